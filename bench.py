@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark: TD site-estimates/s at equal 95% CI (mixed vs FP64 GPU, vs host CPU).
+
+Workload (one "step"): the compliance TWoS estimator over every interior
+site of the noise-displaced icosphere -- subdivision 7 (327,680 triangles),
+vertices scaled radially by 1 + 0.15 * (8 random real spherical harmonics of
+degree <= 6, seed 1), Poisson f = 1 with u = 0 on the surface, sites = the
+64^3 cell centres of the bounding box kept when inside the mesh (ray parity),
+4,096 walks per site, epsilon = 1e-4, max 1,024 steps.  Synthetic inputs,
+generated here from seeds.
+
+value    mixed form (FP32 query/position, FP64 accumulation) site-estimates/s,
+         sites resident in HBM, scaled to the FP64 form's 95% CI half-width:
+         rate * (h_mixed / h_fp64)^2, h = median over sites of 1.96 * SE.
+e2e      the same metric through the host-buffer C-ABI call (twos_estimate):
+         pinned host sites in, pinned host rows out, copies inside the timed
+         region.
+fp64     the plain all-FP64 GPU form at the same N (the target comparison).
+cpu_baseline  the CPU oracle (the reference's algorithm and random stream,
+         OpenMP over all host cores) on a bounded random subset of the sites.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun) every rank runs the full workload on its own GPU with
+its own seed (weak scaling, no data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "walking-into-holes_b200"))
+
+METRIC = "TD site-estimates/s at equal 95% CI: mixed vs FP64 GPU, vs host CPU"
+UNIT = "site-estimates/s"
+WORKLOAD = ("noise-displaced icosphere L7 (327,680 tris, SH seed 1), Poisson f=1 u=0, 64^3 grid clipped to "
+            "interior, 4096 walks/site, eps=1e-4")
+# Canonical algorithmic bytes per closest-point query on this workload:
+# 32 B per AABB test + 36 B per triangle test of the canonical binary SAH
+# traversal, counted at the workload's own walk positions by
+# `python oracle/canonical_bytes.py` (96 sites x 64 walks).
+CANONICAL_BYTES_PER_QUERY = 38530.8  # 546.3 AABB + 584.7 triangle tests per query
+CANONICAL_SOURCE = "oracle/canonical_bytes.py --sites 96 --walks 64"
+EPSILON = 1e-4
+MAX_STEPS = 1024
+SEED = 20260912
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--walks", type=int, default=4096)
+    ap.add_argument("--grid", type=int, default=64)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------- workload
+def workload(grid_n):
+    from twos_b200 import geometry
+    V, F = geometry.noise_sphere(7, 1)
+    grid = geometry.grid_points(V.min(0), V.max(0), grid_n)
+    return V, F, grid
+
+
+def source_terms():
+    from twos_b200 import sources
+    return sources.constant(1.0)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU oracle leg
+def cpu_leg(V, F, sites, walks, seconds, repeat=0, threads=None):
+    """Times the oracle (reference algorithm and mt19937_64 stream, OpenMP) on a
+    random subset of the sites sized for about `seconds` of work."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+    oracle.build()
+    threads = threads or oracle.default_threads()
+    om = oracle.OracleMesh(V, F)
+    kw = dict(walks=walks, seed=SEED, epsilon=EPSILON, max_steps=MAX_STEPS,
+              source=[oracle.term(oracle.TERM_CONST, 1.0)], weight_order=0, threads=threads, repeat=repeat)
+    rng = np.random.default_rng(1234 + repeat)
+    pilot = sites[rng.choice(len(sites), size=min(len(sites), threads), replace=False)]
+    t = time.perf_counter()
+    om.estimate(pilot, **kw)
+    per_round = time.perf_counter() - t
+    rounds = max(1, int(seconds / max(per_round, 1e-3)))
+    count = min(len(sites), threads * rounds)
+    idx = rng.choice(len(sites), size=count, replace=False)
+    t = time.perf_counter()
+    est = om.estimate(sites[idx], site_ids=idx, **kw)
+    dt = time.perf_counter() - t
+    return {"sites": count, "seconds": dt, "rate": count / dt, "threads": threads,
+            "h_median": float(np.median(1.96 * est["score_se"]))}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import twos_b200 as tb
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    V, F, grid = workload(args.grid)
+    mesh = tb.Mesh(V, F, device=local)
+    info = mesh.info()
+    sites = grid[mesh.inside(grid)]
+    n = len(sites)
+    stream = torch.cuda.Stream()
+    mesh.set_stream(stream)
+    d_sites = torch.tensor(sites, dtype=torch.float64, device="cuda")
+    d_out = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    base = dict(walks=args.walks, mode="compliance", seed=SEED + rank, epsilon=EPSILON, max_steps=MAX_STEPS,
+                source=source_terms(), query_radius=4.0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(cfg, steps, warmup, host=None):
+        for w in range(warmup):
+            cfg.repeat = 1000 + w
+            if host is None:
+                mesh.estimate_device(d_sites, n, d_out, cfg)
+            else:
+                mesh.estimate(host[0], cfg, out=host[1])
+        ms, summs = [], []
+        barrier()
+        for k in range(steps):
+            cfg.repeat = k
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if host is None:
+                    summs.append(mesh.estimate_device(d_sites, n, d_out, cfg))
+                else:
+                    summs.append(mesh.estimate(host[0], cfg, out=host[1])[1])
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        barrier()
+        total = sum(ms)
+        if dist is not None:
+            t = torch.tensor([total], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total, ms, summs
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    cfg_mixed = tb.Config(precision="mixed", **base)
+    t_mixed, ms_mixed, s_mixed = timed(cfg_mixed, args.steps, args.warmup)
+    rows_mixed = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+    clock_info = clocks.stop()
+    h_mixed = float(np.median(1.96 * rows_mixed["score_se"]))
+
+    # e2e: host-buffer entry point, pinned host memory, copies inside the timed region.
+    h_sites = torch.from_numpy(np.ascontiguousarray(sites)).pin_memory()
+    h_out = torch.zeros((n, 7), dtype=torch.float64).pin_memory()
+    host = (h_sites.numpy(), h_out.numpy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1))
+    t_e2e, ms_e2e, s_e2e = timed(tb.Config(precision="mixed", **base), args.steps, 1, host=host)
+
+    fp64 = None
+    if not args.no_fp64:
+        t64, ms64, s64 = timed(tb.Config(precision="fp64", **base), args.fp64_steps, 1)
+        rows64 = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        h64 = float(np.median(1.96 * rows64["score_se"]))
+        fp64 = {"rate": world * n * len(ms64) / (t64 / 1e3), "ms_per_step": t64 / len(ms64), "steps": len(ms64),
+                "h_median": h64, "walk_seconds": float(np.mean([s["walk_seconds"] for s in s64]))}
+    h_ref = fp64["h_median"] if fp64 else h_mixed
+    scale = (h_mixed / h_ref) ** 2
+    rate_mixed = world * n * args.steps / (t_mixed / 1e3)
+    value = rate_mixed * scale
+    rate_e2e = world * n * args.steps / (t_e2e / 1e3) * scale
+
+    out = None
+    if rank == 0:
+        queries = np.mean([s["queries"] for s in s_mixed])
+        walk_s = float(np.mean([s["walk_seconds"] for s in s_mixed]))
+        peak, peak_kind = measured_peaks()
+        roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None, "traffic": None,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "queries_per_launch": float(queries), "walk_kernel_seconds": walk_s,
+                "queries_per_second": float(queries / walk_s)}
+        if CANONICAL_BYTES_PER_QUERY:
+            ach = CANONICAL_BYTES_PER_QUERY * queries / walk_s / 1e9
+            roof.update({"achieved": ach, "frac": ach / peak, "bytes_per_query": CANONICAL_BYTES_PER_QUERY,
+                         "bytes_source": CANONICAL_SOURCE})
+        cpu = None
+        if not args.no_cpu and world == 1:
+            c = cpu_leg(V, F, sites, args.walks, args.cpu_seconds)
+            cpu = {"value": c["rate"] * (c["h_median"] / h_ref) ** 2, "unit": UNIT, "cores": c["threads"],
+                   "kind": "port",
+                   "sample": f"{c['sites']} random interior sites x {args.walks} walks, oracle (reference "
+                             f"algorithm + mt19937_64 stream), OpenMP {c['threads']} threads, {c['seconds']:.1f} s"}
+        launches = int(sum(s["launches"] for s in s_mixed))
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 query/position, f64 accumulation",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites": int(n), "walks": args.walks, "epsilon": EPSILON,
+                       "max_steps": MAX_STEPS, "mesh_triangles": int(info["faces"]),
+                       "bvh_nodes": int(info["bvh_nodes"]), "mixed_delta": info["mixed_delta"],
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+            "ci": {"h_mixed_median": h_mixed, "h_fp64_median": h_ref, "scale": scale,
+                   "rate_mixed_unscaled": rate_mixed},
+            "fp64_form": fp64,
+            "mixed_over_fp64": (value / fp64["rate"]) if fp64 else None,
+            "e2e": {"value": rate_e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
+                    "d2h_bytes_per_step": int(n * 56), "ms_per_step": t_e2e / args.steps},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clock_info,
+        }
+        if cpu:
+            out["gpu_over_cpu"] = value / cpu["value"]
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    mesh.close()
+    return out
+
+
+def run_reference(args):
+    """The reference's algorithm on the host cores: the oracle (restatement of
+    wih_twos.cpp's compliance walk with its mt19937_64 stream), OpenMP over all
+    threads, each step a bounded random sample of the workload's sites."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    V, F, grid = workload(args.grid)
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+    oracle.build()
+    # Interior sites by the oracle's exact distance + ray parity is not needed:
+    # the star-shaped surface gives the interior test directly.
+    from twos_b200 import geometry
+    r = np.linalg.norm(grid, axis=1)
+    keep = r > 1e-12
+    g = grid[keep]
+    rad = 1.0 + 0.15 * geometry.sh_field(g / r[keep][:, None], 1)
+    sites = g[r[keep] < rad]
+    per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
+    for w in range(args.warmup):
+        cpu_leg(V, F, sites, args.walks, per_step / 4, repeat=100 + w)
+    runs = [cpu_leg(V, F, sites, args.walks, per_step, repeat=k) for k in range(args.steps)]
+    total_sites = sum(c["sites"] for c in runs)
+    total_s = sum(c["seconds"] for c in runs)
+    value = total_sites / total_s
+    threads = runs[0]["threads"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "walks": args.walks, "epsilon": EPSILON, "max_steps": MAX_STEPS,
+                   "parallelism": f"OpenMP x{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{total_sites} random interior sites over {args.steps} steps x {args.walks} "
+                                   "walks (oracle: reference algorithm + mt19937_64 stream)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

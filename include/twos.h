@@ -1,0 +1,236 @@
+/*
+ * twos.h -- C ABI of the B200-native TWoS (Topological Walk on Spheres)
+ * estimator, libtwos.so.
+ *
+ * This is the drop-in boundary for the reference's compiled Embree/OpenMP
+ * backend (hertjo/walking-into-holes).  The reference exposes that backend to
+ * Python only as executables driven by argv, files and a --serve pipe
+ * (benchmarks/compiled_bunny/src/wih_twos.cpp:137-240, 1799-1864;
+ * benchmarks/distinct_adjoint/adjoint.cpp:91-158).  The executables built
+ * from this library (wih_twos, wih_adjoint) keep that contract byte for byte;
+ * this header is the in-process call underneath them, which a ctypes, cgo or
+ * JNI binding can reach directly.  Each entry point names the reference code
+ * it replaces.
+ *
+ * Conventions
+ *   - Return codes: TWOS_OK (0), TWOS_ERR_RUNTIME (1: cap hit, non-finite
+ *     distance, CUDA error, device wait limit), TWOS_ERR_USAGE (2: invalid
+ *     argument).  These are the reference's process exit codes
+ *     (wih_twos.cpp:134, 1860-1863).  twos_last_error() gives the message
+ *     (thread-local, valid until the next call on the same thread).
+ *   - Buffers passed to the host entry points are caller-owned host memory;
+ *     device buffers are owned by the mesh session.  No C++ exception crosses
+ *     this ABI.
+ *   - A session is not thread-safe; it issues all work on one CUDA stream.
+ *   - Points, cavities and vertices are arrays of 3 doubles (x, y, z).
+ */
+#ifndef TWOS_H
+#define TWOS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TWOS_ABI_VERSION 1
+
+enum { TWOS_OK = 0, TWOS_ERR_RUNTIME = 1, TWOS_ERR_USAGE = 2 };
+
+/* Estimator modes.
+ *   COMPLIANCE: one walk set, U = sum f r^2/6; score = (S^2 - S2)/(N(N-1))
+ *               (wih_twos.cpp:674-717, the compliance TD -D_T = u^2).
+ *   PAIRED:     one walk set with two payoffs u (source) and p (adjoint
+ *               source) at a shared Green point; score = (SuSp - Sup)/(N(N-1))
+ *               (adjoint.cpp:18-42, study.cpp:80-120).
+ *   HOT:        PAIRED with the adjoint switched off; score = mean u
+ *               (adjoint.cpp:38, --hot-only 1). */
+enum { TWOS_MODE_COMPLIANCE = 0, TWOS_MODE_PAIRED = 1, TWOS_MODE_HOT = 2 };
+
+/* Arithmetic of the walk.
+ *   FP64:  positions, BVH boxes, triangles and distances in FP64 (the plain
+ *          form; termination at r <= epsilon exactly as wih_twos.cpp:647).
+ *   MIXED: positions, boxes, triangles and distances in FP32 about the mesh
+ *          centre; each step radius is shrunk by a bound delta on the FP32
+ *          distance error, and the walk stops when the shrunk radius is
+ *          <= epsilon, so no walk steps through the boundary.  Per-site
+ *          U-statistic accumulation stays in FP64. */
+enum { TWOS_PREC_FP64 = 0, TWOS_PREC_MIXED = 1 };
+
+/* Source terms; a source f(x) is the ordered sum of up to TWOS_MAX_TERMS terms.
+ *   CONST  amp
+ *   LINEAR amp * (x[axis] + offset)                 (affine, wih_twos.cpp:551)
+ *   GAUSS  amp * exp(-sum_k ((x_k - c_k)/w_k)^2)     (housing, wih_twos.cpp:553-565)
+ *   BUMP   amp * max(0, 1 - |x-c|^2/w0^2)^2 / div   (sensor, adjoint.cpp:11-15,
+ *                                                    study.cpp:45-47)
+ *   BOX    amp if c <= x <= w componentwise, else 0
+ *   BALL   amp if |x - c| <= w0, else 0 */
+enum {
+  TWOS_TERM_CONST = 0,
+  TWOS_TERM_LINEAR = 1,
+  TWOS_TERM_GAUSS = 2,
+  TWOS_TERM_BUMP = 3,
+  TWOS_TERM_BOX = 4,
+  TWOS_TERM_BALL = 5
+};
+
+#define TWOS_MAX_TERMS 8
+
+typedef struct twos_source_term {
+  int32_t kind;
+  int32_t axis;
+  double amp;
+  double offset;
+  double div;
+  double c[3];
+  double w[3];
+} twos_source_term; /* 80 bytes */
+
+/* One estimation request (the reference's Options, wih_twos.cpp:73-101, plus
+ * the paired flags of adjoint.cpp:95-107). */
+typedef struct twos_request {
+  int32_t mode;       /* TWOS_MODE_* */
+  int32_t precision;  /* TWOS_PREC_* */
+  int32_t walks;      /* N >= 2 walks per site (--walks) */
+  int32_t max_steps;  /* step cap per walk (--max-steps); reaching it is an error */
+  uint64_t seed;      /* --seed */
+  uint32_t repeat;    /* repeat index, part of the sample key */
+  uint32_t stream;    /* independent stream id (0 estimate, 1 fresh validation, ...) */
+  double epsilon;     /* termination shell (--epsilon) */
+  double cavity_radius;  /* common radius of the spherical cavities (--cavity-radius) */
+  double query_radius;   /* initial closest-point radius; nothing at or beyond it is
+                            found (wih_twos.cpp:348 uses 4.0); <= 0 means unbounded */
+  int32_t green;         /* 1: evaluate sources at a Beta(2,2) Green point in each
+                            ball (housing mode); 0: at the ball centre (affine) */
+  int32_t n_source;
+  int32_t n_adjoint;
+  int32_t skip_cavity_sites; /* 1: sites inside a cavity get all-zero rows
+                                (adjoint.cpp:123-126) */
+  uint32_t site_offset;      /* added to the site index in the sample key */
+  uint32_t reserved;
+  twos_source_term source[TWOS_MAX_TERMS];
+  twos_source_term adjoint[TWOS_MAX_TERMS];
+} twos_request;
+
+/* Per-site result (SiteResult wih_twos.cpp:666-672 and PairValue
+ * adjoint.cpp:16).  COMPLIANCE fills u = mean, score, score_se (jackknife),
+ * p = u and same_index = sum u^2 / N.  PAIRED/HOT fill u, p (means), score,
+ * score_se (jackknife of the cross statistic), same_index = sum u p / N. */
+typedef struct twos_site_result {
+  double u;
+  double p;
+  double score;
+  double score_se;
+  double same_index;
+  uint64_t steps;
+  uint64_t caps;
+} twos_site_result; /* 56 bytes */
+
+typedef struct twos_summary {
+  double kernel_seconds;   /* device time of the walk + finalize kernels */
+  double walk_seconds;     /* device time of the walk kernel alone */
+  double total_seconds;    /* host wall time of the call */
+  uint64_t paths;          /* walks run */
+  uint64_t steps;          /* sum of steps */
+  uint64_t caps;           /* walks that hit max_steps */
+  uint64_t queries;        /* closest-point queries = steps + paths (wih_twos.cpp:1779) */
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint32_t launches;       /* kernels launched by the call */
+  uint32_t error_flags;    /* TWOS_DEVERR_* bits raised on the device */
+} twos_summary;
+
+/* Device-side error bits (set by kernels, never by a trap). */
+enum {
+  TWOS_DEVERR_QUERY = 1u,     /* no surface point within query_radius / non-finite */
+  TWOS_DEVERR_STACK = 2u,     /* traversal stack bound exceeded */
+  TWOS_DEVERR_ITER = 4u,      /* traversal iteration bound exceeded */
+  TWOS_DEVERR_CONFIG = 8u
+};
+
+typedef struct twos_mesh twos_mesh;
+
+typedef struct twos_mesh_info {
+  uint64_t vertices;
+  uint64_t faces;
+  uint64_t bvh_nodes;
+  uint32_t bvh_depth;
+  uint32_t device;
+  double bounds_min[3];
+  double bounds_max[3];
+  double center[3];
+  double mixed_delta;         /* FP32 distance error bound used by TWOS_PREC_MIXED */
+  double build_seconds;       /* host BVH build + upload */
+  uint64_t device_bytes;      /* BVH + triangle bytes resident on the device */
+} twos_mesh_info;
+
+/* Library version and the message of the last failed call on this thread. */
+int twos_abi_version(void);
+const char *twos_last_error(void);
+
+/* Build a session from an in-memory triangle mesh: host BVH build, upload of
+ * the FP32 and FP64 layouts to `device`.  Replaces EmbreeMesh's constructor
+ * (wih_twos.cpp:298-325; rtcCommitScene is the BVH build). */
+int twos_mesh_open(const double *vertices, uint64_t n_vertices, const uint32_t *faces,
+                   uint64_t n_faces, int device, twos_mesh **out);
+
+/* Same from an ASCII PLY file with the reference's accept/reject rules and
+ * messages (EmbreeMesh::load_ascii_ply, wih_twos.cpp:437-493). */
+int twos_mesh_open_ply(const char *path, int device, twos_mesh **out);
+
+void twos_mesh_close(twos_mesh *mesh);
+
+int twos_mesh_get_info(const twos_mesh *mesh, twos_mesh_info *info);
+
+/* Issue the session's work on `stream` (a cudaStream_t of the session's
+ * device) instead of its own stream; NULL restores the session's stream.
+ * Lets a caller time the kernels with events on its own stream.  No
+ * reference counterpart (the reference has no device work). */
+int twos_mesh_set_stream(twos_mesh *mesh, void *stream);
+
+/* Batched unsigned distance and closest point to the mesh surface
+ * (EmbreeMesh::closest_point + point_query_callback, wih_twos.cpp:339-359,
+ * 416-430).  `closest` may be NULL.  Host buffers. */
+int twos_closest_point(twos_mesh *mesh, int precision, const double *points, uint64_t n,
+                       double query_radius, double *distance, double *closest);
+
+/* Per-site TWoS estimates for n_sites sites (the OpenMP site loop of
+ * wih_twos.cpp:1825-1841 with evaluate_site 674-717, or the paired loop of
+ * adjoint.cpp:121-127 with paired_site 18-42).  Host buffers; `summary` may
+ * be NULL.  Returns TWOS_ERR_RUNTIME when any walk hit max_steps (the rows
+ * are still written, with caps > 0) or a device error bit was raised. */
+int twos_estimate(twos_mesh *mesh, const twos_request *request, const double *sites,
+                  uint32_t n_sites, const double *cavities, uint32_t n_cavities,
+                  twos_site_result *out, twos_summary *summary);
+
+/* As twos_estimate with device-resident sites (d_sites, 3 doubles each) and
+ * results (d_out); cavities stay host memory.  Work is ordered on the
+ * session's stream and the call returns after it completes. */
+int twos_estimate_device(twos_mesh *mesh, const twos_request *request, const double *d_sites,
+                         uint32_t n_sites, const double *cavities, uint32_t n_cavities,
+                         twos_site_result *d_out, twos_summary *summary);
+
+/* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
+ * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid
+ * out [site][walk].  Host buffers.  Used by parity tests. */
+int twos_walk_samples(twos_mesh *mesh, const twos_request *request, const double *sites,
+                      uint32_t n_sites, const double *cavities, uint32_t n_cavities, double *u,
+                      double *p, uint32_t *steps);
+
+/* Ray-parity point membership (EmbreeMesh::inside, wih_twos.cpp:361-394):
+ * inside[i] = 1 when a ray in the reference's fixed oblique direction crosses
+ * the surface an odd number of times.  Host buffers. */
+int twos_inside(twos_mesh *mesh, const double *points, uint64_t n, uint8_t *inside);
+
+/* Indices of the k largest keys, highest first, ties to the lower index
+ * (np.argpartition(...)[-k:] of run_bunny_benchmark.py:324 with a
+ * deterministic order).  Device buffers, k <= 1024. */
+int twos_topk_device(twos_mesh *mesh, const double *d_keys, uint32_t n, uint32_t k,
+                     uint32_t *d_index);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TWOS_H */

@@ -1,0 +1,362 @@
+"""TEST INFRASTRUCTURE ONLY -- Python side of the CPU oracle.
+
+The oracle restates the reference TWoS backend on the host so the CUDA product
+can be checked against it.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg import this module; the product never does.
+
+Contents
+--------
+* ctypes bindings to ``oracle/_build/libtwos_oracle.so`` (``twos_oracle.cpp``):
+  FP64 closest point (BVH or brute force, with box/triangle test counts),
+  per-walk samples and per-site estimates in the reference's own
+  ``mt19937_64`` stream or in the GPU's counter stream.
+* numpy restatements of the reference's readers and statistics:
+  ``load_ascii_ply`` (benchmarks/compiled_bunny/src/wih_twos.cpp:437-493),
+  ``read_points`` (wih_twos.cpp:508-522), ``crossfit_square``
+  (benchmarks/stanford_bunny/run_bunny_benchmark.py:257-269),
+  ``crossfit_product`` (experiments/run_controlled_experiments.py:79-87) and
+  the shortlist/rescore selection rule (run_bunny_benchmark.py:302-337).
+"""
+from __future__ import annotations
+
+import ctypes
+import gzip
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libtwos_oracle.so"
+
+MODE_COMPLIANCE, MODE_PAIRED, MODE_HOT = 0, 1, 2
+RNG_REFERENCE, RNG_COUNTER = 0, 1
+TERM_CONST, TERM_LINEAR, TERM_GAUSS, TERM_BUMP, TERM_BOX, TERM_BALL = range(6)
+
+
+class Term(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("axis", ctypes.c_int32),
+        ("amp", ctypes.c_double), ("offset", ctypes.c_double), ("div", ctypes.c_double),
+        ("c", ctypes.c_double * 3), ("w", ctypes.c_double * 3),
+    ]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32), ("rng", ctypes.c_int32),
+        ("walks", ctypes.c_int32), ("max_steps", ctypes.c_int32),
+        ("seed", ctypes.c_uint64), ("repeat", ctypes.c_uint32), ("stream", ctypes.c_uint32),
+        ("epsilon", ctypes.c_double), ("cavity_radius", ctypes.c_double),
+        ("query_radius", ctypes.c_double),
+        ("green", ctypes.c_int32), ("n_source", ctypes.c_int32), ("n_adjoint", ctypes.c_int32),
+        ("skip_cavity_sites", ctypes.c_int32), ("weight_order", ctypes.c_int32),
+        ("threads", ctypes.c_int32),
+        ("source", Term * 8), ("adjoint", Term * 8),
+    ]
+
+
+class Site(ctypes.Structure):
+    _fields_ = [
+        ("u", ctypes.c_double), ("p", ctypes.c_double), ("score", ctypes.c_double),
+        ("score_se", ctypes.c_double), ("same_index", ctypes.c_double),
+        ("steps", ctypes.c_uint64), ("caps", ctypes.c_uint64),
+    ]
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (system g++, no FMA contraction)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.oracle_mesh_new.restype = ctypes.c_void_p
+        L.oracle_mesh_new.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]
+        L.oracle_mesh_free.argtypes = [ctypes.c_void_p]
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_bvh_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_int)]
+        L.oracle_closest_point.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_double,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_walk_samples.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+            ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p]
+        L.oracle_estimate.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+            ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        assert L.oracle_sizeof_params() == ctypes.sizeof(Params)
+        assert L.oracle_sizeof_site() == ctypes.sizeof(Site)
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+# --------------------------------------------------------------------------- sources
+def term(kind, amp=1.0, axis=0, offset=0.0, div=1.0, c=(0.0, 0.0, 0.0), w=(1.0, 1.0, 1.0)) -> Term:
+    t = Term()
+    t.kind, t.axis, t.amp, t.offset, t.div = kind, axis, amp, offset, div
+    t.c[:] = list(c)
+    t.w[:] = list(w)
+    return t
+
+
+def affine_source(slope=0.65):
+    """wih_twos.cpp:550-552: f = 1 + slope*(y + 0.5)."""
+    return [term(TERM_CONST, 1.0), term(TERM_LINEAR, slope, axis=1, offset=0.5)]
+
+
+def housing_source():
+    """wih_twos.cpp:553-565: 0.08 + 5.2 chip_a + 4.6 chip_b + 2.0 regulator."""
+    return [
+        term(TERM_CONST, 0.08),
+        term(TERM_GAUSS, 5.2, c=(-0.48, -0.18, -0.08), w=(0.24, 0.22, 0.16)),
+        term(TERM_GAUSS, 4.6, c=(0.43, 0.19, -0.07), w=(0.21, 0.20, 0.15)),
+        term(TERM_GAUSS, 2.0, c=(0.02, -0.31, -0.02), w=(0.30, 0.16, 0.19)),
+    ]
+
+
+def sensor_source(side=1):
+    """adjoint.cpp:11-15 with the --sensor-side flip of adjoint.cpp:98-102."""
+    return [term(TERM_BUMP, 1.0, c=(0.55 * side, 0.18 * side, -0.03), w=(0.13, 0.0, 0.0))]
+
+
+# --------------------------------------------------------------------------- mesh
+class OracleMesh:
+    def __init__(self, vertices: np.ndarray, faces: np.ndarray):
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
+        self.faces = np.ascontiguousarray(faces, dtype=np.uint32)
+        h = lib().oracle_mesh_new(_ptr(self.vertices), len(self.vertices), _ptr(self.faces), len(self.faces))
+        if not h:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().oracle_mesh_free(self.handle)
+            self.handle = None
+
+    def bvh_info(self):
+        n = ctypes.c_uint64()
+        d = ctypes.c_int()
+        lib().oracle_bvh_info(self.handle, ctypes.byref(n), ctypes.byref(d))
+        return int(n.value), int(d.value)
+
+    def closest_point(self, points, brute=False, radius=np.inf, threads=0):
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        n = len(pts)
+        dist = np.empty(n)
+        closest = np.empty((n, 3))
+        tri = np.empty(n, dtype=np.uint32)
+        counts = np.zeros((n, 2), dtype=np.uint64)
+        lib().oracle_closest_point(self.handle, _ptr(pts), n, int(brute), float(radius),
+                                   _ptr(dist), _ptr(closest), _ptr(tri), _ptr(counts), threads)
+        return dist, closest, tri, counts
+
+    def _params(self, **kw) -> Params:
+        p = Params()
+        p.mode = kw.get("mode", MODE_COMPLIANCE)
+        p.rng = kw.get("rng", RNG_REFERENCE)
+        p.walks = kw["walks"]
+        p.max_steps = kw.get("max_steps", 512)
+        p.seed = kw.get("seed", 20260912)
+        p.repeat = kw.get("repeat", 0)
+        p.stream = kw.get("stream", 0)
+        p.epsilon = kw.get("epsilon", 5e-4)
+        p.cavity_radius = kw.get("cavity_radius", 0.0)
+        p.query_radius = kw.get("query_radius", 4.0)
+        p.green = int(kw.get("green", False))
+        src = kw.get("source", affine_source())
+        adj = kw.get("adjoint", [])
+        p.n_source, p.n_adjoint = len(src), len(adj)
+        for i, t in enumerate(src):
+            p.source[i] = t
+        for i, t in enumerate(adj):
+            p.adjoint[i] = t
+        p.skip_cavity_sites = int(kw.get("skip_cavity_sites", p.mode != MODE_COMPLIANCE))
+        p.weight_order = kw.get("weight_order", 0 if p.mode == MODE_COMPLIANCE else 1)
+        p.threads = kw.get("threads", 0)
+        return p
+
+    def walk_samples(self, sites, site_ids=None, cavities=None, count_tests=False, **kw):
+        p = self._params(**kw)
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        ids = None if site_ids is None else np.ascontiguousarray(site_ids, dtype=np.uint64)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64)
+        n = len(s)
+        u = np.empty((n, p.walks))
+        pp = np.empty((n, p.walks))
+        st = np.empty((n, p.walks), dtype=np.uint32)
+        tests = np.zeros((n, p.walks, 2), dtype=np.uint64) if count_tests else None
+        rc = lib().oracle_walk_samples(self.handle, ctypes.byref(p), _ptr(s), _ptr(ids), n, _ptr(cav),
+                                       len(cav), _ptr(u), _ptr(pp), _ptr(st), _ptr(tests))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        out = {"u": u, "p": pp, "steps": st & 0x7FFFFFFF, "caps": (st >> 31).astype(bool)}
+        if count_tests:
+            out["aabb_tests"] = tests[..., 0]
+            out["tri_tests"] = tests[..., 1]
+        return out
+
+    def estimate(self, sites, site_ids=None, cavities=None, **kw):
+        p = self._params(**kw)
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        ids = None if site_ids is None else np.ascontiguousarray(site_ids, dtype=np.uint64)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64)
+        n = len(s)
+        out = (Site * n)()
+        rc = lib().oracle_estimate(self.handle, ctypes.byref(p), _ptr(s), _ptr(ids), n, _ptr(cav), len(cav),
+                                   ctypes.cast(out, ctypes.c_void_p))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        arr = np.frombuffer(out, dtype=np.dtype([
+            ("u", "f8"), ("p", "f8"), ("score", "f8"), ("score_se", "f8"), ("same_index", "f8"),
+            ("steps", "u8"), ("caps", "u8")]), count=n)
+        return arr.copy()
+
+
+# --------------------------------------------------------------------------- readers
+def _open_text(path):
+    path = str(path)
+    if path.endswith(".gz"):
+        return gzip.open(path, "rt")
+    return open(path, "r")
+
+
+def load_ascii_ply(path):
+    """Restates wih_twos.cpp:437-493: ASCII triangle PLY, FP64 vertices.
+
+    The header must declare ``format ascii``, a vertex and a face count and
+    end with ``end_header``; every face must be a triangle with indices in
+    range.  Errors carry the reference's messages.
+    """
+    with _open_text(path) as fh:
+        vertex_count = face_count = 0
+        ascii = header_done = False
+        for line in fh:
+            words = line.split()
+            if not words:
+                continue
+            if words[0] == "format":
+                ascii = len(words) > 1 and words[1] == "ascii"
+            elif words[0] == "element":
+                kind = words[1] if len(words) > 1 else ""
+                count = int(words[2]) if len(words) > 2 else 0
+                if kind == "vertex":
+                    vertex_count = count
+                if kind == "face":
+                    face_count = count
+            elif words[0] == "end_header":
+                header_done = True
+                break
+        if not ascii or not header_done or vertex_count == 0 or face_count == 0:
+            raise RuntimeError("expected a nonempty ASCII triangle PLY mesh")
+        vertices = np.empty((vertex_count, 3))
+        for i in range(vertex_count):
+            parts = fh.readline().split()
+            if len(parts) < 3:
+                raise RuntimeError("truncated PLY vertex section")
+            vertices[i] = [float(parts[0]), float(parts[1]), float(parts[2])]
+        faces = np.empty((face_count, 3), dtype=np.uint32)
+        for i in range(face_count):
+            parts = fh.readline().split()
+            if len(parts) < 4 or int(parts[0]) != 3:
+                raise RuntimeError("expected valid triangular PLY faces")
+            idx = [int(parts[1]), int(parts[2]), int(parts[3])]
+            if min(idx) < 0 or max(idx) >= vertex_count:
+                raise RuntimeError("expected valid triangular PLY faces")
+            faces[i] = idx
+    return vertices, faces
+
+
+def read_points(path):
+    """Restates wih_twos.cpp:508-522: comma or whitespace x,y,z rows; '#' comments."""
+    pts = []
+    with _open_text(path) as fh:
+        for line in fh:
+            line = line.rstrip("\n")
+            if not line or line[0] == "#":
+                continue
+            parts = line.replace(",", " ").split()
+            if len(parts) >= 3:
+                try:
+                    pts.append([float(parts[0]), float(parts[1]), float(parts[2])])
+                except ValueError:
+                    continue
+    if not pts:
+        raise RuntimeError("points file contains no points")
+    return np.array(pts)
+
+
+# --------------------------------------------------------------------------- statistics
+def crossfit_square(samples):
+    """run_bunny_benchmark.py:257-269: U-statistic of u^2 and jackknife SE."""
+    samples = np.asarray(samples, dtype=float)
+    n = samples.shape[1]
+    sums = samples.sum(axis=1)
+    sums2 = np.sum(samples ** 2, axis=1)
+    estimate = (sums ** 2 - sums2) / (n * (n - 1))
+    leave_sums = sums[:, None] - samples
+    leave_sums2 = sums2[:, None] - samples ** 2
+    leave = (leave_sums ** 2 - leave_sums2) / ((n - 1) * (n - 2))
+    leave_mean = leave.mean(axis=1, keepdims=True)
+    se = np.sqrt((n - 1) / n * np.sum((leave - leave_mean) ** 2, axis=1))
+    return estimate, se
+
+
+def crossfit_product(a, b):
+    """experiments/run_controlled_experiments.py:79-87: the off-diagonal mean of a_i b_j."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    n = a.shape[-1]
+    return (a.sum(axis=-1) * b.sum(axis=-1) - np.sum(a * b, axis=-1)) / (n * (n - 1))
+
+
+def cross_jackknife_se(a, b):
+    """Leave-one-out jackknife SE of the cross statistic (the compliance
+    formula of wih_twos.cpp:698-712 applied to the product a_i b_j, i != j)."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    n = a.shape[-1]
+    sa = a.sum(axis=-1, keepdims=True)
+    sb = b.sum(axis=-1, keepdims=True)
+    sab = np.sum(a * b, axis=-1, keepdims=True)
+    leave = ((sa - a) * (sb - b) - (sab - a * b)) / ((n - 1) * (n - 2))
+    lm = leave.mean(axis=-1, keepdims=True)
+    return np.sqrt((n - 1) / n * np.sum((leave - lm) ** 2, axis=-1))
+
+
+def select_shortlist_rescore(scout, shortlist, validation, validation_se, z=1.96):
+    """run_bunny_benchmark.py:323-331: top-`shortlist` by scout score, then
+    argmax of validation - z*se.  Returns (chosen candidate index, lower)."""
+    scout = np.asarray(scout, dtype=float)
+    k = min(shortlist, len(scout))
+    # Deterministic top-k: highest score first, lowest index on ties.
+    order = np.lexsort((np.arange(len(scout)), -scout))[:k]
+    lower = np.asarray(validation, dtype=float) - z * np.asarray(validation_se, dtype=float)
+    local = int(np.argmax(lower))
+    return int(order[local]), float(lower[local]), order
+
+
+def topk_indices(score, k):
+    """Top-k indices by score descending, ties broken by the lower index."""
+    score = np.asarray(score, dtype=float)
+    return np.lexsort((np.arange(len(score)), -score))[:k]
+
+
+def default_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)

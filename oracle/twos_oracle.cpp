@@ -1,0 +1,792 @@
+// TEST INFRASTRUCTURE ONLY -- the CPU oracle for the TWoS estimator.
+//
+// This file restates, on the host and in plain FP64, the algorithm of the
+// reference backend (hertjo/walking-into-holes,
+// benchmarks/compiled_bunny/src/wih_twos.cpp and
+// benchmarks/distinct_adjoint/adjoint.cpp).  It is the checker that the CUDA
+// product is compared with; nothing in the product links, loads or calls it.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+//
+// Two random streams are provided:
+//   * RNG_REFERENCE -- the reference's own per-walk std::mt19937_64 stream,
+//     keyed exactly as wih_twos.cpp:681-686 (compliance) and adjoint.cpp:22
+//     (paired).  Because the same libstdc++ <random> and libm are used, the
+//     integer step counts reproduce the reference's tracked output files.
+//   * RNG_COUNTER -- the counter-based Philox4x32-10 stream that the GPU
+//     kernels use (a pure function of seed, stream, repeat, site, walk, step,
+//     draw), so GPU and oracle walk the same paths from the same samples.
+//
+// Closest-point queries use an exact FP64 minimum over triangles through a
+// binary SAH BVH (<= 4 triangles per leaf, nearest-child-first traversal,
+// pruning a box when its lower-bound distance is >= the current best).  The
+// same traversal is instrumented to count AABB and triangle tests; those
+// counts define the algorithmic bytes per query used for the roofline.
+//
+// Build: g++ -O2 -fopenmp -ffp-contract=off -shared -fPIC (no -march flags, so
+// no FMA contraction, matching the reference's default x86-64 Release build).
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct Vec3 {
+  double x = 0.0, y = 0.0, z = 0.0;
+};
+inline Vec3 operator+(const Vec3 &a, const Vec3 &b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline Vec3 operator-(const Vec3 &a, const Vec3 &b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline Vec3 operator*(const Vec3 &a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(const Vec3 &a, const Vec3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline double norm(const Vec3 &a) { return std::sqrt(dot(a, a)); }
+inline double coord(const Vec3 &v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+// Ericson's closest point on a triangle (Real-Time Collision Detection,
+// section 5.1.5), the case analysis wih_twos.cpp:247-289 uses.
+Vec3 closest_point_triangle(const Vec3 &p, const Vec3 &a, const Vec3 &b, const Vec3 &c) {
+  const Vec3 ab = b - a, ac = c - a, ap = p - a;
+  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0.0 && d2 <= 0.0) return a;
+  const Vec3 bp = p - b;
+  const double d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0.0 && d4 <= d3) return b;
+  const double vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+    const double v = d1 / (d1 - d3);
+    return a + ab * v;
+  }
+  const Vec3 cp = p - c;
+  const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0 && d5 <= d6) return c;
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+    const double w = d2 / (d2 - d6);
+    return a + ac * w;
+  }
+  const double va = d3 * d6 - d5 * d4;
+  if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+    const Vec3 bc = c - b;
+    const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    return b + bc * w;
+  }
+  const double denom = 1.0 / (va + vb + vc);
+  const double v = vb * denom, w = vc * denom;
+  return a + ab * v + ac * w;
+}
+
+struct Box {
+  Vec3 lo{std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+          std::numeric_limits<double>::infinity()};
+  Vec3 hi{-std::numeric_limits<double>::infinity(), -std::numeric_limits<double>::infinity(),
+          -std::numeric_limits<double>::infinity()};
+  void grow(const Vec3 &p) {
+    lo = {std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z)};
+    hi = {std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z)};
+  }
+  void grow(const Box &b) {
+    grow(b.lo);
+    grow(b.hi);
+  }
+  double area() const {
+    const double dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    if (!(dx >= 0.0)) return 0.0;
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+  }
+  // Squared distance from p to the box (0 inside).
+  double dist2(const Vec3 &p) const {
+    double s = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double g = std::max({0.0, coord(lo, a) - coord(p, a), coord(p, a) - coord(hi, a)});
+      s += g * g;
+    }
+    return s;
+  }
+};
+
+// Binary SAH BVH with at most 4 triangles per leaf (the canonical traversal).
+struct Bvh {
+  struct Node {
+    Box box;
+    int left = -1, right = -1;  // internal: children; leaf: left = -1
+    int begin = 0, count = 0;   // leaf triangle range into order
+  };
+  std::vector<Node> nodes;
+  std::vector<uint32_t> order;
+  int depth = 0;
+};
+
+struct Mesh {
+  std::vector<Vec3> v;
+  std::vector<std::array<uint32_t, 3>> f;
+  Bvh bvh;
+};
+
+constexpr int kLeafMax = 4;
+constexpr int kBins = 32;
+
+int build_node(Mesh &m, std::vector<Box> &tb, std::vector<Vec3> &cent, int begin, int end, int depth) {
+  Bvh &b = m.bvh;
+  const int index = static_cast<int>(b.nodes.size());
+  b.nodes.emplace_back();
+  b.depth = std::max(b.depth, depth);
+  Box box, cbox;
+  for (int i = begin; i < end; ++i) {
+    box.grow(tb[b.order[i]]);
+    cbox.grow(cent[b.order[i]]);
+  }
+  b.nodes[index].box = box;
+  const int n = end - begin;
+  if (n <= kLeafMax) {
+    b.nodes[index].begin = begin;
+    b.nodes[index].count = n;
+    return index;
+  }
+  // Binned SAH over centroid bounds on every axis.
+  double best_cost = std::numeric_limits<double>::infinity();
+  int best_axis = -1, best_split = -1;
+  for (int axis = 0; axis < 3; ++axis) {
+    const double lo = coord(cbox.lo, axis), hi = coord(cbox.hi, axis);
+    if (!(hi > lo)) continue;
+    std::array<Box, kBins> bins;
+    std::array<int, kBins> counts{};
+    const double scale = kBins / (hi - lo);
+    for (int i = begin; i < end; ++i) {
+      int k = static_cast<int>((coord(cent[b.order[i]], axis) - lo) * scale);
+      k = std::min(std::max(k, 0), kBins - 1);
+      bins[k].grow(tb[b.order[i]]);
+      ++counts[k];
+    }
+    std::array<double, kBins> right_area{};
+    std::array<int, kBins> right_count{};
+    Box acc;
+    int cnt = 0;
+    for (int k = kBins - 1; k > 0; --k) {
+      acc.grow(bins[k]);
+      cnt += counts[k];
+      right_area[k] = acc.area();
+      right_count[k] = cnt;
+    }
+    Box lacc;
+    int lcnt = 0;
+    for (int k = 0; k < kBins - 1; ++k) {
+      lacc.grow(bins[k]);
+      lcnt += counts[k];
+      if (lcnt == 0 || right_count[k + 1] == 0) continue;
+      const double cost = lacc.area() * lcnt + right_area[k + 1] * right_count[k + 1];
+      if (cost < best_cost) {
+        best_cost = cost;
+        best_axis = axis;
+        best_split = k;
+      }
+    }
+  }
+  int mid;
+  if (best_axis < 0) {
+    mid = begin + n / 2;  // all centroids coincide: split by index
+  } else {
+    const double lo = coord(cbox.lo, best_axis), hi = coord(cbox.hi, best_axis);
+    const double scale = kBins / (hi - lo);
+    auto it = std::partition(b.order.begin() + begin, b.order.begin() + end, [&](uint32_t t) {
+      int k = static_cast<int>((coord(cent[t], best_axis) - lo) * scale);
+      k = std::min(std::max(k, 0), kBins - 1);
+      return k <= best_split;
+    });
+    mid = static_cast<int>(it - b.order.begin());
+    if (mid == begin || mid == end) mid = begin + n / 2;
+  }
+  const int l = build_node(m, tb, cent, begin, mid, depth + 1);
+  const int r = build_node(m, tb, cent, mid, end, depth + 1);
+  b.nodes[index].left = l;
+  b.nodes[index].right = r;
+  return index;
+}
+
+void build_bvh(Mesh &m) {
+  const size_t nf = m.f.size();
+  std::vector<Box> tb(nf);
+  std::vector<Vec3> cent(nf);
+  for (size_t i = 0; i < nf; ++i) {
+    Box b;
+    b.grow(m.v[m.f[i][0]]);
+    b.grow(m.v[m.f[i][1]]);
+    b.grow(m.v[m.f[i][2]]);
+    tb[i] = b;
+    cent[i] = (b.lo + b.hi) * 0.5;
+  }
+  m.bvh.order.resize(nf);
+  std::iota(m.bvh.order.begin(), m.bvh.order.end(), 0u);
+  m.bvh.nodes.reserve(2 * nf + 1);
+  build_node(m, tb, cent, 0, static_cast<int>(nf), 0);
+}
+
+struct QueryStats {
+  uint64_t aabb = 0, tri = 0;
+};
+
+struct Closest {
+  double distance = std::numeric_limits<double>::infinity();
+  Vec3 point;
+  uint32_t tri = 0xffffffffu;
+};
+
+// Exact FP64 closest point; counts box and triangle tests of the canonical
+// traversal.  `radius` plays the role of the reference's initial query radius
+// (wih_twos.cpp:348, 4.0F): nothing at or beyond it is reported.
+Closest closest_point(const Mesh &m, const Vec3 &p, double radius, QueryStats *stats) {
+  Closest out;
+  double best2 = radius * radius;
+  const Bvh &b = m.bvh;
+  struct Entry {
+    int node;
+    double d2;
+  };
+  Entry stack[128];
+  int sp = 0;
+  // The root's box is tested like every other box.
+  if (stats) ++stats->aabb;
+  const double root_d2 = b.nodes[0].box.dist2(p);
+  if (root_d2 < best2) stack[sp++] = {0, root_d2};
+  while (sp > 0) {
+    const Entry e = stack[--sp];
+    if (!(e.d2 < best2)) continue;
+    const Bvh::Node &n = b.nodes[e.node];
+    if (n.left < 0) {
+      for (int i = 0; i < n.count; ++i) {
+        const uint32_t t = b.order[n.begin + i];
+        if (stats) ++stats->tri;
+        const auto &f = m.f[t];
+        const Vec3 q = closest_point_triangle(p, m.v[f[0]], m.v[f[1]], m.v[f[2]]);
+        const Vec3 d = p - q;
+        const double d2 = dot(d, d);
+        if (d2 < best2) {
+          best2 = d2;
+          out.point = q;
+          out.tri = t;
+        }
+      }
+      continue;
+    }
+    const Bvh::Node &l = b.nodes[n.left], &r = b.nodes[n.right];
+    if (stats) stats->aabb += 2;
+    const double dl = l.box.dist2(p), dr = r.box.dist2(p);
+    // Push the farther child first so the nearer one is visited next.
+    if (dl <= dr) {
+      if (dr < best2) stack[sp++] = {n.right, dr};
+      if (dl < best2) stack[sp++] = {n.left, dl};
+    } else {
+      if (dl < best2) stack[sp++] = {n.left, dl};
+      if (dr < best2) stack[sp++] = {n.right, dr};
+    }
+    if (sp > 120) throw std::runtime_error("oracle BVH stack overflow");
+  }
+  if (out.tri != 0xffffffffu) out.distance = norm(p - out.point);
+  return out;
+}
+
+Closest closest_point_brute(const Mesh &m, const Vec3 &p) {
+  Closest out;
+  double best2 = std::numeric_limits<double>::infinity();
+  for (uint32_t t = 0; t < m.f.size(); ++t) {
+    const auto &f = m.f[t];
+    const Vec3 q = closest_point_triangle(p, m.v[f[0]], m.v[f[1]], m.v[f[2]]);
+    const Vec3 d = p - q;
+    const double d2 = dot(d, d);
+    if (d2 < best2) {
+      best2 = d2;
+      out.point = q;
+      out.tri = t;
+    }
+  }
+  out.distance = norm(p - out.point);
+  return out;
+}
+
+// ---------------------------------------------------------------- sources
+// One source term; a source is the ordered sum of its terms.
+struct Term {
+  int32_t kind;  // 0 const, 1 linear, 2 gauss, 3 bump, 4 box, 5 ball
+  int32_t axis;
+  double amp, offset, div;
+  double c[3], w[3];
+};
+static_assert(sizeof(Term) == 80, "term layout");
+
+double term_value(const Term &t, const Vec3 &x) {
+  switch (t.kind) {
+    case 0:
+      return t.amp;
+    case 1:
+      return t.amp * (coord(x, t.axis) + t.offset);
+    case 2: {
+      // wih_twos.cpp:553-556: exp(-((x-c0)/w0)^2 - ((y-c1)/w1)^2 - ((z-c2)/w2)^2)
+      const double a = (x.x - t.c[0]) / t.w[0], b = (x.y - t.c[1]) / t.w[1], c = (x.z - t.c[2]) / t.w[2];
+      return t.amp * std::exp(-(a * a) - (b * b) - (c * c));
+    }
+    case 3: {
+      // adjoint.cpp:11-15: (max(0, 1 - |x-c|^2/r^2))^2
+      const Vec3 d{x.x - t.c[0], x.y - t.c[1], x.z - t.c[2]};
+      const double s = std::max(0.0, 1.0 - dot(d, d) / (t.w[0] * t.w[0]));
+      return t.amp * (s * s) / t.div;
+    }
+    case 4:
+      return (x.x >= t.c[0] && x.x <= t.w[0] && x.y >= t.c[1] && x.y <= t.w[1] && x.z >= t.c[2] &&
+              x.z <= t.w[2])
+                 ? t.amp
+                 : 0.0;
+    case 5: {
+      const Vec3 d{x.x - t.c[0], x.y - t.c[1], x.z - t.c[2]};
+      return dot(d, d) <= t.w[0] * t.w[0] ? t.amp : 0.0;
+    }
+    default:
+      return 0.0;
+  }
+}
+
+double source_value(const Term *terms, int n, const Vec3 &x) {
+  if (n <= 0) return 0.0;
+  double s = term_value(terms[0], x);
+  for (int i = 1; i < n; ++i) s = s + term_value(terms[i], x);
+  return s;
+}
+
+// ---------------------------------------------------------------- random streams
+uint64_t splitmix64(uint64_t x) {
+  // SplitMix64 finaliser (Steele, Lea & Flood 2014), as wih_twos.cpp:529-534 uses it.
+  x += 0x9e3779b97f4a7c15ULL;
+  x = (x ^ (x >> 30U)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27U)) * 0x94d049bb133111ebULL;
+  return x ^ (x >> 31U);
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11).
+struct Philox {
+  static void block(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                    uint32_t out[4]) {
+    for (int r = 0; r < 10; ++r) {
+      const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+      const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+      const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+      const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+      c0 = hi1 ^ c1 ^ k0;
+      c1 = lo1;
+      c2 = hi0 ^ c3 ^ k1;
+      c3 = lo0;
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+  }
+};
+
+inline double u53(uint32_t hi, uint32_t lo) {
+  const uint64_t v = (static_cast<uint64_t>(hi) << 32) | lo;
+  return static_cast<double>(v >> 11) * 0x1.0p-53;
+}
+
+// Counter stream of one walk: counter = (step, walk, site, repeat*8 + draw block).
+struct CounterStream {
+  uint32_t k0, k1, walk, site, repeat;
+  // Two FP64 uniforms from block j of step s.
+  void uniforms(uint32_t step, uint32_t j, double &a, double &b) const {
+    uint32_t o[4];
+    Philox::block(k0, k1, step, walk, site, (repeat << 3) | j, o);
+    a = u53(o[0], o[1]);
+    b = u53(o[2], o[3]);
+  }
+};
+
+inline void counter_key(uint64_t seed, uint32_t stream, uint32_t &k0, uint32_t &k1) {
+  const uint64_t k = splitmix64(seed + 0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(stream) + 1));
+  k0 = static_cast<uint32_t>(k);
+  k1 = static_cast<uint32_t>(k >> 32);
+}
+
+// Uniform direction on S^2 from two uniforms: z = 1 - 2a, phi = 2*pi*b.
+inline Vec3 direction_from(double a, double b) {
+  const double z = 1.0 - 2.0 * a;
+  const double phi = 2.0 * 3.141592653589793 * b;
+  const double radial = std::sqrt(std::max(0.0, 1.0 - z * z));
+  return {radial * std::cos(phi), radial * std::sin(phi), z};
+}
+
+inline double median3(double a, double b, double c) {
+  return std::max(std::min(a, b), std::min(std::max(a, b), c));
+}
+
+// Reference stream pieces (wih_twos.cpp:536-542, 569-575).
+Vec3 random_unit_vector(std::mt19937_64 &rng) {
+  std::uniform_real_distribution<double> uniform(0.0, 1.0);
+  const double z = 1.0 - 2.0 * uniform(rng);
+  const double phi = 2.0 * std::acos(-1.0) * uniform(rng);
+  const double radial = std::sqrt(std::max(0.0, 1.0 - z * z));
+  return {radial * std::cos(phi), radial * std::sin(phi), z};
+}
+
+double beta_22(std::mt19937_64 &rng) {
+  std::uniform_real_distribution<double> uniform(0.0, 1.0);
+  while (true) {
+    const double value = uniform(rng);
+    if (uniform(rng) <= 4.0 * value * (1.0 - value)) return value;
+  }
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+struct oracle_params {
+  int32_t mode;       // 0 compliance, 1 paired, 2 hot (paired with primal only)
+  int32_t rng;        // 0 reference mt19937_64 stream, 1 counter (GPU) stream
+  int32_t walks;
+  int32_t max_steps;
+  uint64_t seed;
+  uint32_t repeat;
+  uint32_t stream;
+  double epsilon;
+  double cavity_radius;
+  double query_radius;
+  int32_t green;       // evaluate sources at a Beta(2,2) Green point
+  int32_t n_source;
+  int32_t n_adjoint;
+  int32_t skip_cavity_sites;
+  int32_t weight_order;  // reference association: 0 (f*r*r)/6 [wih_twos walk], 1 (r*r/6)*f [paired_site]
+  int32_t threads;
+  Term source[8];
+  Term adjoint[8];
+};
+
+struct oracle_site {
+  double u, p, score, score_se, same_index;
+  uint64_t steps, caps;
+};
+
+struct oracle_mesh {
+  Mesh m;
+};
+
+static thread_local std::string g_error;
+
+const char *oracle_last_error() { return g_error.c_str(); }
+
+oracle_mesh *oracle_mesh_new(const double *vertices, uint32_t nv, const uint32_t *faces, uint32_t nf) {
+  try {
+    auto *om = new oracle_mesh;
+    om->m.v.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) om->m.v[i] = {vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]};
+    om->m.f.resize(nf);
+    for (uint32_t i = 0; i < nf; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        if (faces[3 * i + k] >= nv) throw std::runtime_error("face index out of range");
+        om->m.f[i][k] = faces[3 * i + k];
+      }
+    }
+    if (nf == 0) throw std::runtime_error("empty mesh");
+    build_bvh(om->m);
+    return om;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    return nullptr;
+  }
+}
+
+void oracle_mesh_free(oracle_mesh *om) { delete om; }
+
+int oracle_bvh_info(const oracle_mesh *om, uint64_t *nodes, int *depth) {
+  *nodes = om->m.bvh.nodes.size();
+  *depth = om->m.bvh.depth;
+  return 0;
+}
+
+// Batched closest point.  mode 0: BVH traversal (counts box/triangle tests
+// into counts[2*i], counts[2*i+1] when counts != null); mode 1: brute force.
+int oracle_closest_point(const oracle_mesh *om, const double *pts, uint64_t n, int brute, double radius,
+                         double *dist, double *closest, uint32_t *tri, uint64_t *counts, int threads) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+    const Vec3 p{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    QueryStats st;
+    const Closest c = brute ? closest_point_brute(om->m, p) : closest_point(om->m, p, radius, &st);
+    dist[i] = c.distance;
+    if (closest) {
+      closest[3 * i] = c.point.x;
+      closest[3 * i + 1] = c.point.y;
+      closest[3 * i + 2] = c.point.z;
+    }
+    if (tri) tri[i] = c.tri;
+    if (counts) {
+      counts[2 * i] = st.aabb;
+      counts[2 * i + 1] = st.tri;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct WalkOut {
+  double u = 0.0, p = 0.0;
+  uint32_t steps = 0;
+  bool cap = false;
+  bool failed = false;
+  uint64_t aabb = 0, tri = 0;
+};
+
+inline double domain_distance(const Mesh &m, const Vec3 &x, const double *cav, uint32_t ncav, double cr,
+                              double query_radius, QueryStats *st, bool &failed) {
+  const Closest c = closest_point(m, x, query_radius, st);
+  if (!std::isfinite(c.distance)) failed = true;
+  double d = c.distance;
+  for (uint32_t i = 0; i < ncav; ++i) {
+    const Vec3 cc{cav[3 * i], cav[3 * i + 1], cav[3 * i + 2]};
+    d = std::min(d, norm(x - cc) - cr);
+  }
+  return d;
+}
+
+inline bool inside_cavity(const Vec3 &x, const double *cav, uint32_t ncav, double cr) {
+  for (uint32_t i = 0; i < ncav; ++i) {
+    const Vec3 cc{cav[3 * i], cav[3 * i + 1], cav[3 * i + 2]};
+    if (norm(x - cc) <= cr) return true;
+  }
+  return false;
+}
+
+// One walk.  Reference stream: wih_twos.cpp:635-664 (compliance) and
+// adjoint.cpp:18-37 (paired).  Counter stream: the GPU kernel's draw layout.
+WalkOut walk(const Mesh &m, const oracle_params &o, const double *cav, uint32_t ncav, Vec3 y, uint64_t site,
+             uint32_t sample, bool count_tests) {
+  WalkOut out;
+  QueryStats st;
+  QueryStats *stp = count_tests ? &st : nullptr;
+  const bool primal_only = (o.mode != 1);  // compliance and hot keep only u
+  const bool want_p = (o.mode == 1);
+  if (o.rng == 0) {
+    std::mt19937_64 rng;
+    if (o.mode == 0) {
+      // wih_twos.cpp:681-686: XOR of four hashed keys, reseeded through splitmix64.
+      const uint64_t key = splitmix64(o.seed + 0x2d358dccaa6c78a5ULL) ^
+                           splitmix64(static_cast<uint64_t>(o.repeat) + 0x8bb84b93962eacc9ULL) ^
+                           splitmix64(site + 0x4b33a62ed433d4a3ULL) ^
+                           splitmix64(static_cast<uint64_t>(sample) + 0x4d5a2da51de1aa47ULL);
+      rng.seed(splitmix64(key));
+    } else {
+      // adjoint.cpp:22
+      rng.seed(splitmix64(o.seed) ^ splitmix64(site + 91347) ^ splitmix64(static_cast<uint64_t>(sample) + 571));
+    }
+    for (int k = 0; k < o.max_steps; ++k) {
+      const double r = domain_distance(m, y, cav, ncav, o.cavity_radius, o.query_radius, stp, out.failed);
+      if (!(r > o.epsilon)) {
+        out.aabb = st.aabb;
+        out.tri = st.tri;
+        return out;
+      }
+      Vec3 a = y;
+      if (o.green) {
+        // The scale operand (and so beta_22) is evaluated before the
+        // direction, as g++ sequences `operator*(random_unit_vector(rng),
+        // radius * beta_22(rng))`; the tracked fixtures pin this order.
+        const double scale = r * beta_22(rng);
+        const Vec3 dir = random_unit_vector(rng);
+        a = y + dir * scale;
+      }
+      if (o.weight_order == 0) {
+        out.u += source_value(o.source, o.n_source, a) * r * r / 6.0;
+      } else {
+        out.u += r * r / 6 * source_value(o.source, o.n_source, a);
+        if (want_p) out.p += r * r / 6 * source_value(o.adjoint, o.n_adjoint, a);
+      }
+      y = y + random_unit_vector(rng) * r;
+      ++out.steps;
+    }
+    out.cap = true;
+  } else {
+    CounterStream cs;
+    counter_key(o.seed, o.stream, cs.k0, cs.k1);
+    cs.walk = sample;
+    cs.site = static_cast<uint32_t>(site);
+    cs.repeat = o.repeat;
+    for (int k = 0; k < o.max_steps; ++k) {
+      const double r = domain_distance(m, y, cav, ncav, o.cavity_radius, o.query_radius, stp, out.failed);
+      if (!(r > o.epsilon)) {
+        out.aabb = st.aabb;
+        out.tri = st.tri;
+        return out;
+      }
+      double a0, a1;
+      cs.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
+      Vec3 a = y;
+      if (o.green) {
+        double g0, g1, b0, b1, b2, spare;
+        cs.uniforms(static_cast<uint32_t>(k), 1, g0, g1);
+        cs.uniforms(static_cast<uint32_t>(k), 2, b0, b1);
+        cs.uniforms(static_cast<uint32_t>(k), 3, b2, spare);
+        const double beta = median3(b0, b1, b2);
+        a = y + direction_from(g0, g1) * (r * beta);
+      }
+      const double w = r * r / 6.0;
+      out.u += w * source_value(o.source, o.n_source, a);
+      if (want_p) out.p += w * source_value(o.adjoint, o.n_adjoint, a);
+      y = y + direction_from(a0, a1) * r;
+      ++out.steps;
+    }
+    out.cap = true;
+  }
+  (void)primal_only;
+  out.aabb = st.aabb;
+  out.tri = st.tri;
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per-walk samples for n_sites sites (site ids site_ids[i], or i when null).
+// u, p: [n_sites * walks]; steps: [n_sites * walks] with bit 31 set on a cap.
+int oracle_walk_samples(const oracle_mesh *om, const oracle_params *o, const double *sites,
+                        const uint64_t *site_ids, uint32_t n_sites, const double *cav, uint32_t ncav, double *u,
+                        double *p, uint32_t *steps, uint64_t *tests) {
+  std::atomic<int> failed{0};
+#ifdef _OPENMP
+  if (o->threads > 0) omp_set_num_threads(o->threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int64_t i = 0; i < static_cast<int64_t>(n_sites); ++i) {
+    const Vec3 x{sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]};
+    const uint64_t sid = site_ids ? site_ids[i] : static_cast<uint64_t>(i);
+    const bool skip = o->skip_cavity_sites && inside_cavity(x, cav, ncav, o->cavity_radius);
+    for (int w = 0; w < o->walks; ++w) {
+      const size_t slot = static_cast<size_t>(i) * o->walks + w;
+      if (skip) {
+        u[slot] = 0.0;
+        if (p) p[slot] = 0.0;
+        steps[slot] = 0;
+        continue;
+      }
+      const WalkOut r = walk(om->m, *o, cav, ncav, x, sid, static_cast<uint32_t>(w), tests != nullptr);
+      if (r.failed) failed = 1;
+      u[slot] = r.u;
+      if (p) p[slot] = r.p;
+      steps[slot] = r.steps | (r.cap ? 0x80000000u : 0u);
+      if (tests) {
+        tests[2 * slot] = r.aabb;
+        tests[2 * slot + 1] = r.tri;
+      }
+    }
+  }
+  if (failed) {
+    g_error = "closest-point query failed";
+    return 1;
+  }
+  return 0;
+}
+
+// Per-site estimates.  Compliance: wih_twos.cpp:691-715 (mean, U-statistic
+// (S^2 - S2)/(n(n-1)), leave-one-out jackknife SE).  Paired/hot:
+// adjoint.cpp:36-41 (score (SuSp - Sup)/(n(n-1)), same_index Sup/n, hot
+// score = mean u) plus the jackknife SE of the cross statistic.
+int oracle_estimate(const oracle_mesh *om, const oracle_params *o, const double *sites, const uint64_t *site_ids,
+                    uint32_t n_sites, const double *cav, uint32_t ncav, oracle_site *out) {
+  const size_t total = static_cast<size_t>(n_sites) * o->walks;
+  std::vector<double> u(total), p(total);
+  std::vector<uint32_t> st(total);
+  const int rc = oracle_walk_samples(om, o, sites, site_ids, n_sites, cav, ncav, u.data(), p.data(), st.data(),
+                                     nullptr);
+  const double n = o->walks;
+  for (uint32_t i = 0; i < n_sites; ++i) {
+    const double *U = &u[static_cast<size_t>(i) * o->walks];
+    const double *P = &p[static_cast<size_t>(i) * o->walks];
+    const uint32_t *S = &st[static_cast<size_t>(i) * o->walks];
+    oracle_site r{};
+    for (int w = 0; w < o->walks; ++w) {
+      r.steps += S[w] & 0x7fffffffu;
+      r.caps += (S[w] >> 31) & 1u;
+    }
+    if (o->mode == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < o->walks; ++w) sum += U[w];
+      double sum2 = 0.0;
+      for (int w = 0; w < o->walks; ++w) sum2 += U[w] * U[w];
+      r.u = sum / n;
+      r.score = (sum * sum - sum2) / (n * (n - 1.0));
+      if (o->walks >= 4) {
+        std::vector<double> leave(o->walks);
+        for (int w = 0; w < o->walks; ++w) {
+          const double ls = sum - U[w], ls2 = sum2 - U[w] * U[w];
+          leave[w] = (ls * ls - ls2) / ((n - 1.0) * (n - 2.0));
+        }
+        double lm = 0.0;
+        for (double v : leave) lm += v;
+        lm /= n;
+        double spread = 0.0;
+        for (double v : leave) spread += (v - lm) * (v - lm);
+        r.score_se = std::sqrt((n - 1.0) / n * spread);
+      } else {
+        r.score_se = std::numeric_limits<double>::quiet_NaN();
+      }
+      r.p = r.u;
+      r.same_index = sum2 / n;
+    } else {
+      double su = 0.0, sp = 0.0, same = 0.0;
+      for (int w = 0; w < o->walks; ++w) {
+        su += U[w];
+        sp += P[w];
+        same += U[w] * P[w];
+      }
+      const bool hot = (o->mode == 2);
+      r.score = hot ? su / n : (su * sp - same) / (n * (n - 1));
+      if (o->walks >= 4) {
+        std::vector<double> leave(o->walks);
+        for (int w = 0; w < o->walks; ++w) {
+          if (hot) {
+            leave[w] = (su - U[w]) / (n - 1.0);
+          } else {
+            leave[w] = ((su - U[w]) * (sp - P[w]) - (same - U[w] * P[w])) / ((n - 1.0) * (n - 2.0));
+          }
+        }
+        double lm = 0.0;
+        for (double v : leave) lm += v;
+        lm /= n;
+        double spread = 0.0;
+        for (double v : leave) spread += (v - lm) * (v - lm);
+        r.score_se = std::sqrt((n - 1.0) / n * spread);
+      } else {
+        r.score_se = std::numeric_limits<double>::quiet_NaN();
+      }
+      r.same_index = same / n;
+      r.u = su / n;
+      r.p = sp / n;
+    }
+    out[i] = r;
+  }
+  return rc;
+}
+
+// Reference-identical paired output fields (adjoint.cpp:36-41): the site
+// loop skips sites inside a cavity (adjoint.cpp:123-126).
+int oracle_sizeof_params() { return static_cast<int>(sizeof(oracle_params)); }
+int oracle_sizeof_site() { return static_cast<int>(sizeof(oracle_site)); }
+
+}  // extern "C"

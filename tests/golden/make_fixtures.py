@@ -1,0 +1,87 @@
+"""Extract the golden fixtures used by the parity tests from the reference tree.
+
+Run once in a container where the reference checkout is mounted:
+
+    python tests/golden/make_fixtures.py /path/to/walking-into-holes
+
+It copies (meshes gzip-compressed) the reference's own tracked inputs and
+outputs for the TWoS backend:
+
+* compliance fields of benchmarks/compiled_bunny/output/ (wih_twos --mode twos,
+  affine source, eps 5e-4, max-steps 512, slope 0.65; argv from
+  run_compiled_benchmark.py:133-159, seeds from :676-760);
+* paired primal/adjoint requests of
+  benchmarks/distinct_adjoint/persistent_output/ (wih_adjoint, housing
+  source, sensor bump, Green-point sampling), with each request's argv.
+
+The fixtures are committed, so tests never read the reference at run time.
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import shutil
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+COMPLIANCE_FILES = [
+    "evaluation-points.csv",
+    "field-bunny-01000-faces.csv",
+    "field-bunny-04000-faces.csv",
+    "field-reference.csv",
+    "field-twos-0016.csv",
+    "reference-summary.json",
+    "summary-bunny-01000-faces.json",
+]
+MESHES = {
+    "benchmarks/compiled_bunny/output/bunny-01000-faces.ply": "bunny-01000-faces.ply.gz",
+    "benchmarks/compiled_bunny/output/bunny-04000-faces.ply": "bunny-04000-faces.ply.gz",
+    "benchmarks/stanford_bunny/output/stanford-bunny-watertight.ply": "stanford-bunny-watertight.ply.gz",
+    "benchmarks/engineering_housing/assets/stylized-finned-housing.ply": "stylized-finned-housing.ply.gz",
+}
+PAIRED = [
+    "side1/seed2026091500/twos_sparse/round1/scout",
+    "side1/seed2026091500/twos_dense/round2/rescore",
+    "side1/seed2026091500/wos_hot/round3/scout",
+    "side-1/seed2026091500/twos_sparse/round4/rescore",
+]
+
+
+def main(reference: Path) -> None:
+    out = HERE
+    for src, dst in MESHES.items():
+        with open(reference / src, "rb") as fh, gzip.GzipFile(out / dst, "wb", compresslevel=9, mtime=0) as gz:
+            shutil.copyfileobj(fh, gz)
+    comp = out / "compiled_bunny"
+    comp.mkdir(exist_ok=True)
+    for name in COMPLIANCE_FILES:
+        shutil.copyfile(reference / "benchmarks/compiled_bunny/output" / name, comp / name)
+    paired = out / "distinct_adjoint"
+    paired.mkdir(exist_ok=True)
+    base = reference / "benchmarks/distinct_adjoint/persistent_output"
+    index = []
+    for rel in PAIRED:
+        src = base / rel
+        tag = rel.replace("/", "_")
+        dst = paired / tag
+        dst.mkdir(exist_ok=True)
+        for name in ("points.csv", "holes.csv", "field.csv"):
+            if (src / name).exists():
+                shutil.copyfile(src / name, dst / name)
+        summary = json.loads((src / "summary.json").read_text())
+        argv = summary["command"][1:]
+        # Paths in the recorded argv are remapped to the fixture's own files.
+        keep = {}
+        for key, value in zip(argv[0::2], argv[1::2]):
+            if key in ("--mesh", "--points", "--output", "--summary", "--cavities"):
+                continue
+            keep[key] = value
+        (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
+        index.append(tag)
+    (paired / "index.json").write_text(json.dumps(index, indent=1) + "\n")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

@@ -1,0 +1,873 @@
+// CUDA kernels of libtwos.so (sm_100a).
+//
+//   wos_kernel       persistent walk-on-spheres: every lane runs one walk at a
+//                    time and refills from a device work queue when its walk
+//                    ends on the epsilon shell, so walks of very different
+//                    lengths do not idle a warp.  Replaces the OpenMP site loop
+//                    + evaluate_site/paired_site + walk of the reference
+//                    (wih_twos.cpp:635-717, 1825-1841; adjoint.cpp:18-42).
+//   nearest()        BVH closest-point query used by every step: 16-byte node
+//                    and triangle loads, nearest-child-first order, a traversal
+//                    stack in shared memory, pruning on push and pop.  Replaces
+//                    rtcPointQuery + point_query_callback (wih_twos.cpp:339-359,
+//                    416-430).
+//   finalize_kernel  one warp per site: FP64 U-statistic, means and the
+//                    leave-one-out jackknife SE over the per-walk samples with
+//                    warp-shuffle reductions in a fixed order (wih_twos.cpp:
+//                    691-715; adjoint.cpp:36-41).
+//   closest_kernel   batched closest point (tests and the queries/s figure).
+//   topk kernels     block-local bitonic top-k then a merge block.
+//
+// Compiled with -fmad=false: FP64 arithmetic is evaluated exactly as written
+// (no contraction), so it matches a plain IEEE FP64 evaluation on the host;
+// the FP32 path asks for FMAs explicitly where it wants them.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "twos_internal.h"
+
+namespace twos {
+
+// ================================================================ random stream
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): counter = (step, walk, site, repeat*8 + block).
+struct Philox4 {
+  uint32_t x, y, z, w;
+};
+
+__device__ __forceinline__ Philox4 philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2,
+                                          uint32_t c3) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    c0 = hi1 ^ c1 ^ k0;
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ k1;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return {c0, c1, c2, c3};
+}
+
+// Uniforms in [0,1): FP64 takes the top 53 bits of (hi:lo); FP32 takes the
+// top 24, i.e. the FP64 value truncated, so both forms share samples.
+template <typename T> __device__ __forceinline__ T uniform(uint32_t hi, uint32_t lo);
+template <> __device__ __forceinline__ double uniform<double>(uint32_t hi, uint32_t lo) {
+  const uint64_t v = (static_cast<uint64_t>(hi) << 32) | lo;
+  return static_cast<double>(v >> 11) * 0x1.0p-53;
+}
+template <> __device__ __forceinline__ float uniform<float>(uint32_t hi, uint32_t) {
+  return static_cast<float>(hi >> 8) * 0x1.0p-24f;
+}
+
+template <typename T> struct Vec {
+  T x, y, z;
+};
+
+__device__ __forceinline__ void sincos_pi(double a, double *s, double *c) { sincospi(a, s, c); }
+__device__ __forceinline__ void sincos_pi(float a, float *s, float *c) { sincospif(a, s, c); }
+
+// Uniform direction on S^2: z = 1 - 2a, phi = 2*pi*b (the parametrisation of
+// random_unit_vector, wih_twos.cpp:536-542).
+template <typename T> __device__ __forceinline__ Vec<T> direction(T a, T b) {
+  const T z = T(1) - T(2) * a;
+  const T zz = z * z;
+  const T radial = sqrt(fmax(T(0), T(1) - zz));
+  T s, c;
+  sincos_pi(T(2) * b, &s, &c);
+  return {radial * c, radial * s, z};
+}
+
+template <typename T> __device__ __forceinline__ T median3(T a, T b, T c) {
+  return fmax(fmin(a, b), fmin(fmax(a, b), c));
+}
+
+// ================================================================ arithmetic helpers
+// madd: FMA in FP32, plain multiply-add in FP64 (bit-identical to host FP64).
+__device__ __forceinline__ float madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double madd(double a, double b, double c) { return a * b + c; }
+
+__device__ __forceinline__ float dot3(const Vec<float> &a, const Vec<float> &b) {
+  return __fmaf_rn(a.x, b.x, __fmaf_rn(a.y, b.y, a.z * b.z));
+}
+__device__ __forceinline__ double dot3(const Vec<double> &a, const Vec<double> &b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename T> __device__ __forceinline__ Vec<T> sub(const Vec<T> &a, const Vec<T> &b) {
+  return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <typename T> __device__ __forceinline__ Vec<T> add_scaled(const Vec<T> &a, const Vec<T> &d, T s) {
+  return {a.x + d.x * s, a.y + d.y * s, a.z + d.z * s};
+}
+
+// Squared distance from p to the closest point of triangle (a, b, c):
+// Ericson's Voronoi-region case analysis (Real-Time Collision Detection,
+// 5.1.5), the algorithm of closest_point_triangle (wih_twos.cpp:247-289).
+template <typename T>
+__device__ __forceinline__ Vec<T> tri_closest(const Vec<T> &p, const Vec<T> &a, const Vec<T> &b, const Vec<T> &c) {
+  const Vec<T> ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+  const T d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  Vec<T> q;
+  if (d1 <= T(0) && d2 <= T(0)) {
+    q = a;
+  } else {
+    const Vec<T> bp = sub(p, b);
+    const T d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= T(0) && d4 <= d3) {
+      q = b;
+    } else {
+      const T vc = d1 * d4 - d3 * d2;
+      if (vc <= T(0) && d1 >= T(0) && d3 <= T(0)) {
+        const T v = d1 / (d1 - d3);
+        q = add_scaled(a, ab, v);
+      } else {
+        const Vec<T> cp = sub(p, c);
+        const T d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+        if (d6 >= T(0) && d5 <= d6) {
+          q = c;
+        } else {
+          const T vb = d5 * d2 - d1 * d6;
+          if (vb <= T(0) && d2 >= T(0) && d6 <= T(0)) {
+            const T w = d2 / (d2 - d6);
+            q = add_scaled(a, ac, w);
+          } else {
+            const T va = d3 * d6 - d5 * d4;
+            if (va <= T(0) && (d4 - d3) >= T(0) && (d5 - d6) >= T(0)) {
+              const T w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+              q = add_scaled(b, sub(c, b), w);
+            } else {
+              const T denom = T(1) / (va + vb + vc);
+              const T v = vb * denom, w = vc * denom;
+              const Vec<T> t = add_scaled(a, ab, v);
+              q = add_scaled(t, ac, w);
+            }
+          }
+        }
+      }
+    }
+  }
+  return q;
+}
+
+template <typename T>
+__device__ __forceinline__ T tri_dist2(const Vec<T> &p, const Vec<T> &a, const Vec<T> &b, const Vec<T> &c) {
+  const Vec<T> d = sub(p, tri_closest(p, a, b, c));
+  return dot3(d, d);
+}
+
+// ================================================================ BVH traversal
+template <typename T> struct Layout;
+template <> struct Layout<float> {
+  using Node = NodeF;
+  using Tri = TriF;
+};
+template <> struct Layout<double> {
+  using Node = NodeD;
+  using Tri = TriD;
+};
+
+__device__ __forceinline__ float gap(float lo, float hi, float p) { return fmaxf(fmaxf(lo - p, p - hi), 0.f); }
+__device__ __forceinline__ double gap(double lo, double hi, double p) { return fmax(fmax(lo - p, p - hi), 0.0); }
+
+__device__ __forceinline__ void node_dist2(const NodeF *__restrict__ nodes, int idx, const Vec<float> &p,
+                                           float &dl, float &dr, int &cl, int &cr) {
+  const float4 x = __ldg(&nodes[idx].x);
+  const float4 y = __ldg(&nodes[idx].y);
+  const float4 z = __ldg(&nodes[idx].z);
+  const int4 ch = __ldg(&nodes[idx].child);
+  const float lx = gap(x.x, x.z, p.x), rx = gap(x.y, x.w, p.x);
+  const float ly = gap(y.x, y.z, p.y), ry = gap(y.y, y.w, p.y);
+  const float lz = gap(z.x, z.z, p.z), rz = gap(z.y, z.w, p.z);
+  dl = __fmaf_rn(lx, lx, __fmaf_rn(ly, ly, lz * lz));
+  dr = __fmaf_rn(rx, rx, __fmaf_rn(ry, ry, rz * rz));
+  cl = ch.x;
+  cr = ch.y;
+}
+
+__device__ __forceinline__ void node_dist2(const NodeD *__restrict__ nodes, int idx, const Vec<double> &p,
+                                           double &dl, double &dr, int &cl, int &cr) {
+  const double2 xl = __ldg(&nodes[idx].xlo), xh = __ldg(&nodes[idx].xhi);
+  const double2 yl = __ldg(&nodes[idx].ylo), yh = __ldg(&nodes[idx].yhi);
+  const double2 zl = __ldg(&nodes[idx].zlo), zh = __ldg(&nodes[idx].zhi);
+  const int4 ch = __ldg(&nodes[idx].child);
+  const double lx = gap(xl.x, xh.x, p.x), rx = gap(xl.y, xh.y, p.x);
+  const double ly = gap(yl.x, yh.x, p.y), ry = gap(yl.y, yh.y, p.y);
+  const double lz = gap(zl.x, zh.x, p.z), rz = gap(zl.y, zh.y, p.z);
+  dl = lx * lx + ly * ly + lz * lz;
+  dr = rx * rx + ry * ry + rz * rz;
+  cl = ch.x;
+  cr = ch.y;
+}
+
+__device__ __forceinline__ void load_tri(const TriF *__restrict__ tris, uint32_t i, Vec<float> &a, Vec<float> &b,
+                                         Vec<float> &c) {
+  const float4 A = __ldg(&tris[i].a), B = __ldg(&tris[i].b), C = __ldg(&tris[i].c);
+  a = {A.x, A.y, A.z};
+  b = {B.x, B.y, B.z};
+  c = {C.x, C.y, C.z};
+}
+__device__ __forceinline__ void load_tri(const TriD *__restrict__ tris, uint32_t i, Vec<double> &a,
+                                         Vec<double> &b, Vec<double> &c) {
+  const double2 p0 = __ldg(&tris[i].axy), p1 = __ldg(&tris[i].azbx), p2 = __ldg(&tris[i].bybz);
+  const double2 p3 = __ldg(&tris[i].cxy), p4 = __ldg(&tris[i].czid);
+  a = {p0.x, p0.y, p1.x};
+  b = {p1.y, p2.x, p2.y};
+  c = {p3.x, p3.y, p4.x};
+}
+
+__device__ __forceinline__ float lower_f(float v) { return v; }
+__device__ __forceinline__ float lower_f(double v) { return __double2float_rd(v); }
+
+// Closest-point query: on return best2 holds the squared distance to the
+// nearest triangle strictly closer than sqrt(best2) on entry; returns false
+// when there is none.  The stack lives in shared memory, `stack` pointing at
+// this thread's column (stride `stride` entries).  Bounded: at most kStack
+// pushes outstanding and `max_iter` node/leaf visits; overruns set `err`.
+template <typename T>
+__device__ bool nearest(const typename Layout<T>::Node *__restrict__ nodes,
+                        const typename Layout<T>::Tri *__restrict__ tris, uint32_t max_iter, const Vec<T> &p,
+                        T &best2, uint32_t &best_tri, uint2 *stack, int stride, uint32_t &err) {
+  bool found = false;
+  int sp = 0;
+  int node = 0;
+  bool have = true;
+  uint32_t iter = 0;
+  while (have) {
+    if (++iter > max_iter) {
+      err |= TWOS_DEVERR_ITER;
+      break;
+    }
+    if (node >= 0) {
+      T dl, dr;
+      int cl, cr;
+      node_dist2(nodes, node, p, dl, dr, cl, cr);
+      const bool vl = dl < best2, vr = dr < best2;
+      if (vl && vr) {
+        if (dr < dl) {
+          const T td = dl;
+          dl = dr;
+          dr = td;
+          const int tc = cl;
+          cl = cr;
+          cr = tc;
+        }
+        if (sp >= kStack) {
+          err |= TWOS_DEVERR_STACK;
+          break;
+        }
+        stack[sp * stride] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+        ++sp;
+        node = cl;
+        continue;
+      }
+      if (vl) {
+        node = cl;
+        continue;
+      }
+      if (vr) {
+        node = cr;
+        continue;
+      }
+    } else {
+      const uint32_t enc = ~static_cast<uint32_t>(node);
+      const uint32_t first = enc >> 3, count = enc & 7u;
+      for (uint32_t i = 0; i < count; ++i) {
+        Vec<T> a, b, c;
+        load_tri(tris, first + i, a, b, c);
+        const T d2 = tri_dist2(p, a, b, c);
+        if (d2 < best2) {
+          best2 = d2;
+          best_tri = first + i;
+          found = true;
+        }
+      }
+    }
+    // Pop the next entry still closer than the current best.
+    have = false;
+    while (sp > 0) {
+      --sp;
+      const uint2 e = stack[sp * stride];
+      if (static_cast<T>(__uint_as_float(e.y)) < best2) {
+        node = static_cast<int>(e.x);
+        have = true;
+        break;
+      }
+    }
+  }
+  return found;
+}
+
+// ================================================================ sources
+template <typename T> struct TermT {
+  int kind, axis;
+  T amp, offset, div;
+  T c[3], w[3];
+};
+
+template <typename T> __device__ __forceinline__ T coord(const Vec<T> &v, int a) {
+  return a == 0 ? v.x : (a == 1 ? v.y : v.z);
+}
+
+template <typename T> __device__ __forceinline__ T term_value(const TermT<T> &t, const Vec<T> &x) {
+  switch (t.kind) {
+    case TWOS_TERM_CONST:
+      return t.amp;
+    case TWOS_TERM_LINEAR:
+      return t.amp * (coord(x, t.axis) + t.offset);
+    case TWOS_TERM_GAUSS: {
+      const T a = (x.x - t.c[0]) / t.w[0], b = (x.y - t.c[1]) / t.w[1], c = (x.z - t.c[2]) / t.w[2];
+      return t.amp * exp(-(a * a) - (b * b) - (c * c));
+    }
+    case TWOS_TERM_BUMP: {
+      const Vec<T> d{x.x - t.c[0], x.y - t.c[1], x.z - t.c[2]};
+      const T dd = d.x * d.x + d.y * d.y + d.z * d.z;
+      const T s = fmax(T(0), T(1) - dd / (t.w[0] * t.w[0]));
+      return t.amp * (s * s) / t.div;
+    }
+    case TWOS_TERM_BOX:
+      return (x.x >= t.c[0] && x.x <= t.w[0] && x.y >= t.c[1] && x.y <= t.w[1] && x.z >= t.c[2] &&
+              x.z <= t.w[2])
+                 ? t.amp
+                 : T(0);
+    case TWOS_TERM_BALL: {
+      const Vec<T> d{x.x - t.c[0], x.y - t.c[1], x.z - t.c[2]};
+      const T dd = d.x * d.x + d.y * d.y + d.z * d.z;
+      return dd <= t.w[0] * t.w[0] ? t.amp : T(0);
+    }
+    default:
+      return T(0);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T source_value(const TermT<T> *terms, uint32_t begin, uint32_t n, const Vec<T> &x) {
+  if (n == 0) return T(0);
+  T s = term_value(terms[begin], x);
+  for (uint32_t i = 1; i < n; ++i) s = s + term_value(terms[begin + i], x);
+  return s;
+}
+
+// ================================================================ WoS kernel
+constexpr int kWosBlock = 128;
+constexpr int kMaxSmemJobs = 32;
+constexpr int kMaxSmemGeos = 32;
+constexpr int kMaxSmemTerms = 64;
+
+template <typename T> __device__ __forceinline__ T to_T(double v);
+template <> __device__ __forceinline__ double to_T<double>(double v) { return v; }
+template <> __device__ __forceinline__ float to_T<float>(double v) { return static_cast<float>(v); }
+
+// Position of a site/cavity in the geometry frame: FP64 keeps the original
+// coordinates; FP32 is taken about the geometry centre.
+template <typename T> __device__ __forceinline__ Vec<T> to_frame(const double *xyz, const GeoDesc &g);
+template <> __device__ __forceinline__ Vec<double> to_frame<double>(const double *xyz, const GeoDesc &) {
+  return {xyz[0], xyz[1], xyz[2]};
+}
+template <> __device__ __forceinline__ Vec<float> to_frame<float>(const double *xyz, const GeoDesc &g) {
+  return {static_cast<float>(xyz[0] - g.center[0]), static_cast<float>(xyz[1] - g.center[1]),
+          static_cast<float>(xyz[2] - g.center[2])};
+}
+
+template <typename T> __device__ __forceinline__ const typename Layout<T>::Node *geo_nodes(const GeoDesc &g);
+template <> __device__ __forceinline__ const NodeF *geo_nodes<float>(const GeoDesc &g) { return g.nodes_f; }
+template <> __device__ __forceinline__ const NodeD *geo_nodes<double>(const GeoDesc &g) { return g.nodes_d; }
+template <typename T> __device__ __forceinline__ const typename Layout<T>::Tri *geo_tris(const GeoDesc &g);
+template <> __device__ __forceinline__ const TriF *geo_tris<float>(const GeoDesc &g) { return g.tris_f; }
+template <> __device__ __forceinline__ const TriD *geo_tris<double>(const GeoDesc &g) { return g.tris_d; }
+
+__device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, uint64_t wid) {
+  uint32_t lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].walk_begin <= wid)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// MODE: TWOS_MODE_*.  The per-walk value type is T (FP32 accumulation in the
+// mixed form, FP64 in the plain form).
+template <typename T, int MODE, bool GREEN>
+__global__ void __launch_bounds__(kWosBlock, 4) wos_kernel(const WosLaunch L) {
+  __shared__ uint2 s_stack[kStack * kWosBlock];
+  __shared__ JobDesc s_jobs[kMaxSmemJobs];
+  __shared__ GeoDesc s_geos[kMaxSmemGeos];
+  __shared__ TermT<T> s_terms[kMaxSmemTerms];
+
+  for (uint32_t i = threadIdx.x; i < L.n_jobs; i += blockDim.x) s_jobs[i] = L.jobs[i];
+  for (uint32_t i = threadIdx.x; i < L.n_geos; i += blockDim.x) s_geos[i] = L.geos[i];
+  for (uint32_t i = threadIdx.x; i < L.n_terms; i += blockDim.x) {
+    const TermDev &d = L.terms[i];
+    TermT<T> t;
+    t.kind = d.kind;
+    t.axis = d.axis;
+    t.amp = to_T<T>(d.amp);
+    t.offset = to_T<T>(d.offset);
+    t.div = to_T<T>(d.div);
+    for (int k = 0; k < 3; ++k) {
+      t.c[k] = to_T<T>(d.c[k]);
+      t.w[k] = to_T<T>(d.w[k]);
+    }
+    s_terms[i] = t;
+  }
+  __syncthreads();
+
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned full = 0xffffffffu;
+  uint2 *stack = s_stack + threadIdx.x;
+  uint32_t err = 0;
+
+  bool active = false;
+  bool exhausted = false;  // warp-uniform
+  uint64_t wid = 0;
+  uint32_t job = 0, site = 0, walk = 0, steps = 0;
+  Vec<T> pos{T(0), T(0), T(0)};
+  T u = T(0), pv = T(0);
+
+  for (;;) {
+    // ---- refill idle lanes from the work queue
+    const unsigned idle = __ballot_sync(full, !active);
+    if (!exhausted && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
+      unsigned long long base = 0;
+      const int leader = __ffs(idle) - 1;
+      if (static_cast<int>(lane) == leader) base = atomicAdd(L.counter, static_cast<unsigned long long>(__popc(idle)));
+      base = __shfl_sync(full, base, leader);
+      if (base + __popc(idle) >= L.total_walks) exhausted = true;
+      if (!active) {
+        const uint64_t id = base + __popc(idle & ((1u << lane) - 1u));
+        if (id < L.total_walks) {
+          wid = id;
+          job = find_job(s_jobs, L.n_jobs, id);
+          const JobDesc &J = s_jobs[job];
+          const uint64_t local = id - J.walk_begin;
+          site = static_cast<uint32_t>(local / J.walks);
+          walk = static_cast<uint32_t>(local - static_cast<uint64_t>(site) * J.walks);
+          const GeoDesc &G = s_geos[J.geo];
+          pos = to_frame<T>(L.sites + 3ull * (J.site_begin + site), G);
+          u = T(0);
+          pv = T(0);
+          steps = 0;
+          active = true;
+          if (J.flags & kJobSkipCavitySites) {
+            const T R = to_T<T>(J.cavity_radius);
+            for (uint32_t c = 0; c < J.n_cav; ++c) {
+              const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
+              const Vec<T> d = sub(pos, cc);
+              if (sqrt(dot3(d, d)) <= R) active = false;
+            }
+            if (!active) {
+              static_cast<T *>(L.u_out)[wid] = T(0);
+              if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+              L.steps_out[wid] = 0u;
+            }
+          }
+        }
+      }
+    }
+    if (__ballot_sync(full, active) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+
+    // ---- one walk-on-spheres step
+    const JobDesc &J = s_jobs[job];
+    const GeoDesc &G = s_geos[J.geo];
+    T best2 = static_cast<T>(J.query_radius2);
+    uint32_t best_tri = 0;
+    const bool found =
+        nearest<T>(geo_nodes<T>(G), geo_tris<T>(G), G.max_iter, pos, best2, best_tri, stack, kWosBlock, err);
+    T d = sqrt(best2);
+    if (!found) {
+      err |= TWOS_DEVERR_QUERY;
+      d = T(0);  // ends the walk; the call reports the failure
+    }
+    const T R = to_T<T>(J.cavity_radius);
+    for (uint32_t c = 0; c < J.n_cav; ++c) {
+      const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
+      const Vec<T> dv = sub(pos, cc);
+      const T dc = sqrt(dot3(dv, dv)) - R;
+      d = dc < d ? dc : d;
+    }
+    const T r = d - static_cast<T>(G.delta);  // delta is 0 in the FP64 form
+    bool done = !(r > to_T<T>(J.epsilon));
+    bool cap = false;
+    if (!done) {
+      const uint32_t ctr3 = J.repeat << 3;
+      const Philox4 q0 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 0u);
+      Vec<T> a = pos;
+      if (GREEN) {
+        const Philox4 q1 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 1u);
+        const Philox4 q2 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 2u);
+        const Philox4 q3 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 3u);
+        const T beta = median3(uniform<T>(q2.x, q2.y), uniform<T>(q2.z, q2.w), uniform<T>(q3.x, q3.y));
+        const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
+        a = add_scaled(pos, g, r * beta);
+      }
+      const T w = r * r / T(6);
+      u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
+      if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+      const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
+      pos = add_scaled(pos, dir, r);
+      ++steps;
+      if (static_cast<int>(steps) >= J.max_steps) {
+        done = true;
+        cap = true;
+      }
+    }
+    if (done) {
+      static_cast<T *>(L.u_out)[wid] = u;
+      if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
+      L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
+      active = false;
+    }
+  }
+  if (err) atomicOr(L.error, err);
+}
+
+template <typename T, int MODE, bool GREEN> static const void *wos_fn() {
+  return reinterpret_cast<const void *>(&wos_kernel<T, MODE, GREEN>);
+}
+
+static const void *select_wos(int precision, int mode, bool green) {
+  // Paired and hot share the paired instantiation's layout except for p.
+#define TWOS_PICK(T)                                                                          \
+  if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true>() : wos_fn<T, 0, false>(); \
+  if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true>() : wos_fn<T, 1, false>();     \
+  return green ? wos_fn<T, 2, true>() : wos_fn<T, 2, false>();
+  if (precision == TWOS_PREC_MIXED) {
+    TWOS_PICK(float)
+  }
+  TWOS_PICK(double)
+#undef TWOS_PICK
+}
+
+cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
+                       cudaStream_t s) {
+  if (block != kWosBlock) return cudaErrorInvalidValue;
+  if (L.n_jobs == 0 || L.n_jobs > static_cast<uint32_t>(kMaxSmemJobs) || L.n_geos > static_cast<uint32_t>(kMaxSmemGeos) ||
+      L.n_terms > static_cast<uint32_t>(kMaxSmemTerms))
+    return cudaErrorInvalidValue;
+  const void *fn = select_wos(precision, mode, green);
+  WosLaunch copy = L;
+  void *args[] = {&copy};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+}
+
+int wos_max_blocks_per_sm(int precision, int mode, bool green, int block) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, select_wos(precision, mode, green), block, 0) !=
+      cudaSuccess)
+    return 0;
+  return n;
+}
+
+// ================================================================ finalize
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename V, int MODE>
+__global__ void __launch_bounds__(256) finalize_kernel(const FinalizeLaunch F) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t g = warp; g < F.total_sites; g += nwarps) {
+    // Job of launch site g (jobs ordered by site_rank).
+    uint32_t lo = 0, hi = F.n_jobs - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (F.jobs[mid].site_rank <= g)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const JobDesc &J = F.jobs[lo];
+    const uint32_t s = g - J.site_rank;
+    const uint64_t base = J.walk_begin + static_cast<uint64_t>(s) * J.walks;
+    const V *U = static_cast<const V *>(F.u) + base;
+    const V *P = static_cast<const V *>(F.p) + base;
+    const uint32_t *S = F.steps + base;
+    const uint32_t n = J.walks;
+    const double nd = static_cast<double>(n);
+    double a = 0.0, b = 0.0, c = 0.0;
+    unsigned long long st = 0, caps = 0;
+    for (uint32_t w = lane; w < n; w += 32) {
+      const double x = static_cast<double>(U[w]);
+      const uint32_t sw = S[w];
+      st += sw & 0x7fffffffu;
+      caps += sw >> 31;
+      if (MODE == TWOS_MODE_PAIRED) {
+        const double y = static_cast<double>(P[w]);
+        a += x;
+        b += y;
+        c += x * y;
+      } else {
+        a += x;
+        b += x * x;
+      }
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    st = warp_sum_u64(st);
+    caps = warp_sum_u64(caps);
+    twos_site_result r;
+    r.steps = st;
+    r.caps = caps;
+    // Leave-one-out values, their mean and spread (two more passes over the
+    // samples, which are L2-resident at this point).
+    double lsum = 0.0;
+    for (uint32_t w = lane; w < n; w += 32) {
+      const double x = static_cast<double>(U[w]);
+      double leave;
+      if (MODE == TWOS_MODE_COMPLIANCE) {
+        const double ls = a - x, ls2 = b - x * x;
+        leave = (ls * ls - ls2) / ((nd - 1.0) * (nd - 2.0));
+      } else if (MODE == TWOS_MODE_PAIRED) {
+        const double y = static_cast<double>(P[w]);
+        leave = ((a - x) * (b - y) - (c - x * y)) / ((nd - 1.0) * (nd - 2.0));
+      } else {
+        leave = (a - x) / (nd - 1.0);
+      }
+      lsum += leave;
+    }
+    const double lmean = warp_sum(lsum) / nd;
+    double spread = 0.0;
+    for (uint32_t w = lane; w < n; w += 32) {
+      const double x = static_cast<double>(U[w]);
+      double leave;
+      if (MODE == TWOS_MODE_COMPLIANCE) {
+        const double ls = a - x, ls2 = b - x * x;
+        leave = (ls * ls - ls2) / ((nd - 1.0) * (nd - 2.0));
+      } else if (MODE == TWOS_MODE_PAIRED) {
+        const double y = static_cast<double>(P[w]);
+        leave = ((a - x) * (b - y) - (c - x * y)) / ((nd - 1.0) * (nd - 2.0));
+      } else {
+        leave = (a - x) / (nd - 1.0);
+      }
+      const double dv = leave - lmean;
+      spread += dv * dv;
+    }
+    spread = warp_sum(spread);
+    const double se = n >= 4 ? sqrt((nd - 1.0) / nd * spread) : CUDART_NAN;
+    if (MODE == TWOS_MODE_COMPLIANCE) {
+      r.u = a / nd;
+      r.p = r.u;
+      r.score = (a * a - b) / (nd * (nd - 1.0));
+      r.same_index = b / nd;
+    } else if (MODE == TWOS_MODE_PAIRED) {
+      r.u = a / nd;
+      r.p = b / nd;
+      r.score = (a * b - c) / (nd * (nd - 1.0));
+      r.same_index = c / nd;
+    } else {
+      r.u = a / nd;
+      r.p = 0.0;
+      r.score = a / nd;
+      r.same_index = 0.0;
+    }
+    r.score_se = se;
+    if (lane == 0) {
+      F.out[J.site_begin + s] = r;
+      if (F.totals) {
+        atomicAdd(&F.totals[0], st);
+        atomicAdd(&F.totals[1], caps);
+      }
+    }
+  }
+}
+
+cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s) {
+  if (F.total_sites == 0) return cudaSuccess;
+  const int block = 256;
+  const uint64_t warps = F.total_sites;
+  int grid = static_cast<int>(std::min<uint64_t>((warps * 32 + block - 1) / block, 148ull * 16));
+  FinalizeLaunch copy = F;
+  void *args[] = {&copy};
+  const void *fn;
+  if (precision == TWOS_PREC_MIXED) {
+    fn = mode == TWOS_MODE_COMPLIANCE ? reinterpret_cast<const void *>(&finalize_kernel<float, 0>)
+         : mode == TWOS_MODE_PAIRED   ? reinterpret_cast<const void *>(&finalize_kernel<float, 1>)
+                                      : reinterpret_cast<const void *>(&finalize_kernel<float, 2>);
+  } else {
+    fn = mode == TWOS_MODE_COMPLIANCE ? reinterpret_cast<const void *>(&finalize_kernel<double, 0>)
+         : mode == TWOS_MODE_PAIRED   ? reinterpret_cast<const void *>(&finalize_kernel<double, 1>)
+                                      : reinterpret_cast<const void *>(&finalize_kernel<double, 2>);
+  }
+  return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+}
+
+// ================================================================ batched closest point
+template <typename T>
+__global__ void __launch_bounds__(kWosBlock) closest_kernel(const GeoDesc *geo, const double *pts, uint64_t n,
+                                                            double query_radius2, double *dist, double *closest,
+                                                            uint32_t *error) {
+  __shared__ uint2 s_stack[kStack * kWosBlock];
+  __shared__ GeoDesc G;
+  if (threadIdx.x == 0) G = *geo;
+  __syncthreads();
+  uint32_t err = 0;
+  uint2 *stack = s_stack + threadIdx.x;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const Vec<T> p = to_frame<T>(pts + 3 * i, G);
+    T best2 = static_cast<T>(query_radius2);
+    uint32_t best_tri = 0;
+    const bool found =
+        nearest<T>(geo_nodes<T>(G), geo_tris<T>(G), G.max_iter, p, best2, best_tri, stack, kWosBlock, err);
+    dist[i] = found ? static_cast<double>(sqrt(best2)) : CUDART_INF;
+    if (closest) {
+      double q[3] = {CUDART_NAN, CUDART_NAN, CUDART_NAN};
+      if (found) {
+        Vec<T> a, b, c;
+        load_tri(geo_tris<T>(G), best_tri, a, b, c);
+        const Vec<T> cp = tri_closest(p, a, b, c);
+        const bool f32 = sizeof(T) == 4;
+        q[0] = static_cast<double>(cp.x) + (f32 ? G.center[0] : 0.0);
+        q[1] = static_cast<double>(cp.y) + (f32 ? G.center[1] : 0.0);
+        q[2] = static_cast<double>(cp.z) + (f32 ? G.center[2] : 0.0);
+      }
+      closest[3 * i] = q[0];
+      closest[3 * i + 1] = q[1];
+      closest[3 * i + 2] = q[2];
+    }
+  }
+  if (err) atomicOr(error, err);
+}
+
+cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
+                           double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int block = kWosBlock;
+  const int grid = static_cast<int>(std::min<uint64_t>((n + block - 1) / block, 148ull * 32));
+  if (precision == TWOS_PREC_MIXED)
+    closest_kernel<float><<<grid, block, 0, s>>>(geo_dev, pts, n, query_radius2, dist, closest, error);
+  else
+    closest_kernel<double><<<grid, block, 0, s>>>(geo_dev, pts, n, query_radius2, dist, closest, error);
+  return cudaGetLastError();
+}
+
+// ================================================================ top-k
+// Keys compare by (value desc, index asc); NaN sorts last.
+struct KeyIdx {
+  double v;
+  uint32_t i;
+};
+__device__ __forceinline__ bool before(const KeyIdx &a, const KeyIdx &b) {
+  const bool an = isnan(a.v), bn = isnan(b.v);
+  if (an != bn) return bn;
+  if (a.v != b.v) return a.v > b.v;
+  return a.i < b.i;
+}
+
+constexpr int kTopkTile = 2048;
+
+// Sorts one tile of kTopkTile keys in shared memory (bitonic) and writes its
+// first k entries.
+__global__ void __launch_bounds__(1024) topk_tile_kernel(const double *keys, uint32_t n, uint32_t k,
+                                                         KeyIdx *partial) {
+  __shared__ double sv[kTopkTile];
+  __shared__ uint32_t si[kTopkTile];
+  const uint32_t base = blockIdx.x * kTopkTile;
+  for (uint32_t t = threadIdx.x; t < kTopkTile; t += blockDim.x) {
+    const uint32_t g = base + t;
+    sv[t] = g < n ? keys[g] : -CUDART_INF;
+    si[t] = g < n ? g : 0xffffffffu;
+  }
+  __syncthreads();
+  for (uint32_t size = 2; size <= kTopkTile; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t t = threadIdx.x; t < kTopkTile / 2; t += blockDim.x) {
+        const uint32_t pos = 2 * t - (t & (stride - 1));
+        const uint32_t a = pos, b = pos + stride;
+        const bool up = ((pos & size) == 0);
+        const KeyIdx ka{sv[a], si[a]}, kb{sv[b], si[b]};
+        const bool swap = up ? before(kb, ka) : before(ka, kb);
+        if (swap) {
+          sv[a] = kb.v;
+          si[a] = kb.i;
+          sv[b] = ka.v;
+          si[b] = ka.i;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t t = threadIdx.x; t < k; t += blockDim.x) partial[blockIdx.x * k + t] = {sv[t], si[t]};
+}
+
+// Merges the per-tile candidates by repeated selection of the best remaining
+// (k <= 1024, candidates <= a few hundred thousand).
+__global__ void __launch_bounds__(1024) topk_merge_kernel(const KeyIdx *partial, uint32_t m, uint32_t k,
+                                                          uint32_t *index) {
+  __shared__ KeyIdx red[32];
+  __shared__ KeyIdx last;
+  if (threadIdx.x == 0) last = {CUDART_INF, 0u};
+  __syncthreads();
+  for (uint32_t r = 0; r < k; ++r) {
+    KeyIdx best{-CUDART_INF, 0xffffffffu};
+    bool have = false;
+    for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) {
+      const KeyIdx c = partial[t];
+      if (c.i == 0xffffffffu) continue;
+      if (r > 0 && !before(last, c)) continue;  // already taken
+      if (!have || before(c, best)) {
+        best = c;
+        have = true;
+      }
+    }
+    // Block reduction.
+    for (int o = 16; o > 0; o >>= 1) {
+      KeyIdx other{__shfl_xor_sync(0xffffffffu, best.v, o), __shfl_xor_sync(0xffffffffu, best.i, o)};
+      if (other.i != 0xffffffffu && (best.i == 0xffffffffu || before(other, best))) best = other;
+    }
+    if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      KeyIdx b2 = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : KeyIdx{-CUDART_INF, 0xffffffffu};
+      for (int o = 16; o > 0; o >>= 1) {
+        KeyIdx other{__shfl_xor_sync(0xffffffffu, b2.v, o), __shfl_xor_sync(0xffffffffu, b2.i, o)};
+        if (other.i != 0xffffffffu && (b2.i == 0xffffffffu || before(other, b2))) b2 = other;
+      }
+      if (threadIdx.x == 0) {
+        index[r] = b2.i;
+        last = b2;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+size_t topk_scratch_bytes(uint32_t n, uint32_t k) {
+  const uint32_t tiles = (n + kTopkTile - 1) / kTopkTile;
+  return static_cast<size_t>(tiles) * k * sizeof(KeyIdx);
+}
+
+cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *index, void *scratch,
+                        size_t scratch_bytes, cudaStream_t s) {
+  if (n == 0 || k == 0) return cudaSuccess;
+  if (k > 1024 || k > static_cast<uint32_t>(kTopkTile)) return cudaErrorInvalidValue;
+  if (scratch_bytes < topk_scratch_bytes(n, k)) return cudaErrorInvalidValue;
+  const uint32_t tiles = (n + kTopkTile - 1) / kTopkTile;
+  KeyIdx *partial = static_cast<KeyIdx *>(scratch);
+  topk_tile_kernel<<<tiles, 1024, 0, s>>>(keys, n, k, partial);
+  topk_merge_kernel<<<1, 1024, 0, s>>>(partial, tiles * k, k, index);
+  return cudaGetLastError();
+}
+
+}  // namespace twos

@@ -1,0 +1,616 @@
+// C ABI of libtwos.so (include/twos.h): mesh sessions, request validation,
+// device memory, chunked kernel launches and the mapping of device error bits
+// and step caps onto the reference's error behaviour.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "twos_internal.h"
+
+namespace twos {
+
+static thread_local std::string g_error;
+
+static int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+void counter_key(uint64_t seed, uint32_t stream, uint32_t &k0, uint32_t &k1) {
+  uint64_t x = seed + 0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(stream) + 1);
+  // SplitMix64 finaliser (Steele, Lea & Flood 2014).
+  x += 0x9e3779b97f4a7c15ULL;
+  x = (x ^ (x >> 30U)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27U)) * 0x94d049bb133111ebULL;
+  x = x ^ (x >> 31U);
+  k0 = static_cast<uint32_t>(x);
+  k1 = static_cast<uint32_t>(x >> 32);
+}
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+static void check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Grow-only device allocation.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    check(cudaMalloc(&ptr, std::max<size_t>(n, 256)), "cudaMalloc");
+    bytes = std::max<size_t>(n, 256);
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+}  // namespace twos
+
+using namespace twos;
+
+struct twos_mesh {
+  int device = 0;
+  std::vector<double> vertices;
+  std::vector<uint32_t> faces;
+  HostBvh bvh;
+  double bmin[3], bmax[3], center[3];
+  double delta = 0.0;
+  double build_seconds = 0.0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;   // stream in use
+  cudaStream_t own_stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
+  DevBuf nodes_f, tris_f, nodes_d, tris_d;
+  DevBuf geo;  // one GeoDesc
+  GeoDesc geo_host{};
+  uint64_t resident_bytes = 0;
+  // Scratch, grown on demand.
+  DevBuf jobs, terms, cavities, sites, out, u, p, steps, counter, totals, points, dist, closest, topk;
+  size_t max_launch_walks = size_t(1) << 30;
+  int refill = 1;
+};
+
+namespace {
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, twos_mesh **out) {
+  if (!out) return fail(TWOS_ERR_USAGE, "null output pointer");
+  *out = nullptr;
+  if (f.empty() || v.empty()) return fail(TWOS_ERR_USAGE, "expected a nonempty triangle mesh");
+  const size_t nv = v.size() / 3;
+  for (uint32_t idx : f)
+    if (idx >= nv) return fail(TWOS_ERR_USAGE, "face index out of range");
+  for (double x : v)
+    if (!std::isfinite(x)) return fail(TWOS_ERR_USAGE, "non-finite vertex coordinate");
+  auto m = std::make_unique<twos_mesh>();
+  m->device = device;
+  m->vertices = std::move(v);
+  m->faces = std::move(f);
+  try {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop;
+    check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    m->num_sms = prop.multiProcessorCount;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int a = 0; a < 3; ++a) {
+      m->bmin[a] = std::numeric_limits<double>::infinity();
+      m->bmax[a] = -std::numeric_limits<double>::infinity();
+    }
+    for (size_t i = 0; i < nv; ++i)
+      for (int a = 0; a < 3; ++a) {
+        m->bmin[a] = std::min(m->bmin[a], m->vertices[3 * i + a]);
+        m->bmax[a] = std::max(m->bmax[a], m->vertices[3 * i + a]);
+      }
+    double reach = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      m->center[a] = 0.5 * (m->bmin[a] + m->bmax[a]);
+      reach = std::max(reach, 0.5 * (m->bmax[a] - m->bmin[a]));
+    }
+    // FP32 distance error bound for the mixed form: coordinates within
+    // `reach` of the centre carry at most ulp(reach)/2 representation error
+    // each; the closest-point arithmetic adds a few ulps.  32 * 2^-24 * reach
+    // covers both with margin (checked against FP64 in the tests).
+    m->delta = 32.0 * std::ldexp(1.0, -24) * std::max(reach, 1e-30);
+    build_bvh(m->vertices, m->faces, m->bvh);
+    std::vector<NodeF> nf;
+    std::vector<TriF> tf;
+    std::vector<NodeD> nd;
+    std::vector<TriD> td;
+    pack_bvh_f32(m->bvh, m->vertices, m->faces, m->center, nf, tf);
+    pack_bvh_f64(m->bvh, m->vertices, m->faces, nd, td);
+    check(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    m->stream = m->own_stream;
+    check(cudaEventCreate(&m->ev0), "cudaEventCreate");
+    check(cudaEventCreate(&m->ev1), "cudaEventCreate");
+    check(cudaEventCreate(&m->evw), "cudaEventCreate");
+    m->nodes_f.reserve(nf.size() * sizeof(NodeF));
+    m->tris_f.reserve(tf.size() * sizeof(TriF));
+    m->nodes_d.reserve(nd.size() * sizeof(NodeD));
+    m->tris_d.reserve(td.size() * sizeof(TriD));
+    check(cudaMemcpy(m->nodes_f.ptr, nf.data(), nf.size() * sizeof(NodeF), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(m->tris_f.ptr, tf.data(), tf.size() * sizeof(TriF), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(m->nodes_d.ptr, nd.data(), nd.size() * sizeof(NodeD), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(m->tris_d.ptr, td.data(), td.size() * sizeof(TriD), cudaMemcpyHostToDevice), "upload");
+    m->resident_bytes = nf.size() * sizeof(NodeF) + tf.size() * sizeof(TriF) + nd.size() * sizeof(NodeD) +
+                        td.size() * sizeof(TriD);
+    GeoDesc &g = m->geo_host;
+    g.nodes_f = m->nodes_f.as<NodeF>();
+    g.tris_f = m->tris_f.as<TriF>();
+    g.nodes_d = m->nodes_d.as<NodeD>();
+    g.tris_d = m->tris_d.as<TriD>();
+    for (int a = 0; a < 3; ++a) g.center[a] = m->center[a];
+    g.delta = static_cast<float>(m->delta);
+    g.max_iter = static_cast<uint32_t>(std::min<uint64_t>(4ull * m->bvh.nodes.size() + 16, 0xffffffffull));
+    m->geo.reserve(sizeof(GeoDesc));
+    check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
+    m->counter.reserve(16);
+    m->totals.reserve(32);
+    m->build_seconds = seconds_since(t0);
+    if (const char *e = std::getenv("TWOS_MAX_LAUNCH_WALKS")) m->max_launch_walks = std::strtoull(e, nullptr, 10);
+    if (const char *e = std::getenv("TWOS_REFILL")) m->refill = std::max(1, std::atoi(e));
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  *out = m.release();
+  return TWOS_OK;
+}
+
+int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav) {
+  if (!r) return fail(TWOS_ERR_USAGE, "null request");
+  if (r->mode < 0 || r->mode > 2) return fail(TWOS_ERR_USAGE, "invalid mode");
+  if (r->precision != TWOS_PREC_FP64 && r->precision != TWOS_PREC_MIXED)
+    return fail(TWOS_ERR_USAGE, "invalid precision");
+  if (r->walks < 2) return fail(TWOS_ERR_USAGE, "walks must be at least 2");
+  if (r->max_steps < 1) return fail(TWOS_ERR_USAGE, "max_steps must be at least 1");
+  if (!(r->epsilon > 0.0)) return fail(TWOS_ERR_USAGE, "epsilon must be positive");
+  if (r->cavity_radius < 0.0 || (n_cav > 0 && !(r->cavity_radius > 0.0)))
+    return fail(TWOS_ERR_USAGE, "cavities need a positive cavity radius");
+  if (r->n_source < 0 || r->n_source > TWOS_MAX_TERMS || r->n_adjoint < 0 || r->n_adjoint > TWOS_MAX_TERMS)
+    return fail(TWOS_ERR_USAGE, "too many source terms");
+  for (int i = 0; i < r->n_source + r->n_adjoint; ++i) {
+    const twos_source_term &t = i < r->n_source ? r->source[i] : r->adjoint[i - r->n_source];
+    if (t.kind < TWOS_TERM_CONST || t.kind > TWOS_TERM_BALL) return fail(TWOS_ERR_USAGE, "unknown source term");
+    if (t.kind == TWOS_TERM_LINEAR && (t.axis < 0 || t.axis > 2)) return fail(TWOS_ERR_USAGE, "bad term axis");
+  }
+  if (n_cav > 4096) return fail(TWOS_ERR_USAGE, "at most 4096 cavities per request");
+  (void)n_sites;
+  return TWOS_OK;
+}
+
+// Translates a term into the FP32 frame about `c` (identity for FP64).
+TermDev frame_term(const twos_source_term &t, const double c[3]) {
+  TermDev d;
+  std::memcpy(&d, &t, sizeof(d));
+  switch (t.kind) {
+    case TWOS_TERM_LINEAR:
+      d.offset = t.offset + c[t.axis];
+      break;
+    case TWOS_TERM_GAUSS:
+    case TWOS_TERM_BUMP:
+    case TWOS_TERM_BALL:
+      for (int a = 0; a < 3; ++a) d.c[a] = t.c[a] - c[a];
+      break;
+    case TWOS_TERM_BOX:
+      for (int a = 0; a < 3; ++a) {
+        d.c[a] = t.c[a] - c[a];
+        d.w[a] = t.w[a] - c[a];
+      }
+      break;
+    default:
+      break;
+  }
+  return d;
+}
+
+struct RunOut {
+  double kernel_seconds = 0.0;
+  double walk_seconds = 0.0;
+  uint32_t launches = 0;
+  uint32_t error_flags = 0;
+  uint64_t steps = 0, caps = 0;
+};
+
+// Runs the estimator over device-resident sites into device-resident rows.
+// When `keep` is non-null, per-walk samples of the (single) launch are left in
+// the session's u/p/steps buffers.
+void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, uint32_t n_sites,
+                  const double *cav, uint32_t n_cav, twos_site_result *d_out, RunOut &ro, bool keep) {
+  const bool mixed = r->precision == TWOS_PREC_MIXED;
+  const int mode = r->mode;
+  const bool paired = mode == TWOS_MODE_PAIRED;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const double *frame = mixed ? m->center : zero;
+  std::vector<TermDev> terms;
+  for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
+  for (int i = 0; i < r->n_adjoint; ++i) terms.push_back(frame_term(r->adjoint[i], frame));
+  if (terms.empty()) terms.push_back(TermDev{});
+  m->terms.reserve(terms.size() * sizeof(TermDev));
+  check(cudaMemcpyAsync(m->terms.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice,
+                        m->stream),
+        "upload terms");
+  m->cavities.reserve(std::max<size_t>(1, n_cav) * 3 * sizeof(double));
+  if (n_cav)
+    check(cudaMemcpyAsync(m->cavities.ptr, cav, n_cav * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
+          "upload cavities");
+  const size_t walks = static_cast<size_t>(r->walks);
+  const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
+  const size_t chunk_sites =
+      std::max<size_t>(1, std::min<size_t>(n_sites, std::max<size_t>(1, m->max_launch_walks / walks)));
+  if (keep && chunk_sites < n_sites) throw std::runtime_error("sample request exceeds one launch");
+  const size_t chunk_walks = chunk_sites * walks;
+  m->u.reserve(chunk_walks * vbytes);
+  if (paired) m->p.reserve(chunk_walks * vbytes);
+  m->steps.reserve(chunk_walks * sizeof(uint32_t));
+  m->jobs.reserve(sizeof(JobDesc));
+  check(cudaMemsetAsync(m->totals.ptr, 0, 2 * sizeof(unsigned long long) + sizeof(uint32_t), m->stream),
+        "memset");
+  uint32_t k0, k1;
+  counter_key(r->seed, r->stream, k0, k1);
+  const int block = 128;
+  const int per_sm = wos_max_blocks_per_sm(r->precision, mode, r->green != 0, block);
+  if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
+  const int grid = per_sm * m->num_sms;
+  const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
+  float ms_total = 0.f, ms_walk = 0.f;
+  for (size_t first = 0; first < n_sites; first += chunk_sites) {
+    const uint32_t count = static_cast<uint32_t>(std::min<size_t>(chunk_sites, n_sites - first));
+    JobDesc J{};
+    J.walk_begin = 0;
+    J.n_sites = count;
+    J.walks = static_cast<uint32_t>(r->walks);
+    J.site_begin = static_cast<uint32_t>(first);
+    J.site_offset = r->site_offset + static_cast<uint32_t>(first);
+    J.geo = 0;
+    J.k0 = k0;
+    J.k1 = k1;
+    J.repeat = r->repeat;
+    J.max_steps = r->max_steps;
+    J.flags = (r->green ? kJobGreen : 0u) | (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
+    J.epsilon = r->epsilon;
+    J.query_radius2 = qr * qr;
+    J.cavity_radius = r->cavity_radius;
+    J.src_begin = 0;
+    J.n_src = static_cast<uint32_t>(r->n_source);
+    J.adj_begin = static_cast<uint32_t>(r->n_source);
+    J.n_adj = static_cast<uint32_t>(r->n_adjoint);
+    J.cav_begin = 0;
+    J.n_cav = n_cav;
+    J.site_rank = 0;
+    check(cudaMemcpyAsync(m->jobs.ptr, &J, sizeof(J), cudaMemcpyHostToDevice, m->stream), "upload job");
+    check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+    WosLaunch L{};
+    L.jobs = m->jobs.as<JobDesc>();
+    L.n_jobs = 1;
+    L.geos = m->geo.as<GeoDesc>();
+    L.n_geos = 1;
+    L.sites = d_sites;
+    L.terms = m->terms.as<TermDev>();
+    L.n_terms = static_cast<uint32_t>(terms.size());
+    L.cavities = m->cavities.as<double>();
+    L.total_walks = static_cast<uint64_t>(count) * walks;
+    L.counter = m->counter.as<unsigned long long>();
+    L.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    L.u_out = m->u.ptr;
+    L.p_out = paired ? m->p.ptr : nullptr;
+    L.steps_out = m->steps.as<uint32_t>();
+    L.refill = m->refill;
+    FinalizeLaunch F{};
+    F.jobs = L.jobs;
+    F.n_jobs = 1;
+    F.total_sites = count;
+    F.totals = m->totals.as<unsigned long long>();
+    F.u = L.u_out;
+    F.p = L.p_out;
+    F.steps = L.steps_out;
+    F.out = d_out;
+    check(cudaEventRecord(m->ev0, m->stream), "event");
+    check(launch_wos(r->precision, mode, r->green != 0, L, grid, block, m->stream), "WoS launch");
+    check(cudaEventRecord(m->evw, m->stream), "event");
+    check(launch_finalize(r->precision, mode, F, m->stream), "finalize launch");
+    check(cudaEventRecord(m->ev1, m->stream), "event");
+    check(cudaEventSynchronize(m->ev1), "WoS kernels");
+    float ms = 0.f, msw = 0.f;
+    check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
+    check(cudaEventElapsedTime(&msw, m->ev0, m->evw), "event time");
+    ms_total += ms;
+    ms_walk += msw;
+    ro.launches += 2;
+  }
+  unsigned long long tot[3] = {0, 0, 0};
+  check(cudaMemcpyAsync(tot, m->totals.ptr, 2 * sizeof(unsigned long long) + sizeof(uint32_t),
+                        cudaMemcpyDeviceToHost, m->stream),
+        "download totals");
+  check(cudaStreamSynchronize(m->stream), "sync");
+  ro.steps = tot[0];
+  ro.caps = tot[1];
+  uint32_t err = 0;
+  std::memcpy(&err, &tot[2], sizeof(uint32_t));
+  ro.error_flags = err;
+  ro.kernel_seconds = ms_total * 1e-3;
+  ro.walk_seconds = ms_walk * 1e-3;
+}
+
+int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summary *summary, double t_total,
+           uint64_t h2d, uint64_t d2h) {
+  if (summary) {
+    summary->kernel_seconds = ro.kernel_seconds;
+    summary->walk_seconds = ro.walk_seconds;
+    summary->total_seconds = t_total;
+    summary->paths = static_cast<uint64_t>(n_sites) * static_cast<uint64_t>(r->walks);
+    summary->steps = ro.steps;
+    summary->caps = ro.caps;
+    summary->queries = ro.steps + summary->paths;
+    summary->h2d_bytes = h2d;
+    summary->d2h_bytes = d2h;
+    summary->launches = ro.launches;
+    summary->error_flags = ro.error_flags;
+  }
+  if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
+  if (ro.error_flags & TWOS_DEVERR_STACK) return fail(TWOS_ERR_RUNTIME, "BVH traversal stack bound exceeded");
+  if (ro.error_flags & TWOS_DEVERR_ITER) return fail(TWOS_ERR_RUNTIME, "BVH traversal iteration bound exceeded");
+  if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  if (ro.caps) return fail(TWOS_ERR_RUNTIME, "one or more paths hit --max-steps");
+  return TWOS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int twos_abi_version(void) { return TWOS_ABI_VERSION; }
+
+const char *twos_last_error(void) { return g_error.c_str(); }
+
+int twos_mesh_open(const double *vertices, uint64_t n_vertices, const uint32_t *faces, uint64_t n_faces,
+                   int device, twos_mesh **out) {
+  if (!vertices || !faces) return fail(TWOS_ERR_USAGE, "null mesh buffers");
+  std::vector<double> v(vertices, vertices + 3 * n_vertices);
+  std::vector<uint32_t> f(faces, faces + 3 * n_faces);
+  return open_impl(std::move(v), std::move(f), device, out);
+}
+
+int twos_mesh_open_ply(const char *path, int device, twos_mesh **out) {
+  if (!path) return fail(TWOS_ERR_USAGE, "null path");
+  std::vector<double> v;
+  std::vector<uint32_t> f;
+  try {
+    load_ascii_ply(path, v, f);
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return open_impl(std::move(v), std::move(f), device, out);
+}
+
+void twos_mesh_close(twos_mesh *m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->terms, &m->cavities,
+                    &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->counter, &m->totals, &m->points, &m->dist,
+                    &m->closest, &m->topk})
+    b->release();
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->evw) cudaEventDestroy(m->evw);
+  if (m->own_stream) cudaStreamDestroy(m->own_stream);
+  delete m;
+}
+
+int twos_mesh_set_stream(twos_mesh *m, void *stream) {
+  if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
+  cudaSetDevice(m->device);
+  cudaStreamSynchronize(m->stream);
+  m->stream = stream ? static_cast<cudaStream_t>(stream) : m->own_stream;
+  return TWOS_OK;
+}
+
+int twos_mesh_get_info(const twos_mesh *m, twos_mesh_info *info) {
+  if (!m || !info) return fail(TWOS_ERR_USAGE, "null argument");
+  info->vertices = m->vertices.size() / 3;
+  info->faces = m->faces.size() / 3;
+  info->bvh_nodes = m->bvh.nodes.size();
+  info->bvh_depth = static_cast<uint32_t>(m->bvh.depth);
+  info->device = static_cast<uint32_t>(m->device);
+  for (int a = 0; a < 3; ++a) {
+    info->bounds_min[a] = m->bmin[a];
+    info->bounds_max[a] = m->bmax[a];
+    info->center[a] = m->center[a];
+  }
+  info->mixed_delta = m->delta;
+  info->build_seconds = m->build_seconds;
+  info->device_bytes = m->resident_bytes;
+  return TWOS_OK;
+}
+
+int twos_closest_point(twos_mesh *m, int precision, const double *points, uint64_t n, double query_radius,
+                       double *distance, double *closest) {
+  if (!m || (!points && n) || (!distance && n)) return fail(TWOS_ERR_USAGE, "null argument");
+  if (precision != TWOS_PREC_FP64 && precision != TWOS_PREC_MIXED) return fail(TWOS_ERR_USAGE, "invalid precision");
+  if (n == 0) return TWOS_OK;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->points.reserve(n * 3 * sizeof(double));
+    m->dist.reserve(n * sizeof(double));
+    if (closest) m->closest.reserve(n * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->points.ptr, points, n * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
+          "upload points");
+    check(cudaMemsetAsync(m->totals.ptr, 0, 32, m->stream), "memset");
+    const double qr = query_radius > 0.0 ? query_radius : std::numeric_limits<double>::infinity();
+    uint32_t *err = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    check(launch_closest(precision, m->geo.as<GeoDesc>(), m->points.as<double>(), n, qr * qr,
+                         m->dist.as<double>(), closest ? m->closest.as<double>() : nullptr, err, m->stream),
+          "closest launch");
+    check(cudaMemcpyAsync(distance, m->dist.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+          "download");
+    if (closest)
+      check(cudaMemcpyAsync(closest, m->closest.ptr, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+            "download");
+    uint32_t e = 0;
+    check(cudaMemcpyAsync(&e, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, m->stream), "download");
+    check(cudaStreamSynchronize(m->stream), "closest kernel");
+    if (e & (TWOS_DEVERR_STACK | TWOS_DEVERR_ITER)) return fail(TWOS_ERR_RUNTIME, "BVH traversal bound exceeded");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return TWOS_OK;
+}
+
+int twos_estimate_device(twos_mesh *m, const twos_request *r, const double *d_sites, uint32_t n_sites,
+                         const double *cavities, uint32_t n_cavities, twos_site_result *d_out,
+                         twos_summary *summary) {
+  if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
+  if (int rc = validate_request(r, n_sites, n_cavities)) return rc;
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  if (!d_sites || !d_out || (n_cavities && !cavities)) return fail(TWOS_ERR_USAGE, "null buffer");
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    run_estimate(m, r, d_sites, n_sites, cavities, n_cavities, d_out, ro, false);
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return finish(ro, n_sites, r, summary, seconds_since(t0), 0, 0);
+}
+
+int twos_estimate(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,
+                  const double *cavities, uint32_t n_cavities, twos_site_result *out, twos_summary *summary) {
+  if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
+  if (int rc = validate_request(r, n_sites, n_cavities)) return rc;
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  if (!sites || !out || (n_cavities && !cavities)) return fail(TWOS_ERR_USAGE, "null buffer");
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  const uint64_t h2d = static_cast<uint64_t>(n_sites) * 3 * sizeof(double) + n_cavities * 3 * sizeof(double);
+  const uint64_t d2h = static_cast<uint64_t>(n_sites) * sizeof(twos_site_result);
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    m->out.reserve(static_cast<size_t>(n_sites) * sizeof(twos_site_result));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    run_estimate(m, r, m->sites.as<double>(), n_sites, cavities, n_cavities, m->out.as<twos_site_result>(), ro,
+                 false);
+    check(cudaMemcpyAsync(out, m->out.ptr, d2h, cudaMemcpyDeviceToHost, m->stream), "download results");
+    check(cudaStreamSynchronize(m->stream), "sync");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return finish(ro, n_sites, r, summary, seconds_since(t0), h2d, d2h);
+}
+
+int twos_walk_samples(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,
+                      const double *cavities, uint32_t n_cavities, double *u, double *p, uint32_t *steps) {
+  if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
+  if (int rc = validate_request(r, n_sites, n_cavities)) return rc;
+  if (n_sites == 0) return TWOS_OK;
+  if (!sites || !u || !steps) return fail(TWOS_ERR_USAGE, "null buffer");
+  const size_t total = static_cast<size_t>(n_sites) * static_cast<size_t>(r->walks);
+  if (total > m->max_launch_walks) return fail(TWOS_ERR_USAGE, "too many walks for one sample request");
+  RunOut ro;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    m->out.reserve(static_cast<size_t>(n_sites) * sizeof(twos_site_result));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    run_estimate(m, r, m->sites.as<double>(), n_sites, cavities, n_cavities, m->out.as<twos_site_result>(), ro,
+                 true);
+    const bool mixed = r->precision == TWOS_PREC_MIXED;
+    const bool paired = r->mode == TWOS_MODE_PAIRED;
+    if (mixed) {
+      std::vector<float> tmp(total);
+      check(cudaMemcpy(tmp.data(), m->u.ptr, total * sizeof(float), cudaMemcpyDeviceToHost), "download");
+      for (size_t i = 0; i < total; ++i) u[i] = tmp[i];
+      if (p) {
+        if (paired) {
+          check(cudaMemcpy(tmp.data(), m->p.ptr, total * sizeof(float), cudaMemcpyDeviceToHost), "download");
+          for (size_t i = 0; i < total; ++i) p[i] = tmp[i];
+        } else {
+          std::fill(p, p + total, 0.0);
+        }
+      }
+    } else {
+      check(cudaMemcpy(u, m->u.ptr, total * sizeof(double), cudaMemcpyDeviceToHost), "download");
+      if (p) {
+        if (paired)
+          check(cudaMemcpy(p, m->p.ptr, total * sizeof(double), cudaMemcpyDeviceToHost), "download");
+        else
+          std::fill(p, p + total, 0.0);
+      }
+    }
+    check(cudaMemcpy(steps, m->steps.ptr, total * sizeof(uint32_t), cudaMemcpyDeviceToHost), "download");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
+  if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  return TWOS_OK;
+}
+
+int twos_inside(twos_mesh *m, const double *points, uint64_t n, uint8_t *inside) {
+  if (!m || (n && (!points || !inside))) return fail(TWOS_ERR_USAGE, "null argument");
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint64_t threads = std::min<uint64_t>(hw, std::max<uint64_t>(1, n / 1024));
+  std::vector<std::string> errs(threads);
+  std::vector<int> codes(threads, 0);
+  std::vector<std::thread> pool;
+  for (uint64_t t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t] {
+      for (uint64_t i = t; i < n; i += threads) {
+        bool in = false;
+        if (inside_parity(m->bvh, m->vertices, m->faces, points + 3 * i, in, errs[t])) {
+          codes[t] = 1;
+          return;
+        }
+        inside[i] = in ? 1 : 0;
+      }
+    });
+  }
+  for (auto &th : pool) th.join();
+  for (uint64_t t = 0; t < threads; ++t)
+    if (codes[t]) return fail(TWOS_ERR_RUNTIME, errs[t]);
+  return TWOS_OK;
+}
+
+int twos_topk_device(twos_mesh *m, const double *d_keys, uint32_t n, uint32_t k, uint32_t *d_index) {
+  if (!m || (n && (!d_keys || !d_index))) return fail(TWOS_ERR_USAGE, "null argument");
+  if (k > 1024) return fail(TWOS_ERR_USAGE, "k must be at most 1024");
+  if (k > n) return fail(TWOS_ERR_USAGE, "k must not exceed n");
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    const size_t bytes = topk_scratch_bytes(n, k);
+    m->topk.reserve(bytes);
+    check(launch_topk(d_keys, n, k, d_index, m->topk.ptr, m->topk.bytes, m->stream), "topk launch");
+    check(cudaStreamSynchronize(m->stream), "topk kernels");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return TWOS_OK;
+}
+
+}  // extern "C"

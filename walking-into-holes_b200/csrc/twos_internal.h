@@ -1,0 +1,169 @@
+// Internal layouts shared by the host code (twos_abi.cpp, bvh.cpp) and the
+// CUDA kernels (kernels.cu) of libtwos.so.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "twos.h"
+
+namespace twos {
+
+// ---------------------------------------------------------------- BVH layouts
+// Binary BVH; each node stores both children's boxes so one node fetch gives
+// the two box tests.  Child encoding: >= 0 internal node index; < 0 leaf with
+// ~child = (first_triangle << 3) | count (count 0..7, 0 = empty child whose
+// box is inverted so it is never entered).
+constexpr int kLeafMax = 4;
+constexpr int kMaxDepth = 30;    // builder bound; the traversal stack holds kStack entries
+constexpr int kStack = 32;
+
+// FP32 node: 64 bytes, four 16-byte loads.  x = (l.lo.x, r.lo.x, l.hi.x, r.hi.x),
+// likewise y and z; child = (left, right, -, -).
+struct alignas(64) NodeF {
+  float4 x, y, z;
+  int4 child;
+};
+static_assert(sizeof(NodeF) == 64, "NodeF layout");
+
+// FP64 node: 128 bytes.  lo/hi pairs (left, right) per axis.
+struct alignas(16) NodeD {
+  double2 xlo, xhi, ylo, yhi, zlo, zhi;
+  int4 child;
+  int4 pad;
+};
+static_assert(sizeof(NodeD) == 128, "NodeD layout");
+
+// FP32 triangle: 48 bytes: (a.xyz, id), (b.xyz, 0), (c.xyz, 0).
+struct alignas(16) TriF {
+  float4 a, b, c;
+};
+static_assert(sizeof(TriF) == 48, "TriF layout");
+
+// FP64 triangle: 96 bytes, six 16-byte loads.
+struct alignas(16) TriD {
+  double2 axy, azbx, bybz, cxy, czid, pad;
+};
+static_assert(sizeof(TriD) == 96, "TriD layout");
+
+// Host-side BVH produced by the builder (bvh.cpp).
+struct HostBvh {
+  struct Node {
+    double lo[2][3], hi[2][3];  // child boxes (left, right)
+    int32_t child[2];
+  };
+  std::vector<Node> nodes;      // nodes[0] is the root (always internal)
+  std::vector<uint32_t> order;  // leaf triangle order -> original triangle index
+  int depth = 0;
+};
+
+void build_bvh(const std::vector<double> &vertices, const std::vector<uint32_t> &faces, HostBvh &out);
+
+// Packs the host BVH into device layouts.  FP32 coordinates are taken about
+// `center`; boxes are taken from the rounded FP32 vertices so they contain the
+// FP32 triangles exactly.
+void pack_bvh_f32(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
+                  const double center[3], std::vector<NodeF> &nodes, std::vector<TriF> &tris);
+void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
+                  std::vector<NodeD> &nodes, std::vector<TriD> &tris);
+
+// Host ray-parity membership over the host BVH (EmbreeMesh::inside).
+int inside_parity(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
+                  const double p[3], bool &inside, std::string &err);
+
+// ASCII PLY reader with the reference's rules; throws std::runtime_error.
+void load_ascii_ply(const std::string &path, std::vector<double> &vertices, std::vector<uint32_t> &faces);
+// CSV/whitespace point reader (wih_twos.cpp:508-522); throws when empty.
+std::vector<double> read_points(const std::string &path);
+
+// ---------------------------------------------------------------- launch descriptors
+// One geometry resident on the device.
+struct GeoDesc {
+  const NodeF *nodes_f;
+  const TriF *tris_f;
+  const NodeD *nodes_d;
+  const TriD *tris_d;
+  double center[3];   // FP32 frame origin (mixed form)
+  float delta;        // FP32 distance error bound (mixed form)
+  uint32_t max_iter;  // traversal iteration bound (node + leaf visits)
+};
+
+// One job = one geometry x a contiguous range of sites with one request.
+struct JobDesc {
+  uint64_t walk_begin;   // first global walk id of the job
+  uint32_t n_sites;
+  uint32_t walks;
+  uint32_t site_begin;   // index of the job's first site in the sites/results arrays
+  uint32_t site_offset;  // added to the local site index in the sample key
+  uint32_t geo;
+  uint32_t k0, k1;       // Philox key
+  uint32_t repeat;
+  int32_t max_steps;
+  uint32_t flags;        // kJobGreen | kJobSkipCavitySites
+  double epsilon;
+  double query_radius2;  // squared initial radius (+inf when unbounded)
+  double cavity_radius;
+  uint32_t src_begin, n_src, adj_begin, n_adj;
+  uint32_t cav_begin, n_cav;
+  uint32_t site_rank;    // sites of the launch's earlier jobs (finalize lookup)
+  uint32_t pad;
+};
+constexpr uint32_t kJobGreen = 1u;
+constexpr uint32_t kJobSkipCavitySites = 2u;
+
+struct TermDev {
+  int32_t kind;
+  int32_t axis;
+  double amp, offset, div;
+  double c[3], w[3];
+};
+static_assert(sizeof(TermDev) == sizeof(twos_source_term), "term layout");
+
+struct WosLaunch {
+  const JobDesc *jobs;
+  uint32_t n_jobs;
+  const GeoDesc *geos;
+  uint32_t n_geos;
+  const double *sites;      // [n][3], original coordinates
+  const TermDev *terms;     // job term ranges index this table (frame of the job's geometry)
+  uint32_t n_terms;
+  const double *cavities;   // [n][3]
+  uint64_t total_walks;
+  unsigned long long *counter;  // work-queue head, zeroed before launch
+  uint32_t *error;              // TWOS_DEVERR_* bits
+  void *u_out;                  // per-walk u: float (mixed) or double (fp64)
+  void *p_out;                  // per-walk p (paired), same type
+  uint32_t *steps_out;          // per-walk steps | cap << 31
+  int refill;                   // refill a warp once this many lanes are idle
+};
+
+struct FinalizeLaunch {
+  const JobDesc *jobs;
+  uint32_t n_jobs;
+  uint32_t total_sites;           // sites of this launch (sum of job n_sites)
+  unsigned long long *totals;     // [0] += steps, [1] += caps
+  const void *u;
+  const void *p;
+  const uint32_t *steps;
+  twos_site_result *out;
+};
+
+// Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
+cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
+                       cudaStream_t s);
+int wos_max_blocks_per_sm(int precision, int mode, bool green, int block);
+cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s);
+cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
+                           double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s);
+cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *index, void *scratch,
+                        size_t scratch_bytes, cudaStream_t s);
+size_t topk_scratch_bytes(uint32_t n, uint32_t k);
+
+// Host copy of the counter-based key derivation (shared definition with the
+// device draw layout): key = splitmix64(seed + golden * (stream + 1)).
+void counter_key(uint64_t seed, uint32_t stream, uint32_t &k0, uint32_t &k1);
+
+}  // namespace twos

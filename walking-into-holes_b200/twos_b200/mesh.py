@@ -1,0 +1,195 @@
+"""Python face of libtwos.so: a mesh session and its estimator calls.
+
+``Mesh`` owns a twos_mesh session (BVH resident on one GPU).  Its methods are
+thin wrappers over the C ABI with numpy buffers:
+
+* ``estimate``      per-site (u, p, score, score_se, same_index, steps, caps)
+                    -- evaluate_site / paired_site of the reference
+                    (benchmarks/compiled_bunny/src/wih_twos.cpp:674-717,
+                    benchmarks/distinct_adjoint/adjoint.cpp:18-42);
+* ``estimate_device`` the same with device-resident sites and results (torch
+                    tensors or raw pointers);
+* ``walk_samples``  per-walk u, p and steps;
+* ``closest_point`` batched distance/closest point (wih_twos.cpp:339-359);
+* ``inside``        ray-parity membership (wih_twos.cpp:361-394);
+* ``topk_device``   top-k site indices.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi, sources
+from ._abi import (MODE_COMPLIANCE, MODE_HOT, MODE_PAIRED, PREC_FP64, PREC_MIXED, Request, SITE_DTYPE, Summary,
+                   check)
+
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
+MODES = {"compliance": MODE_COMPLIANCE, "paired": MODE_PAIRED, "hot": MODE_HOT}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Config:
+    """One estimation request (the reference's Options, wih_twos.cpp:73-101)."""
+    walks: int = 16
+    mode: str = "compliance"
+    precision: str = "mixed"
+    max_steps: int = 512
+    seed: int = 20260912
+    repeat: int = 0
+    stream: int = 0
+    epsilon: float = 5e-4
+    cavity_radius: float = 0.0
+    query_radius: float = 4.0
+    green: bool = False
+    source: list = field(default_factory=lambda: sources.affine())
+    adjoint: list = field(default_factory=list)
+    skip_cavity_sites: bool | None = None
+    site_offset: int = 0
+
+    def to_request(self) -> Request:
+        r = Request()
+        r.mode = MODES[self.mode] if isinstance(self.mode, str) else int(self.mode)
+        r.precision = PRECISIONS[self.precision] if isinstance(self.precision, str) else int(self.precision)
+        r.walks = int(self.walks)
+        r.max_steps = int(self.max_steps)
+        r.seed = int(self.seed)
+        r.repeat = int(self.repeat)
+        r.stream = int(self.stream)
+        r.epsilon = float(self.epsilon)
+        r.cavity_radius = float(self.cavity_radius)
+        r.query_radius = float(self.query_radius) if self.query_radius is not None else 0.0
+        r.green = int(bool(self.green))
+        if len(self.source) > _abi.MAX_TERMS or len(self.adjoint) > _abi.MAX_TERMS:
+            raise ValueError("too many source terms")
+        r.n_source, r.n_adjoint = len(self.source), len(self.adjoint)
+        for i, t in enumerate(self.source):
+            r.source[i] = t
+        for i, t in enumerate(self.adjoint):
+            r.adjoint[i] = t
+        skip = self.skip_cavity_sites
+        if skip is None:
+            skip = r.mode != MODE_COMPLIANCE
+        r.skip_cavity_sites = int(bool(skip))
+        r.site_offset = int(self.site_offset)
+        return r
+
+
+def _summary_dict(s: Summary) -> dict:
+    return {k: getattr(s, k) for k, _ in Summary._fields_}
+
+
+class Mesh:
+    """A triangle mesh resident on one GPU, with its BVH (FP32 and FP64)."""
+
+    def __init__(self, vertices=None, faces=None, *, ply: str | None = None, device: int = 0):
+        L = _abi.load()
+        h = ctypes.c_void_p()
+        if ply is not None:
+            check(L.twos_mesh_open_ply(str(ply).encode(), device, ctypes.byref(h)))
+        else:
+            v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+            f = np.ascontiguousarray(faces, dtype=np.uint32).reshape(-1, 3)
+            check(L.twos_mesh_open(_ptr(v), len(v), _ptr(f), len(f), device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _abi.load().twos_mesh_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream=None):
+        """Run the session's work on `stream` (torch.cuda.Stream, a raw handle, or None for its own)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
+
+    def info(self) -> dict:
+        i = _abi.MeshInfo()
+        check(_abi.load().twos_mesh_get_info(self._h, ctypes.byref(i)))
+        return {"vertices": i.vertices, "faces": i.faces, "bvh_nodes": i.bvh_nodes, "bvh_depth": i.bvh_depth,
+                "device": i.device, "bounds_min": list(i.bounds_min), "bounds_max": list(i.bounds_max),
+                "center": list(i.center), "mixed_delta": i.mixed_delta, "build_seconds": i.build_seconds,
+                "device_bytes": i.device_bytes}
+
+    # ------------------------------------------------------------------ queries
+    def closest_point(self, points, precision="fp64", query_radius=0.0, with_points=True):
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        n = len(pts)
+        dist = np.empty(n)
+        closest = np.empty((n, 3)) if with_points else None
+        check(_abi.load().twos_closest_point(self._h, PRECISIONS[precision], _ptr(pts), n, float(query_radius),
+                                             _ptr(dist), _ptr(closest)))
+        return (dist, closest) if with_points else dist
+
+    def inside(self, points):
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(len(pts), dtype=np.uint8)
+        check(_abi.load().twos_inside(self._h, _ptr(pts), len(pts), _ptr(out)))
+        return out.astype(bool)
+
+    # ------------------------------------------------------------------ estimator
+    def estimate(self, sites, config: Config, cavities=None, raise_on_caps=True, out=None):
+        """Per-site estimates (structured array with SITE_DTYPE fields) and the call summary.
+
+        `out` may be a preallocated SITE_DTYPE array (e.g. a view of pinned memory)."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        if out is None:
+            out = np.zeros(len(s), dtype=SITE_DTYPE)
+        elif out.dtype != np.dtype(SITE_DTYPE) or len(out) != len(s) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous SITE_DTYPE array with one row per site")
+        req = config.to_request()
+        summ = Summary()
+        rc = _abi.load().twos_estimate(self._h, ctypes.byref(req), _ptr(s), len(s), _ptr(cav), len(cav), _ptr(out),
+                                       ctypes.byref(summ))
+        if rc != _abi.OK and not (not raise_on_caps and summ.error_flags == 0 and summ.caps > 0):
+            check(rc)
+        return out, _summary_dict(summ)
+
+    def estimate_device(self, d_sites, n_sites, d_out, config: Config, cavities=None):
+        """Device-resident sites (n x 3 float64) and rows (n x 56 bytes); pointers or torch tensors."""
+        def addr(x):
+            return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        req = config.to_request()
+        summ = Summary()
+        check(_abi.load().twos_estimate_device(self._h, ctypes.byref(req), ctypes.c_void_p(addr(d_sites)),
+                                               int(n_sites), _ptr(cav), len(cav), ctypes.c_void_p(addr(d_out)),
+                                               ctypes.byref(summ)))
+        return _summary_dict(summ)
+
+    def walk_samples(self, sites, config: Config, cavities=None):
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        n, w = len(s), int(config.walks)
+        u = np.empty((n, w))
+        p = np.empty((n, w))
+        st = np.empty((n, w), dtype=np.uint32)
+        req = config.to_request()
+        check(_abi.load().twos_walk_samples(self._h, ctypes.byref(req), _ptr(s), n, _ptr(cav), len(cav), _ptr(u),
+                                            _ptr(p), _ptr(st)))
+        return {"u": u, "p": p, "steps": st & 0x7FFFFFFF, "caps": (st >> 31).astype(bool)}
+
+    def topk_device(self, d_keys, n, k, d_index):
+        def addr(x):
+            return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
+        check(_abi.load().twos_topk_device(self._h, ctypes.c_void_p(addr(d_keys)), int(n), int(k),
+                                           ctypes.c_void_p(addr(d_index))))
