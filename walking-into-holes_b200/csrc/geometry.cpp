@@ -258,88 +258,250 @@ void build_bvh(const std::vector<double> &v, const std::vector<uint32_t> &f, Hos
   if (out.depth > kMaxDepth) throw std::runtime_error("BVH depth bound exceeded");
 }
 
+namespace {
+
+float round_down(double x) {
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) > x) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+  return f;
+}
+float round_up(double x) {
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) < x) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+  return f;
+}
+
+struct Range {
+  uint32_t begin = 0, end = 0;
+};
+
+Range code_range(int32_t code, const std::vector<Range> &node_range) {
+  if (code >= 0) return node_range[code];
+  const uint32_t enc = ~static_cast<uint32_t>(code);
+  return {enc >> 3, (enc >> 3) + (enc & 7u)};
+}
+
+// Leaf-order ranges of every node (children always follow their parent).
+std::vector<Range> node_ranges(const HostBvh &bvh) {
+  std::vector<Range> r(bvh.nodes.size());
+  for (size_t ni = bvh.nodes.size(); ni-- > 0;) {
+    const Range a = code_range(bvh.nodes[ni].child[0], r), b = code_range(bvh.nodes[ni].child[1], r);
+    if (a.end == a.begin) {
+      r[ni] = b;
+    } else if (b.end == b.begin) {
+      r[ni] = a;
+    } else {
+      r[ni] = {std::min(a.begin, b.begin), std::max(a.end, b.end)};
+    }
+  }
+  return r;
+}
+
+// Vertex coordinates of leaf-order triangle i in a frame (the FP32 layout
+// passes the rounded FP32 coordinates, the FP64 layout the originals).
+struct TriCoords {
+  std::vector<double> xyz;  // 9 per triangle
+  const double *tri(uint32_t i) const { return &xyz[9 * static_cast<size_t>(i)]; }
+};
+
+void cross(const double *a, const double *b, const double *c, double out[3]) {
+  const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  const double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+  out[0] = e1[1] * e2[2] - e1[2] * e2[1];
+  out[1] = e1[2] * e2[0] - e1[0] * e2[2];
+  out[2] = e1[0] * e2[1] - e1[1] * e2[0];
+}
+
+// Unit mean normal of a triangle range and the interval of n.v over its
+// vertices.  `nq` receives the direction as the kernel stores it (FP32-rounded
+// for the FP32 layout), and the interval is computed with that direction.
+// Returns false (no slab) when the normals cancel.
+bool range_slab(const TriCoords &tc, Range r, bool fp32, double nq[3], double &smin, double &smax) {
+  double N[3] = {0, 0, 0}, total = 0.0;
+  for (uint32_t i = r.begin; i < r.end; ++i) {
+    const double *t = tc.tri(i);
+    double c[3];
+    cross(t, t + 3, t + 6, c);
+    N[0] += c[0];
+    N[1] += c[1];
+    N[2] += c[2];
+    total += std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+  }
+  const double len = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+  if (!(len > 1e-3 * total) || !(len > 0.0)) return false;
+  for (int k = 0; k < 3; ++k) {
+    nq[k] = N[k] / len;
+    if (fp32) nq[k] = static_cast<double>(static_cast<float>(nq[k]));
+  }
+  smin = std::numeric_limits<double>::infinity();
+  smax = -std::numeric_limits<double>::infinity();
+  double mag = 0.0;
+  for (uint32_t i = r.begin; i < r.end; ++i) {
+    const double *t = tc.tri(i);
+    for (int v = 0; v < 3; ++v) {
+      const double *x = t + 3 * v;
+      const double s = nq[0] * x[0] + nq[1] * x[1] + nq[2] * x[2];
+      smin = std::min(smin, s);
+      smax = std::max(smax, s);
+      mag = std::max(mag, std::fabs(nq[0] * x[0]) + std::fabs(nq[1] * x[1]) + std::fabs(nq[2] * x[2]));
+    }
+  }
+  // Rounding of the three-term dot products above (and in the FP64 kernel).
+  const double pad = 8.0 * std::ldexp(1.0, -52) * mag;
+  smin -= pad;
+  smax += pad;
+  return true;
+}
+
+TriCoords leaf_coords(const HostBvh &bvh, const std::vector<double> &v, const std::vector<uint32_t> &f,
+                      const double *center, bool fp32) {
+  const size_t nf = bvh.order.size();
+  TriCoords tc;
+  tc.xyz.resize(9 * nf);
+  for (size_t i = 0; i < nf; ++i) {
+    const uint32_t t = bvh.order[i];
+    for (int k = 0; k < 3; ++k)
+      for (int a = 0; a < 3; ++a) {
+        const double x = v[3 * static_cast<size_t>(f[3 * t + k]) + a];
+        tc.xyz[9 * i + 3 * k + a] =
+            fp32 ? static_cast<double>(static_cast<float>(x - center[a])) : x;
+      }
+  }
+  return tc;
+}
+
+}  // namespace
+
 void pack_bvh_f32(const HostBvh &bvh, const std::vector<double> &v, const std::vector<uint32_t> &f,
                   const double center[3], std::vector<NodeF> &nodes, std::vector<TriF> &tris) {
   const size_t nf = bvh.order.size();
+  const TriCoords tc = leaf_coords(bvh, v, f, center, true);
   tris.resize(nf);
   std::vector<float> tri_lo(3 * nf), tri_hi(3 * nf);
   for (size_t i = 0; i < nf; ++i) {
-    const uint32_t t = bvh.order[i];
+    const double *t = tc.tri(static_cast<uint32_t>(i));
     float p[3][3];
     for (int k = 0; k < 3; ++k)
-      for (int a = 0; a < 3; ++a)
-        p[k][a] = static_cast<float>(v[3 * static_cast<size_t>(f[3 * t + k]) + a] - center[a]);
-    uint32_t id = t;
+      for (int a = 0; a < 3; ++a) p[k][a] = static_cast<float>(t[3 * k + a]);
+    double c[3];
+    cross(t, t + 3, t + 6, c);
+    const double len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    float n[3] = {0.f, 0.f, 0.f};
+    float dmin = 0.f, dmax = 0.f;
+    if (len > 0.0) {
+      for (int a = 0; a < 3; ++a) n[a] = static_cast<float>(c[a] / len);
+      double lo = std::numeric_limits<double>::infinity(), hi = -lo, mag = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        const double s = static_cast<double>(n[0]) * t[3 * k] + static_cast<double>(n[1]) * t[3 * k + 1] +
+                         static_cast<double>(n[2]) * t[3 * k + 2];
+        lo = std::min(lo, s);
+        hi = std::max(hi, s);
+        mag = std::max(mag, std::fabs(n[0] * t[3 * k]) + std::fabs(n[1] * t[3 * k + 1]) +
+                                std::fabs(n[2] * t[3 * k + 2]));
+      }
+      const double pad = 8.0 * std::ldexp(1.0, -52) * mag;
+      dmin = round_down(lo - pad);
+      dmax = round_up(hi + pad);
+    }
+    uint32_t id = bvh.order[i];
     float idf;
     std::memcpy(&idf, &id, 4);
-    tris[i].a = make_float4(p[0][0], p[0][1], p[0][2], idf);
-    tris[i].b = make_float4(p[1][0], p[1][1], p[1][2], 0.f);
+    tris[i].plane = make_float4(n[0], n[1], n[2], dmin);
+    tris[i].a = make_float4(p[0][0], p[0][1], p[0][2], dmax);
+    tris[i].b = make_float4(p[1][0], p[1][1], p[1][2], idf);
     tris[i].c = make_float4(p[2][0], p[2][1], p[2][2], 0.f);
     for (int a = 0; a < 3; ++a) {
       tri_lo[3 * i + a] = std::min({p[0][a], p[1][a], p[2][a]});
       tri_hi[3 * i + a] = std::max({p[0][a], p[1][a], p[2][a]});
     }
   }
-  // Child boxes recomputed from the FP32 triangles (exact min/max).
+  const std::vector<Range> ranges = node_ranges(bvh);
   nodes.resize(bvh.nodes.size());
-  struct Box3 {
-    float lo[3], hi[3];
-  };
-  std::vector<Box3> nodebox(bvh.nodes.size());
-  auto leafbox = [&](int32_t code) {
-    Box3 b;
-    for (int a = 0; a < 3; ++a) {
-      b.lo[a] = std::numeric_limits<float>::infinity();
-      b.hi[a] = -std::numeric_limits<float>::infinity();
-    }
-    const uint32_t enc = ~static_cast<uint32_t>(code);
-    const uint32_t first = enc >> 3, count = enc & 7u;
-    for (uint32_t i = first; i < first + count; ++i)
+  for (size_t ni = 0; ni < bvh.nodes.size(); ++ni) {
+    const HostBvh::Node &hn = bvh.nodes[ni];
+    float lo[2][3], hi[2][3], nv[2][3], smin[2], smax[2];
+    for (int c = 0; c < 2; ++c) {
+      const Range r = code_range(hn.child[c], ranges);
       for (int a = 0; a < 3; ++a) {
-        b.lo[a] = std::min(b.lo[a], tri_lo[3 * i + a]);
-        b.hi[a] = std::max(b.hi[a], tri_hi[3 * i + a]);
+        lo[c][a] = std::numeric_limits<float>::infinity();
+        hi[c][a] = -std::numeric_limits<float>::infinity();
       }
-    return b;
-  };
-  // Children always have larger indices than parents: fill bottom-up.
-  for (size_t ni = bvh.nodes.size(); ni-- > 0;) {
-    const HostBvh::Node &n = bvh.nodes[ni];
-    Box3 cb[2];
-    for (int c = 0; c < 2; ++c) cb[c] = n.child[c] < 0 ? leafbox(n.child[c]) : nodebox[n.child[c]];
-    Box3 all;
-    for (int a = 0; a < 3; ++a) {
-      all.lo[a] = std::min(cb[0].lo[a], cb[1].lo[a]);
-      all.hi[a] = std::max(cb[0].hi[a], cb[1].hi[a]);
+      for (uint32_t i = r.begin; i < r.end; ++i)
+        for (int a = 0; a < 3; ++a) {
+          lo[c][a] = std::min(lo[c][a], tri_lo[3 * i + a]);
+          hi[c][a] = std::max(hi[c][a], tri_hi[3 * i + a]);
+        }
+      double nq[3], s0, s1;
+      if (r.end > r.begin && range_slab(tc, r, true, nq, s0, s1)) {
+        for (int a = 0; a < 3; ++a) nv[c][a] = static_cast<float>(nq[a]);
+        smin[c] = round_down(s0);
+        smax[c] = round_up(s1);
+      } else {
+        nv[c][0] = nv[c][1] = nv[c][2] = 0.f;
+        smin[c] = smax[c] = 0.f;
+      }
     }
-    nodebox[ni] = all;
     NodeF &o = nodes[ni];
-    o.x = make_float4(cb[0].lo[0], cb[1].lo[0], cb[0].hi[0], cb[1].hi[0]);
-    o.y = make_float4(cb[0].lo[1], cb[1].lo[1], cb[0].hi[1], cb[1].hi[1]);
-    o.z = make_float4(cb[0].lo[2], cb[1].lo[2], cb[0].hi[2], cb[1].hi[2]);
-    o.child = make_int4(n.child[0], n.child[1], 0, 0);
+    o.x = make_float4(lo[0][0], lo[1][0], hi[0][0], hi[1][0]);
+    o.y = make_float4(lo[0][1], lo[1][1], hi[0][1], hi[1][1]);
+    o.z = make_float4(lo[0][2], lo[1][2], hi[0][2], hi[1][2]);
+    o.nl = make_float4(nv[0][0], nv[0][1], nv[0][2], smin[0]);
+    o.nr = make_float4(nv[1][0], nv[1][1], nv[1][2], smin[1]);
+    float cl, cr;
+    std::memcpy(&cl, &hn.child[0], 4);
+    std::memcpy(&cr, &hn.child[1], 4);
+    o.tail = make_float4(smax[0], smax[1], cl, cr);
   }
 }
 
 void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &v, const std::vector<uint32_t> &f,
                   std::vector<NodeD> &nodes, std::vector<TriD> &tris) {
   const size_t nf = bvh.order.size();
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const TriCoords tc = leaf_coords(bvh, v, f, zero, false);
   tris.resize(nf);
   for (size_t i = 0; i < nf; ++i) {
-    const uint32_t t = bvh.order[i];
-    const double *a = &v[3 * static_cast<size_t>(f[3 * t])];
-    const double *b = &v[3 * static_cast<size_t>(f[3 * t + 1])];
-    const double *c = &v[3 * static_cast<size_t>(f[3 * t + 2])];
+    const double *t = tc.tri(static_cast<uint32_t>(i));
+    double c[3];
+    cross(t, t + 3, t + 6, c);
+    const double len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    double n[3] = {0.0, 0.0, 0.0}, dmin = 0.0, dmax = 0.0;
+    if (len > 0.0) {
+      for (int a = 0; a < 3; ++a) n[a] = c[a] / len;
+      double lo = std::numeric_limits<double>::infinity(), hi = -lo, mag = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        const double s = n[0] * t[3 * k] + n[1] * t[3 * k + 1] + n[2] * t[3 * k + 2];
+        lo = std::min(lo, s);
+        hi = std::max(hi, s);
+        mag = std::max(mag, std::fabs(n[0] * t[3 * k]) + std::fabs(n[1] * t[3 * k + 1]) +
+                                std::fabs(n[2] * t[3 * k + 2]));
+      }
+      const double pad = 8.0 * std::ldexp(1.0, -52) * mag;
+      dmin = lo - pad;
+      dmax = hi + pad;
+    }
     TriD &o = tris[i];
-    o.axy = make_double2(a[0], a[1]);
-    o.azbx = make_double2(a[2], b[0]);
-    o.bybz = make_double2(b[1], b[2]);
-    o.cxy = make_double2(c[0], c[1]);
-    o.czid = make_double2(c[2], static_cast<double>(t));
-    o.pad = make_double2(0.0, 0.0);
+    o.nxy = make_double2(n[0], n[1]);
+    o.nzmin = make_double2(n[2], dmin);
+    o.dmax_id = make_double2(dmax, static_cast<double>(bvh.order[i]));
+    o.axy = make_double2(t[0], t[1]);
+    o.azbx = make_double2(t[2], t[3]);
+    o.bybz = make_double2(t[4], t[5]);
+    o.cxy = make_double2(t[6], t[7]);
+    o.czpad = make_double2(t[8], 0.0);
   }
+  const std::vector<Range> ranges = node_ranges(bvh);
   nodes.resize(bvh.nodes.size());
   for (size_t ni = 0; ni < bvh.nodes.size(); ++ni) {
     const HostBvh::Node &n = bvh.nodes[ni];
+    double nv[2][3], smin[2], smax[2];
+    for (int c = 0; c < 2; ++c) {
+      const Range r = code_range(n.child[c], ranges);
+      if (!(r.end > r.begin && range_slab(tc, r, false, nv[c], smin[c], smax[c]))) {
+        nv[c][0] = nv[c][1] = nv[c][2] = 0.0;
+        smin[c] = smax[c] = 0.0;
+      }
+    }
     NodeD &o = nodes[ni];
     o.xlo = make_double2(n.lo[0][0], n.lo[1][0]);
     o.xhi = make_double2(n.hi[0][0], n.hi[1][0]);
@@ -347,8 +509,12 @@ void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &v, const std::v
     o.yhi = make_double2(n.hi[0][1], n.hi[1][1]);
     o.zlo = make_double2(n.lo[0][2], n.lo[1][2]);
     o.zhi = make_double2(n.hi[0][2], n.hi[1][2]);
+    o.nl_xy = make_double2(nv[0][0], nv[0][1]);
+    o.nl_zmin = make_double2(nv[0][2], smin[0]);
+    o.nr_xy = make_double2(nv[1][0], nv[1][1]);
+    o.nr_zmin = make_double2(nv[1][2], smin[1]);
+    o.smax = make_double2(smax[0], smax[1]);
     o.child = make_int4(n.child[0], n.child[1], 0, 0);
-    o.pad = make_int4(0, 0, 0, 0);
   }
 }
 

@@ -174,34 +174,70 @@ template <> struct Layout<double> {
 __device__ __forceinline__ float gap(float lo, float hi, float p) { return fmaxf(fmaxf(lo - p, p - hi), 0.f); }
 __device__ __forceinline__ double gap(double lo, double hi, double p) { return fmax(fmax(lo - p, p - hi), 0.0); }
 
+// Lower bound on the squared distance from p to each child: the larger of
+// the box bound and the normal-slab bound (the child's triangles lie between
+// the planes n.x = smin and n.x = smax, so |n.p - [smin, smax]| bounds the
+// distance from below; for a nearly flat patch the slab is thin and the
+// bound is close to the true distance, where the box bound is off by up to
+// the box size).
 __device__ __forceinline__ void node_dist2(const NodeF *__restrict__ nodes, int idx, const Vec<float> &p,
                                            float &dl, float &dr, int &cl, int &cr) {
-  const float4 x = __ldg(&nodes[idx].x);
-  const float4 y = __ldg(&nodes[idx].y);
-  const float4 z = __ldg(&nodes[idx].z);
-  const int4 ch = __ldg(&nodes[idx].child);
+  const NodeF *n = nodes + idx;
+  const float4 x = __ldg(&n->x);
+  const float4 y = __ldg(&n->y);
+  const float4 z = __ldg(&n->z);
+  const float4 nl = __ldg(&n->nl);
+  const float4 nr = __ldg(&n->nr);
+  const float4 t = __ldg(&n->tail);
   const float lx = gap(x.x, x.z, p.x), rx = gap(x.y, x.w, p.x);
   const float ly = gap(y.x, y.z, p.y), ry = gap(y.y, y.w, p.y);
   const float lz = gap(z.x, z.z, p.z), rz = gap(z.y, z.w, p.z);
-  dl = __fmaf_rn(lx, lx, __fmaf_rn(ly, ly, lz * lz));
-  dr = __fmaf_rn(rx, rx, __fmaf_rn(ry, ry, rz * rz));
-  cl = ch.x;
-  cr = ch.y;
+  const float sl = __fmaf_rn(nl.x, p.x, __fmaf_rn(nl.y, p.y, nl.z * p.z));
+  const float sr = __fmaf_rn(nr.x, p.x, __fmaf_rn(nr.y, p.y, nr.z * p.z));
+  const float gl = gap(nl.w, t.x, sl), gr = gap(nr.w, t.y, sr);
+  dl = fmaxf(__fmaf_rn(lx, lx, __fmaf_rn(ly, ly, lz * lz)), gl * gl);
+  dr = fmaxf(__fmaf_rn(rx, rx, __fmaf_rn(ry, ry, rz * rz)), gr * gr);
+  cl = __float_as_int(t.z);
+  cr = __float_as_int(t.w);
 }
 
 __device__ __forceinline__ void node_dist2(const NodeD *__restrict__ nodes, int idx, const Vec<double> &p,
                                            double &dl, double &dr, int &cl, int &cr) {
-  const double2 xl = __ldg(&nodes[idx].xlo), xh = __ldg(&nodes[idx].xhi);
-  const double2 yl = __ldg(&nodes[idx].ylo), yh = __ldg(&nodes[idx].yhi);
-  const double2 zl = __ldg(&nodes[idx].zlo), zh = __ldg(&nodes[idx].zhi);
-  const int4 ch = __ldg(&nodes[idx].child);
+  const NodeD *n = nodes + idx;
+  const double2 xl = __ldg(&n->xlo), xh = __ldg(&n->xhi);
+  const double2 yl = __ldg(&n->ylo), yh = __ldg(&n->yhi);
+  const double2 zl = __ldg(&n->zlo), zh = __ldg(&n->zhi);
+  const double2 l0 = __ldg(&n->nl_xy), l1 = __ldg(&n->nl_zmin);
+  const double2 r0 = __ldg(&n->nr_xy), r1 = __ldg(&n->nr_zmin);
+  const double2 smax = __ldg(&n->smax);
+  const int4 ch = __ldg(&n->child);
   const double lx = gap(xl.x, xh.x, p.x), rx = gap(xl.y, xh.y, p.x);
   const double ly = gap(yl.x, yh.x, p.y), ry = gap(yl.y, yh.y, p.y);
   const double lz = gap(zl.x, zh.x, p.z), rz = gap(zl.y, zh.y, p.z);
-  dl = lx * lx + ly * ly + lz * lz;
-  dr = rx * rx + ry * ry + rz * rz;
+  const double sl = l0.x * p.x + l0.y * p.y + l1.x * p.z;
+  const double sr = r0.x * p.x + r0.y * p.y + r1.x * p.z;
+  const double gl = gap(l1.y, smax.x, sl), gr = gap(r1.y, smax.y, sr);
+  dl = fmax(lx * lx + ly * ly + lz * lz, gl * gl);
+  dr = fmax(rx * rx + ry * ry + rz * rz, gr * gr);
   cl = ch.x;
   cr = ch.y;
+}
+
+// Plane-slab lower bound of a triangle (one or two 16-byte loads); the full
+// closest-point test loads the vertices only when this bound is below best.
+__device__ __forceinline__ float tri_plane_gap2(const TriF *__restrict__ tris, uint32_t i, const Vec<float> &p) {
+  const float4 P = __ldg(&tris[i].plane);
+  const float dmax = __ldg(&tris[i].a.w);
+  const float s = __fmaf_rn(P.x, p.x, __fmaf_rn(P.y, p.y, P.z * p.z));
+  const float g = gap(P.w, dmax, s);
+  return g * g;
+}
+__device__ __forceinline__ double tri_plane_gap2(const TriD *__restrict__ tris, uint32_t i, const Vec<double> &p) {
+  const double2 n = __ldg(&tris[i].nxy), z = __ldg(&tris[i].nzmin);
+  const double dmax = __ldg(&tris[i].dmax_id.x);
+  const double s = n.x * p.x + n.y * p.y + z.x * p.z;
+  const double g = gap(z.y, dmax, s);
+  return g * g;
 }
 
 __device__ __forceinline__ void load_tri(const TriF *__restrict__ tris, uint32_t i, Vec<float> &a, Vec<float> &b,
@@ -214,7 +250,7 @@ __device__ __forceinline__ void load_tri(const TriF *__restrict__ tris, uint32_t
 __device__ __forceinline__ void load_tri(const TriD *__restrict__ tris, uint32_t i, Vec<double> &a,
                                          Vec<double> &b, Vec<double> &c) {
   const double2 p0 = __ldg(&tris[i].axy), p1 = __ldg(&tris[i].azbx), p2 = __ldg(&tris[i].bybz);
-  const double2 p3 = __ldg(&tris[i].cxy), p4 = __ldg(&tris[i].czid);
+  const double2 p3 = __ldg(&tris[i].cxy), p4 = __ldg(&tris[i].czpad);
   a = {p0.x, p0.y, p1.x};
   b = {p1.y, p2.x, p2.y};
   c = {p3.x, p3.y, p4.x};
@@ -277,6 +313,7 @@ __device__ bool nearest(const typename Layout<T>::Node *__restrict__ nodes,
       const uint32_t enc = ~static_cast<uint32_t>(node);
       const uint32_t first = enc >> 3, count = enc & 7u;
       for (uint32_t i = 0; i < count; ++i) {
+        if (!(tri_plane_gap2(tris, first + i, p) < best2)) continue;
         Vec<T> a, b, c;
         load_tri(tris, first + i, a, b, c);
         const T d2 = tri_dist2(p, a, b, c);
@@ -496,7 +533,9 @@ __global__ void __launch_bounds__(kWosBlock, 4) wos_kernel(const WosLaunch L) {
       const T dc = sqrt(dot3(dv, dv)) - R;
       d = dc < d ? dc : d;
     }
-    const T r = d - static_cast<T>(G.delta);  // delta is 0 in the FP64 form
+    // The mixed form shrinks the radius by the FP32 distance error bound; the
+    // FP64 form uses the distance itself (wih_twos.cpp:645-647).
+    const T r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
     bool done = !(r > to_T<T>(J.epsilon));
     bool cap = false;
     if (!done) {

@@ -21,33 +21,44 @@ constexpr int kLeafMax = 4;
 constexpr int kMaxDepth = 30;    // builder bound; the traversal stack holds kStack entries
 constexpr int kStack = 32;
 
-// FP32 node: 64 bytes, four 16-byte loads.  x = (l.lo.x, r.lo.x, l.hi.x, r.hi.x),
-// likewise y and z; child = (left, right, -, -).
-struct alignas(64) NodeF {
-  float4 x, y, z;
-  int4 child;
-};
-static_assert(sizeof(NodeF) == 64, "NodeF layout");
+// Each child also carries a normal slab: a unit direction n (the child's
+// area-weighted mean normal) and the interval [smin, smax] of n.v over its
+// vertices, rounded outward.  A child whose normals cancel gets n = 0 and
+// [0, 0], which bounds nothing.
 
-// FP64 node: 128 bytes.  lo/hi pairs (left, right) per axis.
+// FP32 node: 96 bytes, six 16-byte loads.  x = (l.lo.x, r.lo.x, l.hi.x, r.hi.x),
+// likewise y and z; nl = (l.n, l.smin), nr = (r.n, r.smin);
+// tail = (l.smax, r.smax, left child bits, right child bits).
+struct alignas(32) NodeF {
+  float4 x, y, z;
+  float4 nl, nr;
+  float4 tail;
+};
+static_assert(sizeof(NodeF) == 96, "NodeF layout");
+
+// FP64 node: 192 bytes.  lo/hi pairs (left, right) per axis, slabs, children.
 struct alignas(16) NodeD {
   double2 xlo, xhi, ylo, yhi, zlo, zhi;
+  double2 nl_xy, nl_zmin, nr_xy, nr_zmin, smax;
   int4 child;
-  int4 pad;
 };
-static_assert(sizeof(NodeD) == 128, "NodeD layout");
+static_assert(sizeof(NodeD) == 192, "NodeD layout");
 
-// FP32 triangle: 48 bytes: (a.xyz, id), (b.xyz, 0), (c.xyz, 0).
-struct alignas(16) TriF {
-  float4 a, b, c;
+// FP32 triangle: 64 bytes: plane slab (n.xyz, dmin), (a.xyz, dmax),
+// (b.xyz, original id bits), (c.xyz, 0).  n is the unit normal; the vertices
+// satisfy dmin <= n.v <= dmax (rounded outward); degenerate triangles carry
+// n = 0, which never rejects.
+struct alignas(64) TriF {
+  float4 plane, a, b, c;
 };
-static_assert(sizeof(TriF) == 48, "TriF layout");
+static_assert(sizeof(TriF) == 64, "TriF layout");
 
-// FP64 triangle: 96 bytes, six 16-byte loads.
+// FP64 triangle: 128 bytes, eight 16-byte loads.
 struct alignas(16) TriD {
-  double2 axy, azbx, bybz, cxy, czid, pad;
+  double2 nxy, nzmin, dmax_id;
+  double2 axy, azbx, bybz, cxy, czpad;
 };
-static_assert(sizeof(TriD) == 96, "TriD layout");
+static_assert(sizeof(TriD) == 128, "TriD layout");
 
 // Host-side BVH produced by the builder (bvh.cpp).
 struct HostBvh {
