@@ -264,11 +264,19 @@ def run_ours(args):
     if rank == 0:
         queries = np.mean([s["queries"] for s in s_mixed])
         walk_s = float(np.mean([s["walk_seconds"] for s in s_mixed]))
+        nodes = np.mean([s["node_tests"] for s in s_mixed])
+        planes = np.mean([s["plane_tests"] for s in s_mixed])
+        tris = np.mean([s["triangle_tests"] for s in s_mixed])
+        fetched = 96.0 * nodes + 32.0 * planes + 48.0 * tris
         peak, peak_kind = measured_peaks()
         roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None, "traffic": None,
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "queries_per_launch": float(queries), "walk_kernel_seconds": walk_s,
-                "queries_per_second": float(queries / walk_s)}
+                "queries_per_second": float(queries / walk_s),
+                "node_tests_per_query": float(nodes / queries), "plane_tests_per_query": float(planes / queries),
+                "triangle_tests_per_query": float(tris / queries),
+                "fetched_bytes_per_query": float(fetched / queries),
+                "fetched_gbs": float(fetched / walk_s / 1e9)}
         if CANONICAL_BYTES_PER_QUERY:
             ach = CANONICAL_BYTES_PER_QUERY * queries / walk_s / 1e9
             roof.update({"achieved": ach, "frac": ach / peak, "bytes_per_query": CANONICAL_BYTES_PER_QUERY,

@@ -139,6 +139,9 @@ typedef struct twos_summary {
   uint64_t d2h_bytes;
   uint32_t launches;       /* kernels launched by the call */
   uint32_t error_flags;    /* TWOS_DEVERR_* bits raised on the device */
+  uint64_t node_tests;     /* BVH node fetches (two child bounds each) */
+  uint64_t plane_tests;    /* triangle plane-slab tests */
+  uint64_t triangle_tests; /* full closest-point-on-triangle tests */
 } twos_summary;
 
 /* Device-side error bits (set by kernels, never by a trap). */

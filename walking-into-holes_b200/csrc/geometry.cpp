@@ -220,7 +220,7 @@ struct Builder {
 void build_bvh(const std::vector<double> &v, const std::vector<uint32_t> &f, HostBvh &out) {
   const size_t nf = f.size() / 3;
   if (nf == 0) throw std::runtime_error("empty mesh");
-  if (nf >= (1u << 28)) throw std::runtime_error("mesh too large (>= 2^28 triangles)");
+  if (nf > (static_cast<size_t>(kLeafMax) << kMaxDepth)) throw std::runtime_error("mesh too large (> 4 * 2^24 triangles)");
   std::vector<Aabb> tb(nf);
   std::vector<std::array<double, 3>> cent(nf);
   for (size_t i = 0; i < nf; ++i) {

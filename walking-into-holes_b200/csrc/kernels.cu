@@ -391,9 +391,6 @@ __device__ __forceinline__ T source_value(const TermT<T> *terms, uint32_t begin,
 
 // ================================================================ WoS kernel
 constexpr int kWosBlock = 128;
-constexpr int kMaxSmemJobs = 32;
-constexpr int kMaxSmemGeos = 32;
-constexpr int kMaxSmemTerms = 64;
 
 template <typename T> __device__ __forceinline__ T to_T(double v);
 template <> __device__ __forceinline__ double to_T<double>(double v) { return v; }
@@ -429,14 +426,40 @@ __device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, ui
   return lo;
 }
 
-// MODE: TWOS_MODE_*.  The per-walk value type is T (FP32 accumulation in the
-// mixed form, FP64 in the plain form).
+// Dynamic shared memory: the launch's job, geometry and term tables.
+struct SmemPlan {
+  uint32_t geo_offset, term_offset, bytes;
+};
+template <typename T> __host__ __device__ inline SmemPlan smem_plan(uint32_t n_jobs, uint32_t n_geos, uint32_t n_terms) {
+  SmemPlan p;
+  const uint32_t jobs = n_jobs * static_cast<uint32_t>(sizeof(JobDesc));
+  p.geo_offset = (jobs + 15u) & ~15u;
+  const uint32_t geos = p.geo_offset + n_geos * static_cast<uint32_t>(sizeof(GeoDesc));
+  p.term_offset = (geos + 15u) & ~15u;
+  p.bytes = p.term_offset + n_terms * static_cast<uint32_t>(sizeof(TermT<T>));
+  return p;
+}
+
+enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
+
+// Persistent walk-on-spheres kernel as a per-lane state machine.  Each loop
+// iteration every lane does at most one unit of work: one BVH node test or
+// one triangle test of its current closest-point query.  A lane whose query
+// has finished waits in kStep until at least `step_threshold` lanes of its
+// warp are ready (or no lane is still traversing); those lanes then take
+// their walk step together and start their next query, and lanes whose walk
+// ended refill from the work queue once `refill` lanes are idle.  So lanes
+// never wait for the slowest traversal of the warp, only for the batched
+// step.  MODE: TWOS_MODE_*; the per-walk value type is T (FP32 accumulation
+// in the mixed form, FP64 in the plain form).
 template <typename T, int MODE, bool GREEN>
-__global__ void __launch_bounds__(kWosBlock, 4) wos_kernel(const WosLaunch L) {
+__global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
   __shared__ uint2 s_stack[kStack * kWosBlock];
-  __shared__ JobDesc s_jobs[kMaxSmemJobs];
-  __shared__ GeoDesc s_geos[kMaxSmemGeos];
-  __shared__ TermT<T> s_terms[kMaxSmemTerms];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  const SmemPlan plan = smem_plan<T>(L.n_jobs, L.n_geos, L.n_terms);
+  JobDesc *s_jobs = reinterpret_cast<JobDesc *>(s_dyn);
+  GeoDesc *s_geos = reinterpret_cast<GeoDesc *>(s_dyn + plan.geo_offset);
+  TermT<T> *s_terms = reinterpret_cast<TermT<T> *>(s_dyn + plan.term_offset);
 
   for (uint32_t i = threadIdx.x; i < L.n_jobs; i += blockDim.x) s_jobs[i] = L.jobs[i];
   for (uint32_t i = threadIdx.x; i < L.n_geos; i += blockDim.x) s_geos[i] = L.geos[i];
@@ -460,24 +483,32 @@ __global__ void __launch_bounds__(kWosBlock, 4) wos_kernel(const WosLaunch L) {
   const unsigned full = 0xffffffffu;
   uint2 *stack = s_stack + threadIdx.x;
   uint32_t err = 0;
+  unsigned long long c_nodes = 0, c_planes = 0, c_tris = 0;
 
-  bool active = false;
+  int phase = kIdle;
   bool exhausted = false;  // warp-uniform
+  // Walk state.
   uint64_t wid = 0;
   uint32_t job = 0, site = 0, walk = 0, steps = 0;
   Vec<T> pos{T(0), T(0), T(0)};
   T u = T(0), pv = T(0);
+  // Query state.
+  T best2 = T(0);
+  int node = 0, sp = 0;
+  bool have = false, found = false;
+  uint32_t tri_cur = 0, tri_end = 0, iter = 0;
 
   for (;;) {
     // ---- refill idle lanes from the work queue
-    const unsigned idle = __ballot_sync(full, !active);
+    const unsigned idle = __ballot_sync(full, phase == kIdle);
     if (!exhausted && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
       unsigned long long base = 0;
       const int leader = __ffs(idle) - 1;
-      if (static_cast<int>(lane) == leader) base = atomicAdd(L.counter, static_cast<unsigned long long>(__popc(idle)));
+      if (static_cast<int>(lane) == leader)
+        base = atomicAdd(L.counter, static_cast<unsigned long long>(__popc(idle)));
       base = __shfl_sync(full, base, leader);
       if (base + __popc(idle) >= L.total_walks) exhausted = true;
-      if (!active) {
+      if (phase == kIdle) {
         const uint64_t id = base + __popc(idle & ((1u << lane) - 1u));
         if (id < L.total_walks) {
           wid = id;
@@ -491,84 +522,188 @@ __global__ void __launch_bounds__(kWosBlock, 4) wos_kernel(const WosLaunch L) {
           u = T(0);
           pv = T(0);
           steps = 0;
-          active = true;
+          bool skip = false;
           if (J.flags & kJobSkipCavitySites) {
             const T R = to_T<T>(J.cavity_radius);
             for (uint32_t c = 0; c < J.n_cav; ++c) {
               const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
-              const Vec<T> d = sub(pos, cc);
-              if (sqrt(dot3(d, d)) <= R) active = false;
+              const Vec<T> dv = sub(pos, cc);
+              if (sqrt(dot3(dv, dv)) <= R) skip = true;
             }
-            if (!active) {
-              static_cast<T *>(L.u_out)[wid] = T(0);
-              if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
-              L.steps_out[wid] = 0u;
-            }
+          }
+          if (skip) {
+            static_cast<T *>(L.u_out)[wid] = T(0);
+            if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+            L.steps_out[wid] = 0u;
+          } else {
+            best2 = static_cast<T>(J.query_radius2);
+            node = 0;
+            sp = 0;
+            have = true;
+            found = false;
+            tri_cur = tri_end = 0;
+            iter = 0;
+            phase = kTraverse;
           }
         }
       }
     }
-    if (__ballot_sync(full, active) == 0u) {
+
+    // ---- batched walk step for lanes whose query has finished
+    const unsigned ready = __ballot_sync(full, phase == kStep);
+    const unsigned trav = __ballot_sync(full, phase == kTraverse);
+    if (ready != 0u && (__popc(ready) >= L.step_threshold || trav == 0u) && phase == kStep) {
+      const JobDesc &J = s_jobs[job];
+      const GeoDesc &G = s_geos[J.geo];
+      T d = sqrt(best2);
+      if (!found) {
+        err |= TWOS_DEVERR_QUERY;
+        d = T(0);  // ends the walk; the call reports the failure
+      }
+      const T R = to_T<T>(J.cavity_radius);
+      for (uint32_t c = 0; c < J.n_cav; ++c) {
+        const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
+        const Vec<T> dv = sub(pos, cc);
+        const T dc = sqrt(dot3(dv, dv)) - R;
+        d = dc < d ? dc : d;
+      }
+      // The mixed form shrinks the radius by the FP32 distance error bound;
+      // the FP64 form uses the distance itself (wih_twos.cpp:645-647).
+      const T r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
+      bool done = !(r > to_T<T>(J.epsilon));
+      bool cap = false;
+      if (!done) {
+        const uint32_t ctr3 = J.repeat << 3;
+        const Philox4 q0 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 0u);
+        Vec<T> a = pos;
+        if (GREEN) {
+          const Philox4 q1 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 1u);
+          const Philox4 q2 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 2u);
+          const Philox4 q3 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 3u);
+          const T beta = median3(uniform<T>(q2.x, q2.y), uniform<T>(q2.z, q2.w), uniform<T>(q3.x, q3.y));
+          const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
+          a = add_scaled(pos, g, r * beta);
+        }
+        const T w = r * r / T(6);
+        u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
+        if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+        const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
+        pos = add_scaled(pos, dir, r);
+        ++steps;
+        if (static_cast<int>(steps) >= J.max_steps) {
+          done = true;
+          cap = true;
+        }
+      }
+      if (done) {
+        static_cast<T *>(L.u_out)[wid] = u;
+        if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
+        L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
+        phase = kIdle;
+      } else {
+        best2 = static_cast<T>(J.query_radius2);
+        node = 0;
+        sp = 0;
+        have = true;
+        found = false;
+        tri_cur = tri_end = 0;
+        iter = 0;
+        phase = kTraverse;
+      }
+    }
+
+    if (__ballot_sync(full, phase != kIdle) == 0u) {
       if (exhausted) break;
       continue;
     }
-    if (!active) continue;
 
-    // ---- one walk-on-spheres step
-    const JobDesc &J = s_jobs[job];
-    const GeoDesc &G = s_geos[J.geo];
-    T best2 = static_cast<T>(J.query_radius2);
-    uint32_t best_tri = 0;
-    const bool found =
-        nearest<T>(geo_nodes<T>(G), geo_tris<T>(G), G.max_iter, pos, best2, best_tri, stack, kWosBlock, err);
-    T d = sqrt(best2);
-    if (!found) {
-      err |= TWOS_DEVERR_QUERY;
-      d = T(0);  // ends the walk; the call reports the failure
-    }
-    const T R = to_T<T>(J.cavity_radius);
-    for (uint32_t c = 0; c < J.n_cav; ++c) {
-      const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
-      const Vec<T> dv = sub(pos, cc);
-      const T dc = sqrt(dot3(dv, dv)) - R;
-      d = dc < d ? dc : d;
-    }
-    // The mixed form shrinks the radius by the FP32 distance error bound; the
-    // FP64 form uses the distance itself (wih_twos.cpp:645-647).
-    const T r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
-    bool done = !(r > to_T<T>(J.epsilon));
-    bool cap = false;
-    if (!done) {
-      const uint32_t ctr3 = J.repeat << 3;
-      const Philox4 q0 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 0u);
-      Vec<T> a = pos;
-      if (GREEN) {
-        const Philox4 q1 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 1u);
-        const Philox4 q2 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 2u);
-        const Philox4 q3 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 3u);
-        const T beta = median3(uniform<T>(q2.x, q2.y), uniform<T>(q2.z, q2.w), uniform<T>(q3.x, q3.y));
-        const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
-        a = add_scaled(pos, g, r * beta);
+    // ---- one unit of closest-point traversal
+    if (phase == kTraverse) {
+      const GeoDesc &G = s_geos[s_jobs[job].geo];
+      if (++iter > G.max_iter) {
+        err |= TWOS_DEVERR_ITER;
+        found = false;
+        phase = kStep;
+      } else if (tri_cur < tri_end) {
+        const typename Layout<T>::Tri *tris = geo_tris<T>(G);
+        ++c_planes;
+        if (tri_plane_gap2(tris, tri_cur, pos) < best2) {
+          ++c_tris;
+          Vec<T> a, b, c;
+          load_tri(tris, tri_cur, a, b, c);
+          const T d2 = tri_dist2(pos, a, b, c);
+          if (d2 < best2) {
+            best2 = d2;
+            found = true;
+          }
+        }
+        ++tri_cur;
+      } else {
+        // Pop the next entry still closer than the current best.
+        while (!have && sp > 0) {
+          --sp;
+          const uint2 e = stack[sp * kWosBlock];
+          if (static_cast<T>(__uint_as_float(e.y)) < best2) {
+            node = static_cast<int>(e.x);
+            have = true;
+          }
+        }
+        if (!have) {
+          phase = kStep;
+        } else if (node >= 0) {
+          ++c_nodes;
+          T dl, dr;
+          int cl, cr;
+          node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
+          const bool vl = dl < best2, vr = dr < best2;
+          if (vl && vr) {
+            if (dr < dl) {
+              const T td = dl;
+              dl = dr;
+              dr = td;
+              const int tc = cl;
+              cl = cr;
+              cr = tc;
+            }
+            if (sp >= kStack) {
+              err |= TWOS_DEVERR_STACK;
+              found = false;
+              phase = kStep;
+            } else {
+              stack[sp * kWosBlock] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+              ++sp;
+              node = cl;
+            }
+          } else if (vl) {
+            node = cl;
+          } else if (vr) {
+            node = cr;
+          } else {
+            have = false;
+          }
+        } else {
+          const uint32_t enc = ~static_cast<uint32_t>(node);
+          tri_cur = enc >> 3;
+          tri_end = tri_cur + (enc & 7u);
+          have = false;
+        }
       }
-      const T w = r * r / T(6);
-      u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
-      if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
-      const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
-      pos = add_scaled(pos, dir, r);
-      ++steps;
-      if (static_cast<int>(steps) >= J.max_steps) {
-        done = true;
-        cap = true;
-      }
-    }
-    if (done) {
-      static_cast<T *>(L.u_out)[wid] = u;
-      if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
-      L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
-      active = false;
     }
   }
   if (err) atomicOr(L.error, err);
+  if (L.counters) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      c_nodes += __shfl_xor_sync(full, c_nodes, o);
+      c_planes += __shfl_xor_sync(full, c_planes, o);
+      c_tris += __shfl_xor_sync(full, c_tris, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&L.counters[0], c_nodes);
+      atomicAdd(&L.counters[1], c_planes);
+      atomicAdd(&L.counters[2], c_tris);
+    }
+  }
 }
 
 template <typename T, int MODE, bool GREEN> static const void *wos_fn() {
@@ -576,7 +711,6 @@ template <typename T, int MODE, bool GREEN> static const void *wos_fn() {
 }
 
 static const void *select_wos(int precision, int mode, bool green) {
-  // Paired and hot share the paired instantiation's layout except for p.
 #define TWOS_PICK(T)                                                                          \
   if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true>() : wos_fn<T, 0, false>(); \
   if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true>() : wos_fn<T, 1, false>();     \
@@ -588,23 +722,32 @@ static const void *select_wos(int precision, int mode, bool green) {
 #undef TWOS_PICK
 }
 
+static uint32_t wos_dyn_smem(int precision, const WosLaunch &L) {
+  return precision == TWOS_PREC_MIXED ? smem_plan<float>(L.n_jobs, L.n_geos, L.n_terms).bytes
+                                      : smem_plan<double>(L.n_jobs, L.n_geos, L.n_terms).bytes;
+}
+
 cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
                        cudaStream_t s) {
   if (block != kWosBlock) return cudaErrorInvalidValue;
-  if (L.n_jobs == 0 || L.n_jobs > static_cast<uint32_t>(kMaxSmemJobs) || L.n_geos > static_cast<uint32_t>(kMaxSmemGeos) ||
-      L.n_terms > static_cast<uint32_t>(kMaxSmemTerms))
-    return cudaErrorInvalidValue;
+  if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
+  const uint32_t dyn = wos_dyn_smem(precision, L);
+  if (dyn > 64 * 1024) return cudaErrorInvalidValue;
   const void *fn = select_wos(precision, mode, green);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
+  if (e != cudaSuccess) return e;
   WosLaunch copy = L;
   void *args[] = {&copy};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+  return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, dyn, s);
 }
 
-int wos_max_blocks_per_sm(int precision, int mode, bool green, int block) {
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, select_wos(precision, mode, green), block, 0) !=
-      cudaSuccess)
+int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L) {
+  const uint32_t dyn = wos_dyn_smem(precision, L);
+  const void *fn = select_wos(precision, mode, green);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block, dyn) != cudaSuccess) return 0;
   return n;
 }
 

@@ -86,7 +86,9 @@ struct twos_mesh {
   // Scratch, grown on demand.
   DevBuf jobs, terms, cavities, sites, out, u, p, steps, counter, totals, points, dist, closest, topk;
   size_t max_launch_walks = size_t(1) << 30;
-  int refill = 1;
+  int refill = 1;          // lanes idle before a warp refills from the queue
+  int step_threshold = 1;  // finished queries before a warp takes its walk step
+  int blocks_per_sm = 0;   // 0: as many as fit
 };
 
 namespace {
@@ -162,14 +164,18 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     g.tris_d = m->tris_d.as<TriD>();
     for (int a = 0; a < 3; ++a) g.center[a] = m->center[a];
     g.delta = static_cast<float>(m->delta);
-    g.max_iter = static_cast<uint32_t>(std::min<uint64_t>(4ull * m->bvh.nodes.size() + 16, 0xffffffffull));
+    // A query visits each node and tests each triangle at most once.
+    g.max_iter = static_cast<uint32_t>(
+        std::min<uint64_t>(2ull * (m->bvh.nodes.size() + m->faces.size() / 3) + 16, 0xffffffffull));
     m->geo.reserve(sizeof(GeoDesc));
     check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
     m->counter.reserve(16);
-    m->totals.reserve(32);
+    m->totals.reserve(64);
     m->build_seconds = seconds_since(t0);
     if (const char *e = std::getenv("TWOS_MAX_LAUNCH_WALKS")) m->max_launch_walks = std::strtoull(e, nullptr, 10);
     if (const char *e = std::getenv("TWOS_REFILL")) m->refill = std::max(1, std::atoi(e));
+    if (const char *e = std::getenv("TWOS_STEP_THRESHOLD")) m->step_threshold = std::max(1, std::atoi(e));
+    if (const char *e = std::getenv("TWOS_BLOCKS_PER_SM")) m->blocks_per_sm = std::max(0, std::atoi(e));
   } catch (const std::exception &e) {
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
@@ -230,6 +236,7 @@ struct RunOut {
   uint32_t launches = 0;
   uint32_t error_flags = 0;
   uint64_t steps = 0, caps = 0;
+  uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0;
 };
 
 // Runs the estimator over device-resident sites into device-resident rows.
@@ -264,14 +271,11 @@ void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, ui
   if (paired) m->p.reserve(chunk_walks * vbytes);
   m->steps.reserve(chunk_walks * sizeof(uint32_t));
   m->jobs.reserve(sizeof(JobDesc));
-  check(cudaMemsetAsync(m->totals.ptr, 0, 2 * sizeof(unsigned long long) + sizeof(uint32_t), m->stream),
-        "memset");
+  // totals: [0] steps, [1] caps, [2] error bits, [3..5] traversal counters.
+  check(cudaMemsetAsync(m->totals.ptr, 0, 8 * sizeof(unsigned long long), m->stream), "memset");
   uint32_t k0, k1;
   counter_key(r->seed, r->stream, k0, k1);
   const int block = 128;
-  const int per_sm = wos_max_blocks_per_sm(r->precision, mode, r->green != 0, block);
-  if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
-  const int grid = per_sm * m->num_sms;
   const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
   float ms_total = 0.f, ms_walk = 0.f;
   for (size_t first = 0; first < n_sites; first += chunk_sites) {
@@ -316,6 +320,11 @@ void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, ui
     L.p_out = paired ? m->p.ptr : nullptr;
     L.steps_out = m->steps.as<uint32_t>();
     L.refill = m->refill;
+    L.step_threshold = m->step_threshold;
+    L.counters = m->totals.as<unsigned long long>() + 3;
+    const int per_sm = wos_max_blocks_per_sm(r->precision, mode, r->green != 0, block, L);
+    if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
+    const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
     FinalizeLaunch F{};
     F.jobs = L.jobs;
     F.n_jobs = 1;
@@ -338,9 +347,8 @@ void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, ui
     ms_walk += msw;
     ro.launches += 2;
   }
-  unsigned long long tot[3] = {0, 0, 0};
-  check(cudaMemcpyAsync(tot, m->totals.ptr, 2 * sizeof(unsigned long long) + sizeof(uint32_t),
-                        cudaMemcpyDeviceToHost, m->stream),
+  unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  check(cudaMemcpyAsync(tot, m->totals.ptr, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, m->stream),
         "download totals");
   check(cudaStreamSynchronize(m->stream), "sync");
   ro.steps = tot[0];
@@ -348,6 +356,9 @@ void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, ui
   uint32_t err = 0;
   std::memcpy(&err, &tot[2], sizeof(uint32_t));
   ro.error_flags = err;
+  ro.node_tests = tot[3];
+  ro.plane_tests = tot[4];
+  ro.triangle_tests = tot[5];
   ro.kernel_seconds = ms_total * 1e-3;
   ro.walk_seconds = ms_walk * 1e-3;
 }
@@ -366,6 +377,9 @@ int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summa
     summary->d2h_bytes = d2h;
     summary->launches = ro.launches;
     summary->error_flags = ro.error_flags;
+    summary->node_tests = ro.node_tests;
+    summary->plane_tests = ro.plane_tests;
+    summary->triangle_tests = ro.triangle_tests;
   }
   if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
   if (ro.error_flags & TWOS_DEVERR_STACK) return fail(TWOS_ERR_RUNTIME, "BVH traversal stack bound exceeded");
@@ -456,7 +470,7 @@ int twos_closest_point(twos_mesh *m, int precision, const double *points, uint64
     if (closest) m->closest.reserve(n * 3 * sizeof(double));
     check(cudaMemcpyAsync(m->points.ptr, points, n * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
           "upload points");
-    check(cudaMemsetAsync(m->totals.ptr, 0, 32, m->stream), "memset");
+    check(cudaMemsetAsync(m->totals.ptr, 0, 64, m->stream), "memset");
     const double qr = query_radius > 0.0 ? query_radius : std::numeric_limits<double>::infinity();
     uint32_t *err = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
     check(launch_closest(precision, m->geo.as<GeoDesc>(), m->points.as<double>(), n, qr * qr,

@@ -18,8 +18,8 @@ namespace twos {
 // ~child = (first_triangle << 3) | count (count 0..7, 0 = empty child whose
 // box is inverted so it is never entered).
 constexpr int kLeafMax = 4;
-constexpr int kMaxDepth = 30;    // builder bound; the traversal stack holds kStack entries
-constexpr int kStack = 32;
+constexpr int kMaxDepth = 24;    // builder bound (<= 4 * 2^24 triangles); one stack entry per level
+constexpr int kStack = 24;
 
 // Each child also carries a normal slab: a unit direction n (the child's
 // area-weighted mean normal) and the interval [smin, smax] of n.v over its
@@ -149,6 +149,8 @@ struct WosLaunch {
   void *p_out;                  // per-walk p (paired), same type
   uint32_t *steps_out;          // per-walk steps | cap << 31
   int refill;                   // refill a warp once this many lanes are idle
+  int step_threshold;           // step a warp's walks once this many queries are done
+  unsigned long long *counters; // [0] node tests, [1] triangle plane tests, [2] full triangle tests
 };
 
 struct FinalizeLaunch {
@@ -165,7 +167,7 @@ struct FinalizeLaunch {
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
 cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
                        cudaStream_t s);
-int wos_max_blocks_per_sm(int precision, int mode, bool green, int block);
+int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L);
 cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s);
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
                            double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s);

@@ -62,6 +62,7 @@ class Summary(ctypes.Structure):
         ("paths", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("caps", ctypes.c_uint64),
         ("queries", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("launches", ctypes.c_uint32), ("error_flags", ctypes.c_uint32),
+        ("node_tests", ctypes.c_uint64), ("plane_tests", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
     ]
 
 
