@@ -144,6 +144,22 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# ---------------------------------------------------------------- ranks
+def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
+    """Max of a per-rank time over all ranks (identity without a process group)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank: int) -> int:
+    """Each rank's replica of the workload draws an independent stream."""
+    return SEED + rank
+
+
 # ---------------------------------------------------------------- CPU oracle leg
 def cpu_leg(V, F, sites, walks, seconds, repeat=0, threads=None):
     """Times the oracle (reference algorithm and mt19937_64 stream, OpenMP) on a
@@ -195,7 +211,7 @@ def run_ours(args):
     d_sites = torch.tensor(sites, dtype=torch.float64, device="cuda")
     d_out = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
-    base = dict(walks=args.walks, mode="compliance", seed=SEED + rank, epsilon=EPSILON, max_steps=MAX_STEPS,
+    base = dict(walks=args.walks, mode="compliance", seed=replica_seed(rank), epsilon=EPSILON, max_steps=MAX_STEPS,
                 source=source_terms(), query_radius=4.0)
 
     def barrier():
@@ -227,10 +243,7 @@ def run_ours(args):
             ms.append(e0.elapsed_time(e1))
         barrier()
         total = sum(ms)
-        if dist is not None:
-            t = torch.tensor([total], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, dist, "cuda")
         return total, ms, summs
 
     clocks = ClockSampler(local)

@@ -214,6 +214,20 @@ int twos_estimate_device(twos_mesh *mesh, const twos_request *request, const dou
                          uint32_t n_sites, const double *cavities, uint32_t n_cavities,
                          twos_site_result *d_out, twos_summary *summary);
 
+/* Several meshes in ONE persistent launch: job j runs request[j] over
+ * sites[j] (n_sites[j] sites, 3 doubles each) on meshes[j] with cavities[j]
+ * (may be NULL when n_cavities[j] == 0) and writes out[j].  All meshes must be
+ * sessions on the same device; all requests must share mode, precision and the
+ * Green-point flag.  Walks of every job share one device work queue, so a
+ * batch of uneven meshes, site counts and walk counts keeps every SM busy.
+ * Results equal those of one twos_estimate call per job with the same
+ * requests.  The work runs on meshes[0]'s stream; `summary` totals the batch.
+ * Replaces a driver loop of one process call per geometry (e.g.
+ * benchmarks/bunny_budget/run_study.py:41-62). */
+int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, uint32_t n_jobs,
+                        const double *const *sites, const uint32_t *n_sites, const double *const *cavities,
+                        const uint32_t *n_cavities, twos_site_result *const *out, twos_summary *summary);
+
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid
  * out [site][walk].  Host buffers.  Used by parity tests. */

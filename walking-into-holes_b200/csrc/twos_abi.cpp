@@ -84,7 +84,7 @@ struct twos_mesh {
   GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
   // Scratch, grown on demand.
-  DevBuf jobs, terms, cavities, sites, out, u, p, steps, counter, totals, points, dist, closest, topk;
+  DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, counter, totals, points, dist, closest, topk;
   size_t max_launch_walks = size_t(1) << 30;
   int refill = 1;          // lanes idle before a warp refills from the queue
   int step_threshold = 1;  // finished queries before a warp takes its walk step
@@ -239,114 +239,146 @@ struct RunOut {
   uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0;
 };
 
-// Runs the estimator over device-resident sites into device-resident rows.
-// When `keep` is non-null, per-walk samples of the (single) launch are left in
-// the session's u/p/steps buffers.
-void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, uint32_t n_sites,
-                  const double *cav, uint32_t n_cav, twos_site_result *d_out, RunOut &ro, bool keep) {
-  const bool mixed = r->precision == TWOS_PREC_MIXED;
-  const int mode = r->mode;
+// One job of a launch plan, before device layout.
+struct JobSpec {
+  twos_mesh *mesh;
+  const twos_request *r;
+  uint32_t n_sites;
+  uint32_t site_begin;   // into the launch's site / result arrays
+  uint32_t site_offset;  // RNG site index base
+  const double *cav;     // host cavities
+  uint32_t n_cav;
+};
+
+// Runs one persistent launch over a group of jobs (walk kernel + finalize)
+// on `owner`'s stream; sites and rows are device arrays indexed by
+// JobSpec::site_begin.  All jobs share mode, precision and the Green flag.
+void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const double *d_sites, twos_site_result *d_out,
+                RunOut &ro) {
+  const twos_request *r0 = specs.front().r;
+  const bool mixed = r0->precision == TWOS_PREC_MIXED;
+  const int mode = r0->mode;
   const bool paired = mode == TWOS_MODE_PAIRED;
-  const double zero[3] = {0.0, 0.0, 0.0};
-  const double *frame = mixed ? m->center : zero;
+  const bool green = r0->green != 0;
+  std::vector<JobDesc> jobs;
+  std::vector<GeoDesc> geos;
+  std::vector<twos_mesh *> geo_mesh;
   std::vector<TermDev> terms;
-  for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
-  for (int i = 0; i < r->n_adjoint; ++i) terms.push_back(frame_term(r->adjoint[i], frame));
-  if (terms.empty()) terms.push_back(TermDev{});
-  m->terms.reserve(terms.size() * sizeof(TermDev));
-  check(cudaMemcpyAsync(m->terms.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice,
-                        m->stream),
-        "upload terms");
-  m->cavities.reserve(std::max<size_t>(1, n_cav) * 3 * sizeof(double));
-  if (n_cav)
-    check(cudaMemcpyAsync(m->cavities.ptr, cav, n_cav * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
-          "upload cavities");
-  const size_t walks = static_cast<size_t>(r->walks);
-  const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
-  const size_t chunk_sites =
-      std::max<size_t>(1, std::min<size_t>(n_sites, std::max<size_t>(1, m->max_launch_walks / walks)));
-  if (keep && chunk_sites < n_sites) throw std::runtime_error("sample request exceeds one launch");
-  const size_t chunk_walks = chunk_sites * walks;
-  m->u.reserve(chunk_walks * vbytes);
-  if (paired) m->p.reserve(chunk_walks * vbytes);
-  m->steps.reserve(chunk_walks * sizeof(uint32_t));
-  m->jobs.reserve(sizeof(JobDesc));
-  // totals: [0] steps, [1] caps, [2] error bits, [3..5] traversal counters.
-  check(cudaMemsetAsync(m->totals.ptr, 0, 8 * sizeof(unsigned long long), m->stream), "memset");
-  uint32_t k0, k1;
-  counter_key(r->seed, r->stream, k0, k1);
-  const int block = 128;
-  const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
-  float ms_total = 0.f, ms_walk = 0.f;
-  for (size_t first = 0; first < n_sites; first += chunk_sites) {
-    const uint32_t count = static_cast<uint32_t>(std::min<size_t>(chunk_sites, n_sites - first));
+  std::vector<double> cav;
+  uint64_t walk_total = 0;
+  uint32_t site_total = 0;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  for (const JobSpec &js : specs) {
+    const twos_request *r = js.r;
+    uint32_t geo = 0;
+    while (geo < geo_mesh.size() && geo_mesh[geo] != js.mesh) ++geo;
+    if (geo == geo_mesh.size()) {
+      geo_mesh.push_back(js.mesh);
+      geos.push_back(js.mesh->geo_host);
+    }
+    const double *frame = mixed ? js.mesh->center : zero;
     JobDesc J{};
-    J.walk_begin = 0;
-    J.n_sites = count;
+    J.walk_begin = walk_total;
+    J.n_sites = js.n_sites;
     J.walks = static_cast<uint32_t>(r->walks);
-    J.site_begin = static_cast<uint32_t>(first);
-    J.site_offset = r->site_offset + static_cast<uint32_t>(first);
-    J.geo = 0;
-    J.k0 = k0;
-    J.k1 = k1;
+    J.site_begin = js.site_begin;
+    J.site_offset = js.site_offset;
+    J.geo = geo;
+    counter_key(r->seed, r->stream, J.k0, J.k1);
     J.repeat = r->repeat;
     J.max_steps = r->max_steps;
     J.flags = (r->green ? kJobGreen : 0u) | (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
     J.epsilon = r->epsilon;
+    const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
     J.query_radius2 = qr * qr;
     J.cavity_radius = r->cavity_radius;
-    J.src_begin = 0;
+    J.src_begin = static_cast<uint32_t>(terms.size());
     J.n_src = static_cast<uint32_t>(r->n_source);
-    J.adj_begin = static_cast<uint32_t>(r->n_source);
+    for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
+    J.adj_begin = static_cast<uint32_t>(terms.size());
     J.n_adj = static_cast<uint32_t>(r->n_adjoint);
-    J.cav_begin = 0;
-    J.n_cav = n_cav;
-    J.site_rank = 0;
-    check(cudaMemcpyAsync(m->jobs.ptr, &J, sizeof(J), cudaMemcpyHostToDevice, m->stream), "upload job");
-    check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
-    WosLaunch L{};
-    L.jobs = m->jobs.as<JobDesc>();
-    L.n_jobs = 1;
-    L.geos = m->geo.as<GeoDesc>();
-    L.n_geos = 1;
-    L.sites = d_sites;
-    L.terms = m->terms.as<TermDev>();
-    L.n_terms = static_cast<uint32_t>(terms.size());
-    L.cavities = m->cavities.as<double>();
-    L.total_walks = static_cast<uint64_t>(count) * walks;
-    L.counter = m->counter.as<unsigned long long>();
-    L.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
-    L.u_out = m->u.ptr;
-    L.p_out = paired ? m->p.ptr : nullptr;
-    L.steps_out = m->steps.as<uint32_t>();
-    L.refill = m->refill;
-    L.step_threshold = m->step_threshold;
-    L.counters = m->totals.as<unsigned long long>() + 3;
-    const int per_sm = wos_max_blocks_per_sm(r->precision, mode, r->green != 0, block, L);
-    if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
-    const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
-    FinalizeLaunch F{};
-    F.jobs = L.jobs;
-    F.n_jobs = 1;
-    F.total_sites = count;
-    F.totals = m->totals.as<unsigned long long>();
-    F.u = L.u_out;
-    F.p = L.p_out;
-    F.steps = L.steps_out;
-    F.out = d_out;
-    check(cudaEventRecord(m->ev0, m->stream), "event");
-    check(launch_wos(r->precision, mode, r->green != 0, L, grid, block, m->stream), "WoS launch");
-    check(cudaEventRecord(m->evw, m->stream), "event");
-    check(launch_finalize(r->precision, mode, F, m->stream), "finalize launch");
-    check(cudaEventRecord(m->ev1, m->stream), "event");
-    check(cudaEventSynchronize(m->ev1), "WoS kernels");
-    float ms = 0.f, msw = 0.f;
-    check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
-    check(cudaEventElapsedTime(&msw, m->ev0, m->evw), "event time");
-    ms_total += ms;
-    ms_walk += msw;
-    ro.launches += 2;
+    for (int i = 0; i < r->n_adjoint; ++i) terms.push_back(frame_term(r->adjoint[i], frame));
+    J.cav_begin = static_cast<uint32_t>(cav.size() / 3);
+    J.n_cav = js.n_cav;
+    cav.insert(cav.end(), js.cav, js.cav + 3 * static_cast<size_t>(js.n_cav));
+    J.site_rank = site_total;
+    jobs.push_back(J);
+    walk_total += static_cast<uint64_t>(js.n_sites) * static_cast<uint64_t>(r->walks);
+    site_total += js.n_sites;
   }
+  if (terms.empty()) terms.push_back(TermDev{});
+  twos_mesh *m = owner;
+  const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
+  m->jobs.reserve(jobs.size() * sizeof(JobDesc));
+  m->geos.reserve(geos.size() * sizeof(GeoDesc));
+  m->terms.reserve(terms.size() * sizeof(TermDev));
+  m->cavities.reserve(std::max<size_t>(1, cav.size()) * sizeof(double));
+  m->u.reserve(walk_total * vbytes);
+  if (paired) m->p.reserve(walk_total * vbytes);
+  m->steps.reserve(walk_total * sizeof(uint32_t));
+  check(cudaMemcpyAsync(m->jobs.ptr, jobs.data(), jobs.size() * sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream),
+        "upload jobs");
+  check(cudaMemcpyAsync(m->geos.ptr, geos.data(), geos.size() * sizeof(GeoDesc), cudaMemcpyHostToDevice, m->stream),
+        "upload geometries");
+  check(cudaMemcpyAsync(m->terms.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice,
+                        m->stream),
+        "upload terms");
+  if (!cav.empty())
+    check(cudaMemcpyAsync(m->cavities.ptr, cav.data(), cav.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          m->stream),
+          "upload cavities");
+  check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+  WosLaunch L{};
+  L.jobs = m->jobs.as<JobDesc>();
+  L.n_jobs = static_cast<uint32_t>(jobs.size());
+  L.geos = m->geos.as<GeoDesc>();
+  L.n_geos = static_cast<uint32_t>(geos.size());
+  L.sites = d_sites;
+  L.terms = m->terms.as<TermDev>();
+  L.n_terms = static_cast<uint32_t>(terms.size());
+  L.cavities = m->cavities.as<double>();
+  L.total_walks = walk_total;
+  L.counter = m->counter.as<unsigned long long>();
+  L.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+  L.u_out = m->u.ptr;
+  L.p_out = paired ? m->p.ptr : nullptr;
+  L.steps_out = m->steps.as<uint32_t>();
+  L.refill = m->refill;
+  L.step_threshold = m->step_threshold;
+  L.counters = m->totals.as<unsigned long long>() + 3;
+  const int block = 128;
+  const int per_sm = wos_max_blocks_per_sm(r0->precision, mode, green, block, L);
+  if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
+  const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
+  FinalizeLaunch F{};
+  F.jobs = L.jobs;
+  F.n_jobs = L.n_jobs;
+  F.total_sites = site_total;
+  F.totals = m->totals.as<unsigned long long>();
+  F.u = L.u_out;
+  F.p = L.p_out;
+  F.steps = L.steps_out;
+  F.out = d_out;
+  check(cudaEventRecord(m->ev0, m->stream), "event");
+  check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
+  check(cudaEventRecord(m->evw, m->stream), "event");
+  check(launch_finalize(r0->precision, mode, F, m->stream), "finalize launch");
+  check(cudaEventRecord(m->ev1, m->stream), "event");
+  check(cudaEventSynchronize(m->ev1), "WoS kernels");
+  float ms = 0.f, msw = 0.f;
+  check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
+  check(cudaEventElapsedTime(&msw, m->ev0, m->evw), "event time");
+  ro.kernel_seconds += ms * 1e-3;
+  ro.walk_seconds += msw * 1e-3;
+  ro.launches += 2;
+}
+
+void begin_totals(twos_mesh *m) {
+  // totals: [0] steps, [1] caps, [2] error bits, [3..5] traversal counters.
+  check(cudaMemsetAsync(m->totals.ptr, 0, 8 * sizeof(unsigned long long), m->stream), "memset");
+}
+
+void end_totals(twos_mesh *m, RunOut &ro) {
   unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   check(cudaMemcpyAsync(tot, m->totals.ptr, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, m->stream),
         "download totals");
@@ -359,8 +391,25 @@ void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, ui
   ro.node_tests = tot[3];
   ro.plane_tests = tot[4];
   ro.triangle_tests = tot[5];
-  ro.kernel_seconds = ms_total * 1e-3;
-  ro.walk_seconds = ms_walk * 1e-3;
+}
+
+// Runs the estimator over device-resident sites into device-resident rows,
+// chunked by sites so one launch holds at most max_launch_walks walks.  With
+// `keep`, the request must fit one launch and its per-walk samples stay in
+// the session's u/p/steps buffers.
+void run_estimate(twos_mesh *m, const twos_request *r, const double *d_sites, uint32_t n_sites,
+                  const double *cav, uint32_t n_cav, twos_site_result *d_out, RunOut &ro, bool keep) {
+  const size_t walks = static_cast<size_t>(r->walks);
+  const size_t chunk_sites =
+      std::max<size_t>(1, std::min<size_t>(n_sites, std::max<size_t>(1, m->max_launch_walks / walks)));
+  if (keep && chunk_sites < n_sites) throw std::runtime_error("sample request exceeds one launch");
+  begin_totals(m);
+  for (size_t first = 0; first < n_sites; first += chunk_sites) {
+    const uint32_t count = static_cast<uint32_t>(std::min<size_t>(chunk_sites, n_sites - first));
+    JobSpec js{m, r, count, static_cast<uint32_t>(first), r->site_offset + static_cast<uint32_t>(first), cav, n_cav};
+    run_launch(m, {js}, d_sites, d_out, ro);
+  }
+  end_totals(m, ro);
 }
 
 int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summary *summary, double t_total,
@@ -421,7 +470,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (!m) return;
   cudaSetDevice(m->device);
   if (m->stream) cudaStreamSynchronize(m->stream);
-  for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->terms, &m->cavities,
+  for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->counter, &m->totals, &m->points, &m->dist,
                     &m->closest, &m->topk})
     b->release();
@@ -534,6 +583,84 @@ int twos_estimate(twos_mesh *m, const twos_request *r, const double *sites, uint
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
   return finish(ro, n_sites, r, summary, seconds_since(t0), h2d, d2h);
+}
+
+int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, uint32_t n_jobs,
+                        const double *const *sites, const uint32_t *n_sites, const double *const *cavities,
+                        const uint32_t *n_cavities, twos_site_result *const *out, twos_summary *summary) {
+  if (!meshes || !requests || !sites || !n_sites || !out || n_jobs == 0)
+    return fail(TWOS_ERR_USAGE, "null argument");
+  twos_mesh *owner = meshes[0];
+  uint64_t total_sites = 0, total_paths = 0, h2d = 0;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    if (!meshes[j]) return fail(TWOS_ERR_USAGE, "null mesh in batch");
+    if (meshes[j]->device != owner->device) return fail(TWOS_ERR_USAGE, "batch meshes must share one device");
+    const uint32_t nc = n_cavities ? n_cavities[j] : 0;
+    if (int rc = validate_request(&requests[j], n_sites[j], nc)) return rc;
+    if (requests[j].mode != requests[0].mode || requests[j].precision != requests[0].precision ||
+        (requests[j].green != 0) != (requests[0].green != 0))
+      return fail(TWOS_ERR_USAGE, "batch requests must share mode, precision and green");
+    if ((n_sites[j] && (!sites[j] || !out[j])) || (nc && (!cavities || !cavities[j])))
+      return fail(TWOS_ERR_USAGE, "null buffer in batch");
+    if (nc > 4096) return fail(TWOS_ERR_USAGE, "at most 4096 cavities per job");
+    total_sites += n_sites[j];
+    total_paths += static_cast<uint64_t>(n_sites[j]) * static_cast<uint64_t>(requests[j].walks);
+    h2d += static_cast<uint64_t>(n_sites[j]) * 3 * sizeof(double) + nc * 3 * sizeof(double);
+  }
+  if (total_sites > 0xffffffffull) return fail(TWOS_ERR_USAGE, "too many sites in one batch");
+  if (n_jobs > 256) return fail(TWOS_ERR_USAGE, "at most 256 jobs per batch");
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  try {
+    check(cudaSetDevice(owner->device), "cudaSetDevice");
+    owner->sites.reserve(std::max<uint64_t>(1, total_sites) * 3 * sizeof(double));
+    owner->out.reserve(std::max<uint64_t>(1, total_sites) * sizeof(twos_site_result));
+    std::vector<uint32_t> begin(n_jobs);
+    uint32_t at = 0;
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+      begin[j] = at;
+      if (n_sites[j])
+        check(cudaMemcpyAsync(owner->sites.as<double>() + 3ull * at, sites[j], n_sites[j] * 3 * sizeof(double),
+                              cudaMemcpyHostToDevice, owner->stream),
+              "upload sites");
+      at += n_sites[j];
+    }
+    // Group consecutive jobs into launches of at most max_launch_walks walks
+    // (a single larger job runs alone).
+    begin_totals(owner);
+    std::vector<JobSpec> group;
+    uint64_t group_walks = 0;
+    for (uint32_t j = 0; j <= n_jobs; ++j) {
+      const uint64_t w = j < n_jobs ? static_cast<uint64_t>(n_sites[j]) * requests[j].walks : 0;
+      if (!group.empty() && (j == n_jobs || group_walks + w > owner->max_launch_walks)) {
+        run_launch(owner, group, owner->sites.as<double>(), owner->out.as<twos_site_result>(), ro);
+        group.clear();
+        group_walks = 0;
+      }
+      if (j == n_jobs) break;
+      if (n_sites[j] == 0) continue;
+      const uint32_t nc = n_cavities ? n_cavities[j] : 0;
+      group.push_back(JobSpec{meshes[j], &requests[j], n_sites[j], begin[j], requests[j].site_offset,
+                              nc ? cavities[j] : nullptr, nc});
+      group_walks += w;
+    }
+    end_totals(owner, ro);
+    for (uint32_t j = 0; j < n_jobs; ++j)
+      if (n_sites[j])
+        check(cudaMemcpyAsync(out[j], owner->out.as<twos_site_result>() + begin[j],
+                              n_sites[j] * sizeof(twos_site_result), cudaMemcpyDeviceToHost, owner->stream),
+              "download results");
+    check(cudaStreamSynchronize(owner->stream), "sync");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  twos_request agg = requests[0];
+  const int rc = finish(ro, 0, &agg, summary, seconds_since(t0), h2d, total_sites * sizeof(twos_site_result));
+  if (summary) {
+    summary->paths = total_paths;
+    summary->queries = ro.steps + total_paths;
+  }
+  return rc;
 }
 
 int twos_walk_samples(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,

@@ -193,3 +193,30 @@ class Mesh:
             return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
         check(_abi.load().twos_topk_device(self._h, ctypes.c_void_p(addr(d_keys)), int(n), int(k),
                                            ctypes.c_void_p(addr(d_index))))
+
+
+def estimate_batch(meshes, sites_list, configs, cavities_list=None):
+    """Several (mesh, sites, config) jobs in one persistent launch
+    (twos_estimate_batch).  Returns one SITE_DTYPE array per job and the
+    batch summary."""
+    n = len(meshes)
+    if not (len(sites_list) == len(configs) == n):
+        raise ValueError("meshes, sites_list and configs must have the same length")
+    cavities_list = cavities_list or [None] * n
+    sites = [np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 3) for s in sites_list]
+    cavs = [np.zeros((0, 3)) if c is None else np.ascontiguousarray(c, dtype=np.float64).reshape(-1, 3)
+            for c in cavities_list]
+    outs = [np.zeros(len(s), dtype=SITE_DTYPE) for s in sites]
+    reqs = (Request * n)(*[c.to_request() for c in configs])
+    vp = ctypes.c_void_p
+    mesh_arr = (vp * n)(*[m._h.value for m in meshes])
+    site_arr = (vp * n)(*[s.ctypes.data for s in sites])
+    nsite_arr = (ctypes.c_uint32 * n)(*[len(s) for s in sites])
+    cav_arr = (vp * n)(*[c.ctypes.data if len(c) else None for c in cavs])
+    ncav_arr = (ctypes.c_uint32 * n)(*[len(c) for c in cavs])
+    out_arr = (vp * n)(*[o.ctypes.data for o in outs])
+    summ = Summary()
+    check(_abi.load().twos_estimate_batch(mesh_arr, reqs, n, site_arr, nsite_arr, cav_arr, ncav_arr, out_arr,
+                                          ctypes.byref(summ)))
+    return outs, _summary_dict(summ)
+
