@@ -228,6 +228,44 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
                         const double *const *sites, const uint32_t *n_sites, const double *const *cavities,
                         const uint32_t *n_cavities, twos_site_result *const *out, twos_summary *summary);
 
+/* Design loop (select_twos, benchmarks/stanford_bunny/run_bunny_benchmark.py:
+ * 302-337, and run_design 450-491): each iteration scouts every feasible
+ * candidate with `scout`, rescored the top `shortlist` by scout score with
+ * `validate` (its own stream, so fresh samples), takes the argmax of
+ * lower = score - z * score_se, and inserts a ball cavity of radius
+ * cavity_radius at it when lower > accept_threshold.  A candidate is feasible
+ * when its surface distance is >= cavity_radius + outer_clearance and it is
+ * at least 2 * cavity_radius + pair_gap from every cavity (feasible_mask,
+ * run_bunny_benchmark.py:290-299).  Every decision is taken on the device;
+ * with use_graph one iteration is captured as a CUDA graph and replayed. */
+typedef struct twos_design_params {
+  uint32_t iterations;
+  uint32_t shortlist;       /* <= 1024 */
+  double cavity_radius;
+  double z;                 /* confidence multiplier (1.96) */
+  double accept_threshold;
+  double outer_clearance;
+  double pair_gap;
+  int32_t use_graph;
+  int32_t reserved;
+} twos_design_params;
+
+typedef struct twos_design_step {
+  uint32_t chosen;          /* candidate index, UINT32_MAX when none was feasible */
+  uint32_t accepted;
+  double scout_score;
+  double score;             /* validation estimate */
+  double score_se;
+  double lower;             /* score - z * score_se */
+} twos_design_step;
+
+/* history[iterations]; cavities_out holds up to n_cavities + iterations
+ * centres (initial ones first); *n_cavities_out is set.  Host buffers. */
+int twos_design_loop(twos_mesh *mesh, const twos_request *scout, const twos_request *validate,
+                     const double *candidates, uint32_t n_candidates, const double *cavities,
+                     uint32_t n_cavities, const twos_design_params *params, twos_design_step *history,
+                     double *cavities_out, uint32_t *n_cavities_out, twos_summary *summary);
+
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid
  * out [site][walk].  Host buffers.  Used by parity tests. */

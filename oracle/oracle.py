@@ -352,6 +352,45 @@ def select_shortlist_rescore(scout, shortlist, validation, validation_se, z=1.96
     return int(order[local]), float(lower[local]), order
 
 
+def design_loop(mesh: "OracleMesh", candidates, scout_kw, validate_kw, iterations, shortlist, cavity_radius,
+                z=1.96, accept_threshold=0.0, outer_clearance=0.0, pair_gap=0.0, cavities=None):
+    """FP64 restatement of the design loop on the GPU's counter stream:
+    select_twos (run_bunny_benchmark.py:302-337) -- feasible scout, top-k by
+    score, fresh rescore, argmax of score - z*se (run_bunny_benchmark.py:330-331)
+    -- with insertion when the bound clears accept_threshold and the feasibility
+    mask of run_bunny_benchmark.py:290-299.  Iteration i uses repeat = i;
+    scout walks are keyed by candidate index, validation walks by shortlist
+    slot.  Returns (history list of dicts, cavities array)."""
+    cand = np.asarray(candidates, dtype=np.float64).reshape(-1, 3)
+    cav = np.zeros((0, 3)) if cavities is None else np.asarray(cavities, dtype=np.float64).reshape(-1, 3)
+    dist, _, _, _ = mesh.closest_point(cand)
+    pair = 2.0 * cavity_radius + pair_gap
+    feasible = dist >= cavity_radius + outer_clearance
+    for c in cav:
+        feasible &= np.sum((cand - c) ** 2, axis=1) >= pair * pair
+    history = []
+    ids = np.arange(len(cand), dtype=np.uint64)
+    for it in range(iterations):
+        scout = mesh.estimate(cand, site_ids=ids, cavities=cav, cavity_radius=cavity_radius, repeat=it,
+                              rng=RNG_COUNTER, weight_order=1, **scout_kw)
+        keys = np.where(feasible & ~np.isnan(scout["score"]), scout["score"], -np.inf)
+        short = topk_indices(keys, shortlist)
+        val = mesh.estimate(cand[short], site_ids=np.arange(len(short), dtype=np.uint64), cavities=cav,
+                            cavity_radius=cavity_radius, repeat=it, rng=RNG_COUNTER, weight_order=1, **validate_kw)
+        lower = val["score"] - z * val["score_se"]
+        lower = np.where(np.isnan(lower), -np.inf, lower)
+        slot = int(np.argmax(lower))
+        c = int(short[slot])
+        accepted = bool(lower[slot] > accept_threshold)
+        history.append({"chosen": c, "accepted": accepted, "scout_score": float(scout["score"][c]),
+                        "score": float(val["score"][slot]), "score_se": float(val["score_se"][slot]),
+                        "lower": float(lower[slot])})
+        if accepted:
+            cav = np.vstack([cav, cand[c][None, :]])
+            feasible &= np.sum((cand - cand[c]) ** 2, axis=1) >= pair * pair
+    return history, cav
+
+
 def topk_indices(score, k):
     """Top-k indices by score descending, ties broken by the lower index."""
     score = np.asarray(score, dtype=float)

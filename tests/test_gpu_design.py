@@ -1,0 +1,85 @@
+"""Design loop on the device (twos_design_loop): scout -> top-k -> fresh
+validation -> lower-bound argmax -> accept/insert, captured as a CUDA graph.
+
+* FP64 form vs the oracle's FP64 restatement on the same counter-stream
+  samples: identical chosen candidates, accept decisions and cavities (bit
+  exact); scores to rtol 1e-9.
+* Graph replay vs plain launches: identical histories.
+* Mixed vs FP64 form under shared samples: identical decisions wherever the
+  FP64 lower bounds of the best two shortlist entries differ by more than the
+  mixed form's perturbation.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tb(lib_built):
+    import twos_b200
+    return twos_b200
+
+
+def _setup(tb):
+    V, F = tb.geometry.icosphere(3)
+    cand = tb.geometry.uniform_ball(1500, 0.85, seed=1)
+    return V, F, cand
+
+
+KW = dict(iterations=6, shortlist=16, cavity_radius=0.05, z=1.96, accept_threshold=0.02, outer_clearance=0.02,
+          pair_gap=0.01)
+
+
+def _configs(tb, precision):
+    scout = tb.Config(walks=64, precision=precision, seed=31, stream=0, epsilon=1e-4, max_steps=1024,
+                      source=tb.sources.constant(1.0))
+    val = tb.Config(walks=256, precision=precision, seed=31, stream=1, epsilon=1e-4, max_steps=1024,
+                    source=tb.sources.constant(1.0))
+    return scout, val
+
+
+def test_fp64_design_loop_matches_oracle(tb, oracle_mod):
+    V, F, cand = _setup(tb)
+    scout, val = _configs(tb, "fp64")
+    with tb.Mesh(V, F) as mesh:
+        hist, cav, summ = mesh.design_loop(cand, scout, val, use_graph=True, **KW)
+    om = oracle_mod.OracleMesh(V, F)
+    ref, ref_cav = oracle_mod.design_loop(
+        om, cand, dict(walks=64, seed=31, stream=0, epsilon=1e-4, max_steps=1024,
+                       source=[oracle_mod.term(oracle_mod.TERM_CONST, 1.0)]),
+        dict(walks=256, seed=31, stream=1, epsilon=1e-4, max_steps=1024,
+             source=[oracle_mod.term(oracle_mod.TERM_CONST, 1.0)]),
+        KW["iterations"], KW["shortlist"], KW["cavity_radius"], KW["z"], KW["accept_threshold"],
+        KW["outer_clearance"], KW["pair_gap"])
+    assert [int(h["chosen"]) for h in hist] == [r["chosen"] for r in ref]
+    assert [bool(h["accepted"]) for h in hist] == [r["accepted"] for r in ref]
+    assert any(r["accepted"] for r in ref) and not all(r["accepted"] for r in ref)
+    np.testing.assert_array_equal(cav, ref_cav)
+    for k in ("scout_score", "score", "score_se", "lower"):
+        np.testing.assert_allclose(hist[k], [r[k] for r in ref], rtol=1e-9, err_msg=k)
+    assert summ["caps"] == 0
+
+
+def test_graph_replay_equals_plain_launches(tb):
+    V, F, cand = _setup(tb)
+    scout, val = _configs(tb, "mixed")
+    with tb.Mesh(V, F) as mesh:
+        h1, c1, _ = mesh.design_loop(cand, scout, val, use_graph=True, **KW)
+        h0, c0, _ = mesh.design_loop(cand, scout, val, use_graph=False, **KW)
+    np.testing.assert_array_equal(h1, h0)
+    np.testing.assert_array_equal(c1, c0)
+
+
+def test_mixed_decisions_match_fp64(tb):
+    V, F, cand = _setup(tb)
+    with tb.Mesh(V, F) as mesh:
+        h64, c64, _ = mesh.design_loop(cand, *_configs(tb, "fp64"), **KW)
+        h32, c32, _ = mesh.design_loop(cand, *_configs(tb, "mixed"), **KW)
+    for it in range(KW["iterations"]):
+        if h64["chosen"][it] != h32["chosen"][it]:
+            # Only a near tie may flip the choice; after it the paths diverge.
+            assert abs(h64["lower"][it] - h32["lower"][it]) < 0.05 * abs(h64["lower"][it])
+            break
+        assert h64["accepted"][it] == h32["accepted"][it]
+    assert h64["chosen"][0] == h32["chosen"][0]

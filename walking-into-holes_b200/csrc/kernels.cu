@@ -535,6 +535,11 @@ __global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
             static_cast<T *>(L.u_out)[wid] = T(0);
             if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
             L.steps_out[wid] = 0u;
+          } else if (L.site_best2) {
+            // First query answered by the per-site pre-pass.
+            best2 = static_cast<const T *>(L.site_best2)[J.site_rank + site];
+            found = best2 >= T(0);
+            phase = kStep;
           } else {
             best2 = static_cast<T>(J.query_radius2);
             node = 0;
@@ -704,6 +709,45 @@ __global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
       atomicAdd(&L.counters[2], c_tris);
     }
   }
+}
+
+// Per-site first query: one closest-point traversal per site of the launch
+// (the N walks of a site all start there), written as the squared mesh
+// distance, or -1 when no surface point lies within the query radius.
+template <typename T>
+__global__ void __launch_bounds__(kWosBlock) site_prepass_kernel(const WosLaunch L) {
+  __shared__ uint2 s_stack[kStack * kWosBlock];
+  uint2 *stack = s_stack + threadIdx.x;
+  uint32_t err = 0;
+  T *out = static_cast<T *>(L.site_best2);
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < L.total_sites; g += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = L.n_jobs - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (L.jobs[mid].site_rank <= g)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const JobDesc &J = L.jobs[lo];
+    const GeoDesc &G = L.geos[J.geo];
+    const Vec<T> p = to_frame<T>(L.sites + 3ull * (J.site_begin + (g - J.site_rank)), G);
+    T best2 = static_cast<T>(J.query_radius2);
+    uint32_t tri = 0;
+    const bool found = nearest<T>(geo_nodes<T>(G), geo_tris<T>(G), G.max_iter, p, best2, tri, stack, kWosBlock, err);
+    out[g] = found ? best2 : T(-1);
+  }
+  if (err) atomicOr(L.error, err);
+}
+
+cudaError_t launch_site_prepass(int precision, const WosLaunch &L, cudaStream_t s) {
+  if (!L.site_best2 || L.total_sites == 0) return cudaSuccess;
+  const int grid = static_cast<int>(std::min<uint32_t>((L.total_sites + kWosBlock - 1) / kWosBlock, 148u * 16));
+  if (precision == TWOS_PREC_MIXED)
+    site_prepass_kernel<float><<<grid, kWosBlock, 0, s>>>(L);
+  else
+    site_prepass_kernel<double><<<grid, kWosBlock, 0, s>>>(L);
+  return cudaGetLastError();
 }
 
 template <typename T, int MODE, bool GREEN> static const void *wos_fn() {

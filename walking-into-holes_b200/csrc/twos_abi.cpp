@@ -84,7 +84,7 @@ struct twos_mesh {
   GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
   // Scratch, grown on demand.
-  DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, counter, totals, points, dist, closest, topk;
+  DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, first, counter, totals, points, dist, closest, topk;
   size_t max_launch_walks = size_t(1) << 30;
   int refill = 1;          // lanes idle before a warp refills from the queue
   int step_threshold = 1;  // finished queries before a warp takes its walk step
@@ -239,6 +239,40 @@ struct RunOut {
   uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0;
 };
 
+// The device descriptor of one job; its source terms are appended to `terms`
+// in the job geometry's frame.
+JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint32_t site_begin,
+                 uint32_t site_offset, uint32_t geo, uint64_t walk_begin, uint32_t site_rank, uint32_t cav_begin,
+                 uint32_t n_cav, std::vector<TermDev> &terms) {
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const double *frame = r->precision == TWOS_PREC_MIXED ? mesh->center : zero;
+  JobDesc J{};
+  J.walk_begin = walk_begin;
+  J.n_sites = n_sites;
+  J.walks = static_cast<uint32_t>(r->walks);
+  J.site_begin = site_begin;
+  J.site_offset = site_offset;
+  J.geo = geo;
+  counter_key(r->seed, r->stream, J.k0, J.k1);
+  J.repeat = r->repeat;
+  J.max_steps = r->max_steps;
+  J.flags = (r->green ? kJobGreen : 0u) | (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
+  J.epsilon = r->epsilon;
+  const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
+  J.query_radius2 = qr * qr;
+  J.cavity_radius = r->cavity_radius;
+  J.src_begin = static_cast<uint32_t>(terms.size());
+  J.n_src = static_cast<uint32_t>(r->n_source);
+  for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
+  J.adj_begin = static_cast<uint32_t>(terms.size());
+  J.n_adj = static_cast<uint32_t>(r->n_adjoint);
+  for (int i = 0; i < r->n_adjoint; ++i) terms.push_back(frame_term(r->adjoint[i], frame));
+  J.cav_begin = cav_begin;
+  J.n_cav = n_cav;
+  J.site_rank = site_rank;
+  return J;
+}
+
 // One job of a launch plan, before device layout.
 struct JobSpec {
   twos_mesh *mesh;
@@ -267,7 +301,6 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   std::vector<double> cav;
   uint64_t walk_total = 0;
   uint32_t site_total = 0;
-  const double zero[3] = {0.0, 0.0, 0.0};
   for (const JobSpec &js : specs) {
     const twos_request *r = js.r;
     uint32_t geo = 0;
@@ -276,32 +309,9 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
       geo_mesh.push_back(js.mesh);
       geos.push_back(js.mesh->geo_host);
     }
-    const double *frame = mixed ? js.mesh->center : zero;
-    JobDesc J{};
-    J.walk_begin = walk_total;
-    J.n_sites = js.n_sites;
-    J.walks = static_cast<uint32_t>(r->walks);
-    J.site_begin = js.site_begin;
-    J.site_offset = js.site_offset;
-    J.geo = geo;
-    counter_key(r->seed, r->stream, J.k0, J.k1);
-    J.repeat = r->repeat;
-    J.max_steps = r->max_steps;
-    J.flags = (r->green ? kJobGreen : 0u) | (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
-    J.epsilon = r->epsilon;
-    const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
-    J.query_radius2 = qr * qr;
-    J.cavity_radius = r->cavity_radius;
-    J.src_begin = static_cast<uint32_t>(terms.size());
-    J.n_src = static_cast<uint32_t>(r->n_source);
-    for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
-    J.adj_begin = static_cast<uint32_t>(terms.size());
-    J.n_adj = static_cast<uint32_t>(r->n_adjoint);
-    for (int i = 0; i < r->n_adjoint; ++i) terms.push_back(frame_term(r->adjoint[i], frame));
-    J.cav_begin = static_cast<uint32_t>(cav.size() / 3);
-    J.n_cav = js.n_cav;
+    JobDesc J = make_job(js.mesh, r, js.n_sites, js.site_begin, js.site_offset, geo, walk_total, site_total,
+                         static_cast<uint32_t>(cav.size() / 3), js.n_cav, terms);
     cav.insert(cav.end(), js.cav, js.cav + 3 * static_cast<size_t>(js.n_cav));
-    J.site_rank = site_total;
     jobs.push_back(J);
     walk_total += static_cast<uint64_t>(js.n_sites) * static_cast<uint64_t>(r->walks);
     site_total += js.n_sites;
@@ -316,6 +326,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   m->u.reserve(walk_total * vbytes);
   if (paired) m->p.reserve(walk_total * vbytes);
   m->steps.reserve(walk_total * sizeof(uint32_t));
+  m->first.reserve(static_cast<size_t>(site_total) * sizeof(double));
   check(cudaMemcpyAsync(m->jobs.ptr, jobs.data(), jobs.size() * sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream),
         "upload jobs");
   check(cudaMemcpyAsync(m->geos.ptr, geos.data(), geos.size() * sizeof(GeoDesc), cudaMemcpyHostToDevice, m->stream),
@@ -346,6 +357,8 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.refill = m->refill;
   L.step_threshold = m->step_threshold;
   L.counters = m->totals.as<unsigned long long>() + 3;
+  L.site_best2 = m->first.ptr;
+  L.total_sites = site_total;
   const int block = 128;
   const int per_sm = wos_max_blocks_per_sm(r0->precision, mode, green, block, L);
   if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
@@ -360,6 +373,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   F.steps = L.steps_out;
   F.out = d_out;
   check(cudaEventRecord(m->ev0, m->stream), "event");
+  check(launch_site_prepass(r0->precision, L, m->stream), "site pre-pass");
   check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
   check(cudaEventRecord(m->evw, m->stream), "event");
   check(launch_finalize(r0->precision, mode, F, m->stream), "finalize launch");
@@ -370,7 +384,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   check(cudaEventElapsedTime(&msw, m->ev0, m->evw), "event time");
   ro.kernel_seconds += ms * 1e-3;
   ro.walk_seconds += msw * 1e-3;
-  ro.launches += 2;
+  ro.launches += 3;
 }
 
 void begin_totals(twos_mesh *m) {
@@ -471,7 +485,7 @@ void twos_mesh_close(twos_mesh *m) {
   cudaSetDevice(m->device);
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
-                    &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->counter, &m->totals, &m->points, &m->dist,
+                    &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
                     &m->closest, &m->topk})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -659,6 +673,228 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
   if (summary) {
     summary->paths = total_paths;
     summary->queries = ro.steps + total_paths;
+  }
+  return rc;
+}
+
+int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request *validate,
+                     const double *candidates, uint32_t n, const double *cavities, uint32_t n_cav0,
+                     const twos_design_params *P, twos_design_step *history, double *cavities_out,
+                     uint32_t *n_cavities_out, twos_summary *summary) {
+  if (!m || !scout || !validate || !candidates || !P || !history || !cavities_out || !n_cavities_out)
+    return fail(TWOS_ERR_USAGE, "null argument");
+  if (n == 0 || P->iterations == 0) return fail(TWOS_ERR_USAGE, "need candidates and iterations");
+  if (P->shortlist == 0 || P->shortlist > 1024 || P->shortlist > n)
+    return fail(TWOS_ERR_USAGE, "shortlist must be in [1, min(1024, candidates)]");
+  if (!(P->cavity_radius > 0.0) || !(P->z >= 0.0)) return fail(TWOS_ERR_USAGE, "invalid design parameters");
+  if (n_cav0 && !cavities) return fail(TWOS_ERR_USAGE, "null cavities");
+  twos_request rs = *scout, rv = *validate;
+  rs.cavity_radius = rv.cavity_radius = P->cavity_radius;
+  // Iteration i draws its samples with repeat = i; validation walks are keyed
+  // by their shortlist slot, on the validate request's own stream.
+  rs.repeat = rv.repeat = 0;
+  const uint32_t max_cav = n_cav0 + P->iterations;
+  if (int rc = validate_request(&rs, n, max_cav)) return rc;
+  if (int rc = validate_request(&rv, P->shortlist, max_cav)) return rc;
+  if (rs.precision != rv.precision || rs.mode != rv.mode || rs.mode == TWOS_MODE_HOT)
+    return fail(TWOS_ERR_USAGE, "scout and validate must share precision and a TD mode");
+  const uint32_t k = P->shortlist;
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  DevBuf cand, feas, keys, idx, vsites, rows_s, rows_v, cav, jobs_s, jobs_v, iter, hist, terms_d, topk, dist,
+      first_v;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    cand.reserve(static_cast<size_t>(n) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(cand.ptr, candidates, static_cast<size_t>(n) * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                          m->stream),
+          "upload candidates");
+    // Feasibility against the surface and the initial cavities (host, once).
+    dist.reserve(static_cast<size_t>(n) * sizeof(double));
+    check(launch_closest(TWOS_PREC_FP64, m->geo.as<GeoDesc>(), cand.as<double>(), n,
+                         std::numeric_limits<double>::infinity(), dist.as<double>(), nullptr,
+                         reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2), m->stream),
+          "closest launch");
+    std::vector<double> d(n);
+    check(cudaMemcpyAsync(d.data(), dist.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
+    check(cudaStreamSynchronize(m->stream), "sync");
+    const double pair = 2.0 * P->cavity_radius + P->pair_gap;
+    std::vector<uint8_t> mask(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      bool ok = d[i] >= P->cavity_radius + P->outer_clearance;
+      for (uint32_t c = 0; c < n_cav0 && ok; ++c) {
+        const double dx = candidates[3 * i] - cavities[3 * c], dy = candidates[3 * i + 1] - cavities[3 * c + 1],
+                     dz = candidates[3 * i + 2] - cavities[3 * c + 2];
+        ok = dx * dx + dy * dy + dz * dz >= pair * pair;
+      }
+      mask[i] = ok ? 1 : 0;
+    }
+    feas.reserve(n);
+    check(cudaMemcpyAsync(feas.ptr, mask.data(), n, cudaMemcpyHostToDevice, m->stream), "upload mask");
+    keys.reserve(static_cast<size_t>(n) * sizeof(double));
+    idx.reserve(k * sizeof(uint32_t));
+    vsites.reserve(static_cast<size_t>(k) * 3 * sizeof(double));
+    rows_s.reserve(static_cast<size_t>(n) * sizeof(twos_site_result));
+    rows_v.reserve(static_cast<size_t>(k) * sizeof(twos_site_result));
+    cav.reserve(static_cast<size_t>(max_cav) * 3 * sizeof(double));
+    if (n_cav0)
+      check(cudaMemcpyAsync(cav.ptr, cavities, n_cav0 * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
+            "upload cavities");
+    std::vector<TermDev> terms;
+    const JobDesc Js = make_job(m, &rs, n, 0, rs.site_offset, 0, 0, 0, 0, n_cav0, terms);
+    const JobDesc Jv = make_job(m, &rv, k, 0, rv.site_offset, 0, 0, 0, 0, n_cav0, terms);
+    if (terms.empty()) terms.push_back(TermDev{});
+    terms_d.reserve(terms.size() * sizeof(TermDev));
+    jobs_s.reserve(sizeof(JobDesc));
+    jobs_v.reserve(sizeof(JobDesc));
+    check(cudaMemcpyAsync(terms_d.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice,
+                          m->stream),
+          "upload terms");
+    check(cudaMemcpyAsync(jobs_s.ptr, &Js, sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream), "upload job");
+    check(cudaMemcpyAsync(jobs_v.ptr, &Jv, sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream), "upload job");
+    iter.reserve(sizeof(uint32_t));
+    check(cudaMemsetAsync(iter.ptr, 0, sizeof(uint32_t), m->stream), "memset");
+    hist.reserve(static_cast<size_t>(P->iterations) * sizeof(DesignStep));
+    const bool mixed = rs.precision == TWOS_PREC_MIXED;
+    const bool paired = rs.mode == TWOS_MODE_PAIRED;
+    const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
+    const size_t walks_max = std::max<size_t>(static_cast<size_t>(n) * rs.walks, static_cast<size_t>(k) * rv.walks);
+    m->u.reserve(walks_max * vbytes);
+    if (paired) m->p.reserve(walks_max * vbytes);
+    m->steps.reserve(walks_max * sizeof(uint32_t));
+    const size_t tk = topk_scratch_bytes(n, k);
+    topk.reserve(tk);
+    begin_totals(m);
+
+    WosLaunch Ls{};
+    Ls.jobs = jobs_s.as<JobDesc>();
+    Ls.n_jobs = 1;
+    Ls.geos = m->geo.as<GeoDesc>();
+    Ls.n_geos = 1;
+    Ls.sites = cand.as<double>();
+    Ls.terms = terms_d.as<TermDev>();
+    Ls.n_terms = static_cast<uint32_t>(terms.size());
+    Ls.cavities = cav.as<double>();
+    Ls.total_walks = static_cast<uint64_t>(n) * rs.walks;
+    Ls.counter = m->counter.as<unsigned long long>();
+    Ls.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    Ls.u_out = m->u.ptr;
+    Ls.p_out = paired ? m->p.ptr : nullptr;
+    Ls.steps_out = m->steps.as<uint32_t>();
+    Ls.refill = m->refill;
+    Ls.step_threshold = m->step_threshold;
+    Ls.counters = m->totals.as<unsigned long long>() + 3;
+    m->first.reserve(static_cast<size_t>(n) * sizeof(double));
+    first_v.reserve(static_cast<size_t>(k) * sizeof(double));
+    Ls.site_best2 = m->first.ptr;
+    Ls.total_sites = n;
+    WosLaunch Lv = Ls;
+    Lv.site_best2 = first_v.ptr;
+    Lv.total_sites = k;
+    Lv.jobs = jobs_v.as<JobDesc>();
+    Lv.sites = vsites.as<double>();
+    Lv.total_walks = static_cast<uint64_t>(k) * rv.walks;
+    FinalizeLaunch Fs{};
+    Fs.jobs = Ls.jobs;
+    Fs.n_jobs = 1;
+    Fs.total_sites = n;
+    Fs.totals = m->totals.as<unsigned long long>();
+    Fs.u = Ls.u_out;
+    Fs.p = Ls.p_out;
+    Fs.steps = Ls.steps_out;
+    Fs.out = rows_s.as<twos_site_result>();
+    FinalizeLaunch Fv = Fs;
+    Fv.jobs = Lv.jobs;
+    Fv.total_sites = k;
+    Fv.out = rows_v.as<twos_site_result>();
+    DesignLaunch D{};
+    D.candidates = cand.as<double>();
+    D.n_candidates = n;
+    D.k = k;
+    D.scout_rows = rows_s.as<twos_site_result>();
+    D.feasible = feas.as<uint8_t>();
+    D.keys = keys.as<double>();
+    D.shortlist = idx.as<uint32_t>();
+    D.val_sites = vsites.as<double>();
+    D.val_rows = rows_v.as<twos_site_result>();
+    D.scout_job = jobs_s.as<JobDesc>();
+    D.val_job = jobs_v.as<JobDesc>();
+    D.cavities = cav.as<double>();
+    D.max_cav = max_cav;
+    D.max_iterations = P->iterations;
+    D.z = P->z;
+    D.threshold = P->accept_threshold;
+    D.pair_clearance = pair;
+    D.iteration = iter.as<uint32_t>();
+    D.history = hist.as<DesignStep>();
+    const int block = 128;
+    const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green != 0, block, Ls);
+    const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green != 0, block, Lv);
+    if (per_s <= 0 || per_v <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
+    const int cap = m->blocks_per_sm > 0 ? m->blocks_per_sm : 1 << 20;
+    const int grid_s = std::min(per_s, cap) * m->num_sms, grid_v = std::min(per_v, cap) * m->num_sms;
+    auto iteration = [&]() {
+      check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+      check(launch_site_prepass(rs.precision, Ls, m->stream), "scout pre-pass");
+      check(launch_wos(rs.precision, rs.mode, rs.green != 0, Ls, grid_s, block, m->stream), "scout launch");
+      check(launch_finalize(rs.precision, rs.mode, Fs, m->stream), "scout finalize");
+      check(launch_design_keys(D, m->stream), "keys");
+      check(launch_topk(D.keys, n, k, idx.as<uint32_t>(), topk.ptr, topk.bytes, m->stream), "top-k");
+      check(launch_design_gather(D, m->stream), "gather");
+      check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+      check(launch_site_prepass(rv.precision, Lv, m->stream), "validate pre-pass");
+      check(launch_wos(rv.precision, rv.mode, rv.green != 0, Lv, grid_v, block, m->stream), "validate launch");
+      check(launch_finalize(rv.precision, rv.mode, Fv, m->stream), "validate finalize");
+      check(launch_design_select(D, m->stream), "select");
+      check(launch_design_mask(D, m->stream), "mask");
+    };
+    if (P->use_graph) {
+      check(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+      iteration();
+      check(cudaStreamEndCapture(m->stream, &graph), "end capture");
+      check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    }
+    check(cudaEventRecord(m->ev0, m->stream), "event");
+    for (uint32_t it = 0; it < P->iterations; ++it) {
+      if (exec)
+        check(cudaGraphLaunch(exec, m->stream), "graph launch");
+      else
+        iteration();
+    }
+    check(cudaEventRecord(m->ev1, m->stream), "event");
+    check(cudaEventSynchronize(m->ev1), "design loop");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
+    ro.kernel_seconds = ms * 1e-3;
+    ro.launches = P->iterations * 11;
+    check(cudaMemcpyAsync(history, hist.ptr, P->iterations * sizeof(DesignStep), cudaMemcpyDeviceToHost, m->stream),
+          "download history");
+    JobDesc Jout{};
+    check(cudaMemcpyAsync(&Jout, jobs_s.ptr, sizeof(JobDesc), cudaMemcpyDeviceToHost, m->stream), "download job");
+    check(cudaMemcpyAsync(cavities_out, cav.ptr, max_cav * 3 * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+          "download cavities");
+    end_totals(m, ro);
+    *n_cavities_out = Jout.n_cav;
+  } catch (const std::exception &e) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (DevBuf *b : {&cand, &feas, &keys, &idx, &vsites, &rows_s, &rows_v, &cav, &jobs_s, &jobs_v, &iter, &hist,
+                      &terms_d, &topk, &dist, &first_v})
+      b->release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  for (DevBuf *b : {&cand, &feas, &keys, &idx, &vsites, &rows_s, &rows_v, &cav, &jobs_s, &jobs_v, &iter, &hist,
+                    &terms_d, &topk, &dist, &first_v})
+    b->release();
+  const int rc = finish(ro, 0, &rs, summary, seconds_since(t0), 0, 0);
+  if (summary) {
+    summary->paths = static_cast<uint64_t>(P->iterations) *
+                     (static_cast<uint64_t>(n) * rs.walks + static_cast<uint64_t>(k) * rv.walks);
+    summary->queries = ro.steps + summary->paths;
   }
   return rc;
 }

@@ -151,7 +151,15 @@ struct WosLaunch {
   int refill;                   // refill a warp once this many lanes are idle
   int step_threshold;           // step a warp's walks once this many queries are done
   unsigned long long *counters; // [0] node tests, [1] triangle plane tests, [2] full triangle tests
+  // Squared mesh distance at each launch site (index site_rank + site), from
+  // the pre-pass; every walk of a site starts from the same point, so its
+  // first query is answered from here (-1 when nothing is within range).
+  void *site_best2;
+  uint32_t total_sites;
 };
+
+// Fills L.site_best2 (T per site, T = float for mixed, double for FP64).
+cudaError_t launch_site_prepass(int precision, const WosLaunch &L, cudaStream_t s);
 
 struct FinalizeLaunch {
   const JobDesc *jobs;
@@ -163,6 +171,40 @@ struct FinalizeLaunch {
   const uint32_t *steps;
   twos_site_result *out;
 };
+
+// One design-loop iteration record (layout of twos_design_step).
+struct DesignStep {
+  uint32_t chosen;
+  uint32_t accepted;
+  double scout_score, score, score_se, lower;
+};
+static_assert(sizeof(DesignStep) == sizeof(twos_design_step), "design step layout");
+
+// Device buffers of the design loop (design.cu).
+struct DesignLaunch {
+  const double *candidates;            // [n][3]
+  uint32_t n_candidates;
+  uint32_t k;                          // shortlist size
+  const twos_site_result *scout_rows;  // [n]
+  uint8_t *feasible;                   // [n]
+  double *keys;                        // [n]
+  const uint32_t *shortlist;           // [k]
+  double *val_sites;                   // [k][3]
+  const twos_site_result *val_rows;    // [k]
+  JobDesc *scout_job;
+  JobDesc *val_job;
+  double *cavities;                    // [max_cav][3]
+  uint32_t max_cav;
+  uint32_t max_iterations;
+  double z, threshold, pair_clearance;
+  uint32_t *iteration;
+  DesignStep *history;                 // [max_iterations]
+};
+
+cudaError_t launch_design_keys(const DesignLaunch &D, cudaStream_t s);
+cudaError_t launch_design_gather(const DesignLaunch &D, cudaStream_t s);
+cudaError_t launch_design_select(const DesignLaunch &D, cudaStream_t s);
+cudaError_t launch_design_mask(const DesignLaunch &D, cudaStream_t s);
 
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
 cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,

@@ -23,7 +23,7 @@ DEVERR_QUERY, DEVERR_STACK, DEVERR_ITER, DEVERR_CONFIG = 1, 2, 4, 8
 EXPORTED = [
     "twos_abi_version", "twos_last_error", "twos_mesh_open", "twos_mesh_open_ply", "twos_mesh_close",
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
-    "twos_estimate_batch", "twos_walk_samples", "twos_inside", "twos_topk_device",
+    "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
 ]
 
 
@@ -76,6 +76,26 @@ class MeshInfo(ctypes.Structure):
     ]
 
 
+class DesignParams(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_uint32), ("shortlist", ctypes.c_uint32),
+        ("cavity_radius", ctypes.c_double), ("z", ctypes.c_double), ("accept_threshold", ctypes.c_double),
+        ("outer_clearance", ctypes.c_double), ("pair_gap", ctypes.c_double),
+        ("use_graph", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
+class DesignStep(ctypes.Structure):
+    _fields_ = [
+        ("chosen", ctypes.c_uint32), ("accepted", ctypes.c_uint32),
+        ("scout_score", ctypes.c_double), ("score", ctypes.c_double), ("score_se", ctypes.c_double),
+        ("lower", ctypes.c_double),
+    ]
+
+
+DESIGN_DTYPE = [("chosen", "u4"), ("accepted", "u4"), ("scout_score", "f8"), ("score", "f8"),
+                ("score_se", "f8"), ("lower", "f8")]
+
 assert ctypes.sizeof(SourceTerm) == 80
 assert ctypes.sizeof(SiteResult) == 56
 
@@ -113,6 +133,8 @@ def load(path: Path | str | None = None):
     L.twos_estimate.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_estimate_device.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_estimate_batch.argtypes = [vp, ctypes.POINTER(Request), u32, vp, vp, vp, vp, vp, ctypes.POINTER(Summary)]
+    L.twos_design_loop.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(Request), vp, u32, vp, u32,
+                                   ctypes.POINTER(DesignParams), vp, vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
     L.twos_topk_device.argtypes = [vp, vp, u32, u32, vp]

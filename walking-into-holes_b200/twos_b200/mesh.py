@@ -176,6 +176,27 @@ class Mesh:
                                                ctypes.byref(summ)))
         return _summary_dict(summ)
 
+    def design_loop(self, candidates, scout: Config, validate: Config, iterations=20, shortlist=64,
+                    cavity_radius=0.03, z=1.96, accept_threshold=0.0, outer_clearance=0.0, pair_gap=0.0,
+                    cavities=None, use_graph=True):
+        """Scout -> top-k -> fresh validation -> lower-bound argmax -> accept/insert, on the
+        device (twos_design_loop).  Returns (history, cavities, summary)."""
+        cand = np.ascontiguousarray(candidates, dtype=np.float64).reshape(-1, 3)
+        cav0 = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        P = _abi.DesignParams()
+        P.iterations, P.shortlist = int(iterations), int(shortlist)
+        P.cavity_radius, P.z, P.accept_threshold = float(cavity_radius), float(z), float(accept_threshold)
+        P.outer_clearance, P.pair_gap, P.use_graph = float(outer_clearance), float(pair_gap), int(bool(use_graph))
+        hist = np.zeros(int(iterations), dtype=_abi.DESIGN_DTYPE)
+        cav_out = np.zeros((len(cav0) + int(iterations), 3))
+        n_out = ctypes.c_uint32()
+        rs, rv = scout.to_request(), validate.to_request()
+        summ = Summary()
+        check(_abi.load().twos_design_loop(self._h, ctypes.byref(rs), ctypes.byref(rv), _ptr(cand), len(cand),
+                                           _ptr(cav0) if len(cav0) else None, len(cav0), ctypes.byref(P),
+                                           _ptr(hist), _ptr(cav_out), ctypes.byref(n_out), ctypes.byref(summ)))
+        return hist, cav_out[: n_out.value].copy(), _summary_dict(summ)
+
     def walk_samples(self, sites, config: Config, cavities=None):
         s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
         cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
