@@ -13,13 +13,13 @@
 #include <thread>
 #include <vector>
 
-#include "twos_internal.h"
+#include "twos_session.h"
 
 namespace twos {
 
 static thread_local std::string g_error;
 
-static int fail(int code, const std::string &msg) {
+int fail(int code, const std::string &msg) {
   g_error = msg;
   return code;
 }
@@ -39,59 +39,15 @@ struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
-static void check(cudaError_t e, const char *what) {
+void check(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-// Grow-only device allocation.
-struct DevBuf {
-  void *ptr = nullptr;
-  size_t bytes = 0;
-  void reserve(size_t n) {
-    if (n <= bytes) return;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-    check(cudaMalloc(&ptr, std::max<size_t>(n, 256)), "cudaMalloc");
-    bytes = std::max<size_t>(n, 256);
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  template <typename T> T *as() const { return static_cast<T *>(ptr); }
-};
 
 }  // namespace twos
 
 using namespace twos;
 
-struct twos_mesh {
-  int device = 0;
-  std::vector<double> vertices;
-  std::vector<uint32_t> faces;
-  HostBvh bvh;
-  double bmin[3], bmax[3], center[3];
-  double delta = 0.0;
-  double build_seconds = 0.0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;   // stream in use
-  cudaStream_t own_stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
-  DevBuf nodes_f, tris_f, nodes_d, tris_d;
-  DevBuf geo;  // one GeoDesc
-  GeoDesc geo_host{};
-  uint64_t resident_bytes = 0;
-  // Scratch, grown on demand.
-  DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, first, counter, totals, points, dist, closest, topk;
-  size_t max_launch_walks = size_t(1) << 30;
-  int refill = 1;          // lanes idle before a warp refills from the queue
-  int step_threshold = 1;  // finished queries before a warp takes its walk step
-  int blocks_per_sm = 0;   // 0: as many as fit
-};
-
-namespace {
+namespace twos {
 
 double seconds_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

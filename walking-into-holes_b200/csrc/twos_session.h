@@ -1,0 +1,69 @@
+// The mesh session of libtwos.so and the host helpers its entry points share
+// (twos_abi.cpp, noalloc.cu).  Not part of the public ABI.
+#pragma once
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "twos_internal.h"
+
+namespace twos {
+
+// Records `msg` as this thread's last error and returns `code`.
+int fail(int code, const std::string &msg);
+// Throws std::runtime_error naming `what` when `e` is not cudaSuccess.
+void check(cudaError_t e, const char *what);
+
+// Grow-only device allocation.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    check(cudaMalloc(&ptr, std::max<size_t>(n, 256)), "cudaMalloc");
+    bytes = std::max<size_t>(n, 256);
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav);
+JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint32_t site_begin,
+                 uint32_t site_offset, uint32_t geo, uint64_t walk_begin, uint32_t site_rank, uint32_t cav_begin,
+                 uint32_t n_cav, std::vector<TermDev> &terms);
+
+}  // namespace twos
+
+struct twos_mesh {
+  int device = 0;
+  std::vector<double> vertices;
+  std::vector<uint32_t> faces;
+  twos::HostBvh bvh;
+  double bmin[3], bmax[3], center[3];
+  double delta = 0.0;
+  double build_seconds = 0.0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;  // stream in use
+  cudaStream_t own_stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
+  twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
+  twos::DevBuf geo;  // one GeoDesc
+  twos::GeoDesc geo_host{};
+  uint64_t resident_bytes = 0;
+  // Scratch, grown on demand.
+  twos::DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, first, counter, totals, points, dist, closest,
+      topk;
+  size_t max_launch_walks = size_t(1) << 30;
+  int refill = 1;          // lanes idle before a warp refills from the queue
+  int step_threshold = 1;  // finished queries before a warp takes its walk step
+  int blocks_per_sm = 0;   // 0: as many as fit
+};
