@@ -214,6 +214,37 @@ int twos_estimate_device(twos_mesh *mesh, const twos_request *request, const dou
                          uint32_t n_sites, const double *cavities, uint32_t n_cavities,
                          twos_site_result *d_out, twos_summary *summary);
 
+/* twos_estimate_device for callers that cannot allocate device memory.  No
+ * counterpart in the reference (whose backend has no device code).
+ *
+ * Some callers must not call cudaMalloc: code running while a framework owns
+ * the device memory pool (a raw cudaMalloc bypasses its allocator and
+ * fragments memory it manages), code on paths that must not synchronise the
+ * device (cudaMalloc/cudaFree may), and services with a fixed memory budget.
+ * This entry point allocates nothing: every per-call device buffer (launch
+ * tables, cavities, first-query distances, queue counter, totals and the
+ * per-walk samples) is carved out of one static device array of
+ * TWOS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits.  The mesh session (opened earlier with twos_mesh_open*),
+ * the sites (d_sites, 3 doubles each) and the result rows (d_out) belong to
+ * the caller.
+ *
+ * Limit: the scratch holds the per-walk samples of one call, so
+ * n_sites * walks may be at most about 4 M in mixed compliance mode (8 bytes
+ * per walk), 1.3 M in FP64 paired mode (20 bytes per walk); larger requests
+ * are rejected with TWOS_ERR_USAGE and a message giving the bytes needed.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the one array and it keeps the previous call's contents (the call clears
+ * what must start at zero): calls that overlap on the GPU, from different
+ * threads, streams or sessions, race on it and must be serialised by the
+ * caller.  Work runs on the session's stream and the call returns after it
+ * completes.  Results equal twos_estimate_device's. */
+#define TWOS_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int twos_estimate_noalloc(twos_mesh *mesh, const twos_request *request, const double *d_sites,
+                          uint32_t n_sites, const double *cavities, uint32_t n_cavities,
+                          twos_site_result *d_out, twos_summary *summary);
+
 /* Several meshes in ONE persistent launch: job j runs request[j] over
  * sites[j] (n_sites[j] sites, 3 doubles each) on meshes[j] with cavities[j]
  * (may be NULL when n_cavities[j] == 0) and writes out[j].  All meshes must be

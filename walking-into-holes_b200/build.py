@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-I", str(INCLUDE), "-I", str(CSRC)]
 CUDA_FLAGS = ARCH + ["-lineinfo", "-fmad=false", "--expt-relaxed-constexpr"]
 
-LIB_SOURCES = ["kernels.cu", "design.cu", "twos_abi.cpp", "geometry.cpp"]
+LIB_SOURCES = ["kernels.cu", "design.cu", "noalloc.cu", "twos_abi.cpp", "geometry.cpp"]
 CLI = {"wih_twos": "cli_twos.cpp", "wih_adjoint": "cli_adjoint.cpp"}
 HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h"]
 
