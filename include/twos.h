@@ -192,6 +192,24 @@ int twos_mesh_get_info(const twos_mesh *mesh, twos_mesh_info *info);
  * reference counterpart (the reference has no device work). */
 int twos_mesh_set_stream(twos_mesh *mesh, void *stream);
 
+/* Launch tuning of a session's walk kernel (chosen by the autotuner of
+ * twos_b200/autotune.py; no reference counterpart).
+ *   block:          threads per block, 128, 256 or 512
+ *   refill:         a warp refills from the work queue once this many lanes
+ *                   are idle (1..32)
+ *   step_threshold: a warp takes its batched walk step once this many lanes
+ *                   have finished their closest-point query (1..32)
+ *   blocks_per_sm:  resident blocks per SM, 0 = as many as fit */
+typedef struct twos_tuning {
+  int32_t block;
+  int32_t refill;
+  int32_t step_threshold;
+  int32_t blocks_per_sm;
+} twos_tuning;
+
+int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);
+int twos_mesh_get_tuning(const twos_mesh *mesh, twos_tuning *tuning);
+
 /* Batched unsigned distance and closest point to the mesh surface
  * (EmbreeMesh::closest_point + point_query_callback, wih_twos.cpp:339-359,
  * 416-430).  `closest` may be NULL.  Host buffers. */

@@ -1,0 +1,49 @@
+"""Launch tuning (twos_mesh_set_tuning) and the autotuner: results are a pure
+function of the request and the samples, so every block size, refill
+threshold, step threshold and occupancy cap gives bit-identical rows."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tb(lib_built):
+    import twos_b200
+    return twos_b200
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision):
+    cfg = tb.Config(walks=96, precision=precision, seed=3, source=tb.sources.affine(0.65))
+    with tb.Mesh(*bunny1000) as mesh:
+        ref, _ = mesh.estimate(eval_points, cfg)
+        for block, refill, step, bps in [(256, 1, 1, 0), (512, 1, 1, 0), (128, 8, 8, 0), (128, 32, 32, 2),
+                                         (256, 4, 16, 1)]:
+            mesh.set_tuning(block=block, refill=refill, step_threshold=step, blocks_per_sm=bps)
+            assert mesh.get_tuning() == {"block": block, "refill": refill, "step_threshold": step,
+                                         "blocks_per_sm": bps}
+            out, _ = mesh.estimate(eval_points, cfg)
+            for k in ("u", "score", "score_se", "steps"):
+                np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {block} {refill} {step} {bps}")
+
+
+def test_invalid_tuning_is_usage_error(tb, bunny1000):
+    with tb.Mesh(*bunny1000) as mesh:
+        for bad in [dict(block=96), dict(refill=0), dict(step_threshold=33), dict(blocks_per_sm=-1)]:
+            with pytest.raises(tb.TwosError) as e:
+                mesh.set_tuning(**bad)
+            assert e.value.code == 2
+
+
+def test_autotuner_picks_a_grid_point(tb, bunny1000, eval_points, tmp_path):
+    from twos_b200.autotune import autotune, DEFAULT_GRID
+    cfg = tb.Config(walks=256, precision="mixed", seed=1, source=tb.sources.affine(0.65))
+    cache = tmp_path / "tuning.json"
+    with tb.Mesh(*bunny1000) as mesh:
+        best, results = autotune(mesh, eval_points, cfg, calib_sites=256, calib_walks=64, repeats=1, cache=cache)
+        assert mesh.get_tuning() == best
+        assert len(results) == np.prod([len(v) for v in DEFAULT_GRID.values()])
+        assert all(t > 0 for _, t in results)
+        again, cached = autotune(mesh, eval_points, cfg, cache=cache)
+        assert again == best and cached == []

@@ -180,15 +180,21 @@ __device__ __forceinline__ double gap(double lo, double hi, double p) { return f
 // distance from below; for a nearly flat patch the slab is thin and the
 // bound is close to the true distance, where the box bound is off by up to
 // the box size).
+// 32-byte read-only load (two float4) of 32-byte aligned data: one L1
+// request instead of two.
+__device__ __forceinline__ void ldg32(const void *p, float4 &a, float4 &b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
 __device__ __forceinline__ void node_dist2(const NodeF *__restrict__ nodes, int idx, const Vec<float> &p,
                                            float &dl, float &dr, int &cl, int &cr) {
   const NodeF *n = nodes + idx;
-  const float4 x = __ldg(&n->x);
-  const float4 y = __ldg(&n->y);
-  const float4 z = __ldg(&n->z);
-  const float4 nl = __ldg(&n->nl);
-  const float4 nr = __ldg(&n->nr);
-  const float4 t = __ldg(&n->tail);
+  float4 x, y, z, nl, nr, t;
+  ldg32(&n->x, x, y);
+  ldg32(&n->z, z, nl);
+  ldg32(&n->nr, nr, t);
   const float lx = gap(x.x, x.z, p.x), rx = gap(x.y, x.w, p.x);
   const float ly = gap(y.x, y.z, p.y), ry = gap(y.y, y.w, p.y);
   const float lz = gap(z.x, z.z, p.z), rz = gap(z.y, z.w, p.z);
@@ -256,6 +262,40 @@ __device__ __forceinline__ void load_tri(const TriD *__restrict__ tris, uint32_t
   c = {p3.x, p3.y, p4.x};
 }
 
+// One triangle against the current best: the plane-slab bound first, the
+// full closest-point test only when the bound is below best.  Returns true
+// when the triangle is strictly closer (best2 updated); `full` counts full tests.
+__device__ __forceinline__ bool tri_test(const TriF *__restrict__ tris, uint32_t i, const Vec<float> &p, float &best2,
+                                         unsigned long long &full) {
+  float4 P, A;
+  ldg32(&tris[i].plane, P, A);
+  const float s = __fmaf_rn(P.x, p.x, __fmaf_rn(P.y, p.y, P.z * p.z));
+  const float g = gap(P.w, A.w, s);
+  if (!(g * g < best2)) return false;
+  ++full;
+  float4 B, C;
+  ldg32(&tris[i].b, B, C);
+  const float d2 = tri_dist2(p, Vec<float>{A.x, A.y, A.z}, Vec<float>{B.x, B.y, B.z}, Vec<float>{C.x, C.y, C.z});
+  if (d2 < best2) {
+    best2 = d2;
+    return true;
+  }
+  return false;
+}
+__device__ __forceinline__ bool tri_test(const TriD *__restrict__ tris, uint32_t i, const Vec<double> &p,
+                                         double &best2, unsigned long long &full) {
+  if (!(tri_plane_gap2(tris, i, p) < best2)) return false;
+  ++full;
+  Vec<double> a, b, c;
+  load_tri(tris, i, a, b, c);
+  const double d2 = tri_dist2(p, a, b, c);
+  if (d2 < best2) {
+    best2 = d2;
+    return true;
+  }
+  return false;
+}
+
 __device__ __forceinline__ float lower_f(float v) { return v; }
 __device__ __forceinline__ float lower_f(double v) { return __double2float_rd(v); }
 
@@ -313,12 +353,8 @@ __device__ bool nearest(const typename Layout<T>::Node *__restrict__ nodes,
       const uint32_t enc = ~static_cast<uint32_t>(node);
       const uint32_t first = enc >> 3, count = enc & 7u;
       for (uint32_t i = 0; i < count; ++i) {
-        if (!(tri_plane_gap2(tris, first + i, p) < best2)) continue;
-        Vec<T> a, b, c;
-        load_tri(tris, first + i, a, b, c);
-        const T d2 = tri_dist2(p, a, b, c);
-        if (d2 < best2) {
-          best2 = d2;
+        unsigned long long full = 0;
+        if (tri_test(tris, first + i, p, best2, full)) {
           best_tri = first + i;
           found = true;
         }
@@ -452,14 +488,17 @@ enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
 // never wait for the slowest traversal of the warp, only for the batched
 // step.  MODE: TWOS_MODE_*; the per-walk value type is T (FP32 accumulation
 // in the mixed form, FP64 in the plain form).
-template <typename T, int MODE, bool GREEN>
-__global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
-  __shared__ uint2 s_stack[kStack * kWosBlock];
+template <typename T, int MODE, bool GREEN, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_kernel(const WosLaunch L) {
+  // Dynamic shared memory: the traversal stacks (kStack entries per thread,
+  // column-major so a warp's accesses hit distinct banks), then the tables.
   extern __shared__ __align__(16) unsigned char s_dyn[];
+  uint2 *s_stack = reinterpret_cast<uint2 *>(s_dyn);
+  unsigned char *s_tab = s_dyn + kStack * BLOCK * sizeof(uint2);
   const SmemPlan plan = smem_plan<T>(L.n_jobs, L.n_geos, L.n_terms);
-  JobDesc *s_jobs = reinterpret_cast<JobDesc *>(s_dyn);
-  GeoDesc *s_geos = reinterpret_cast<GeoDesc *>(s_dyn + plan.geo_offset);
-  TermT<T> *s_terms = reinterpret_cast<TermT<T> *>(s_dyn + plan.term_offset);
+  JobDesc *s_jobs = reinterpret_cast<JobDesc *>(s_tab);
+  GeoDesc *s_geos = reinterpret_cast<GeoDesc *>(s_tab + plan.geo_offset);
+  TermT<T> *s_terms = reinterpret_cast<TermT<T> *>(s_tab + plan.term_offset);
 
   for (uint32_t i = threadIdx.x; i < L.n_jobs; i += blockDim.x) s_jobs[i] = L.jobs[i];
   for (uint32_t i = threadIdx.x; i < L.n_geos; i += blockDim.x) s_geos[i] = L.geos[i];
@@ -622,8 +661,15 @@ __global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
       continue;
     }
 
-    // ---- one unit of closest-point traversal
-    if (phase == kTraverse) {
+    // ---- one unit of closest-point traversal.  The warp runs one kind of
+    // unit per iteration -- triangle tests or node tests/pops -- whichever
+    // more of its traversing lanes need, so each iteration executes one code
+    // path instead of the union of both.
+    const bool want_tri = phase == kTraverse && tri_cur < tri_end;
+    const unsigned vt = __ballot_sync(full, want_tri);
+    const unsigned vn = __ballot_sync(full, phase == kTraverse && !want_tri);
+    const bool tri_turn = __popc(vt) >= __popc(vn);
+    if (phase == kTraverse && (!L.vote || want_tri == tri_turn)) {
       const GeoDesc &G = s_geos[s_jobs[job].geo];
       if (++iter > G.max_iter) {
         err |= TWOS_DEVERR_ITER;
@@ -632,22 +678,13 @@ __global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
       } else if (tri_cur < tri_end) {
         const typename Layout<T>::Tri *tris = geo_tris<T>(G);
         ++c_planes;
-        if (tri_plane_gap2(tris, tri_cur, pos) < best2) {
-          ++c_tris;
-          Vec<T> a, b, c;
-          load_tri(tris, tri_cur, a, b, c);
-          const T d2 = tri_dist2(pos, a, b, c);
-          if (d2 < best2) {
-            best2 = d2;
-            found = true;
-          }
-        }
+        if (tri_test(tris, tri_cur, pos, best2, c_tris)) found = true;
         ++tri_cur;
       } else {
         // Pop the next entry still closer than the current best.
         while (!have && sp > 0) {
           --sp;
-          const uint2 e = stack[sp * kWosBlock];
+          const uint2 e = stack[sp * BLOCK];
           if (static_cast<T>(__uint_as_float(e.y)) < best2) {
             node = static_cast<int>(e.x);
             have = true;
@@ -675,7 +712,7 @@ __global__ void __launch_bounds__(kWosBlock, 6) wos_kernel(const WosLaunch L) {
               found = false;
               phase = kStep;
             } else {
-              stack[sp * kWosBlock] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+              stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
               ++sp;
               node = cl;
             }
@@ -750,15 +787,15 @@ cudaError_t launch_site_prepass(int precision, const WosLaunch &L, cudaStream_t 
   return cudaGetLastError();
 }
 
-template <typename T, int MODE, bool GREEN> static const void *wos_fn() {
-  return reinterpret_cast<const void *>(&wos_kernel<T, MODE, GREEN>);
+template <typename T, int MODE, bool GREEN, int BLOCK> static const void *wos_fn() {
+  return reinterpret_cast<const void *>(&wos_kernel<T, MODE, GREEN, BLOCK>);
 }
 
-static const void *select_wos(int precision, int mode, bool green) {
-#define TWOS_PICK(T)                                                                          \
-  if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true>() : wos_fn<T, 0, false>(); \
-  if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true>() : wos_fn<T, 1, false>();     \
-  return green ? wos_fn<T, 2, true>() : wos_fn<T, 2, false>();
+template <int BLOCK> static const void *select_wos_block(int precision, int mode, bool green) {
+#define TWOS_PICK(T)                                                                                          \
+  if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true, BLOCK>() : wos_fn<T, 0, false, BLOCK>(); \
+  if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true, BLOCK>() : wos_fn<T, 1, false, BLOCK>();     \
+  return green ? wos_fn<T, 2, true, BLOCK>() : wos_fn<T, 2, false, BLOCK>();
   if (precision == TWOS_PREC_MIXED) {
     TWOS_PICK(float)
   }
@@ -766,18 +803,33 @@ static const void *select_wos(int precision, int mode, bool green) {
 #undef TWOS_PICK
 }
 
-static uint32_t wos_dyn_smem(int precision, const WosLaunch &L) {
-  return precision == TWOS_PREC_MIXED ? smem_plan<float>(L.n_jobs, L.n_geos, L.n_terms).bytes
-                                      : smem_plan<double>(L.n_jobs, L.n_geos, L.n_terms).bytes;
+// Walk kernel instantiations: block sizes 128, 256 and 512 threads.
+static const void *select_wos(int precision, int mode, bool green, int block) {
+  switch (block) {
+    case 128:
+      return select_wos_block<128>(precision, mode, green);
+    case 256:
+      return select_wos_block<256>(precision, mode, green);
+    case 512:
+      return select_wos_block<512>(precision, mode, green);
+    default:
+      return nullptr;
+  }
+}
+
+static uint32_t wos_dyn_smem(int precision, const WosLaunch &L, int block) {
+  const uint32_t stack = static_cast<uint32_t>(kStack * block * sizeof(uint2));
+  return stack + (precision == TWOS_PREC_MIXED ? smem_plan<float>(L.n_jobs, L.n_geos, L.n_terms).bytes
+                                               : smem_plan<double>(L.n_jobs, L.n_geos, L.n_terms).bytes);
 }
 
 cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
                        cudaStream_t s) {
-  if (block != kWosBlock) return cudaErrorInvalidValue;
   if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
-  const uint32_t dyn = wos_dyn_smem(precision, L);
-  if (dyn > 64 * 1024) return cudaErrorInvalidValue;
-  const void *fn = select_wos(precision, mode, green);
+  const uint32_t dyn = wos_dyn_smem(precision, L, block);
+  if (dyn > 200 * 1024) return cudaErrorInvalidValue;
+  const void *fn = select_wos(precision, mode, green, block);
+  if (!fn) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
   WosLaunch copy = L;
@@ -786,8 +838,9 @@ cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, 
 }
 
 int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L) {
-  const uint32_t dyn = wos_dyn_smem(precision, L);
-  const void *fn = select_wos(precision, mode, green);
+  const uint32_t dyn = wos_dyn_smem(precision, L, block);
+  const void *fn = select_wos(precision, mode, green, block);
+  if (!fn || dyn > 200 * 1024) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;
   int n = 0;

@@ -148,10 +148,11 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.steps_out = reinterpret_cast<uint32_t *>(base + lay.steps);
     L.refill = m->refill;
     L.step_threshold = m->step_threshold;
+    L.vote = m->vote;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;
-    const int block = 128;
+    const int block = m->block;
     const int per_sm = wos_max_blocks_per_sm(r->precision, r->mode, r->green != 0, block, L);
     if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
     const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;

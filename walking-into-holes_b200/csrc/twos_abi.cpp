@@ -132,6 +132,11 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_REFILL")) m->refill = std::max(1, std::atoi(e));
     if (const char *e = std::getenv("TWOS_STEP_THRESHOLD")) m->step_threshold = std::max(1, std::atoi(e));
     if (const char *e = std::getenv("TWOS_BLOCKS_PER_SM")) m->blocks_per_sm = std::max(0, std::atoi(e));
+    if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
+    if (const char *e = std::getenv("TWOS_BLOCK")) {
+      const int b = std::atoi(e);
+      if (b == 128 || b == 256 || b == 512) m->block = b;
+    }
   } catch (const std::exception &e) {
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
@@ -312,10 +317,11 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.steps_out = m->steps.as<uint32_t>();
   L.refill = m->refill;
   L.step_threshold = m->step_threshold;
+  L.vote = m->vote;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
-  const int block = 128;
+  const int block = m->block;
   const int per_sm = wos_max_blocks_per_sm(r0->precision, mode, green, block, L);
   if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
   const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
@@ -456,6 +462,27 @@ int twos_mesh_set_stream(twos_mesh *m, void *stream) {
   cudaSetDevice(m->device);
   cudaStreamSynchronize(m->stream);
   m->stream = stream ? static_cast<cudaStream_t>(stream) : m->own_stream;
+  return TWOS_OK;
+}
+
+int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
+  if (!m || !t) return fail(TWOS_ERR_USAGE, "null argument");
+  if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
+      t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0)
+    return fail(TWOS_ERR_USAGE, "invalid tuning");
+  m->block = t->block;
+  m->refill = t->refill;
+  m->step_threshold = t->step_threshold;
+  m->blocks_per_sm = t->blocks_per_sm;
+  return TWOS_OK;
+}
+
+int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
+  if (!m || !t) return fail(TWOS_ERR_USAGE, "null argument");
+  t->block = m->block;
+  t->refill = m->refill;
+  t->step_threshold = m->step_threshold;
+  t->blocks_per_sm = m->blocks_per_sm;
   return TWOS_OK;
 }
 
@@ -741,6 +768,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.steps_out = m->steps.as<uint32_t>();
     Ls.refill = m->refill;
     Ls.step_threshold = m->step_threshold;
+    Ls.vote = m->vote;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -785,7 +813,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     D.pair_clearance = pair;
     D.iteration = iter.as<uint32_t>();
     D.history = hist.as<DesignStep>();
-    const int block = 128;
+    const int block = m->block;
     const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green != 0, block, Ls);
     const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green != 0, block, Lv);
     if (per_s <= 0 || per_v <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");

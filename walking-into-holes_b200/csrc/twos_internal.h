@@ -156,6 +156,7 @@ struct WosLaunch {
   // first query is answered from here (-1 when nothing is within range).
   void *site_best2;
   uint32_t total_sites;
+  int vote;  // 1: a warp runs one kind of traversal unit per iteration (majority vote)
 };
 
 // Fills L.site_best2 (T per site, T = float for mixed, double for FP64).

@@ -63,7 +63,9 @@ struct twos_mesh {
   twos::DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, first, counter, totals, points, dist, closest,
       topk;
   size_t max_launch_walks = size_t(1) << 30;
+  int block = 128;         // walk-kernel threads per block
   int refill = 1;          // lanes idle before a warp refills from the queue
   int step_threshold = 1;  // finished queries before a warp takes its walk step
   int blocks_per_sm = 0;   // 0: as many as fit
+  int vote = 0;            // 1: one kind of traversal unit per warp iteration
 };

@@ -24,7 +24,7 @@ EXPORTED = [
     "twos_abi_version", "twos_last_error", "twos_mesh_open", "twos_mesh_open_ply", "twos_mesh_close",
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
-    "twos_estimate_noalloc",
+    "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning",
 ]
 
 
@@ -75,6 +75,11 @@ class MeshInfo(ctypes.Structure):
         ("center", ctypes.c_double * 3), ("mixed_delta", ctypes.c_double),
         ("build_seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
     ]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int32), ("refill", ctypes.c_int32), ("step_threshold", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32)]
 
 
 class DesignParams(ctypes.Structure):
@@ -133,7 +138,9 @@ def load(path: Path | str | None = None):
     L.twos_closest_point.argtypes = [vp, i32, vp, u64, dbl, vp, vp]
     L.twos_estimate.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_estimate_device.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
-    L.twos_estimate_noalloc.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
+    L.twos_mesh_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.twos_mesh_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.twos_estimate_noalloc.argtypes =[vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_estimate_batch.argtypes =[vp, ctypes.POINTER(Request), u32, vp, vp, vp, vp, vp, ctypes.POINTER(Summary)]
     L.twos_design_loop.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(Request), vp, u32, vp, u32,
                                    ctypes.POINTER(DesignParams), vp, vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]

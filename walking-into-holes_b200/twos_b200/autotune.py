@@ -1,0 +1,70 @@
+"""Autotuner for the walk kernel's launch parameters.
+
+Times a calibration estimate (a seeded random subset of the workload's sites,
+the workload's own request with fewer walks) for every candidate setting of
+
+* block size (threads per block): 128, 256, 512;
+* queue-refill threshold: idle lanes before a warp refills from the queue;
+* step threshold: finished queries before a warp takes its batched step;
+* resident blocks per SM (occupancy cap);
+
+and leaves the fastest (walk-kernel device time per closest-point query) set
+on the mesh.  Results can be cached in a JSON file keyed by the mesh's size and
+the request's precision/mode, so a service tunes once per geometry class.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+from dataclasses import replace
+from pathlib import Path
+
+import numpy as np
+
+DEFAULT_GRID = {
+    "block": (128, 256, 512),
+    "refill": (1, 4),
+    "step_threshold": (1, 4),
+    "blocks_per_sm": (0,),
+}
+
+
+def _key(mesh, config) -> str:
+    info = mesh.info()
+    return f"faces={info['faces']}|precision={config.precision}|mode={config.mode}|green={int(config.green)}"
+
+
+def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, repeats=2, seed=0,
+             cache: str | Path | None = None, cavities=None):
+    """Pick the fastest launch tuning for `config` on `mesh`; returns
+    (best tuning dict, list of (tuning, seconds per query))."""
+    key = _key(mesh, config)
+    if cache is not None and Path(cache).exists():
+        table = json.loads(Path(cache).read_text())
+        if key in table:
+            mesh.set_tuning(**table[key])
+            return table[key], []
+    grid = grid or DEFAULT_GRID
+    sites = np.asarray(sites, dtype=np.float64).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    pick = sites[rng.choice(len(sites), size=min(calib_sites, len(sites)), replace=False)]
+    calib = replace(config, walks=min(config.walks, calib_walks))
+    results = []
+    names = list(grid)
+    for values in itertools.product(*(grid[n] for n in names)):
+        tuning = dict(zip(names, values))
+        mesh.set_tuning(**tuning)
+        times = []
+        for r in range(repeats + 1):
+            calib.repeat = 5000 + r
+            _, s = mesh.estimate(pick, calib, cavities=cavities)
+            if r:  # the first run is a warm-up
+                times.append(s["walk_seconds"] / max(1, s["queries"]))
+        results.append((tuning, float(np.median(times))))
+    best = min(results, key=lambda t: t[1])[0]
+    mesh.set_tuning(**best)
+    if cache is not None:
+        table = json.loads(Path(cache).read_text()) if Path(cache).exists() else {}
+        table[key] = best
+        Path(cache).write_text(json.dumps(table, indent=1, sort_keys=True) + "\n")
+    return best, results

@@ -121,6 +121,16 @@ class Mesh:
         handle = getattr(stream, "cuda_stream", stream)
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
+    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0):
+        t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm))
+        check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _abi.Tuning()
+        check(_abi.load().twos_mesh_get_tuning(self._h, ctypes.byref(t)))
+        return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
+                "blocks_per_sm": t.blocks_per_sm}
+
     def info(self) -> dict:
         i = _abi.MeshInfo()
         check(_abi.load().twos_mesh_get_info(self._h, ctypes.byref(i)))
