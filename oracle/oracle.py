@@ -96,6 +96,10 @@ def lib():
         L.oracle_estimate.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_diffwos.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p]
         assert L.oracle_sizeof_params() == ctypes.sizeof(Params)
         assert L.oracle_sizeof_site() == ctypes.sizeof(Site)
         _lib = L
@@ -133,6 +137,18 @@ def housing_source():
 def sensor_source(side=1):
     """adjoint.cpp:11-15 with the --sensor-side flip of adjoint.cpp:98-102."""
     return [term(TERM_BUMP, 1.0, c=(0.55 * side, 0.18 * side, -0.03), w=(0.13, 0.0, 0.0))]
+
+
+def load_study_config(path):
+    """benchmarks/submission_study/study.cpp:37-42: a sensor line (x y z r)
+    then heat lines (x y z r A).  Returns (sensor (x, y, z, r), heat source
+    terms: sum of A * (1 - |x-c|^2/r^2)_+^2 in file order, study.cpp:27-35)."""
+    rows = [list(map(float, line.split())) for line in open(path) if line.strip()]
+    sensor = tuple(rows[0][:4])
+    heat = [term(TERM_BUMP, r[4], c=tuple(r[:3]), w=(r[3], 0.0, 0.0)) for r in rows[1:]]
+    if not heat:
+        raise RuntimeError("missing compact heat sources")
+    return sensor, heat
 
 
 # --------------------------------------------------------------------------- mesh
@@ -211,6 +227,24 @@ class OracleMesh:
             out["aabb_tests"] = tests[..., 0]
             out["tri_tests"] = tests[..., 1]
         return out
+
+    def diffwos(self, sites, cavities, diff_offset, site_ids=None, enclosure_fallback=True, **kw):
+        """evaluate_differential_site over sites (wih_twos.cpp:839-928) in the
+        reference stream.  Returns (derivs [n, ncav, 8] = dc(3), dc_se(3), dR,
+        dR_se; stats [n, 7]; totals (distance queries, parity rays, fallbacks))."""
+        p = self._params(**kw)
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        ids = None if site_ids is None else np.ascontiguousarray(site_ids, dtype=np.uint64)
+        out = np.zeros((len(s), len(cav), 8))
+        stats = np.zeros((len(s), 7), dtype=np.uint64)
+        totals = np.zeros(3, dtype=np.uint64)
+        rc = lib().oracle_diffwos(self.handle, ctypes.byref(p), float(diff_offset), int(bool(enclosure_fallback)),
+                                  _ptr(s), _ptr(ids), len(s), _ptr(cav), len(cav), _ptr(out), _ptr(stats),
+                                  _ptr(totals))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return out, stats, totals
 
     def estimate(self, sites, site_ids=None, cavities=None, **kw):
         p = self._params(**kw)

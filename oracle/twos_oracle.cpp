@@ -790,3 +790,307 @@ int oracle_sizeof_params() { return static_cast<int>(sizeof(oracle_params)); }
 int oracle_sizeof_site() { return static_cast<int>(sizeof(oracle_site)); }
 
 }  // extern "C"
+
+// ================================================================ Differential WoS
+// Restates evaluate_differential_site (wih_twos.cpp:839-928) with
+// walk_to_boundary (725-740), closest_boundary (602-626),
+// classify_offset_safety (765-837, with the WIH_ENCLOSURE_FALLBACK branch of
+// benchmarks/submission_study/study.cpp:7) and EmbreeMesh::inside (361-394),
+// in the reference's mt19937_64 stream.  Distance queries and parity rays are
+// counted as note_query(0)/(1)/(2) count them (study.cpp:8-16).
+
+namespace {
+
+struct Counters {
+  uint64_t queries = 0, rays = 0, fallbacks = 0;
+};
+
+// Closest hit t of a ray in [tnear, tfar] (Moller-Trumbore, FP64), or -1.
+double ray_triangle(const Vec3 &o, const Vec3 &d, const Vec3 &a, const Vec3 &b, const Vec3 &c) {
+  const Vec3 e1 = b - a, e2 = c - a;
+  const Vec3 pv{d.y * e2.z - d.z * e2.y, d.z * e2.x - d.x * e2.z, d.x * e2.y - d.y * e2.x};
+  const double det = dot(e1, pv);
+  if (det == 0.0) return -1.0;
+  const double inv = 1.0 / det;
+  const Vec3 tv = o - a;
+  const double u = dot(tv, pv) * inv;
+  if (u < 0.0 || u > 1.0) return -1.0;
+  const Vec3 qv{tv.y * e1.z - tv.z * e1.y, tv.z * e1.x - tv.x * e1.z, tv.x * e1.y - tv.y * e1.x};
+  const double w = dot(d, qv) * inv;
+  if (w < 0.0 || u + w > 1.0) return -1.0;
+  return dot(e2, qv) * inv;
+}
+
+bool ray_box(const Box &b, const Vec3 &o, const Vec3 &inv, double tmin, double tmax) {
+  for (int a = 0; a < 3; ++a) {
+    double t0 = (coord(b.lo, a) - coord(o, a)) * coord(inv, a), t1 = (coord(b.hi, a) - coord(o, a)) * coord(inv, a);
+    if (t0 > t1) std::swap(t0, t1);
+    tmin = std::max(tmin, t0);
+    tmax = std::min(tmax, t1);
+    if (tmin > tmax) return false;
+  }
+  return true;
+}
+
+double first_hit(const Mesh &m, const Vec3 &o, const Vec3 &d, double tnear, double tfar) {
+  const Vec3 inv{1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
+  double best = -1.0, lim = tfar;
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const Bvh::Node &n = m.bvh.nodes[stack[--sp]];
+    if (!ray_box(n.box, o, inv, tnear, lim)) continue;
+    if (n.left < 0) {
+      for (int i = 0; i < n.count; ++i) {
+        const auto &f = m.f[m.bvh.order[n.begin + i]];
+        const double t = ray_triangle(o, d, m.v[f[0]], m.v[f[1]], m.v[f[2]]);
+        if (t >= tnear && t <= lim) {
+          lim = t;
+          best = t;
+        }
+      }
+    } else {
+      stack[sp++] = n.left;
+      stack[sp++] = n.right;
+    }
+  }
+  return best;
+}
+
+// EmbreeMesh::inside: parity of hits along a fixed oblique ray, re-shot from
+// each hit (t + 2e-6), at most 128 hits.
+bool inside_parity(const Mesh &m, const Vec3 &p, Counters &cnt) {
+  Vec3 dir{1.0, 0.3713906763541037, 0.1570796326794897};
+  dir = dir * (1.0 / norm(dir));
+  Vec3 origin = p;
+  unsigned hits = 0;
+  for (; hits < 128; ++hits) {
+    ++cnt.rays;
+    const double t = first_hit(m, origin, dir, 1.0e-6, 4.0);
+    if (t < 0.0) break;
+    origin = origin + dir * (t + 2.0e-6);
+  }
+  if (hits == 128) throw std::runtime_error("ray-parity traversal exceeded 128 intersections");
+  return hits % 2U == 1U;
+}
+
+struct Hit {
+  double distance = std::numeric_limits<double>::infinity();
+  Vec3 point, normal;
+  int cavity = -1;
+};
+
+Hit closest_boundary(const Mesh &m, const Vec3 &x, const std::vector<Vec3> &cav, double R, Counters &cnt) {
+  ++cnt.queries;
+  const Closest c = closest_point(m, x, 4.0, nullptr);
+  if (!std::isfinite(c.distance)) throw std::runtime_error("closest-point query failed");
+  Hit h;
+  h.distance = c.distance;
+  h.point = c.point;
+  if (c.distance > 0.0) h.normal = (c.point - x) * (1.0 / c.distance);
+  for (size_t i = 0; i < cav.size(); ++i) {
+    const Vec3 radial = x - cav[i];
+    const double len = norm(radial);
+    const double d = len - R;
+    if (d < h.distance && len > 0.0) {
+      const Vec3 dir = radial * (1.0 / len);
+      h.distance = d;
+      h.point = cav[i] + dir * R;
+      h.normal = dir * -1.0;
+      h.cavity = static_cast<int>(i);
+    }
+  }
+  return h;
+}
+
+double domain_distance_counted(const Mesh &m, const Vec3 &x, const std::vector<Vec3> &cav, double R, Counters &cnt) {
+  ++cnt.queries;
+  const Closest c = closest_point(m, x, 4.0, nullptr);
+  if (!std::isfinite(c.distance)) throw std::runtime_error("closest-point query failed");
+  double d = c.distance;
+  for (const Vec3 &cc : cav) d = std::min(d, norm(x - cc) - R);
+  return d;
+}
+
+struct DiffSite {
+  std::vector<double> sums, sq;  // per cavity: cx, cy, cz, r
+  uint64_t outer_steps = 0, nested_steps = 0, cav_terms = 0, near_seam = 0, seg_unsafe = 0, unsafe = 0, limits = 0;
+};
+
+}  // namespace
+
+extern "C" {
+
+// Per-site results: out[site][cavity][8] = dc (3), dc_se (3), dR, dR_se;
+// stats[site][7] = outer_steps, nested_steps, cavity_terminations,
+// near_seam, segment_unsafe, unsafe_offset, limits; totals[3] = distance
+// queries, parity rays, enclosure fallbacks.
+int oracle_diffwos(const oracle_mesh *om, const oracle_params *o, double diff_offset, int enclosure_fallback,
+                   const double *sites, const uint64_t *site_ids, uint32_t n_sites, const double *cav_xyz,
+                   uint32_t ncav, double *out, uint64_t *stats, uint64_t *totals) {
+  const Mesh &m = om->m;
+  std::vector<Vec3> cav(ncav);
+  for (uint32_t i = 0; i < ncav; ++i) cav[i] = {cav_xyz[3 * i], cav_xyz[3 * i + 1], cav_xyz[3 * i + 2]};
+  const double R = o->cavity_radius, eps = o->epsilon;
+  std::atomic<uint64_t> tq{0}, tr{0}, tf{0};
+  std::atomic<int> failed{0};
+#ifdef _OPENMP
+  if (o->threads > 0) omp_set_num_threads(o->threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int64_t si = 0; si < static_cast<int64_t>(n_sites); ++si) {
+    try {
+      Counters cnt;
+      const Vec3 x0{sites[3 * si], sites[3 * si + 1], sites[3 * si + 2]};
+      const uint64_t site = site_ids ? site_ids[si] : static_cast<uint64_t>(si);
+      DiffSite r;
+      r.sums.assign(4 * ncav, 0.0);
+      r.sq.assign(4 * ncav, 0.0);
+      for (int sample = 0; sample < o->walks; ++sample) {
+        const uint64_t outer_key = splitmix64(o->seed + 0x6a09e667f3bcc909ULL) ^
+                                   splitmix64(static_cast<uint64_t>(o->repeat) + 0xbb67ae8584caa73bULL) ^
+                                   splitmix64(site + 0x3c6ef372fe94f82bULL) ^
+                                   splitmix64(static_cast<uint64_t>(sample) + 0xa54ff53a5f1d36f1ULL);
+        // walk_to_boundary
+        std::mt19937_64 rng(splitmix64(outer_key));
+        Vec3 y = x0;
+        Hit hit;
+        int steps = 0;
+        bool limit = true;
+        for (int k = 0; k < o->max_steps; ++k) {
+          hit = closest_boundary(m, y, cav, R, cnt);
+          if (!(hit.distance > eps)) {
+            limit = false;
+            break;
+          }
+          y = y + random_unit_vector(rng) * hit.distance;
+          ++steps;
+        }
+        r.outer_steps += steps;
+        if (limit) {
+          ++r.limits;
+          continue;
+        }
+        if (hit.cavity < 0) continue;
+        ++r.cav_terms;
+        const Vec3 offset = hit.point - hit.normal * diff_offset;
+        // classify_offset_safety
+        bool near_seam = false, seg_unsafe = false;
+        const Vec3 segment = offset - hit.point;
+        const double seg2 = dot(segment, segment);
+        const double tol = 1.0e-10 * std::max(1.0, std::abs(R));
+        const double coll2 = (R + tol) * (R + tol);
+        const Vec3 &hc = cav[hit.cavity];
+        for (size_t i = 0; i < cav.size(); ++i) {
+          if (static_cast<int>(i) == hit.cavity) continue;
+          const Vec3 cd = cav[i] - hc;
+          const double cdist = norm(cd);
+          if (cdist > tol && cdist < 2.0 * R) {
+            const Vec3 axis = cd * (1.0 / cdist);
+            const Vec3 seam_center = (hc + cav[i]) * 0.5;
+            const double seam_r = std::sqrt(std::max(0.0, R * R - 0.25 * (cdist * cdist)));
+            const Vec3 rel = hit.point - seam_center;
+            const double axial = dot(rel, axis);
+            const Vec3 radial = rel - axis * axial;
+            const double nr = norm(radial) - seam_r;
+            const double seam_d = std::sqrt(axial * axial + nr * nr);
+            near_seam = near_seam || seam_d <= diff_offset;
+          }
+          if (seg2 > 0.0) {
+            const double par = std::clamp(dot(cav[i] - hit.point, segment) / seg2, 0.0, 1.0);
+            const Vec3 cl = hit.point + segment * par;
+            if (dot(cl - cav[i], cl - cav[i]) <= coll2) seg_unsafe = true;
+          }
+        }
+        bool inside = inside_parity(m, offset, cnt);
+        if (enclosure_fallback && !inside && inside_parity(m, hc, cnt)) {
+          ++cnt.queries;
+          const Closest cc = closest_point(m, hc, 4.0, nullptr);
+          if (cc.distance > R + diff_offset + eps && norm(offset - hc) <= R + diff_offset + eps * 0.5) {
+            inside = true;
+            ++cnt.fallbacks;
+          }
+        }
+        if (!inside || !(domain_distance_counted(m, offset, cav, R, cnt) > eps)) seg_unsafe = true;
+        r.near_seam += near_seam;
+        r.seg_unsafe += seg_unsafe;
+        if (near_seam || seg_unsafe) {
+          ++r.unsafe;
+          continue;
+        }
+        // nested walk (wih_twos.cpp walk, counted queries)
+        const uint64_t nested_key = splitmix64(outer_key ^ 0x510e527fade682d1ULL);
+        std::mt19937_64 nr(splitmix64(nested_key));
+        Vec3 z = offset;
+        double value = 0.0;
+        int nsteps = 0;
+        bool nlimit = true;
+        for (int k = 0; k < o->max_steps; ++k) {
+          const double rr = domain_distance_counted(m, z, cav, R, cnt);
+          if (!(rr > eps)) {
+            nlimit = false;
+            break;
+          }
+          Vec3 a = z;
+          if (o->green) {
+            const double scale = rr * beta_22(nr);
+            const Vec3 dir = random_unit_vector(nr);
+            a = z + dir * scale;
+          }
+          value += source_value(o->source, o->n_source, a) * rr * rr / 6.0;
+          z = z + random_unit_vector(nr) * rr;
+          ++nsteps;
+        }
+        r.nested_steps += nsteps;
+        r.limits += nlimit ? 1 : 0;
+        const double scale = value / diff_offset;
+        const double sample_v[4] = {hit.normal.x * scale, hit.normal.y * scale, hit.normal.z * scale, -scale};
+        for (int k = 0; k < 4; ++k) {
+          r.sums[4 * hit.cavity + k] += sample_v[k];
+          r.sq[4 * hit.cavity + k] += sample_v[k] * sample_v[k];
+        }
+      }
+      const double n = o->walks;
+      for (uint32_t c = 0; c < ncav; ++c) {
+        double *row = out + (static_cast<size_t>(si) * ncav + c) * 8;
+        for (int k = 0; k < 3; ++k) row[k] = r.sums[4 * c + k] * (1.0 / n);
+        row[6] = r.sums[4 * c + 3] / n;
+        const double den = n * (n - 1.0);
+        for (int k = 0; k < 4; ++k) {
+          const double v = o->walks > 1 ? std::sqrt(std::max(0.0, (r.sq[4 * c + k] - r.sums[4 * c + k] *
+                                                                                            r.sums[4 * c + k] / n) /
+                                                                        den))
+                                        : 0.0;
+          if (k < 3)
+            row[3 + k] = v;
+          else
+            row[7] = v;
+        }
+      }
+      uint64_t *st = stats + 7 * static_cast<size_t>(si);
+      st[0] = r.outer_steps;
+      st[1] = r.nested_steps;
+      st[2] = r.cav_terms;
+      st[3] = r.near_seam;
+      st[4] = r.seg_unsafe;
+      st[5] = r.unsafe;
+      st[6] = r.limits;
+      tq += cnt.queries;
+      tr += cnt.rays;
+      tf += cnt.fallbacks;
+    } catch (const std::exception &) {
+      failed = 1;
+    }
+  }
+  totals[0] = tq;
+  totals[1] = tr;
+  totals[2] = tf;
+  if (failed) {
+    g_error = "differential walk failed";
+    return 1;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -41,6 +41,13 @@ MESHES = {
     "benchmarks/stanford_bunny/output/stanford-bunny-watertight.ply": "stanford-bunny-watertight.ply.gz",
     "benchmarks/engineering_housing/assets/stylized-finned-housing.ply": "stylized-finned-housing.ply.gz",
 }
+MESHES["benchmarks/submission_study/assets/branch.ply"] = "branch.ply.gz"
+# Differential-WoS requests of the study backend (wih_study --diff 1): argv in
+# request.json, totals in kernel.json, per-cavity derivatives in field.csv.
+GRADIENT = [
+    "gradient-0.004-6",
+    "gradient-0.008-0",
+]
 PAIRED = [
     "side1/seed2026091500/twos_sparse/round1/scout",
     "side1/seed2026091500/twos_dense/round2/rescore",
@@ -81,6 +88,19 @@ def main(reference: Path) -> None:
         (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
         index.append(tag)
     (paired / "index.json").write_text(json.dumps(index, indent=1) + "\n")
+    grad = out / "submission_study"
+    grad.mkdir(exist_ok=True)
+    shutil.copyfile(reference / "benchmarks/submission_study/assets/branch.txt", grad / "branch.txt")
+    gbase = reference / "benchmarks/submission_study/validation-v1-remote-sources/raw"
+    for tag in GRADIENT:
+        dst = grad / tag
+        dst.mkdir(exist_ok=True)
+        for name in ("points.txt", "holes.txt", "field.csv", "kernel.json"):
+            shutil.copyfile(gbase / tag / name, dst / name)
+        argv = json.loads((gbase / tag / "request.json").read_text())[1:]
+        keep = {k: v for k, v in zip(argv[0::2], argv[1::2])
+                if k not in ("--mesh", "--config", "--points", "--cavities", "--output", "--summary")}
+        (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
 
 
 if __name__ == "__main__":
