@@ -315,6 +315,43 @@ int twos_design_loop(twos_mesh *mesh, const twos_request *scout, const twos_requ
                      uint32_t n_cavities, const twos_design_params *params, twos_design_step *history,
                      double *cavities_out, uint32_t *n_cavities_out, twos_summary *summary);
 
+/* Differential WoS (evaluate_differential_site, wih_twos.cpp:839-928;
+ * --mode diffwos, run_differential_wos 1604-1709; study.cpp --diff 1,
+ * 304-316): at each probe site, the derivatives of u with respect to every
+ * cavity's centre and radius.  Each of request->walks outer walks runs to the
+ * boundary; one that ends on cavity i is offset inward by diff_offset along
+ * the normal, checked for seam/segment safety and membership (ray parity,
+ * with the enclosure fallback when enclosure_fallback != 0), and a nested
+ * walk from the offset point gives the samples n u/l (centre) and -u/l
+ * (radius).  out is [n_sites][n_cavities]; stats ([n_sites]) may be NULL.
+ * The request's source terms and green flag drive the nested walks.
+ * Returns TWOS_ERR_RUNTIME when a walk hit max_steps or an offset was unsafe
+ * (rows and stats are still written), as the study backend does
+ * (study.cpp:309-310).  In `summary`, queries counts closest-point queries as
+ * the study backend's note_query(0) does, node_tests the parity rays
+ * (note_query(1)), plane_tests the enclosure fallbacks taken and
+ * triangle_tests the unsafe offsets. */
+typedef struct twos_diff_result {
+  double dc[3];
+  double dc_se[3];
+  double dR;
+  double dR_se;
+} twos_diff_result; /* 64 bytes */
+
+typedef struct twos_diff_stats {
+  uint64_t outer_steps;
+  uint64_t nested_steps;
+  uint64_t cavity_terminations;
+  uint64_t near_seam;
+  uint64_t segment_unsafe;
+  uint64_t unsafe_offset;
+  uint64_t limits;
+} twos_diff_stats;
+
+int twos_diffwos(twos_mesh *mesh, const twos_request *request, double diff_offset, int enclosure_fallback,
+                 const double *sites, uint32_t n_sites, const double *cavities, uint32_t n_cavities,
+                 twos_diff_result *out, twos_diff_stats *stats, twos_summary *summary);
+
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid
  * out [site][walk].  Host buffers.  Used by parity tests. */

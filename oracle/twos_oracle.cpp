@@ -796,8 +796,9 @@ int oracle_sizeof_site() { return static_cast<int>(sizeof(oracle_site)); }
 // walk_to_boundary (725-740), closest_boundary (602-626),
 // classify_offset_safety (765-837, with the WIH_ENCLOSURE_FALLBACK branch of
 // benchmarks/submission_study/study.cpp:7) and EmbreeMesh::inside (361-394),
-// in the reference's mt19937_64 stream.  Distance queries and parity rays are
-// counted as note_query(0)/(1)/(2) count them (study.cpp:8-16).
+// in the reference's mt19937_64 stream (rng 0) or the GPU's counter stream
+// (rng 1).  Distance queries and parity rays are counted as
+// note_query(0)/(1)/(2) count them (study.cpp:8-16).
 
 namespace {
 
@@ -952,8 +953,18 @@ int oracle_diffwos(const oracle_mesh *om, const oracle_params *o, double diff_of
                                    splitmix64(static_cast<uint64_t>(o->repeat) + 0xbb67ae8584caa73bULL) ^
                                    splitmix64(site + 0x3c6ef372fe94f82bULL) ^
                                    splitmix64(static_cast<uint64_t>(sample) + 0xa54ff53a5f1d36f1ULL);
-        // walk_to_boundary
+        // walk_to_boundary.  Counter stream: the outer walk draws block 0 of
+        // (seed, stream); the nested walk is a compliance walk of
+        // (seed, stream + 1), both at counter (step, sample, site, repeat).
         std::mt19937_64 rng(splitmix64(outer_key));
+        CounterStream cs_outer{}, cs_nested{};
+        if (o->rng != 0) {
+          counter_key(o->seed, o->stream, cs_outer.k0, cs_outer.k1);
+          counter_key(o->seed, o->stream + 1, cs_nested.k0, cs_nested.k1);
+          cs_outer.walk = cs_nested.walk = static_cast<uint32_t>(sample);
+          cs_outer.site = cs_nested.site = static_cast<uint32_t>(site);
+          cs_outer.repeat = cs_nested.repeat = o->repeat;
+        }
         Vec3 y = x0;
         Hit hit;
         int steps = 0;
@@ -964,7 +975,13 @@ int oracle_diffwos(const oracle_mesh *om, const oracle_params *o, double diff_of
             limit = false;
             break;
           }
-          y = y + random_unit_vector(rng) * hit.distance;
+          if (o->rng == 0) {
+            y = y + random_unit_vector(rng) * hit.distance;
+          } else {
+            double a0, a1;
+            cs_outer.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
+            y = y + direction_from(a0, a1) * hit.distance;
+          }
           ++steps;
         }
         r.outer_steps += steps;
@@ -1032,14 +1049,30 @@ int oracle_diffwos(const oracle_mesh *om, const oracle_params *o, double diff_of
             nlimit = false;
             break;
           }
-          Vec3 a = z;
-          if (o->green) {
-            const double scale = rr * beta_22(nr);
-            const Vec3 dir = random_unit_vector(nr);
-            a = z + dir * scale;
+          if (o->rng == 0) {
+            Vec3 a = z;
+            if (o->green) {
+              const double scale = rr * beta_22(nr);
+              const Vec3 dir = random_unit_vector(nr);
+              a = z + dir * scale;
+            }
+            value += source_value(o->source, o->n_source, a) * rr * rr / 6.0;
+            z = z + random_unit_vector(nr) * rr;
+          } else {
+            // The GPU walk's draw layout (see walk()).
+            double a0, a1;
+            cs_nested.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
+            Vec3 a = z;
+            if (o->green) {
+              double g0, g1, b0, b1, b2, spare;
+              cs_nested.uniforms(static_cast<uint32_t>(k), 1, g0, g1);
+              cs_nested.uniforms(static_cast<uint32_t>(k), 2, b0, b1);
+              cs_nested.uniforms(static_cast<uint32_t>(k), 3, b2, spare);
+              a = z + direction_from(g0, g1) * (rr * median3(b0, b1, b2));
+            }
+            value += rr * rr / 6.0 * source_value(o->source, o->n_source, a);
+            z = z + direction_from(a0, a1) * rr;
           }
-          value += source_value(o->source, o->n_source, a) * rr * rr / 6.0;
-          z = z + random_unit_vector(nr) * rr;
           ++nsteps;
         }
         r.nested_steps += nsteps;

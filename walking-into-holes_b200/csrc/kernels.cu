@@ -535,6 +535,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
   T best2 = T(0);
   int node = 0, sp = 0;
   bool have = false, found = false;
+  uint32_t best_tri = 0;  // leaf-order index of the nearest triangle (boundary mode)
   uint32_t tri_cur = 0, tri_end = 0, iter = 0;
 
   for (;;) {
@@ -557,12 +558,18 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           site = static_cast<uint32_t>(local / J.walks);
           walk = static_cast<uint32_t>(local - static_cast<uint64_t>(site) * J.walks);
           const GeoDesc &G = s_geos[J.geo];
-          pos = to_frame<T>(L.sites + 3ull * (J.site_begin + site), G);
+          bool skip = false;
+          if (L.walk_start) {
+            const double *st = L.walk_start + 3ull * wid;
+            skip = isnan(st[0]);
+            pos = to_frame<T>(st, G);
+          } else {
+            pos = to_frame<T>(L.sites + 3ull * (J.site_begin + site), G);
+          }
           u = T(0);
           pv = T(0);
           steps = 0;
-          bool skip = false;
-          if (J.flags & kJobSkipCavitySites) {
+          if (!skip && (J.flags & kJobSkipCavitySites)) {
             const T R = to_T<T>(J.cavity_radius);
             for (uint32_t c = 0; c < J.n_cav; ++c) {
               const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
@@ -571,10 +578,11 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
             }
           }
           if (skip) {
-            static_cast<T *>(L.u_out)[wid] = T(0);
+            if (MODE != kModeBoundary) static_cast<T *>(L.u_out)[wid] = T(0);
             if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+            if (MODE == kModeBoundary) L.hits[wid].cavity = -2;
             L.steps_out[wid] = 0u;
-          } else if (L.site_best2) {
+          } else if (L.site_best2 && MODE != kModeBoundary) {
             // First query answered by the per-site pre-pass.
             best2 = static_cast<const T *>(L.site_best2)[J.site_rank + site];
             found = best2 >= T(0);
@@ -605,11 +613,22 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
         d = T(0);  // ends the walk; the call reports the failure
       }
       const T R = to_T<T>(J.cavity_radius);
+      const T dmesh = d;
+      int hit_cav = -1;
       for (uint32_t c = 0; c < J.n_cav; ++c) {
         const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
         const Vec<T> dv = sub(pos, cc);
-        const T dc = sqrt(dot3(dv, dv)) - R;
-        d = dc < d ? dc : d;
+        const T len = sqrt(dot3(dv, dv));
+        const T dc = len - R;
+        if (MODE == kModeBoundary) {
+          // closest_boundary (wih_twos.cpp:612-624): the first strictly nearer cavity.
+          if (dc < d && len > T(0)) {
+            d = dc;
+            hit_cav = static_cast<int>(c);
+          }
+        } else {
+          d = dc < d ? dc : d;
+        }
       }
       // The mixed form shrinks the radius by the FP32 distance error bound;
       // the FP64 form uses the distance itself (wih_twos.cpp:645-647).
@@ -629,7 +648,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           a = add_scaled(pos, g, r * beta);
         }
         const T w = r * r / T(6);
-        u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
+        if (MODE != kModeBoundary) u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
         if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
         const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
         pos = add_scaled(pos, dir, r);
@@ -640,7 +659,44 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
         }
       }
       if (done) {
-        static_cast<T *>(L.u_out)[wid] = u;
+        if (MODE == kModeBoundary) {
+          HitRec h;
+          h.pad = 0;
+          Vec<T> q{T(0), T(0), T(0)}, nrm{T(0), T(0), T(0)};
+          if (cap || !found) {
+            h.cavity = -2;
+          } else if (hit_cav >= 0) {
+            // Point on the sphere along the radial direction; the domain
+            // excludes the sphere, so the outward normal points into it.
+            const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + hit_cav), G);
+            const Vec<T> dv = sub(pos, cc);
+            const T inv = T(1) / sqrt(dot3(dv, dv));
+            const Vec<T> dir{dv.x * inv, dv.y * inv, dv.z * inv};
+            q = add_scaled(cc, dir, R);
+            nrm = {dir.x * T(-1), dir.y * T(-1), dir.z * T(-1)};
+            h.cavity = hit_cav;
+          } else {
+            Vec<T> ta, tb, tc;
+            load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+            q = tri_closest(pos, ta, tb, tc);
+            if (dmesh > T(0)) {
+              const T inv = T(1) / dmesh;
+              const Vec<T> dq = sub(q, pos);
+              nrm = {dq.x * inv, dq.y * inv, dq.z * inv};
+            }
+            h.cavity = -1;
+          }
+          const bool f32 = sizeof(T) == 4;
+          h.point[0] = static_cast<double>(q.x) + (f32 ? G.center[0] : 0.0);
+          h.point[1] = static_cast<double>(q.y) + (f32 ? G.center[1] : 0.0);
+          h.point[2] = static_cast<double>(q.z) + (f32 ? G.center[2] : 0.0);
+          h.normal[0] = static_cast<double>(nrm.x);
+          h.normal[1] = static_cast<double>(nrm.y);
+          h.normal[2] = static_cast<double>(nrm.z);
+          L.hits[wid] = h;
+        } else {
+          static_cast<T *>(L.u_out)[wid] = u;
+        }
         if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
         L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
         phase = kIdle;
@@ -678,7 +734,10 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
       } else if (tri_cur < tri_end) {
         const typename Layout<T>::Tri *tris = geo_tris<T>(G);
         ++c_planes;
-        if (tri_test(tris, tri_cur, pos, best2, c_tris)) found = true;
+        if (tri_test(tris, tri_cur, pos, best2, c_tris)) {
+          found = true;
+          best_tri = tri_cur;
+        }
         ++tri_cur;
       } else {
         // Pop the next entry still closer than the current best.
@@ -792,6 +851,9 @@ template <typename T, int MODE, bool GREEN, int BLOCK> static const void *wos_fn
 }
 
 template <int BLOCK> static const void *select_wos_block(int precision, int mode, bool green) {
+  if (mode == kModeBoundary)
+    return precision == TWOS_PREC_MIXED ? wos_fn<float, kModeBoundary, false, BLOCK>()
+                                        : wos_fn<double, kModeBoundary, false, BLOCK>();
 #define TWOS_PICK(T)                                                                                          \
   if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true, BLOCK>() : wos_fn<T, 0, false, BLOCK>(); \
   if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true, BLOCK>() : wos_fn<T, 1, false, BLOCK>();     \
@@ -1150,3 +1212,6 @@ cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *in
 }
 
 }  // namespace twos
+
+// Differential WoS kernels (use nearest<double> above).
+#include "diffwos.cuh"

@@ -883,6 +883,185 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
   return rc;
 }
 
+int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int enclosure_fallback,
+                 const double *sites, uint32_t n_sites, const double *cavities, uint32_t n_cav,
+                 twos_diff_result *out, twos_diff_stats *stats, twos_summary *summary) {
+  if (!m || !r) return fail(TWOS_ERR_USAGE, "null mesh or request");
+  if (r->mode == TWOS_MODE_PAIRED) return fail(TWOS_ERR_USAGE, "Differential WoS takes one source");
+  if (n_cav == 0 || !cavities) return fail(TWOS_ERR_USAGE, "Differential WoS requires --cavities");
+  if (!(diff_offset > r->epsilon)) return fail(TWOS_ERR_USAGE, "diff_offset must exceed epsilon");
+  if (int rc = validate_request(r, n_sites, n_cav)) return rc;
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  if (!sites || !out) return fail(TWOS_ERR_USAGE, "null buffer");
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  unsigned long long tot[kDiffTotals] = {};
+  DevBuf hits, osteps, flags, start, nu, nsteps, rows, st, dtot;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    const bool mixed = r->precision == TWOS_PREC_MIXED;
+    const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
+    const size_t walks = static_cast<size_t>(r->walks);
+    const size_t chunk = std::max<size_t>(1, std::min<size_t>(n_sites, std::max<size_t>(1, m->max_launch_walks / walks)));
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    m->cavities.reserve(static_cast<size_t>(n_cav) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->cavities.ptr, cavities, static_cast<size_t>(n_cav) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload cavities");
+    const size_t cw = chunk * walks;
+    hits.reserve(cw * sizeof(HitRec));
+    osteps.reserve(cw * sizeof(uint32_t));
+    flags.reserve(cw * sizeof(uint32_t));
+    start.reserve(cw * 3 * sizeof(double));
+    nu.reserve(cw * vbytes);
+    nsteps.reserve(cw * sizeof(uint32_t));
+    rows.reserve(static_cast<size_t>(n_sites) * n_cav * sizeof(twos_diff_result));
+    st.reserve(static_cast<size_t>(n_sites) * sizeof(twos_diff_stats));
+    dtot.reserve(sizeof(tot));
+    check(cudaMemsetAsync(dtot.ptr, 0, sizeof(tot), m->stream), "memset");
+    begin_totals(m);
+    // Outer walks (no payoff) on stream s; nested walks on stream s + 1.
+    twos_request ro_req = *r;
+    ro_req.n_source = ro_req.n_adjoint = 0;
+    ro_req.green = 0;
+    ro_req.skip_cavity_sites = 0;
+    twos_request rn_req = *r;
+    rn_req.mode = TWOS_MODE_COMPLIANCE;
+    rn_req.stream = r->stream + 1;
+    rn_req.skip_cavity_sites = 0;
+    for (size_t first = 0; first < n_sites; first += chunk) {
+      const uint32_t count = static_cast<uint32_t>(std::min<size_t>(chunk, n_sites - first));
+      const uint64_t cwalks = static_cast<uint64_t>(count) * walks;
+      for (int pass = 0; pass < 2; ++pass) {
+        const twos_request *rq = pass == 0 ? &ro_req : &rn_req;
+        std::vector<TermDev> terms;
+        const JobDesc J = make_job(m, rq, count, static_cast<uint32_t>(first), r->site_offset + static_cast<uint32_t>(first),
+                                   0, 0, 0, 0, n_cav, terms);
+        if (terms.empty()) terms.push_back(TermDev{});
+        m->jobs.reserve(sizeof(JobDesc));
+        m->terms.reserve(terms.size() * sizeof(TermDev));
+        check(cudaMemcpyAsync(m->jobs.ptr, &J, sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream), "upload job");
+        check(cudaMemcpyAsync(m->terms.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice,
+                              m->stream),
+              "upload terms");
+        check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+        WosLaunch L{};
+        L.jobs = m->jobs.as<JobDesc>();
+        L.n_jobs = 1;
+        L.geos = m->geo.as<GeoDesc>();
+        L.n_geos = 1;
+        L.sites = m->sites.as<double>();
+        L.terms = m->terms.as<TermDev>();
+        L.n_terms = static_cast<uint32_t>(terms.size());
+        L.cavities = m->cavities.as<double>();
+        L.total_walks = cwalks;
+        L.counter = m->counter.as<unsigned long long>();
+        L.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+        L.refill = m->refill;
+        L.step_threshold = m->step_threshold;
+        L.vote = m->vote;
+        L.counters = m->totals.as<unsigned long long>() + 3;
+        L.site_best2 = nullptr;
+        L.total_sites = count;
+        const int mode = pass == 0 ? kModeBoundary : TWOS_MODE_COMPLIANCE;
+        const bool green = pass == 1 && rq->green != 0;
+        if (pass == 0) {
+          L.hits = hits.as<HitRec>();
+          L.steps_out = osteps.as<uint32_t>();
+          L.u_out = nu.ptr;  // unused in boundary mode
+        } else {
+          L.walk_start = start.as<double>();
+          L.u_out = nu.ptr;
+          L.steps_out = nsteps.as<uint32_t>();
+        }
+        const int block = m->block;
+        const int per_sm = wos_max_blocks_per_sm(r->precision, mode, green, block, L);
+        if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
+        const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
+        check(launch_wos(r->precision, mode, green, L, grid, block, m->stream), "walk launch");
+        ro.launches += 1;
+        if (pass == 0) {
+          DiffLaunch D{};
+          D.geo = m->geo.as<GeoDesc>();
+          D.cavities = m->cavities.as<double>();
+          D.n_cav = n_cav;
+          D.cavity_radius = r->cavity_radius;
+          D.diff_offset = diff_offset;
+          D.epsilon = r->epsilon;
+          D.enclosure_fallback = enclosure_fallback;
+          D.total_walks = cwalks;
+          D.hits = hits.as<HitRec>();
+          D.outer_steps = osteps.as<uint32_t>();
+          D.flags = flags.as<uint32_t>();
+          D.start = start.as<double>();
+          D.totals = dtot.as<unsigned long long>();
+          D.error = L.error;
+          check(launch_diff_classify(D, m->stream), "classify launch");
+          ro.launches += 1;
+        }
+      }
+      DiffLaunch D{};
+      D.n_cav = n_cav;
+      D.diff_offset = diff_offset;
+      D.n_sites = count;
+      D.walks = static_cast<uint32_t>(walks);
+      D.site_begin = static_cast<uint32_t>(first);
+      D.hits = hits.as<HitRec>();
+      D.outer_steps = osteps.as<uint32_t>();
+      D.flags = flags.as<uint32_t>();
+      D.nested_u = nu.ptr;
+      D.nested_steps = nsteps.as<uint32_t>();
+      D.out = rows.as<twos_diff_result>();
+      D.stats = st.as<twos_diff_stats>();
+      D.totals = dtot.as<unsigned long long>();
+      check(launch_diff_reduce(r->precision, D, m->stream), "reduce launch");
+      ro.launches += 1;
+    }
+    check(cudaMemcpyAsync(out, rows.ptr, static_cast<size_t>(n_sites) * n_cav * sizeof(twos_diff_result),
+                          cudaMemcpyDeviceToHost, m->stream),
+          "download rows");
+    if (stats)
+      check(cudaMemcpyAsync(stats, st.ptr, static_cast<size_t>(n_sites) * sizeof(twos_diff_stats),
+                            cudaMemcpyDeviceToHost, m->stream),
+            "download stats");
+    check(cudaMemcpyAsync(tot, dtot.ptr, sizeof(tot), cudaMemcpyDeviceToHost, m->stream), "download totals");
+    end_totals(m, ro);
+  } catch (const std::exception &e) {
+    for (DevBuf *b : {&hits, &osteps, &flags, &start, &nu, &nsteps, &rows, &st, &dtot}) b->release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  for (DevBuf *b : {&hits, &osteps, &flags, &start, &nu, &nsteps, &rows, &st, &dtot}) b->release();
+  const double secs = seconds_since(t0);
+  // Queries as the study backend counts them: one closest-point query per
+  // step of the outer and nested walks plus the terminal one of every walk
+  // that was not capped, and the classification's distance queries.
+  const uint64_t outer_walks = static_cast<uint64_t>(n_sites) * static_cast<uint64_t>(r->walks);
+  const uint64_t nested_walks = tot[7] - tot[6];
+  if (summary) {
+    std::memset(summary, 0, sizeof(*summary));
+    summary->kernel_seconds = secs;
+    summary->total_seconds = secs;
+    summary->paths = outer_walks;
+    summary->steps = tot[3] + tot[4];
+    summary->caps = tot[5];
+    summary->queries = tot[3] + (outer_walks - tot[8]) + tot[4] + (nested_walks - tot[9]) + tot[0];
+    summary->launches = ro.launches;
+    summary->error_flags = ro.error_flags;
+    summary->node_tests = tot[1];       // parity rays
+    summary->plane_tests = tot[2];      // enclosure fallbacks
+    summary->triangle_tests = tot[6];   // unsafe offsets
+  }
+  if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
+  if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  if (tot[6] || tot[5])
+    return fail(TWOS_ERR_RUNTIME, "unsafe differential path: unsafe=" + std::to_string(tot[6]) +
+                                      " caps=" + std::to_string(tot[5]));
+  return TWOS_OK;
+}
+
 int twos_walk_samples(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,
                       const double *cavities, uint32_t n_cavities, double *u, double *p, uint32_t *steps) {
   if (!m) return fail(TWOS_ERR_USAGE, "null mesh");

@@ -157,6 +157,26 @@ struct WosLaunch {
   void *site_best2;
   uint32_t total_sites;
   int vote;  // 1: a warp runs one kind of traversal unit per iteration (majority vote)
+  // Per-walk start points [total_walks][3] (original coordinates); a walk whose
+  // start is NaN is skipped (zero value, zero steps).  Null: walks start at
+  // their site.
+  const double *walk_start;
+  // Boundary mode (kModeBoundary): per-walk boundary hit of the terminal step.
+  struct HitRec *hits;
+};
+
+// Walk-to-boundary mode of the walk kernel (walk_to_boundary,
+// wih_twos.cpp:725-740): no payoff; each walk records its terminal hit.
+constexpr int kModeBoundary = 3;
+
+// Boundary hit of a walk's terminal step (closest_boundary, wih_twos.cpp:
+// 602-626), original coordinates.  cavity = -1 for the mesh, -2 when the
+// walk hit the step cap or was skipped.
+struct HitRec {
+  double point[3];
+  double normal[3];
+  int32_t cavity;
+  int32_t pad;
 };
 
 // Fills L.site_best2 (T per site, T = float for mixed, double for FP64).
@@ -172,6 +192,33 @@ struct FinalizeLaunch {
   const uint32_t *steps;
   twos_site_result *out;
 };
+
+// Differential WoS pass over one chunk of sites (diffwos.cuh).
+constexpr uint32_t kDiffCavity = 1u, kDiffNearSeam = 2u, kDiffSegmentUnsafe = 4u, kDiffUnsafe = 8u;
+struct DiffLaunch {
+  const GeoDesc *geo;             // device
+  const double *cavities;         // [n_cav][3], original coordinates
+  uint32_t n_cav;
+  double cavity_radius, diff_offset, epsilon;
+  int enclosure_fallback;
+  uint64_t total_walks;           // n_sites * walks
+  uint32_t n_sites, walks, site_begin;
+  const HitRec *hits;             // outer walks' terminal hits
+  const uint32_t *outer_steps;    // steps | cap << 31
+  uint32_t *flags;                // kDiff* per walk
+  double *start;                  // nested start points [walks][3] (NaN = none)
+  const void *nested_u;           // nested walk values (float or double)
+  const uint32_t *nested_steps;
+  twos_diff_result *out;          // [sites][n_cav], indexed by site_begin + site
+  twos_diff_stats *stats;         // [sites] or null
+  unsigned long long *totals;     // [0] queries [1] rays [2] fallbacks [3] outer steps [4] nested steps
+                                  // [5] limits [6] unsafe [7] cavity terminations
+                                  // [8] outer caps [9] nested caps (kDiffTotals words)
+  uint32_t *error;
+};
+constexpr int kDiffTotals = 10;
+cudaError_t launch_diff_classify(const DiffLaunch &D, cudaStream_t s);
+cudaError_t launch_diff_reduce(int precision, const DiffLaunch &D, cudaStream_t s);
 
 // One design-loop iteration record (layout of twos_design_step).
 struct DesignStep {

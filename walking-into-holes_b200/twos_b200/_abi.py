@@ -24,7 +24,7 @@ EXPORTED = [
     "twos_abi_version", "twos_last_error", "twos_mesh_open", "twos_mesh_open_ply", "twos_mesh_close",
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
-    "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning",
+    "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
 ]
 
 
@@ -99,6 +99,11 @@ class DesignStep(ctypes.Structure):
     ]
 
 
+# twos_diff_result / twos_diff_stats as numpy record layouts.
+DIFF_DTYPE = [("dc", "f8", (3,)), ("dc_se", "f8", (3,)), ("dR", "f8"), ("dR_se", "f8")]
+DIFF_STATS_DTYPE = [("outer_steps", "u8"), ("nested_steps", "u8"), ("cavity_terminations", "u8"),
+                    ("near_seam", "u8"), ("segment_unsafe", "u8"), ("unsafe_offset", "u8"), ("limits", "u8")]
+
 DESIGN_DTYPE = [("chosen", "u4"), ("accepted", "u4"), ("scout_score", "f8"), ("score", "f8"),
                 ("score_se", "f8"), ("lower", "f8")]
 
@@ -140,12 +145,14 @@ def load(path: Path | str | None = None):
     L.twos_estimate_device.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_mesh_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.twos_mesh_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
-    L.twos_estimate_noalloc.argtypes =[vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
-    L.twos_estimate_batch.argtypes =[vp, ctypes.POINTER(Request), u32, vp, vp, vp, vp, vp, ctypes.POINTER(Summary)]
+    L.twos_estimate_noalloc.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
+    L.twos_estimate_batch.argtypes = [vp, ctypes.POINTER(Request), u32, vp, vp, vp, vp, vp, ctypes.POINTER(Summary)]
     L.twos_design_loop.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(Request), vp, u32, vp, u32,
                                    ctypes.POINTER(DesignParams), vp, vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
+    L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,
+                               ctypes.POINTER(Summary)]
     L.twos_topk_device.argtypes = [vp, vp, u32, u32, vp]
     for name in EXPORTED:
         if name not in ("twos_mesh_close", "twos_last_error"):

@@ -10,6 +10,8 @@ thin wrappers over the C ABI with numpy buffers:
 * ``estimate_device`` the same with device-resident sites and results (torch
                     tensors or raw pointers);
 * ``walk_samples``  per-walk u, p and steps;
+* ``diffwos``       derivatives of u with respect to cavity centres and radii
+                    (evaluate_differential_site, wih_twos.cpp:839-928);
 * ``closest_point`` batched distance/closest point (wih_twos.cpp:339-359);
 * ``inside``        ray-parity membership (wih_twos.cpp:361-394);
 * ``topk_device``   top-k site indices.
@@ -22,8 +24,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi, sources
-from ._abi import (MODE_COMPLIANCE, MODE_HOT, MODE_PAIRED, PREC_FP64, PREC_MIXED, Request, SITE_DTYPE, Summary,
-                   check)
+from ._abi import (DIFF_DTYPE, DIFF_STATS_DTYPE, MODE_COMPLIANCE, MODE_HOT, MODE_PAIRED, OK, PREC_FP64, PREC_MIXED,
+                   Request, SITE_DTYPE, Summary, TwosError, check)
 
 PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 MODES = {"compliance": MODE_COMPLIANCE, "paired": MODE_PAIRED, "hot": MODE_HOT}
@@ -218,6 +220,34 @@ class Mesh:
         check(_abi.load().twos_walk_samples(self._h, ctypes.byref(req), _ptr(s), n, _ptr(cav), len(cav), _ptr(u),
                                             _ptr(p), _ptr(st)))
         return {"u": u, "p": p, "steps": st & 0x7FFFFFFF, "caps": (st >> 31).astype(bool)}
+
+    def diffwos(self, sites, config: Config, cavities, diff_offset: float = 0.02,
+                enclosure_fallback: bool = False, strict: bool = True):
+        """Differential WoS (twos_diffwos): returns (rows [n_sites, n_cav] of
+        DIFF_DTYPE, stats [n_sites] of DIFF_STATS_DTYPE, summary).  With
+        strict=False a capped walk or an unsafe offset is reported in
+        summary["error"] instead of raised, as the study backend's error
+        return carries the rows along (study.cpp:309-310)."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        rows = np.zeros((len(s), len(cav)), dtype=DIFF_DTYPE)
+        stats = np.zeros(len(s), dtype=DIFF_STATS_DTYPE)
+        req = config.to_request()
+        summ = Summary()
+        L = _abi.load()
+        rc = L.twos_diffwos(self._h, ctypes.byref(req), float(diff_offset), int(bool(enclosure_fallback)), _ptr(s),
+                            len(s), _ptr(cav), len(cav), _ptr(rows), _ptr(stats), ctypes.byref(summ))
+        out = _summary_dict(summ)
+        out["parity_rays"] = out.pop("node_tests")
+        out["enclosure_fallbacks"] = out.pop("plane_tests")
+        out["unsafe_offsets"] = out.pop("triangle_tests")
+        out["error"] = None
+        if rc != OK:
+            msg = L.twos_last_error().decode(errors="replace")
+            if strict or not msg.startswith("unsafe differential path"):
+                raise TwosError(rc, msg)
+            out["error"] = msg
+        return rows, stats, out
 
     def topk_device(self, d_keys, n, k, d_index):
         def addr(x):

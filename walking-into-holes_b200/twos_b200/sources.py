@@ -63,3 +63,32 @@ def ball_indicator(center, radius, amp=1.0):
 def ball_mean_density(center, radius):
     """1_{|x-c|<r} / |B_r|: the density of a mean over a ball."""
     return ball_indicator(center, radius, amp=1.0 / (4.0 / 3.0 * math.pi * radius ** 3))
+
+
+def study_heat(rows):
+    """Heat lines (x, y, z, r, A) of a study configuration as the source
+    sum of A (1 - |x-c|^2/r^2)_+^2 in file order
+    (benchmarks/submission_study/study.cpp:27-35)."""
+    return [term(TERM_BUMP, r[4], c=tuple(r[:3]), w=(r[3], 0.0, 0.0)) for r in rows]
+
+
+def load_study_config(path):
+    """A study configuration file (benchmarks/submission_study/study.cpp:37-42):
+    a sensor "x y z r", then heat records "x y z r A", read as one stream of
+    numbers (line breaks do not matter; reading stops at the first token that
+    is not a number or at an incomplete record).  Returns ((x, y, z, r), heat
+    terms).  Raises ValueError on a bad sensor or without heat records."""
+    values = []
+    with open(path) as f:
+        for tok in f.read().split():
+            try:
+                values.append(float(tok))
+            except ValueError:
+                break
+    if len(values) < 4:
+        raise ValueError(f"{path}: bad sensor config")
+    rest = values[4:]
+    heat = [rest[i:i + 5] for i in range(0, len(rest) - 4, 5)]
+    if not heat:
+        raise ValueError(f"{path}: missing compact heat sources")
+    return tuple(values[:4]), study_heat(heat)
