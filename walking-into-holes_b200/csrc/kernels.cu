@@ -535,7 +535,8 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
   T best2 = T(0);
   int node = 0, sp = 0;
   bool have = false, found = false;
-  uint32_t best_tri = 0;  // leaf-order index of the nearest triangle (boundary mode)
+  uint32_t best_tri = 0;  // leaf-order index of the nearest triangle found for this walk
+  bool tri_ok = false;    // best_tri belongs to this walk
   uint32_t tri_cur = 0, tri_end = 0, iter = 0;
 
   for (;;) {
@@ -569,6 +570,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           u = T(0);
           pv = T(0);
           steps = 0;
+          tri_ok = false;
           if (!skip && (J.flags & kJobSkipCavitySites)) {
             const T R = to_T<T>(J.cavity_radius);
             for (uint32_t c = 0; c < J.n_cav; ++c) {
@@ -702,10 +704,20 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
         phase = kIdle;
       } else {
         best2 = static_cast<T>(J.query_radius2);
+        found = false;
+        if (L.warm && tri_ok) {
+          Vec<T> ta, tb, tc;
+          load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+          ++c_tris;
+          const T w2 = tri_dist2(pos, ta, tb, tc);
+          if (w2 < best2) {
+            best2 = w2;
+            found = true;
+          }
+        }
         node = 0;
         sp = 0;
         have = true;
-        found = false;
         tri_cur = tri_end = 0;
         iter = 0;
         phase = kTraverse;
@@ -737,6 +749,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
         if (tri_test(tris, tri_cur, pos, best2, c_tris)) {
           found = true;
           best_tri = tri_cur;
+          tri_ok = true;
         }
         ++tri_cur;
       } else {

@@ -149,6 +149,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.refill = m->refill;
     L.step_threshold = m->step_threshold;
     L.vote = m->vote;
+    L.warm = m->warm;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;

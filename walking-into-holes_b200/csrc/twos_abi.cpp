@@ -133,6 +133,7 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_STEP_THRESHOLD")) m->step_threshold = std::max(1, std::atoi(e));
     if (const char *e = std::getenv("TWOS_BLOCKS_PER_SM")) m->blocks_per_sm = std::max(0, std::atoi(e));
     if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
+    if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
       const int b = std::atoi(e);
       if (b == 128 || b == 256 || b == 512) m->block = b;
@@ -318,6 +319,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.refill = m->refill;
   L.step_threshold = m->step_threshold;
   L.vote = m->vote;
+  L.warm = m->warm;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -769,6 +771,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.refill = m->refill;
     Ls.step_threshold = m->step_threshold;
     Ls.vote = m->vote;
+    Ls.warm = m->warm;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -963,6 +966,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.refill = m->refill;
         L.step_threshold = m->step_threshold;
         L.vote = m->vote;
+        L.warm = m->warm;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;

@@ -157,6 +157,11 @@ struct WosLaunch {
   void *site_best2;
   uint32_t total_sites;
   int vote;  // 1: a warp runs one kind of traversal unit per iteration (majority vote)
+  // 1: a step's query starts from the distance to the previous query's
+  // nearest triangle (an upper bound attained by a real triangle, so the
+  // traversal's minimum -- and every walk -- is unchanged; it only prunes
+  // from the first node on).
+  int warm;
   // Per-walk start points [total_walks][3] (original coordinates); a walk whose
   // start is NaN is skipped (zero value, zero steps).  Null: walks start at
   // their site.

@@ -68,4 +68,5 @@ struct twos_mesh {
   int step_threshold = 1;  // finished queries before a warp takes its walk step
   int blocks_per_sm = 0;   // 0: as many as fit
   int vote = 0;            // 1: one kind of traversal unit per warp iteration
+  int warm = 1;            // 1: seed each step's query with the previous nearest triangle
 };
