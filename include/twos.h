@@ -75,6 +75,21 @@ enum {
   TWOS_TERM_BALL = 5
 };
 
+/* Per-step source integral over the walk's ball B_r(y), added to u (p):
+ *   CENTER  r^2/6 f(y)                          (wih_twos.cpp:648-651, affine)
+ *   GREEN   r^2/6 f(a), a = y + r beta w with beta ~ Beta(2,2), w uniform
+ *           (wih_twos.cpp:569-575; adjoint.cpp:31; study.cpp:106-108)
+ *   EXACT   the exact integral of the ball's Green function against f
+ *           (study.cpp WIH_ANALYTIC_SOURCE, 53-77, 96-104): CONST and
+ *           LINEAR terms contribute r^2/6 f(y) (f harmonic), each BUMP term
+ *           A (1 - |x-c|^2/R^2)_+^2 (A = amp / div) its closed-form Newton-
+ *           potential difference; other term kinds are rejected. */
+enum {
+  TWOS_SOURCE_CENTER = 0,
+  TWOS_SOURCE_GREEN = 1,
+  TWOS_SOURCE_EXACT = 2
+};
+
 #define TWOS_MAX_TERMS 8
 
 typedef struct twos_source_term {
@@ -101,8 +116,8 @@ typedef struct twos_request {
   double cavity_radius;  /* common radius of the spherical cavities (--cavity-radius) */
   double query_radius;   /* initial closest-point radius; nothing at or beyond it is
                             found (wih_twos.cpp:348 uses 4.0); <= 0 means unbounded */
-  int32_t green;         /* 1: evaluate sources at a Beta(2,2) Green point in each
-                            ball (housing mode); 0: at the ball centre (affine) */
+  int32_t green;         /* TWOS_SOURCE_*: how each ball's source integral is
+                            taken (centre, Green point, or exact) */
   int32_t n_source;
   int32_t n_adjoint;
   int32_t skip_cavity_sites; /* 1: sites inside a cavity get all-zero rows
@@ -149,7 +164,9 @@ enum {
   TWOS_DEVERR_QUERY = 1u,     /* no surface point within query_radius / non-finite */
   TWOS_DEVERR_STACK = 2u,     /* traversal stack bound exceeded */
   TWOS_DEVERR_ITER = 4u,      /* traversal iteration bound exceeded */
-  TWOS_DEVERR_CONFIG = 8u
+  TWOS_DEVERR_CONFIG = 8u,
+  TWOS_DEVERR_SOURCE = 16u    /* an exact ball integral came out negative beyond
+                                 round-off (study.cpp:74) */
 };
 
 typedef struct twos_mesh twos_mesh;
@@ -363,6 +380,15 @@ int twos_walk_samples(twos_mesh *mesh, const twos_request *request, const double
  * inside[i] = 1 when a ray in the reference's fixed oblique direction crosses
  * the surface an odd number of times.  Host buffers. */
 int twos_inside(twos_mesh *mesh, const double *points, uint64_t n, uint8_t *inside);
+
+/* The EXACT source's ball integral on the device (exact_bump_green,
+ * study.cpp:64-77, as read by wih_analytic_integral_audit,
+ * analytic_integral_audit.cpp): for case i, cases[4i..4i+3] = (d, r, R, A)
+ * with the bump centred at distance d from the ball centre, out[i] =
+ * integral over B_r of G_r(0, z) A (1 - |z-c|^2/R^2)_+^2 dz.  Host buffers;
+ * runs on `device`.  A negative integral beyond round-off returns
+ * TWOS_ERR_RUNTIME with the values written. */
+int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device);
 
 /* Indices of the k largest keys, highest first, ties to the lower index
  * (np.argpartition(...)[-k:] of run_bunny_benchmark.py:324 with a

@@ -100,6 +100,7 @@ def lib():
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p]
+        L.oracle_exact_bump_green.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
         assert L.oracle_sizeof_params() == ctypes.sizeof(Params)
         assert L.oracle_sizeof_site() == ctypes.sizeof(Site)
         _lib = L
@@ -108,6 +109,47 @@ def lib():
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def exact_bump_green(cases):
+    """exact_bump_green (study.cpp:64-77, long double as the reference) for an
+    [n, 4] array of (d, r, R, A) cases; raises on a negative integral."""
+    c = np.ascontiguousarray(cases, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros(len(c))
+    if lib().oracle_exact_bump_green(_ptr(c), len(c), _ptr(out)):
+        raise RuntimeError(lib().oracle_last_error().decode())
+    return out
+
+
+def green_ball_quadrature(d, r, R, A):
+    """Independent check of the closed form: the Green-volume integral of the
+    bump over the ball, int_0^r (t - t^2/r) <f>_t dt with <f>_t the bump's
+    mean over the sphere of radius t about the ball centre (a restatement of
+    the reference's quadrature check, matched_accuracy/check_integral.py:11-20,
+    written from the same integral), by scipy adaptive quadrature split at
+    the support's kinks."""
+    from scipy.integrate import quad
+
+    def angular(t):
+        # Mean of f over the sphere of radius t: half the integral over the
+        # cosine c in [-1, 1] of A (a - b c)_+^2 (c flipped), with
+        # a = 1 - (d^2 + t^2)/R^2 and b = 2 d t / R^2.
+        if d * t == 0:
+            return A * max(0.0, 1 - (d * d + t * t) / (R * R)) ** 2
+        a = 1 - (d * d + t * t) / (R * R)
+        b = 2 * d * t / (R * R)
+        if a + b <= 0:
+            return 0.0
+        hi = min(1.0, a / b)
+
+        def P(c):
+            return a * a * c - a * b * c * c + b * b * c ** 3 / 3
+
+        return A * (P(hi) - P(-1)) / 2
+
+    cuts = sorted(set([0.0, r] + [t for t in (abs(d - R), d + R) if 0 < t < r]))
+    return sum(quad(lambda t: (t - t * t / r) * angular(t), lo, hi, epsabs=1e-13 * A * R * R, epsrel=1e-10)[0]
+               for lo, hi in zip(cuts[:-1], cuts[1:]))
 
 
 # --------------------------------------------------------------------------- sources

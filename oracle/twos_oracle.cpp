@@ -362,6 +362,61 @@ double source_value(const Term *terms, int n, const Vec3 &x) {
   return s;
 }
 
+// ---------------------------------------------------------------- exact ball integral
+// exact_bump_green (benchmarks/submission_study/study.cpp:53-77, the
+// WIH_ANALYTIC_SOURCE path), restated in long double as the reference
+// computes it: the bump's Newton potential N at the ball centre minus its
+// mean over the ball's sphere, from the primitive P(x) = int_0^x s N(s) ds.
+long double ld_bump_potential(long double d, long double R, long double A) {
+  if (d >= R) return A * R * R * R * (8.0L / 105) / d;
+  const long double t = d / R;
+  return A * R * R * (1.0L / 6 - t * t / 6 + t * t * t * t / 10 - t * t * t * t * t * t / 42);
+}
+
+long double ld_potential_primitive(long double d, long double R, long double A) {
+  const long double t = std::min(d / R, 1.0L), t2 = t * t, t4 = t2 * t2;
+  const long double inner = A * R * R * R * R * (t2 / 12 - t4 / 24 + t4 * t2 / 60 - t4 * t4 / 336);
+  return inner + (d > R ? A * R * R * R * (8.0L / 105) * (d - R) : 0.0L);
+}
+
+double exact_bump_green(double d_, double r_, double R_, double A_, bool &negative) {
+  const long double d = d_, r = r_, R = R_, A = A_;
+  if (d >= r + R) return 0.0;
+  const long double at_center = ld_bump_potential(d, R, A);
+  long double mean;
+  if (d + R <= r)
+    mean = A * R * R * R * (8.0L / 105) / r;
+  else if (d < 1e-12L * R)
+    mean = ld_bump_potential(r, R, A);
+  else
+    mean = (ld_potential_primitive(d + r, R, A) - ld_potential_primitive(std::fabs(d - r), R, A)) / (2 * d * r);
+  const long double value = at_center - mean;
+  if (value < -1e-11L * std::max(1.0L, std::fabs(at_center))) negative = true;
+  return static_cast<double>(std::max(0.0L, value));
+}
+
+// One step's exact source integral over B_r(y) (study.cpp:96-104): the
+// harmonic (constant and linear) terms as r*r/6 f(y), then every bump term's
+// exact integral, in term order.
+double exact_source(const Term *terms, int n, const Vec3 &y, double r, double acc, bool &negative) {
+  double harmonic = 0.0;
+  bool any = false;
+  for (int i = 0; i < n; ++i) {
+    if (terms[i].kind == 0 || terms[i].kind == 1) {
+      harmonic = any ? harmonic + term_value(terms[i], y) : term_value(terms[i], y);
+      any = true;
+    }
+  }
+  if (any) acc += r * r / 6 * harmonic;
+  for (int i = 0; i < n; ++i) {
+    const Term &t = terms[i];
+    if (t.kind != 3) continue;
+    const Vec3 c{t.c[0], t.c[1], t.c[2]};
+    acc += exact_bump_green(norm(y - c), r, t.w[0], t.amp / t.div, negative);
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------- random streams
 uint64_t splitmix64(uint64_t x) {
   // SplitMix64 finaliser (Steele, Lea & Flood 2014), as wih_twos.cpp:529-534 uses it.
@@ -462,7 +517,7 @@ struct oracle_params {
   double epsilon;
   double cavity_radius;
   double query_radius;
-  int32_t green;       // evaluate sources at a Beta(2,2) Green point
+  int32_t green;       // 0 ball centre, 1 Beta(2,2) Green point, 2 exact ball integral
   int32_t n_source;
   int32_t n_adjoint;
   int32_t skip_cavity_sites;
@@ -603,6 +658,16 @@ WalkOut walk(const Mesh &m, const oracle_params &o, const double *cav, uint32_t 
         return out;
       }
       Vec3 a = y;
+      if (o.green == 2) {
+        // The analytic study source (study.cpp:96-104): no Green-point draw.
+        bool negative = false;
+        out.u = exact_source(o.source, o.n_source, y, r, out.u, negative);
+        if (want_p) out.p = exact_source(o.adjoint, o.n_adjoint, y, r, out.p, negative);
+        if (negative) out.failed = true;
+        y = y + random_unit_vector(rng) * r;
+        ++out.steps;
+        continue;
+      }
       if (o.green) {
         // The scale operand (and so beta_22) is evaluated before the
         // direction, as g++ sequences `operator*(random_unit_vector(rng),
@@ -637,6 +702,15 @@ WalkOut walk(const Mesh &m, const oracle_params &o, const double *cav, uint32_t 
       double a0, a1;
       cs.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
       Vec3 a = y;
+      if (o.green == 2) {
+        bool negative = false;
+        out.u = exact_source(o.source, o.n_source, y, r, out.u, negative);
+        if (want_p) out.p = exact_source(o.adjoint, o.n_adjoint, y, r, out.p, negative);
+        if (negative) out.failed = true;
+        y = y + direction_from(a0, a1) * r;
+        ++out.steps;
+        continue;
+      }
       if (o.green) {
         double g0, g1, b0, b1, b2, spare;
         cs.uniforms(static_cast<uint32_t>(k), 1, g0, g1);
@@ -662,6 +736,19 @@ WalkOut walk(const Mesh &m, const oracle_params &o, const double *cav, uint32_t 
 }  // namespace
 
 extern "C" {
+
+// exact_bump_green for cases[4i..4i+3] = (d, r, R, A) (the reader of
+// analytic_integral_audit.cpp).  Returns 1 when an integral came out negative.
+int oracle_exact_bump_green(const double *cases, uint32_t n, double *out) {
+  bool negative = false;
+  for (uint32_t i = 0; i < n; ++i)
+    out[i] = exact_bump_green(cases[4 * i], cases[4 * i + 1], cases[4 * i + 2], cases[4 * i + 3], negative);
+  if (negative) {
+    g_error = "negative analytic Green integral";
+    return 1;
+  }
+  return 0;
+}
 
 // Per-walk samples for n_sites sites (site ids site_ids[i], or i when null).
 // u, p: [n_sites * walks]; steps: [n_sites * walks] with bit 31 set on a cap.

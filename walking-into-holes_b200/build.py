@@ -28,7 +28,7 @@ CUDA_FLAGS = ARCH + ["-lineinfo", "-fmad=false", "--expt-relaxed-constexpr"]
 
 LIB_SOURCES = ["kernels.cu", "design.cu", "noalloc.cu", "twos_abi.cpp", "geometry.cpp"]
 CLI = {"wih_twos": "cli_twos.cpp", "wih_adjoint": "cli_adjoint.cpp"}
-HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h", "diffwos.cuh"]
+HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h", "diffwos.cuh", "ball_green.cuh"]
 
 
 def nvcc() -> str:

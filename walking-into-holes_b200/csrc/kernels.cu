@@ -425,6 +425,44 @@ __device__ __forceinline__ T source_value(const TermT<T> *terms, uint32_t begin,
   return s;
 }
 
+}  // namespace twos
+#include "ball_green.cuh"
+namespace twos {
+
+// One step's EXACT source integral over B_r(x), accumulated into acc as the
+// analytic study backend does (study.cpp:96-104): the harmonic (CONST and
+// LINEAR) terms as r^2/6 f(x) in one product, then each bump's closed-form
+// ball integral added in term order.  Bumps are evaluated in FP64 (double-
+// double inside) from the frame coordinates.
+template <typename T>
+__device__ __forceinline__ T exact_source(T acc, const TermT<T> *terms, uint32_t begin, uint32_t n,
+                                          const Vec<T> &x, T r, uint32_t &err) {
+  T harmonic = T(0);
+  bool any = false;
+  for (uint32_t i = 0; i < n; ++i) {
+    const TermT<T> &t = terms[begin + i];
+    if (t.kind == TWOS_TERM_CONST || t.kind == TWOS_TERM_LINEAR) {
+      harmonic = any ? harmonic + term_value(t, x) : term_value(t, x);
+      any = true;
+    }
+  }
+  if (any) acc = acc + r * r / T(6) * harmonic;
+  for (uint32_t i = 0; i < n; ++i) {
+    const TermT<T> &t = terms[begin + i];
+    if (t.kind != TWOS_TERM_BUMP) continue;
+    const double dx = static_cast<double>(x.x) - static_cast<double>(t.c[0]);
+    const double dy = static_cast<double>(x.y) - static_cast<double>(t.c[1]);
+    const double dz = static_cast<double>(x.z) - static_cast<double>(t.c[2]);
+    bool negative = false;
+    const double v = exact_bump_green(sqrt(dx * dx + dy * dy + dz * dz), static_cast<double>(r),
+                                      static_cast<double>(t.w[0]),
+                                      static_cast<double>(t.amp) / static_cast<double>(t.div), negative);
+    if (negative) err |= TWOS_DEVERR_SOURCE;
+    acc = acc + static_cast<T>(v);
+  }
+  return acc;
+}
+
 // ================================================================ WoS kernel
 constexpr int kWosBlock = 128;
 
@@ -649,9 +687,14 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
           a = add_scaled(pos, g, r * beta);
         }
-        const T w = r * r / T(6);
-        if (MODE != kModeBoundary) u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
-        if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+        if (MODE != kModeBoundary && (J.flags & kJobExactSource)) {
+          u = exact_source(u, s_terms, J.src_begin, J.n_src, pos, r, err);
+          if (MODE == TWOS_MODE_PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
+        } else {
+          const T w = r * r / T(6);
+          if (MODE != kModeBoundary) u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
+          if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+        }
         const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
         pos = add_scaled(pos, dir, r);
         ++steps;
@@ -1102,6 +1145,25 @@ __global__ void __launch_bounds__(kWosBlock) closest_kernel(const GeoDesc *geo, 
     }
   }
   if (err) atomicOr(error, err);
+}
+
+__global__ void ball_green_kernel(const double *__restrict__ cases, uint32_t n, double *__restrict__ out,
+                                  uint32_t *error) {
+  uint32_t err = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    bool negative = false;
+    out[i] = exact_bump_green(cases[4ull * i], cases[4ull * i + 1], cases[4ull * i + 2], cases[4ull * i + 3],
+                              negative);
+    if (negative) err |= TWOS_DEVERR_SOURCE;
+  }
+  if (err) atomicOr(error, err);
+}
+
+cudaError_t launch_ball_green(const double *cases, uint32_t n, double *out, uint32_t *error, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int grid = static_cast<int>(std::min<uint32_t>((n + 127) / 128, 148u * 8));
+  ball_green_kernel<<<grid, 128, 0, s>>>(cases, n, out, error);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,

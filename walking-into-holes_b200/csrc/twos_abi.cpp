@@ -161,7 +161,12 @@ int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav) {
     const twos_source_term &t = i < r->n_source ? r->source[i] : r->adjoint[i - r->n_source];
     if (t.kind < TWOS_TERM_CONST || t.kind > TWOS_TERM_BALL) return fail(TWOS_ERR_USAGE, "unknown source term");
     if (t.kind == TWOS_TERM_LINEAR && (t.axis < 0 || t.axis > 2)) return fail(TWOS_ERR_USAGE, "bad term axis");
+    if (r->green == TWOS_SOURCE_EXACT && t.kind != TWOS_TERM_CONST && t.kind != TWOS_TERM_LINEAR &&
+        t.kind != TWOS_TERM_BUMP)
+      return fail(TWOS_ERR_USAGE, "the exact source integral takes constant, linear and bump terms only");
   }
+  if (r->green < TWOS_SOURCE_CENTER || r->green > TWOS_SOURCE_EXACT)
+    return fail(TWOS_ERR_USAGE, "invalid source integration mode");
   if (n_cav > 4096) return fail(TWOS_ERR_USAGE, "at most 4096 cavities per request");
   (void)n_sites;
   return TWOS_OK;
@@ -218,7 +223,9 @@ JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint3
   counter_key(r->seed, r->stream, J.k0, J.k1);
   J.repeat = r->repeat;
   J.max_steps = r->max_steps;
-  J.flags = (r->green ? kJobGreen : 0u) | (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
+  J.flags = (r->green == TWOS_SOURCE_GREEN ? kJobGreen : 0u) |
+            (r->green == TWOS_SOURCE_EXACT ? kJobExactSource : 0u) |
+            (r->skip_cavity_sites ? kJobSkipCavitySites : 0u);
   J.epsilon = r->epsilon;
   const double qr = r->query_radius > 0.0 ? r->query_radius : std::numeric_limits<double>::infinity();
   J.query_radius2 = qr * qr;
@@ -255,7 +262,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   const bool mixed = r0->precision == TWOS_PREC_MIXED;
   const int mode = r0->mode;
   const bool paired = mode == TWOS_MODE_PAIRED;
-  const bool green = r0->green != 0;
+  const bool green = r0->green == TWOS_SOURCE_GREEN;
   std::vector<JobDesc> jobs;
   std::vector<GeoDesc> geos;
   std::vector<twos_mesh *> geo_mesh;
@@ -411,6 +418,7 @@ int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summa
   if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
   if (ro.error_flags & TWOS_DEVERR_STACK) return fail(TWOS_ERR_RUNTIME, "BVH traversal stack bound exceeded");
   if (ro.error_flags & TWOS_DEVERR_ITER) return fail(TWOS_ERR_RUNTIME, "BVH traversal iteration bound exceeded");
+  if (ro.error_flags & TWOS_DEVERR_SOURCE) return fail(TWOS_ERR_RUNTIME, "negative analytic Green integral");
   if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
   if (ro.caps) return fail(TWOS_ERR_RUNTIME, "one or more paths hit --max-steps");
   return TWOS_OK;
@@ -597,7 +605,7 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
     const uint32_t nc = n_cavities ? n_cavities[j] : 0;
     if (int rc = validate_request(&requests[j], n_sites[j], nc)) return rc;
     if (requests[j].mode != requests[0].mode || requests[j].precision != requests[0].precision ||
-        (requests[j].green != 0) != (requests[0].green != 0))
+        requests[j].green != requests[0].green)
       return fail(TWOS_ERR_USAGE, "batch requests must share mode, precision and green");
     if ((n_sites[j] && (!sites[j] || !out[j])) || (nc && (!cavities || !cavities[j])))
       return fail(TWOS_ERR_USAGE, "null buffer in batch");
@@ -817,22 +825,22 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     D.iteration = iter.as<uint32_t>();
     D.history = hist.as<DesignStep>();
     const int block = m->block;
-    const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green != 0, block, Ls);
-    const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green != 0, block, Lv);
+    const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green == TWOS_SOURCE_GREEN, block, Ls);
+    const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green == TWOS_SOURCE_GREEN, block, Lv);
     if (per_s <= 0 || per_v <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
     const int cap = m->blocks_per_sm > 0 ? m->blocks_per_sm : 1 << 20;
     const int grid_s = std::min(per_s, cap) * m->num_sms, grid_v = std::min(per_v, cap) * m->num_sms;
     auto iteration = [&]() {
       check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
       check(launch_site_prepass(rs.precision, Ls, m->stream), "scout pre-pass");
-      check(launch_wos(rs.precision, rs.mode, rs.green != 0, Ls, grid_s, block, m->stream), "scout launch");
+      check(launch_wos(rs.precision, rs.mode, rs.green == TWOS_SOURCE_GREEN, Ls, grid_s, block, m->stream), "scout launch");
       check(launch_finalize(rs.precision, rs.mode, Fs, m->stream), "scout finalize");
       check(launch_design_keys(D, m->stream), "keys");
       check(launch_topk(D.keys, n, k, idx.as<uint32_t>(), topk.ptr, topk.bytes, m->stream), "top-k");
       check(launch_design_gather(D, m->stream), "gather");
       check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
       check(launch_site_prepass(rv.precision, Lv, m->stream), "validate pre-pass");
-      check(launch_wos(rv.precision, rv.mode, rv.green != 0, Lv, grid_v, block, m->stream), "validate launch");
+      check(launch_wos(rv.precision, rv.mode, rv.green == TWOS_SOURCE_GREEN, Lv, grid_v, block, m->stream), "validate launch");
       check(launch_finalize(rv.precision, rv.mode, Fv, m->stream), "validate finalize");
       check(launch_design_select(D, m->stream), "select");
       check(launch_design_mask(D, m->stream), "mask");
@@ -884,6 +892,30 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     summary->queries = ro.steps + summary->paths;
   }
   return rc;
+}
+
+int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device) {
+  if (n == 0) return TWOS_OK;
+  if (!cases || !out) return fail(TWOS_ERR_USAGE, "null buffer");
+  DevBuf dc, dout, derr;
+  uint32_t err = 0;
+  try {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    dc.reserve(static_cast<size_t>(n) * 4 * sizeof(double));
+    dout.reserve(static_cast<size_t>(n) * sizeof(double));
+    derr.reserve(sizeof(uint32_t));
+    check(cudaMemcpy(dc.ptr, cases, static_cast<size_t>(n) * 4 * sizeof(double), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemset(derr.ptr, 0, sizeof(uint32_t)), "memset");
+    check(launch_ball_green(dc.as<double>(), n, dout.as<double>(), derr.as<uint32_t>(), nullptr), "launch");
+    check(cudaMemcpy(out, dout.ptr, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost), "download");
+    check(cudaMemcpy(&err, derr.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost), "download");
+  } catch (const std::exception &e) {
+    for (DevBuf *b : {&dc, &dout, &derr}) b->release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  for (DevBuf *b : {&dc, &dout, &derr}) b->release();
+  if (err) return fail(TWOS_ERR_RUNTIME, "negative analytic Green integral");
+  return TWOS_OK;
 }
 
 int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int enclosure_fallback,
@@ -971,7 +1003,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.site_best2 = nullptr;
         L.total_sites = count;
         const int mode = pass == 0 ? kModeBoundary : TWOS_MODE_COMPLIANCE;
-        const bool green = pass == 1 && rq->green != 0;
+        const bool green = pass == 1 && rq->green == TWOS_SOURCE_GREEN;
         if (pass == 0) {
           L.hits = hits.as<HitRec>();
           L.steps_out = osteps.as<uint32_t>();

@@ -113,7 +113,7 @@ struct JobDesc {
   uint32_t k0, k1;       // Philox key
   uint32_t repeat;
   int32_t max_steps;
-  uint32_t flags;        // kJobGreen | kJobSkipCavitySites
+  uint32_t flags;        // kJobGreen | kJobSkipCavitySites | kJobExactSource
   double epsilon;
   double query_radius2;  // squared initial radius (+inf when unbounded)
   double cavity_radius;
@@ -124,6 +124,7 @@ struct JobDesc {
 };
 constexpr uint32_t kJobGreen = 1u;
 constexpr uint32_t kJobSkipCavitySites = 2u;
+constexpr uint32_t kJobExactSource = 4u;  // TWOS_SOURCE_EXACT
 
 struct TermDev {
   int32_t kind;
@@ -264,6 +265,8 @@ cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, 
                        cudaStream_t s);
 int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L);
 cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s);
+// Exact ball integrals of bump sources: cases[4i..4i+3] = (d, r, R, A).
+cudaError_t launch_ball_green(const double *cases, uint32_t n, double *out, uint32_t *error, cudaStream_t s);
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
                            double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s);
 cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *index, void *scratch,

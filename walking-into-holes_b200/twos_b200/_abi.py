@@ -16,6 +16,7 @@ BIN_DIR = PKG_ROOT / "_build"
 OK, ERR_RUNTIME, ERR_USAGE = 0, 1, 2
 MODE_COMPLIANCE, MODE_PAIRED, MODE_HOT = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+SOURCE_CENTER, SOURCE_GREEN, SOURCE_EXACT = 0, 1, 2
 TERM_CONST, TERM_LINEAR, TERM_GAUSS, TERM_BUMP, TERM_BOX, TERM_BALL = range(6)
 MAX_TERMS = 8
 DEVERR_QUERY, DEVERR_STACK, DEVERR_ITER, DEVERR_CONFIG = 1, 2, 4, 8
@@ -25,6 +26,7 @@ EXPORTED = [
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
+    "twos_ball_green_integral",
 ]
 
 
@@ -151,6 +153,7 @@ def load(path: Path | str | None = None):
                                    ctypes.POINTER(DesignParams), vp, vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
+    L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
     L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,
                                ctypes.POINTER(Summary)]
     L.twos_topk_device.argtypes = [vp, vp, u32, u32, vp]

@@ -29,6 +29,7 @@ from ._abi import (DIFF_DTYPE, DIFF_STATS_DTYPE, MODE_COMPLIANCE, MODE_HOT, MODE
 
 PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 MODES = {"compliance": MODE_COMPLIANCE, "paired": MODE_PAIRED, "hot": MODE_HOT}
+SOURCE_MODES = {"center": _abi.SOURCE_CENTER, "green": _abi.SOURCE_GREEN, "exact": _abi.SOURCE_EXACT}
 
 
 def _ptr(a):
@@ -48,7 +49,7 @@ class Config:
     epsilon: float = 5e-4
     cavity_radius: float = 0.0
     query_radius: float = 4.0
-    green: bool = False
+    green: bool | int | str = False  # False/"center", True/"green", or "exact" (TWOS_SOURCE_*)
     source: list = field(default_factory=lambda: sources.affine())
     adjoint: list = field(default_factory=list)
     skip_cavity_sites: bool | None = None
@@ -66,7 +67,7 @@ class Config:
         r.epsilon = float(self.epsilon)
         r.cavity_radius = float(self.cavity_radius)
         r.query_radius = float(self.query_radius) if self.query_radius is not None else 0.0
-        r.green = int(bool(self.green))
+        r.green = SOURCE_MODES[self.green] if isinstance(self.green, str) else int(self.green)
         if len(self.source) > _abi.MAX_TERMS or len(self.adjoint) > _abi.MAX_TERMS:
             raise ValueError("too many source terms")
         r.n_source, r.n_adjoint = len(self.source), len(self.adjoint)
@@ -254,6 +255,16 @@ class Mesh:
             return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
         check(_abi.load().twos_topk_device(self._h, ctypes.c_void_p(addr(d_keys)), int(n), int(k),
                                            ctypes.c_void_p(addr(d_index))))
+
+
+def ball_green_integral(cases, device: int = 0):
+    """The EXACT source's closed-form ball integral evaluated on the GPU
+    (twos_ball_green_integral; exact_bump_green, study.cpp:64-77): cases is
+    an [n, 4] array of (d, r, R, A); returns the n integrals."""
+    c = np.ascontiguousarray(cases, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros(len(c))
+    check(_abi.load().twos_ball_green_integral(_ptr(c), len(c), _ptr(out), int(device)))
+    return out
 
 
 def estimate_batch(meshes, sites_list, configs, cavities_list=None):
