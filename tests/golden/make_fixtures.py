@@ -101,6 +101,27 @@ def main(reference: Path) -> None:
         keep = {k: v for k, v in zip(argv[0::2], argv[1::2])
                 if k not in ("--mesh", "--config", "--points", "--cavities", "--output", "--summary")}
         (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
+    # Paired and hot requests of the study's pilot pipeline (wih_study, the
+    # branch geometry, the config's two remote heat sources).
+    sbase = reference / "benchmarks/submission_study"
+    for tag, rel in STUDY_REQUESTS.items():
+        src = sbase / rel
+        dst = grad / tag
+        dst.mkdir(exist_ok=True)
+        for name in ("points.txt", "holes.txt", "field.csv", "kernel.json"):
+            shutil.copyfile(src / name, dst / name)
+        argv = json.loads((src / "request.json").read_text())[1:]
+        keep = {k: v for k, v in zip(argv[0::2], argv[1::2])
+                if k not in ("--mesh", "--config", "--points", "--cavities", "--output", "--summary")}
+        keep["has_cavities"] = bool(dict(zip(argv[0::2], argv[1::2])).get("--cavities"))
+        (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
+
+
+STUDY_REQUESTS = {
+    "paired-rescore": "pilot/pipeline/branch/twos-1611/raw/round2-rescore",
+    "paired-scout": "pilot/pipeline/branch/twos-1611/raw/round3-scout",
+    "hot-refine": "pilot/pipeline/branch/hot-1611/refine-raw/r0-trial1",
+}
 
 
 if __name__ == "__main__":

@@ -27,7 +27,16 @@ COMMON = ["-std=c++17", "-O3", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fP
 CUDA_FLAGS = ARCH + ["-lineinfo", "-fmad=false", "--expt-relaxed-constexpr"]
 
 LIB_SOURCES = ["kernels.cu", "design.cu", "noalloc.cu", "twos_abi.cpp", "geometry.cpp"]
-CLI = {"wih_twos": "cli_twos.cpp", "wih_adjoint": "cli_adjoint.cpp"}
+# Executables: name -> (source, extra defines).  The study variants mirror the
+# reference's macro builds of study.cpp (analytic_query.cpp, compliance_query.cpp).
+CLI = {
+    "wih_twos": ("cli_twos.cpp", []),
+    "wih_adjoint": ("cli_adjoint.cpp", []),
+    "wih_study": ("cli_study.cpp", []),
+    "wih_analytic_query": ("cli_study.cpp", ["-DTWOS_STUDY_ANALYTIC=1"]),
+    "wih_compliance_query": ("cli_study.cpp", ["-DTWOS_STUDY_ANALYTIC=1", "-DTWOS_STUDY_AFFINE=1"]),
+    "wih_analytic_integral_audit": ("cli_audit.cpp", []),
+}
 HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h", "diffwos.cuh", "ball_green.cuh"]
 
 
@@ -72,12 +81,12 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     if force or _stale(lib, objs):
         run([nvcc()] + host_compiler() + ARCH + ["-shared", "-cudart", "static", "-o", str(lib)]
             + [str(o) for o in objs] + ["-lpthread"])
-    for exe, src in CLI.items():
+    for exe, (src, defines) in CLI.items():
         s = CSRC / src
         target = OUT / exe
         if force or _stale(target, [s, lib] + headers):
-            run([nvcc()] + host_compiler() + COMMON + ["-o", str(target), str(s), "-L", str(OUT), "-ltwos",
-                 "-Xlinker", "-rpath,$ORIGIN"])
+            run([nvcc()] + host_compiler() + COMMON + defines + ["-o", str(target), str(s), "-L", str(OUT),
+                 "-ltwos", "-Xlinker", "-rpath,$ORIGIN"])
     return lib
 
 

@@ -62,8 +62,8 @@ inline void print_usage(const std::string &message) {
   std::cerr << "Usage: wih_twos --mesh MESH.ply --points POINTS.csv --output FIELD.csv\n"
             << "                 --summary SUMMARY.json [options]\n\n"
             << "Options (B200 backend):\n"
-            << "  --mode NAME           twos (default); voxel, mg, diffwos and validate are not\n"
-            << "                        provided by this backend\n"
+            << "  --mode NAME           twos (default) or diffwos; voxel, mg and validate are\n"
+            << "                        not provided by this backend\n"
             << "  --walks N             paths per evaluation site (default 16)\n"
             << "  --repeats N           timed repetitions; median is reported (default 3)\n"
             << "  --threads N           accepted for compatibility (host threads)\n"
@@ -268,6 +268,48 @@ inline void throw_on(int rc) {
 
 inline int effective_threads(const Options &o) {
   return o.threads > 0 ? o.threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+}
+
+// Differential field CSV (write_differential_field, wih_twos.cpp:1576-1602):
+// site,x,y,z then per cavity i dc{i}_x,_y,_z, dc{i}_se_x,_y,_z, dR{i},
+// dR{i}_se, at 17 significant digits.
+inline void write_differential_field(const std::string &path, const std::vector<double> &points,
+                                     const std::vector<twos_diff_result> &rows, size_t n_cav) {
+  std::ofstream output(path);
+  if (!output) throw std::runtime_error("cannot write differential field output: " + path);
+  output << "site,x,y,z";
+  for (size_t c = 0; c < n_cav; ++c)
+    output << ",dc" << c << "_x,dc" << c << "_y,dc" << c << "_z,dc" << c << "_se_x,dc" << c << "_se_y,dc" << c
+           << "_se_z,dR" << c << ",dR" << c << "_se";
+  output << "\n" << std::setprecision(17);
+  const size_t n = points.size() / 3;
+  for (size_t s = 0; s < n; ++s) {
+    output << s << ',' << points[3 * s] << ',' << points[3 * s + 1] << ',' << points[3 * s + 2];
+    for (size_t c = 0; c < n_cav; ++c) {
+      const twos_diff_result &d = rows[s * n_cav + c];
+      output << ',' << d.dc[0] << ',' << d.dc[1] << ',' << d.dc[2] << ',' << d.dc_se[0] << ',' << d.dc_se[1] << ','
+             << d.dc_se[2] << ',' << d.dR << ',' << d.dR_se;
+    }
+    output << '\n';
+  }
+}
+
+// Runs twos_diffwos, accepting its "unsafe differential path" return (rows
+// and statistics are written) so the caller applies its own policy to caps
+// and unsafe offsets; any other failure throws.
+inline twos_summary run_diffwos(twos_mesh *mesh, const twos_request &r, double offset, int enclosure_fallback,
+                                const std::vector<double> &points, const std::vector<double> &cavities,
+                                std::vector<twos_diff_result> &rows, std::vector<twos_diff_stats> &stats) {
+  const size_t n = points.size() / 3, n_cav = cavities.size() / 3;
+  rows.assign(n * n_cav, twos_diff_result{});
+  stats.assign(n, twos_diff_stats{});
+  twos_summary s{};
+  const int rc = twos_diffwos(mesh, &r, offset, enclosure_fallback, points.data(), static_cast<uint32_t>(n),
+                              cavities.data(), static_cast<uint32_t>(n_cav), rows.data(), stats.data(), &s);
+  if (rc != TWOS_OK && !(rc == TWOS_ERR_RUNTIME && s.error_flags == 0 &&
+                         std::string(twos_last_error()).rfind("unsafe differential path", 0) == 0))
+    throw_on(rc);
+  return s;
 }
 
 }  // namespace twos_cli

@@ -1,6 +1,6 @@
 // wih_twos: drop-in executable for the reference's compliance TWoS backend
-// (benchmarks/compiled_bunny/src/wih_twos.cpp:1799-1864, --mode twos), on
-// libtwos.so.  Same argv, same field CSV `site,x,y,z,u,score,score_se,steps,
+// (benchmarks/compiled_bunny/src/wih_twos.cpp:1799-1864, --mode twos and
+// --mode diffwos), on libtwos.so.  Same argv, same field CSV `site,x,y,z,u,score,score_se,steps,
 // limit_hits` at 17 significant digits, same summary JSON keys (plus gpu_*
 // keys), same exit codes: 2 for usage errors, 1 with "fatal: ..." for runtime
 // errors, including any retained path that hits --max-steps.
@@ -74,9 +74,96 @@ void write_summary(const std::string &path, const twos_mesh_info &info, size_t n
   out << "]\n}\n";
 }
 
+// --mode diffwos (run_differential_wos, wih_twos.cpp:1604-1709): retained
+// repeat 0, an error when any outer or nested path hit --max-steps (unsafe
+// offsets are counted, not errors, in this executable), field CSV and the
+// differential summary JSON.
+int run_differential(const Options &o, twos_mesh *mesh, const twos_mesh_info &info,
+                     const std::vector<double> &points, const std::vector<double> &cavities) {
+  const size_t n = points.size() / 3, n_cav = cavities.size() / 3;
+  twos_request r = base_request(o);
+  std::vector<double> times;
+  std::vector<twos_diff_result> retained;
+  std::vector<twos_diff_stats> stats;
+  for (int repeat = 0; repeat < o.repeats; ++repeat) {
+    r.repeat = static_cast<uint32_t>(repeat);
+    std::vector<twos_diff_result> rows;
+    std::vector<twos_diff_stats> st;
+    const auto start = std::chrono::steady_clock::now();
+    run_diffwos(mesh, r, o.diff_offset, 0, points, cavities, rows, st);
+    times.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count());
+    if (repeat == 0) {
+      retained = std::move(rows);
+      stats = std::move(st);
+    }
+  }
+  uint64_t outer = 0, nested = 0, cav = 0, seam = 0, seg = 0, unsafe = 0, limits = 0;
+  for (const twos_diff_stats &s : stats) {
+    outer += s.outer_steps;
+    nested += s.nested_steps;
+    cav += s.cavity_terminations;
+    seam += s.near_seam;
+    seg += s.segment_unsafe;
+    unsafe += s.unsafe_offset;
+    limits += s.limits;
+  }
+  if (limits != 0) throw std::runtime_error("one or more differential paths hit --max-steps");
+  write_differential_field(o.output_path, points, retained, n_cav);
+  const double runtime = median(times);
+  const double paths = static_cast<double>(n) * o.walks;
+  std::ofstream out(o.summary_path);
+  if (!out) throw std::runtime_error("cannot write differential summary: " + o.summary_path);
+  out << std::setprecision(17) << "{\n"
+      << "  \"engine\": \"TWoS B200 sm_100a Differential WoS\",\n"
+      << "  \"mode\": \"diffwos\",\n"
+      << "  \"vertices\": " << info.vertices << ",\n"
+      << "  \"faces\": " << info.faces << ",\n"
+      << "  \"source_mode\": \"" << o.source_mode << "\",\n"
+      << "  \"cavities\": " << n_cav << ",\n"
+      << "  \"gradient_parameters\": " << 4 * n_cav << ",\n"
+      << "  \"cavity_radius\": " << o.cavity_radius << ",\n"
+      << "  \"sites\": " << n << ",\n"
+      << "  \"walks_per_site\": " << o.walks << ",\n"
+      << "  \"seed\": " << o.seed << ",\n"
+      << "  \"epsilon\": " << o.epsilon << ",\n"
+      << "  \"normal_offset\": " << o.diff_offset << ",\n"
+      << "  \"seam_strip_multiplier\": 1,\n"
+      << "  \"runtime_seconds_median\": " << runtime << ",\n"
+      << "  \"outer_mean_steps\": " << static_cast<double>(outer) / paths << ",\n"
+      << "  \"nested_mean_steps_per_outer_path\": " << static_cast<double>(nested) / paths << ",\n"
+      << "  \"cavity_termination_fraction\": " << static_cast<double>(cav) / paths << ",\n"
+      << "  \"near_seam_fraction\": " << static_cast<double>(seam) / paths << ",\n"
+      << "  \"segment_unsafe_fraction\": " << static_cast<double>(seg) / paths << ",\n"
+      << "  \"unsafe_offset_fraction\": " << static_cast<double>(unsafe) / paths << ",\n"
+      << "  \"unsafe_given_cavity_fraction\": "
+      << (cav == 0 ? 0.0 : static_cast<double>(unsafe) / static_cast<double>(cav)) << ",\n"
+      << "  \"near_seam_terminations\": " << seam << ",\n"
+      << "  \"segment_unsafe_terminations\": " << seg << ",\n"
+      << "  \"unsafe_offset_terminations\": " << unsafe << ",\n"
+      << "  \"mesh_build_seconds\": " << info.build_seconds << ",\n"
+      << "  \"peak_rss_megabytes\": " << peak_rss_megabytes() << ",\n"
+      << "  \"gpu_precision\": \"" << o.precision << "\",\n"
+      << "  \"timings_seconds\": [";
+  for (size_t i = 0; i < times.size(); ++i) {
+    if (i) out << ", ";
+    out << times[i];
+  }
+  out << "]\n}\n";
+  std::cout << "TWoS B200 Differential WoS: " << n << " sites x " << o.walks << " walks, " << 4 * n_cav
+            << " parameters, median " << runtime << " s\n";
+  return 0;
+}
+
 int run(const Options &o) {
-  if (o.mode != "twos")
+  if (o.mode != "twos" && o.mode != "diffwos")
     throw std::runtime_error("mode " + o.mode + " is not provided by the TWoS B200 backend");
+  if (o.mode == "diffwos") {
+    MeshHandle mesh;
+    throw_on(twos_mesh_open_ply(o.mesh_path.c_str(), o.device, &mesh.m));
+    twos_mesh_info info{};
+    throw_on(twos_mesh_get_info(mesh.m, &info));
+    return run_differential(o, mesh.m, info, read_points(o.points_path), read_optional_points(o.cavities_path));
+  }
   MeshHandle mesh;
   throw_on(twos_mesh_open_ply(o.mesh_path.c_str(), o.device, &mesh.m));
   twos_mesh_info info{};

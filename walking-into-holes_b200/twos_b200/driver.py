@@ -70,3 +70,63 @@ class ServeSession:
         if self._log not in (None, subprocess.DEVNULL):
             self._log.close()
         return code
+
+
+WIH_STUDY = BIN_DIR / "wih_study"
+WIH_ANALYTIC_QUERY = BIN_DIR / "wih_analytic_query"
+WIH_COMPLIANCE_QUERY = BIN_DIR / "wih_compliance_query"
+
+
+class StudySolver:
+    """The study driver's solver (submission_study/run_study.py:19-38
+    ``Solver.call``) over a ``--serve`` child of a wih_study executable: the
+    same argv per request, the same files (points.txt, holes.txt, field.csv,
+    kernel.json, request.json) under ``folder/tag``, and the same return
+    value (field DataFrame, summary dict with request_wall_seconds)."""
+
+    def __init__(self, mesh, config, folder, executable=None):
+        self.mesh, self.config, self.folder = Path(mesh), Path(config), Path(folder)
+        self.executable = str(executable or WIH_STUDY)
+        self.session = None
+        self.calls = []
+
+    def call(self, tag, points, holes=(), radius=.065, mode="twos", walks=128, seed=7, hot=False, fd=False,
+             diff=False, epsilon=.0002, offset=.004, precision=None):
+        import time
+
+        import numpy as np
+        import pandas as pd
+        d = self.folder / tag
+        d.mkdir(parents=True, exist_ok=True)
+        holes = np.asarray(holes).reshape(-1, 3)
+        points = np.asarray(points).reshape(-1, 3)
+        np.savetxt(d / "points.txt", points, fmt="%.17g")
+        np.savetxt(d / "holes.txt", holes, fmt="%.17g")
+        args = ["--mesh", str(self.mesh), "--config", str(self.config), "--points", str(d / "points.txt"),
+                "--cavities", str(d / "holes.txt") if len(holes) else "", "--cavity-radius", str(radius),
+                "--output", str(d / "field.csv"), "--summary", str(d / "kernel.json"), "--mode", mode,
+                "--source-mode", "housing", "--walks", str(walks), "--repeats", "1", "--seed", str(seed),
+                "--threads", "4", "--max-steps", "2048", "--epsilon", str(epsilon), "--hot-only", str(int(hot)),
+                "--fd", str(int(fd)), "--diff", str(int(diff)), "--diff-offset", str(offset)]
+        if precision is not None:
+            args += ["--precision", precision]
+        (d / "request.json").write_text(json.dumps([self.executable] + args, indent=2))
+        if self.session is None:
+            self.folder.mkdir(parents=True, exist_ok=True)
+            self.session = ServeSession(self.executable, log=self.folder / "server.log")
+        start = time.perf_counter()
+        code = self.session.request(args)
+        if code != 0:
+            # The server stops after a failed request (study.cpp:373).
+            self.close()
+            raise RuntimeError(f"{d}: DONE {code} " + (self.folder / "server.log").read_text())
+        meta = json.loads((d / "kernel.json").read_text())
+        meta["request_wall_seconds"] = time.perf_counter() - start
+        (d / "kernel.json").write_text(json.dumps(meta, indent=2))
+        self.calls.append(meta)
+        return pd.read_csv(d / "field.csv"), meta
+
+    def close(self):
+        if self.session is not None:
+            self.session.close()
+            self.session = None
