@@ -390,6 +390,58 @@ int twos_inside(twos_mesh *mesh, const double *points, uint64_t n, uint8_t *insi
  * TWOS_ERR_RUNTIME with the values written. */
 int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device);
 
+/* Certified fresh-sample validation (--mode validate: run_minimum_benefit,
+ * cert_walk, CertDistanceTree and cert_source_lower of
+ * benchmarks/compiled_bunny/src/minimum_benefit.hpp:13-188).  Each of
+ * request->walks walks per site takes as its distance the distance to the
+ * union of the triangles' bounding boxes and to the cavities, every positive
+ * operation rounded one ulp down after rounding to nearest; steps of radius
+ * min(radius_cap, 0.95 d); a rounded-down lower bound of the source at the
+ * ball centre (green 0) or at a Beta(2,2) Green point (green 1) times
+ * r^2/6; the value clipped at value_cap; a walk whose sampled point might
+ * leave its ball stops and is counted as a containment failure.  FP64 in
+ * both precision forms (request->precision is ignored).
+ *
+ * Sources: an optional leading CONST term, then LINEAR (amp >= 0) and GAUSS
+ * (amp >= 0) terms; anything else is TWOS_ERR_USAGE.  Every site must be
+ * inside the mesh (ray parity) and outside every cavity, else
+ * TWOS_ERR_RUNTIME.  samples is [n_sites][walks]; stages is
+ * [n_sites][TWOS_VALIDATE_MAX_STAGES] with *n_stages per site: the prefixes
+ * n in {1024, 4096, 16384, 65536} below walks, then walks, as the
+ * reference's stage JSON.  Containment failures return TWOS_ERR_RUNTIME
+ * with everything written ("validation record must be rejected"). */
+#define TWOS_VALIDATE_MAX_STAGES 5
+
+typedef struct twos_validate_params {
+  double radius_cap; /* --validation-radius-cap */
+  double value_cap;  /* --validation-value-cap */
+} twos_validate_params;
+
+typedef struct twos_cert_sample {
+  double value;
+  uint32_t steps;
+  uint8_t capped;    /* hit max_steps */
+  uint8_t clipped;   /* reached value_cap */
+  uint8_t contained; /* 0: containment failure (the sample must not be used) */
+  uint8_t pad;
+} twos_cert_sample; /* 16 bytes */
+
+typedef struct twos_validate_stage {
+  uint32_t site;
+  uint32_t n;
+  double mean;                   /* long-double sum of the first n values / n */
+  double mean_steps;
+  uint64_t clipped;
+  uint64_t path_caps;
+  double center_clearance_lower; /* certified domain distance at the site */
+  double center_distance;        /* exact FP64 domain distance at the site */
+} twos_validate_stage; /* 56 bytes */
+
+int twos_validate(twos_mesh *mesh, const twos_request *request, const twos_validate_params *params,
+                  const double *sites, uint32_t n_sites, const double *cavities, uint32_t n_cavities,
+                  twos_cert_sample *samples, twos_validate_stage *stages, uint32_t *n_stages,
+                  twos_summary *summary);
+
 /* Indices of the k largest keys, highest first, ties to the lower index
  * (np.argpartition(...)[-k:] of run_bunny_benchmark.py:324 with a
  * deterministic order).  Device buffers, k <= 1024. */

@@ -101,6 +101,10 @@ def lib():
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p]
         L.oracle_exact_bump_green.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_validate.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p]
         assert L.oracle_sizeof_params() == ctypes.sizeof(Params)
         assert L.oracle_sizeof_site() == ctypes.sizeof(Site)
         _lib = L
@@ -287,6 +291,27 @@ class OracleMesh:
         if rc:
             raise RuntimeError(lib().oracle_last_error().decode())
         return out, stats, totals
+
+    def validate(self, sites, radius_cap, value_cap, site_ids=None, cavities=None, **kw):
+        """Certified fresh samples (minimum_benefit.hpp cert_walk) at each site:
+        dict of value, steps, capped, clipped, contained ([n_sites, walks]) and
+        clearance (the certified domain distance at each site)."""
+        p = self._params(**kw)
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        ids = None if site_ids is None else np.ascontiguousarray(site_ids, dtype=np.uint64)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        n, w = len(s), p.walks
+        value = np.zeros((n, w))
+        steps = np.zeros((n, w), dtype=np.uint32)
+        flags = np.zeros((n, w), dtype=np.uint8)
+        clearance = np.zeros(n)
+        rc = lib().oracle_validate(self.handle, ctypes.byref(p), float(radius_cap), float(value_cap), _ptr(s),
+                                   _ptr(ids), n, _ptr(cav), len(cav), _ptr(value), _ptr(steps), _ptr(flags),
+                                   _ptr(clearance))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return {"value": value, "steps": steps, "capped": (flags & 1) != 0, "clipped": (flags & 2) != 0,
+                "contained": (flags & 4) == 0, "clearance": clearance}
 
     def estimate(self, sites, site_ids=None, cavities=None, **kw):
         p = self._params(**kw)

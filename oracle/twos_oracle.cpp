@@ -1214,3 +1214,206 @@ int oracle_diffwos(const oracle_mesh *om, const oracle_params *o, double diff_of
 }
 
 }  // extern "C"
+
+// ================================================================ certified validation
+// Restates the certified fresh-sample validator of
+// benchmarks/compiled_bunny/src/minimum_benefit.hpp (run_minimum_benefit,
+// cert_walk, CertDistanceTree, cert_source_lower): a walk whose distances are
+// rigorous lower bounds (distance to the union of the triangles' bounding
+// boxes, every positive operation rounded one ulp down after rounding to
+// nearest), whose ball radius is min(radius_cap, 0.95 d), whose payoff is a
+// rounded-down lower bound of the source, clipped at value_cap, and which
+// fails closed when a sampled point might leave its ball.
+
+namespace {
+
+inline double rdn(double x) { return std::nextafter(x, -std::numeric_limits<double>::infinity()); }
+inline double rup(double x) { return std::nextafter(x, std::numeric_limits<double>::infinity()); }
+inline double pos_dn(double x) { return std::max(0.0, rdn(x)); }
+
+double cert_box_lower(const Vec3 &lo, const Vec3 &hi, const Vec3 &x) {
+  double sum = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double g = std::max({0.0, rdn(coord(lo, a) - coord(x, a)), rdn(coord(x, a) - coord(hi, a))});
+    sum = pos_dn(sum + pos_dn(g * g));
+  }
+  return pos_dn(std::sqrt(sum));
+}
+
+double cert_point_distance(const Vec3 &a, const Vec3 &b, bool upper) {
+  double sum = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    double d = std::abs(coord(a, k) - coord(b, k));
+    d = upper ? rup(d) : pos_dn(d);
+    const double q = upper ? rup(d * d) : pos_dn(d * d);
+    sum = upper ? rup(sum + q) : pos_dn(sum + q);
+  }
+  return upper ? rup(std::sqrt(sum)) : pos_dn(std::sqrt(sum));
+}
+
+// Minimum over triangles of the lower distance to each triangle's box; the
+// oracle BVH's node boxes (unions of those boxes) prune exactly.
+double cert_mesh_distance(const Mesh &m, const Vec3 &x) {
+  double best = std::numeric_limits<double>::infinity();
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const Bvh::Node &n = m.bvh.nodes[stack[--sp]];
+    if (cert_box_lower(n.box.lo, n.box.hi, x) >= best) continue;
+    if (n.left < 0) {
+      for (int i = 0; i < n.count; ++i) {
+        const auto &f = m.f[m.bvh.order[n.begin + i]];
+        Box b;
+        b.grow(m.v[f[0]]);
+        b.grow(m.v[f[1]]);
+        b.grow(m.v[f[2]]);
+        best = std::min(best, cert_box_lower(b.lo, b.hi, x));
+      }
+    } else {
+      stack[sp++] = n.left;
+      stack[sp++] = n.right;
+    }
+  }
+  return best;
+}
+
+double cert_domain_distance(const Mesh &m, const Vec3 &p, const std::vector<Vec3> &holes, double r) {
+  double d = cert_mesh_distance(m, p);
+  for (const Vec3 &c : holes) d = std::min(d, rdn(cert_point_distance(p, c, false) - r));
+  return std::max(0.0, d);
+}
+
+// (1 - t/1024)^1024 <= exp(-t), every step rounded down.
+double cert_exp_lower(double t_upper) {
+  double a = std::max(0.0, rdn(1.0 - rup(t_upper / 1024.0)));
+  for (int i = 0; i < 10; ++i) a = pos_dn(a * a);
+  return a;
+}
+
+// Lower bound of a source given as terms: a leading constant, then linear
+// terms (down(value + down(amp down(x + offset)))) and Gaussian terms
+// (down(value + pos_dn(amp exp_lower(exponent_up)))); cert_source_lower's
+// affine and housing forms are exactly these sequences.
+double cert_source_lower(const Term *terms, int n, const Vec3 &p) {
+  double value = n > 0 && terms[0].kind == 0 ? terms[0].amp : 0.0;
+  for (int i = (n > 0 && terms[0].kind == 0) ? 1 : 0; i < n; ++i) {
+    const Term &t = terms[i];
+    if (t.kind == 1) {
+      value = rdn(value + rdn(t.amp * rdn(coord(p, t.axis) + t.offset)));
+    } else if (t.kind == 2) {
+      double exponent = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double q = rup(rup(std::abs(coord(p, a) - t.c[a])) / t.w[a]);
+        exponent = rup(exponent + rup(q * q));
+      }
+      value = rdn(value + pos_dn(t.amp * cert_exp_lower(exponent)));
+    } else if (t.kind == 0) {
+      value = rdn(value + t.amp);
+    }
+  }
+  return std::max(0.0, value);
+}
+
+struct CertSample {
+  double value = 0.0;
+  int steps = 0;
+  bool capped = false, clipped = false, contained = true;
+};
+
+CertSample cert_walk(const Mesh &m, const std::vector<Vec3> &holes, Vec3 point, const oracle_params &o,
+                     double radius_cap, double value_cap, uint64_t site, uint32_t sample) {
+  std::mt19937_64 rng;
+  CounterStream cs{};
+  if (o.rng == 0) {
+    rng.seed(splitmix64(splitmix64(o.seed) ^ splitmix64(site + 0xa1224ULL) ^ splitmix64(sample + 0x6242cULL)));
+  } else {
+    counter_key(o.seed, o.stream, cs.k0, cs.k1);
+    cs.walk = sample;
+    cs.site = static_cast<uint32_t>(site);
+    cs.repeat = o.repeat;
+  }
+  CertSample out;
+  for (int k = 0; k < o.max_steps; ++k) {
+    const double d = cert_domain_distance(m, point, holes, o.cavity_radius);
+    if (d <= o.epsilon) return out;
+    const double s = std::min(radius_cap, pos_dn(0.95 * d));
+    Vec3 y = point, next;
+    if (o.rng == 0) {
+      if (o.green) {
+        const double scale = s * beta_22(rng);
+        y = point + random_unit_vector(rng) * scale;
+      }
+      next = point + random_unit_vector(rng) * s;
+    } else {
+      double a0, a1;
+      cs.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
+      if (o.green) {
+        double g0, g1, b0, b1, b2, spare;
+        cs.uniforms(static_cast<uint32_t>(k), 1, g0, g1);
+        cs.uniforms(static_cast<uint32_t>(k), 2, b0, b1);
+        cs.uniforms(static_cast<uint32_t>(k), 3, b2, spare);
+        y = point + direction_from(g0, g1) * (s * median3(b0, b1, b2));
+      }
+      next = point + direction_from(a0, a1) * s;
+    }
+    if (!(cert_point_distance(point, next, true) < d) || !(cert_point_distance(point, y, true) < d)) {
+      out.contained = false;
+      return out;
+    }
+    const double weight = pos_dn(pos_dn(s * s) / 6.0);
+    const double increment = pos_dn(weight * cert_source_lower(o.source, o.n_source, y));
+    out.value = pos_dn(out.value + increment);
+    ++out.steps;
+    if (out.value >= value_cap) {
+      out.value = value_cap;
+      out.clipped = true;
+      return out;
+    }
+    point = next;
+  }
+  out.capped = true;
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Certified samples for n_sites sites (site ids site_ids[i] or i):
+// value/steps [n_sites * walks], flags bit 0 capped, bit 1 clipped, bit 2
+// containment failure; clearance[i] = the certified domain distance at site
+// i.  Returns 1 when a site is outside the mesh or inside a cavity.
+int oracle_validate(const oracle_mesh *om, const oracle_params *o, double radius_cap, double value_cap,
+                    const double *sites, const uint64_t *site_ids, uint32_t n_sites, const double *cav_xyz,
+                    uint32_t ncav, double *value, uint32_t *steps, uint8_t *flags, double *clearance) {
+  const Mesh &m = om->m;
+  std::vector<Vec3> holes(ncav);
+  for (uint32_t i = 0; i < ncav; ++i) holes[i] = {cav_xyz[3 * i], cav_xyz[3 * i + 1], cav_xyz[3 * i + 2]};
+  for (uint32_t s = 0; s < n_sites; ++s) {
+    const Vec3 x{sites[3 * s], sites[3 * s + 1], sites[3 * s + 2]};
+    Counters cnt;
+    bool in_cav = false;
+    for (const Vec3 &c : holes) in_cav = in_cav || norm(x - c) <= o->cavity_radius;
+    if (!inside_parity(m, x, cnt) || in_cav) {
+      g_error = "candidate classified outside; exact driver predicate is also required";
+      return 1;
+    }
+    clearance[s] = cert_domain_distance(m, x, holes, o->cavity_radius);
+    const uint64_t site = site_ids ? site_ids[s] : s;
+#ifdef _OPENMP
+    if (o->threads > 0) omp_set_num_threads(o->threads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int j = 0; j < o->walks; ++j) {
+      const CertSample c = cert_walk(m, holes, x, *o, radius_cap, value_cap, site, static_cast<uint32_t>(j));
+      const size_t slot = static_cast<size_t>(s) * o->walks + j;
+      value[slot] = c.value;
+      steps[slot] = static_cast<uint32_t>(c.steps);
+      flags[slot] = static_cast<uint8_t>((c.capped ? 1 : 0) | (c.clipped ? 2 : 0) | (c.contained ? 0 : 4));
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

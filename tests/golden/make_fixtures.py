@@ -115,7 +115,32 @@ def main(reference: Path) -> None:
                 if k not in ("--mesh", "--config", "--points", "--cavities", "--output", "--summary")}
         keep["has_cavities"] = bool(dict(zip(argv[0::2], argv[1::2])).get("--cavities"))
         (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
+    minimum_benefit(reference, out)
 
+
+def minimum_benefit(reference: Path, out: Path) -> None:
+    """Certified validation attempts of benchmarks/minimum_benefit/
+    pilot-floor-policy: the finalist, the retained cavities, the stage JSON,
+    the decision record and the first 4,096 of the 65,536 samples (enough
+    for the n = 1024 and n = 4096 stages, which use a prefix)."""
+    import gzip
+    base = reference / "benchmarks/minimum_benefit/pilot-floor-policy"
+    dst_root = out / "minimum_benefit"
+    dst_root.mkdir(exist_ok=True)
+    shutil.copyfile(base / "configuration.json", dst_root / "configuration.json")
+    for tag, (kind, attempt) in MIN_BENEFIT.items():
+        src = base / kind / attempt
+        dst = dst_root / tag
+        dst.mkdir(exist_ok=True)
+        for name in ("validation-points.csv", "validation-holes.csv", "validation.json", "decision.json"):
+            shutil.copyfile(src / name, dst / name)
+        with open(src / "validation.csv") as f:
+            head = [next(f) for _ in range(4097)]
+        with gzip.open(dst / "validation-head.csv.gz", "wt") as g:
+            g.writelines(head)
+
+
+MIN_BENEFIT = {"bunny-00": ("bunny", "attempt-00"), "housing-01": ("housing", "attempt-01")}
 
 STUDY_REQUESTS = {
     "paired-rescore": "pilot/pipeline/branch/twos-1611/raw/round2-rescore",

@@ -62,7 +62,7 @@ inline void print_usage(const std::string &message) {
   std::cerr << "Usage: wih_twos --mesh MESH.ply --points POINTS.csv --output FIELD.csv\n"
             << "                 --summary SUMMARY.json [options]\n\n"
             << "Options (B200 backend):\n"
-            << "  --mode NAME           twos (default) or diffwos; voxel, mg and validate are\n"
+            << "  --mode NAME           twos (default), diffwos or validate; voxel and mg are\n"
             << "                        not provided by this backend\n"
             << "  --walks N             paths per evaluation site (default 16)\n"
             << "  --repeats N           timed repetitions; median is reported (default 3)\n"

@@ -154,9 +154,72 @@ int run_differential(const Options &o, twos_mesh *mesh, const twos_mesh_info &in
   return 0;
 }
 
+// --mode validate (run_minimum_benefit, minimum_benefit.hpp:145-188): the
+// per-sample CSV site,sample,value,steps,capped,clipped and the stage JSON;
+// a containment failure fails the request after both are written.  The
+// samples come from the validation stream (stream 2) of --seed.
+int run_validate(const Options &o, twos_mesh *mesh, const twos_mesh_info &info, const std::vector<double> &points,
+                 const std::vector<double> &cavities) {
+  const size_t n = points.size() / 3, n_cav = cavities.size() / 3;
+  twos_request r = base_request(o);
+  r.precision = TWOS_PREC_FP64;
+  r.stream = 2;
+  twos_validate_params vp{o.validation_radius_cap, o.validation_value_cap};
+  std::vector<twos_cert_sample> samples(n * static_cast<size_t>(o.walks));
+  std::vector<twos_validate_stage> stages(n * TWOS_VALIDATE_MAX_STAGES);
+  uint32_t n_stages = 0;
+  twos_summary s{};
+  const int rc = twos_validate(mesh, &r, &vp, points.data(), static_cast<uint32_t>(n), cavities.data(),
+                               static_cast<uint32_t>(n_cav), samples.data(), stages.data(), &n_stages, &s);
+  const bool containment = rc == TWOS_ERR_RUNTIME && s.error_flags == 0 && s.node_tests > 0;
+  if (rc != TWOS_OK && !containment) throw_on(rc);
+  std::ofstream output(o.output_path);
+  if (!output) throw std::runtime_error("cannot write validation output: " + o.output_path);
+  output << std::setprecision(17) << "site,sample,value,steps,capped,clipped\n";
+  for (size_t i = 0; i < n; ++i)
+    for (int j = 0; j < o.walks; ++j) {
+      const twos_cert_sample &v = samples[i * o.walks + j];
+      output << i << ',' << j << ',' << v.value << ',' << v.steps << ',' << int(v.capped) << ',' << int(v.clipped)
+             << '\n';
+    }
+  std::ofstream summary(o.summary_path);
+  if (!summary) throw std::runtime_error("cannot write summary: " + o.summary_path);
+  summary << std::setprecision(17)
+          << "{\"scope\":\"conditional ideal-sampling certificate; conservative box geometry and source "
+             "arithmetic\",\n"
+          << "\"distance_tree_build_seconds\":" << info.build_seconds
+          << ",\n\"distance_mode\":\"triangle_AABB_union_lower_bound\",\n"
+          << "\"sample_cap\":" << o.validation_value_cap << ",\"radius_cap\":" << o.validation_radius_cap
+          << ",\"stages\":[\n";
+  bool first = true;
+  for (size_t i = 0; i < n; ++i)
+    for (uint32_t k = 0; k < n_stages; ++k) {
+      const twos_validate_stage &st = stages[i * TWOS_VALIDATE_MAX_STAGES + k];
+      if (!first) summary << ",\n";
+      first = false;
+      // Device time apportioned to the stage's prefix of the site's walks.
+      const double elapsed = s.kernel_seconds * (static_cast<double>(st.n) / o.walks) / static_cast<double>(n);
+      summary << "{\"site\":" << st.site << ",\"n\":" << st.n << ",\"mean\":" << st.mean
+              << ",\"mean_steps\":" << st.mean_steps << ",\"clipped\":" << st.clipped
+              << ",\"path_caps\":" << st.path_caps << ",\"elapsed_seconds\":" << elapsed
+              << ",\"center_clearance_lower\":" << st.center_clearance_lower
+              << ",\"embree_center_distance\":" << st.center_distance << "}";
+    }
+  summary << "\n],\"containment_failures\":" << s.node_tests << "}\n";
+  if (containment) throw std::runtime_error("sample containment guard failed; validation record must be rejected");
+  return 0;
+}
+
 int run(const Options &o) {
-  if (o.mode != "twos" && o.mode != "diffwos")
+  if (o.mode != "twos" && o.mode != "diffwos" && o.mode != "validate")
     throw std::runtime_error("mode " + o.mode + " is not provided by the TWoS B200 backend");
+  if (o.mode == "validate") {
+    MeshHandle mesh;
+    throw_on(twos_mesh_open_ply(o.mesh_path.c_str(), o.device, &mesh.m));
+    twos_mesh_info info{};
+    throw_on(twos_mesh_get_info(mesh.m, &info));
+    return run_validate(o, mesh.m, info, read_points(o.points_path), read_optional_points(o.cavities_path));
+  }
   if (o.mode == "diffwos") {
     MeshHandle mesh;
     throw_on(twos_mesh_open_ply(o.mesh_path.c_str(), o.device, &mesh.m));

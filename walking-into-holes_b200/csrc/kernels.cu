@@ -1290,3 +1290,6 @@ cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *in
 
 // Differential WoS kernels (use nearest<double> above).
 #include "diffwos.cuh"
+
+// Certified validation kernels (use the stream, direction and nearest<double> above).
+#include "validate.cuh"

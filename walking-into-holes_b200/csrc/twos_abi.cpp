@@ -894,6 +894,166 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
   return rc;
 }
 
+int twos_validate(twos_mesh *m, const twos_request *r, const twos_validate_params *vp, const double *sites,
+                  uint32_t n_sites, const double *cavities, uint32_t n_cav, twos_cert_sample *samples,
+                  twos_validate_stage *stages, uint32_t *n_stages, twos_summary *summary) {
+  if (!m || !r || !vp) return fail(TWOS_ERR_USAGE, "null mesh, request or parameters");
+  if (int rc = validate_request(r, n_sites, n_cav)) return rc;
+  if (r->green != TWOS_SOURCE_CENTER && r->green != TWOS_SOURCE_GREEN)
+    return fail(TWOS_ERR_USAGE, "validation takes the centre or the Green-point source rule");
+  if (!(vp->radius_cap > 0.0) || !(vp->value_cap > 0.0))
+    return fail(TWOS_ERR_USAGE, "validation caps must be positive");
+  for (int i = 0; i < r->n_source; ++i) {
+    const twos_source_term &t = r->source[i];
+    const bool lead_const = i == 0 && t.kind == TWOS_TERM_CONST;
+    const bool ok = lead_const || (t.kind == TWOS_TERM_LINEAR && t.amp >= 0.0) ||
+                    (t.kind == TWOS_TERM_GAUSS && t.amp >= 0.0 && t.w[0] > 0.0 && t.w[1] > 0.0 && t.w[2] > 0.0);
+    if (!ok)
+      return fail(TWOS_ERR_USAGE,
+                  "validation sources: a leading constant, then nonnegative linear and Gaussian terms");
+  }
+  if (n_sites == 0) {
+    if (n_stages) *n_stages = 0;
+    return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  }
+  if (!sites || !samples || !stages || !n_stages || (n_cav && !cavities)) return fail(TWOS_ERR_USAGE, "null buffer");
+  // Every candidate must be inside the mesh and outside every cavity
+  // (minimum_benefit.hpp:158-159).
+  {
+    std::vector<uint8_t> inside(n_sites);
+    if (int rc = twos_inside(m, sites, n_sites, inside.data())) return rc;
+    for (uint32_t s = 0; s < n_sites; ++s) {
+      bool in_cav = false;
+      for (uint32_t c = 0; c < n_cav; ++c) {
+        const double dx = sites[3 * s] - cavities[3 * c], dy = sites[3 * s + 1] - cavities[3 * c + 1],
+                     dz = sites[3 * s + 2] - cavities[3 * c + 2];
+        in_cav = in_cav || std::sqrt(dx * dx + dy * dy + dz * dz) <= r->cavity_radius;
+      }
+      if (!inside[s] || in_cav)
+        return fail(TWOS_ERR_RUNTIME, "candidate classified outside; exact driver predicate is also required");
+    }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  const size_t walks = static_cast<size_t>(r->walks);
+  const size_t total = static_cast<size_t>(n_sites) * walks;
+  DevBuf dsamp, dclear, dcenter, dterms;
+  unsigned long long tot[2] = {0, 0};
+  std::vector<double> clearance(n_sites), center(n_sites);
+  RunOut ro;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    m->cavities.reserve(std::max<size_t>(1, n_cav) * 3 * sizeof(double));
+    if (n_cav)
+      check(cudaMemcpyAsync(m->cavities.ptr, cavities, static_cast<size_t>(n_cav) * 3 * sizeof(double),
+                            cudaMemcpyHostToDevice, m->stream),
+            "upload cavities");
+    dterms.reserve(std::max(1, r->n_source) * sizeof(TermDev));
+    if (r->n_source)
+      check(cudaMemcpyAsync(dterms.ptr, r->source, r->n_source * sizeof(TermDev), cudaMemcpyHostToDevice, m->stream),
+            "upload terms");
+    dsamp.reserve(total * sizeof(twos_cert_sample));
+    dclear.reserve(n_sites * sizeof(double));
+    dcenter.reserve(n_sites * sizeof(double));
+    begin_totals(m);
+    ValidateLaunch V{};
+    V.geo = m->geo.as<GeoDesc>();
+    V.sites = m->sites.as<double>();
+    V.n_sites = n_sites;
+    V.walks = static_cast<uint32_t>(walks);
+    V.cavities = m->cavities.as<double>();
+    V.n_cav = n_cav;
+    V.terms = dterms.as<TermDev>();
+    V.n_terms = static_cast<uint32_t>(r->n_source);
+    V.green = r->green == TWOS_SOURCE_GREEN;
+    counter_key(r->seed, r->stream, V.k0, V.k1);
+    V.repeat = r->repeat;
+    V.site_offset = r->site_offset;
+    V.max_steps = r->max_steps;
+    V.epsilon = r->epsilon;
+    V.cavity_radius = r->cavity_radius;
+    V.radius_cap = vp->radius_cap;
+    V.value_cap = vp->value_cap;
+    V.samples = dsamp.as<twos_cert_sample>();
+    V.clearance = dclear.as<double>();
+    V.center_distance = dcenter.as<double>();
+    V.totals = m->totals.as<unsigned long long>() + 3;  // [3] failures, [4] steps
+    V.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    check(cudaEventRecord(m->ev0, m->stream), "event");
+    check(launch_validate(V, m->stream), "validate launch");
+    check(cudaEventRecord(m->ev1, m->stream), "event");
+    ro.launches = 2;
+    check(cudaMemcpyAsync(samples, dsamp.ptr, total * sizeof(twos_cert_sample), cudaMemcpyDeviceToHost, m->stream),
+          "download samples");
+    check(cudaMemcpyAsync(clearance.data(), dclear.ptr, n_sites * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+          "download clearance");
+    check(cudaMemcpyAsync(center.data(), dcenter.ptr, n_sites * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+          "download centre distance");
+    end_totals(m, ro);
+    tot[0] = ro.node_tests;  // totals[3]: containment failures
+    tot[1] = ro.plane_tests; // totals[4]: steps
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
+    ro.kernel_seconds = ro.walk_seconds = ms / 1e3;
+  } catch (const std::exception &e) {
+    for (DevBuf *b : {&dsamp, &dclear, &dcenter, &dterms}) b->release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  for (DevBuf *b : {&dsamp, &dclear, &dcenter, &dterms}) b->release();
+  // Stage statistics: prefixes n in {1024, 4096, 16384, 65536} below walks,
+  // then walks; sums in long double in sample order (minimum_benefit.hpp:160-176).
+  std::vector<uint32_t> ns;
+  for (uint32_t n : {1024u, 4096u, 16384u, 65536u})
+    if (n < walks) ns.push_back(n);
+  ns.push_back(static_cast<uint32_t>(walks));
+  uint64_t caps_total = 0;
+  for (uint32_t s = 0; s < n_sites; ++s) {
+    const twos_cert_sample *v = samples + static_cast<size_t>(s) * walks;
+    long double sum = 0.0L;
+    uint64_t steps = 0, clipped = 0, capped = 0;
+    uint32_t j = 0;
+    for (size_t k = 0; k < ns.size(); ++k) {
+      for (; j < ns[k]; ++j) {
+        sum += v[j].value;
+        steps += v[j].steps;
+        clipped += v[j].clipped;
+        capped += v[j].capped;
+      }
+      twos_validate_stage &st = stages[static_cast<size_t>(s) * TWOS_VALIDATE_MAX_STAGES + k];
+      st.site = s;
+      st.n = ns[k];
+      st.mean = static_cast<double>(sum / ns[k]);
+      st.mean_steps = static_cast<double>(steps) / ns[k];
+      st.clipped = clipped;
+      st.path_caps = capped;
+      st.center_clearance_lower = clearance[s];
+      st.center_distance = center[s];
+    }
+    caps_total += capped;
+  }
+  *n_stages = static_cast<uint32_t>(ns.size());
+  if (summary) {
+    std::memset(summary, 0, sizeof(*summary));
+    summary->kernel_seconds = summary->walk_seconds = ro.kernel_seconds;
+    summary->total_seconds = seconds_since(t0);
+    summary->paths = total;
+    summary->steps = tot[1];
+    summary->caps = caps_total;
+    summary->launches = ro.launches;
+    summary->error_flags = ro.error_flags;
+    summary->node_tests = tot[0];  // containment failures
+  }
+  if (ro.error_flags & TWOS_DEVERR_STACK) return fail(TWOS_ERR_RUNTIME, "BVH traversal stack bound exceeded");
+  if (ro.error_flags & TWOS_DEVERR_ITER) return fail(TWOS_ERR_RUNTIME, "BVH traversal iteration bound exceeded");
+  if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  if (tot[0])
+    return fail(TWOS_ERR_RUNTIME, "sample containment guard failed; validation record must be rejected");
+  return TWOS_OK;
+}
+
 int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device) {
   if (n == 0) return TWOS_OK;
   if (!cases || !out) return fail(TWOS_ERR_USAGE, "null buffer");

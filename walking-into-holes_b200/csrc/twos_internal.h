@@ -265,6 +265,27 @@ cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, 
                        cudaStream_t s);
 int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L);
 cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s);
+// Certified validation walks (validate.cuh), FP64 with directed rounding.
+struct ValidateLaunch {
+  const GeoDesc *geo;          // device descriptor (FP64 BVH and triangles used)
+  const double *sites;         // [n_sites][3]
+  uint32_t n_sites, walks;
+  const double *cavities;      // [n_cav][3]
+  uint32_t n_cav;
+  const TermDev *terms;        // source terms (validated host-side)
+  uint32_t n_terms;
+  int green;                   // 1: Beta(2,2) Green point per step
+  uint32_t k0, k1, repeat, site_offset;
+  int max_steps;
+  double epsilon, cavity_radius, radius_cap, value_cap;
+  twos_cert_sample *samples;   // [n_sites * walks]
+  double *clearance;           // [n_sites] certified distance at the site
+  double *center_distance;     // [n_sites] FP64 domain distance at the site
+  unsigned long long *totals;  // [0] containment failures [1] steps
+  uint32_t *error;
+};
+cudaError_t launch_validate(const ValidateLaunch &V, cudaStream_t s);
+
 // Exact ball integrals of bump sources: cases[4i..4i+3] = (d, r, R, A).
 cudaError_t launch_ball_green(const double *cases, uint32_t n, double *out, uint32_t *error, cudaStream_t s);
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,

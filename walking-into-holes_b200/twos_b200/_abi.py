@@ -26,7 +26,7 @@ EXPORTED = [
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
-    "twos_ball_green_integral",
+    "twos_ball_green_integral", "twos_validate",
 ]
 
 
@@ -101,6 +101,16 @@ class DesignStep(ctypes.Structure):
     ]
 
 
+class ValidateParams(ctypes.Structure):
+    _fields_ = [("radius_cap", ctypes.c_double), ("value_cap", ctypes.c_double)]
+
+
+VALIDATE_MAX_STAGES = 5
+CERT_SAMPLE_DTYPE = [("value", "f8"), ("steps", "u4"), ("capped", "u1"), ("clipped", "u1"), ("contained", "u1"),
+                     ("pad", "u1")]
+VALIDATE_STAGE_DTYPE = [("site", "u4"), ("n", "u4"), ("mean", "f8"), ("mean_steps", "f8"), ("clipped", "u8"),
+                        ("path_caps", "u8"), ("center_clearance_lower", "f8"), ("center_distance", "f8")]
+
 # twos_diff_result / twos_diff_stats as numpy record layouts.
 DIFF_DTYPE = [("dc", "f8", (3,)), ("dc_se", "f8", (3,)), ("dR", "f8"), ("dR_se", "f8")]
 DIFF_STATS_DTYPE = [("outer_steps", "u8"), ("nested_steps", "u8"), ("cavity_terminations", "u8"),
@@ -154,6 +164,8 @@ def load(path: Path | str | None = None):
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
     L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
+    L.twos_validate.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ValidateParams), vp, u32, vp, u32, vp,
+                                vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,
                                ctypes.POINTER(Summary)]
     L.twos_topk_device.argtypes = [vp, vp, u32, u32, vp]

@@ -250,6 +250,36 @@ class Mesh:
             out["error"] = msg
         return rows, stats, out
 
+    def validate(self, sites, config: Config, cavities=None, radius_cap: float = 0.1, value_cap: float = 0.1,
+                 strict: bool = True):
+        """Certified fresh-sample validation (twos_validate; run_minimum_benefit,
+        minimum_benefit.hpp:145-188).  Returns (samples [n_sites, walks] of
+        CERT_SAMPLE_DTYPE, stages [n_sites, n_stages] of VALIDATE_STAGE_DTYPE,
+        summary).  With strict=False a containment failure is reported in
+        summary["error"] with the samples, instead of raised."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        n, w = len(s), int(config.walks)
+        samples = np.zeros((n, w), dtype=_abi.CERT_SAMPLE_DTYPE)
+        stages = np.zeros((n, _abi.VALIDATE_MAX_STAGES), dtype=_abi.VALIDATE_STAGE_DTYPE)
+        n_stages = ctypes.c_uint32(0)
+        req = config.to_request()
+        params = _abi.ValidateParams(float(radius_cap), float(value_cap))
+        summ = Summary()
+        L = _abi.load()
+        rc = L.twos_validate(self._h, ctypes.byref(req), ctypes.byref(params), _ptr(s), n,
+                             _ptr(cav) if len(cav) else None, len(cav), _ptr(samples), _ptr(stages),
+                             ctypes.byref(n_stages), ctypes.byref(summ))
+        out = _summary_dict(summ)
+        out["containment_failures"] = out.pop("node_tests")
+        out["error"] = None
+        if rc != OK:
+            msg = L.twos_last_error().decode(errors="replace")
+            if strict or "containment" not in msg:
+                raise TwosError(rc, msg)
+            out["error"] = msg
+        return samples, stages[:, : n_stages.value].copy(), out
+
     def topk_device(self, d_keys, n, k, d_index):
         def addr(x):
             return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
