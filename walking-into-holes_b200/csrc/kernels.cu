@@ -525,9 +525,13 @@ enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
 // ended refill from the work queue once `refill` lanes are idle.  So lanes
 // never wait for the slowest traversal of the warp, only for the batched
 // step.  MODE: TWOS_MODE_*; the per-walk value type is T (FP32 accumulation
-// in the mixed form, FP64 in the plain form).
-template <typename T, int MODE, bool GREEN, int BLOCK>
+// in the mixed form, FP64 in the plain form).  SRC: TWOS_SOURCE_* (a
+// template argument, so the exact-integral code of TWOS_SOURCE_EXACT adds no
+// registers to the other forms).
+template <typename T, int MODE, int SRC, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_kernel(const WosLaunch L) {
+  constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
+  constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
   // Dynamic shared memory: the traversal stacks (kStack entries per thread,
   // column-major so a warp's accesses hit distinct banks), then the tables.
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -687,7 +691,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
           a = add_scaled(pos, g, r * beta);
         }
-        if (MODE != kModeBoundary && (J.flags & kJobExactSource)) {
+        if (EXACT) {
           u = exact_source(u, s_terms, J.src_begin, J.n_src, pos, r, err);
           if (MODE == TWOS_MODE_PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
         } else {
@@ -902,18 +906,24 @@ cudaError_t launch_site_prepass(int precision, const WosLaunch &L, cudaStream_t 
   return cudaGetLastError();
 }
 
-template <typename T, int MODE, bool GREEN, int BLOCK> static const void *wos_fn() {
-  return reinterpret_cast<const void *>(&wos_kernel<T, MODE, GREEN, BLOCK>);
+template <typename T, int MODE, int SRC, int BLOCK> static const void *wos_fn() {
+  return reinterpret_cast<const void *>(&wos_kernel<T, MODE, SRC, BLOCK>);
 }
 
-template <int BLOCK> static const void *select_wos_block(int precision, int mode, bool green) {
+template <typename T, int MODE, int BLOCK> static const void *select_src(int src) {
+  if (src == TWOS_SOURCE_GREEN) return wos_fn<T, MODE, TWOS_SOURCE_GREEN, BLOCK>();
+  if (src == TWOS_SOURCE_EXACT) return wos_fn<T, MODE, TWOS_SOURCE_EXACT, BLOCK>();
+  return wos_fn<T, MODE, TWOS_SOURCE_CENTER, BLOCK>();
+}
+
+template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src) {
   if (mode == kModeBoundary)
-    return precision == TWOS_PREC_MIXED ? wos_fn<float, kModeBoundary, false, BLOCK>()
-                                        : wos_fn<double, kModeBoundary, false, BLOCK>();
-#define TWOS_PICK(T)                                                                                          \
-  if (mode == TWOS_MODE_COMPLIANCE) return green ? wos_fn<T, 0, true, BLOCK>() : wos_fn<T, 0, false, BLOCK>(); \
-  if (mode == TWOS_MODE_PAIRED) return green ? wos_fn<T, 1, true, BLOCK>() : wos_fn<T, 1, false, BLOCK>();     \
-  return green ? wos_fn<T, 2, true, BLOCK>() : wos_fn<T, 2, false, BLOCK>();
+    return precision == TWOS_PREC_MIXED ? wos_fn<float, kModeBoundary, TWOS_SOURCE_CENTER, BLOCK>()
+                                        : wos_fn<double, kModeBoundary, TWOS_SOURCE_CENTER, BLOCK>();
+#define TWOS_PICK(T)                                                                 \
+  if (mode == TWOS_MODE_COMPLIANCE) return select_src<T, TWOS_MODE_COMPLIANCE, BLOCK>(src); \
+  if (mode == TWOS_MODE_PAIRED) return select_src<T, TWOS_MODE_PAIRED, BLOCK>(src);         \
+  return select_src<T, TWOS_MODE_HOT, BLOCK>(src);
   if (precision == TWOS_PREC_MIXED) {
     TWOS_PICK(float)
   }
@@ -922,14 +932,14 @@ template <int BLOCK> static const void *select_wos_block(int precision, int mode
 }
 
 // Walk kernel instantiations: block sizes 128, 256 and 512 threads.
-static const void *select_wos(int precision, int mode, bool green, int block) {
+static const void *select_wos(int precision, int mode, int src, int block) {
   switch (block) {
     case 128:
-      return select_wos_block<128>(precision, mode, green);
+      return select_wos_block<128>(precision, mode, src);
     case 256:
-      return select_wos_block<256>(precision, mode, green);
+      return select_wos_block<256>(precision, mode, src);
     case 512:
-      return select_wos_block<512>(precision, mode, green);
+      return select_wos_block<512>(precision, mode, src);
     default:
       return nullptr;
   }
@@ -941,12 +951,12 @@ static uint32_t wos_dyn_smem(int precision, const WosLaunch &L, int block) {
                                                : smem_plan<double>(L.n_jobs, L.n_geos, L.n_terms).bytes);
 }
 
-cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
+cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int grid, int block,
                        cudaStream_t s) {
   if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
   if (dyn > 200 * 1024) return cudaErrorInvalidValue;
-  const void *fn = select_wos(precision, mode, green, block);
+  const void *fn = select_wos(precision, mode, src, block);
   if (!fn) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
@@ -955,9 +965,9 @@ cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, 
   return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, dyn, s);
 }
 
-int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L) {
+int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L) {
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
-  const void *fn = select_wos(precision, mode, green, block);
+  const void *fn = select_wos(precision, mode, src, block);
   if (!fn || dyn > 200 * 1024) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;

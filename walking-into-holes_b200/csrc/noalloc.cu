@@ -154,7 +154,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;
     const int block = m->block;
-    const int per_sm = wos_max_blocks_per_sm(r->precision, r->mode, r->green == TWOS_SOURCE_GREEN, block, L);
+    const int per_sm = wos_max_blocks_per_sm(r->precision, r->mode, r->green, block, L);
     if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
     const int grid = std::min(per_sm, m->blocks_per_sm > 0 ? m->blocks_per_sm : per_sm) * m->num_sms;
     FinalizeLaunch F{};
@@ -168,7 +168,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     F.out = d_out;
     check(cudaEventRecord(m->ev0, st), "event");
     check(launch_site_prepass(r->precision, L, st), "site pre-pass");
-    check(launch_wos(r->precision, r->mode, r->green == TWOS_SOURCE_GREEN, L, grid, block, st), "WoS launch");
+    check(launch_wos(r->precision, r->mode, r->green, L, grid, block, st), "WoS launch");
     check(cudaEventRecord(m->evw, st), "event");
     check(launch_finalize(r->precision, r->mode, F, st), "finalize launch");
     check(cudaEventRecord(m->ev1, st), "event");

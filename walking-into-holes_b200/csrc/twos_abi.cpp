@@ -262,7 +262,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   const bool mixed = r0->precision == TWOS_PREC_MIXED;
   const int mode = r0->mode;
   const bool paired = mode == TWOS_MODE_PAIRED;
-  const bool green = r0->green == TWOS_SOURCE_GREEN;
+  const int green = r0->green;
   std::vector<JobDesc> jobs;
   std::vector<GeoDesc> geos;
   std::vector<twos_mesh *> geo_mesh;
@@ -825,22 +825,22 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     D.iteration = iter.as<uint32_t>();
     D.history = hist.as<DesignStep>();
     const int block = m->block;
-    const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green == TWOS_SOURCE_GREEN, block, Ls);
-    const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green == TWOS_SOURCE_GREEN, block, Lv);
+    const int per_s = wos_max_blocks_per_sm(rs.precision, rs.mode, rs.green, block, Ls);
+    const int per_v = wos_max_blocks_per_sm(rv.precision, rv.mode, rv.green, block, Lv);
     if (per_s <= 0 || per_v <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
     const int cap = m->blocks_per_sm > 0 ? m->blocks_per_sm : 1 << 20;
     const int grid_s = std::min(per_s, cap) * m->num_sms, grid_v = std::min(per_v, cap) * m->num_sms;
     auto iteration = [&]() {
       check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
       check(launch_site_prepass(rs.precision, Ls, m->stream), "scout pre-pass");
-      check(launch_wos(rs.precision, rs.mode, rs.green == TWOS_SOURCE_GREEN, Ls, grid_s, block, m->stream), "scout launch");
+      check(launch_wos(rs.precision, rs.mode, rs.green, Ls, grid_s, block, m->stream), "scout launch");
       check(launch_finalize(rs.precision, rs.mode, Fs, m->stream), "scout finalize");
       check(launch_design_keys(D, m->stream), "keys");
       check(launch_topk(D.keys, n, k, idx.as<uint32_t>(), topk.ptr, topk.bytes, m->stream), "top-k");
       check(launch_design_gather(D, m->stream), "gather");
       check(cudaMemsetAsync(m->counter.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
       check(launch_site_prepass(rv.precision, Lv, m->stream), "validate pre-pass");
-      check(launch_wos(rv.precision, rv.mode, rv.green == TWOS_SOURCE_GREEN, Lv, grid_v, block, m->stream), "validate launch");
+      check(launch_wos(rv.precision, rv.mode, rv.green, Lv, grid_v, block, m->stream), "validate launch");
       check(launch_finalize(rv.precision, rv.mode, Fv, m->stream), "validate finalize");
       check(launch_design_select(D, m->stream), "select");
       check(launch_design_mask(D, m->stream), "mask");
@@ -1163,7 +1163,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.site_best2 = nullptr;
         L.total_sites = count;
         const int mode = pass == 0 ? kModeBoundary : TWOS_MODE_COMPLIANCE;
-        const bool green = pass == 1 && rq->green == TWOS_SOURCE_GREEN;
+        const int green = pass == 1 ? rq->green : TWOS_SOURCE_CENTER;
         if (pass == 0) {
           L.hits = hits.as<HitRec>();
           L.steps_out = osteps.as<uint32_t>();

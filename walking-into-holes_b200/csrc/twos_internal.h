@@ -261,9 +261,9 @@ cudaError_t launch_design_select(const DesignLaunch &D, cudaStream_t s);
 cudaError_t launch_design_mask(const DesignLaunch &D, cudaStream_t s);
 
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
-cudaError_t launch_wos(int precision, int mode, bool green, const WosLaunch &L, int grid, int block,
+cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int grid, int block,
                        cudaStream_t s);
-int wos_max_blocks_per_sm(int precision, int mode, bool green, int block, const WosLaunch &L);
+int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L);
 cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s);
 // Certified validation walks (validate.cuh), FP64 with directed rounding.
 struct ValidateLaunch {
