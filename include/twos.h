@@ -65,14 +65,18 @@ enum { TWOS_PREC_FP64 = 0, TWOS_PREC_MIXED = 1 };
  *   BUMP   amp * max(0, 1 - |x-c|^2/w0^2)^2 / div   (sensor, adjoint.cpp:11-15,
  *                                                    study.cpp:45-47)
  *   BOX    amp if c <= x <= w componentwise, else 0
- *   BALL   amp if |x - c| <= w0, else 0 */
+ *   BALL   amp if |x - c| <= w0, else 0
+ *   QUAD   amp * sum_k w_k (x_k - c_k)^2            (harmonic when sum w = 0;
+ *                                                    boundary data, no
+ *                                                    reference counterpart) */
 enum {
   TWOS_TERM_CONST = 0,
   TWOS_TERM_LINEAR = 1,
   TWOS_TERM_GAUSS = 2,
   TWOS_TERM_BUMP = 3,
   TWOS_TERM_BOX = 4,
-  TWOS_TERM_BALL = 5
+  TWOS_TERM_BALL = 5,
+  TWOS_TERM_QUAD = 6
 };
 
 /* Per-step source integral over the walk's ball B_r(y), added to u (p):
@@ -123,9 +127,16 @@ typedef struct twos_request {
   int32_t skip_cavity_sites; /* 1: sites inside a cavity get all-zero rows
                                 (adjoint.cpp:123-126) */
   uint32_t site_offset;      /* added to the site index in the sample key */
-  uint32_t reserved;
+  uint32_t n_boundary;       /* terms of the primal's Dirichlet data g on the
+                                mesh (0: u = 0 there, as the reference) */
   twos_source_term source[TWOS_MAX_TERMS];
   twos_source_term adjoint[TWOS_MAX_TERMS];
+  /* Dirichlet data of u on the mesh surface, added to a walk's u at its exit
+   * point (the nearest surface point when the walk stops within epsilon of
+   * the mesh; cavities keep u = 0).  No reference counterpart: the
+   * reference's walks carry zero terminal data.  The adjoint keeps zero
+   * data. */
+  twos_source_term boundary[TWOS_MAX_TERMS];
 } twos_request;
 
 /* Per-site result (SiteResult wih_twos.cpp:666-672 and PairValue
@@ -368,6 +379,34 @@ typedef struct twos_diff_stats {
 int twos_diffwos(twos_mesh *mesh, const twos_request *request, double diff_offset, int enclosure_fallback,
                  const double *sites, uint32_t n_sites, const double *cavities, uint32_t n_cavities,
                  twos_diff_result *out, twos_diff_stats *stats, twos_summary *summary);
+
+/* Gradient estimates and the cross-index gradient product (the Neumann-
+ * cavity topological derivative of the plain method, BASELINE config 1; no
+ * reference counterpart: the reference implements only Dirichlet cavities,
+ * paper/sections/03_problem.tex:153).  A paired request (source = the
+ * primal's f, adjoint = the adjoint's source q, boundary = the primal's
+ * Dirichlet data; green CENTER or GREEN) runs one walk set; each walk i
+ * gives gradient samples at the site from its first ball B_R(x):
+ *   grad U_i = (3/R) U'_i w + R (1 - t^3) f(x + t R w') w'
+ * with w the first step direction, U'_i the walk's u after its first step
+ * (the sphere term of the mean-value gradient formula), and t ~ U(0,1), w'
+ * uniform an extra draw for the ball's source term (the gradient of the
+ * ball's Green function, sampled with a bounded weight); likewise grad P_i.
+ * cross = sum_{i != j} grad U_i . grad P_j / (N (N-1)) estimates
+ * grad u . grad p without the i = j bias, with its leave-one-out jackknife
+ * SE.  For a small Neumann sphere at x the topological derivative of
+ * J = int q u is D_T = (3/2) grad u . grad p - q(x) u(x) (the dipole of a
+ * Neumann sphere in a uniform field, 3D polarization 3/2). */
+typedef struct twos_gradient_result {
+  double u, p;
+  double grad_u[3], grad_p[3];
+  double cross, cross_se;
+  uint64_t steps, caps;
+} twos_gradient_result; /* 96 bytes */
+
+int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const double *sites, uint32_t n_sites,
+                           const double *cavities, uint32_t n_cavities, twos_gradient_result *out,
+                           twos_summary *summary);
 
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid

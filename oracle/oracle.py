@@ -54,6 +54,7 @@ class Params(ctypes.Structure):
         ("skip_cavity_sites", ctypes.c_int32), ("weight_order", ctypes.c_int32),
         ("threads", ctypes.c_int32),
         ("source", Term * 8), ("adjoint", Term * 8),
+        ("n_boundary", ctypes.c_int32), ("pad", ctypes.c_int32), ("boundary", Term * 8),
     ]
 
 
@@ -101,6 +102,9 @@ def lib():
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p]
         L.oracle_exact_bump_green.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_estimate_gradient.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+            ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_validate.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
@@ -252,6 +256,10 @@ class OracleMesh:
         p.skip_cavity_sites = int(kw.get("skip_cavity_sites", p.mode != MODE_COMPLIANCE))
         p.weight_order = kw.get("weight_order", 0 if p.mode == MODE_COMPLIANCE else 1)
         p.threads = kw.get("threads", 0)
+        bnd = kw.get("boundary", [])
+        p.n_boundary = len(bnd)
+        for i, t in enumerate(bnd):
+            p.boundary[i] = t
         return p
 
     def walk_samples(self, sites, site_ids=None, cavities=None, count_tests=False, **kw):
@@ -291,6 +299,28 @@ class OracleMesh:
         if rc:
             raise RuntimeError(lib().oracle_last_error().decode())
         return out, stats, totals
+
+    def estimate_gradient(self, sites, cavities=None, samples=False, **kw):
+        """The GPU gradient form in the counter stream (rng must be the counter
+        stream): rows (u, p, grad_u, grad_p, cross, cross_se), steps/caps, and
+        optionally the per-walk samples [n, walks, 8]."""
+        p = self._params(**kw)
+        if p.rng != RNG_COUNTER:
+            raise ValueError("the gradient form is defined in the counter stream")
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        rows = np.zeros((len(s), 10))
+        counts = np.zeros((len(s), 2), dtype=np.uint64)
+        walks = np.zeros((len(s), p.walks, 8)) if samples else None
+        rc = lib().oracle_estimate_gradient(self.handle, ctypes.byref(p), _ptr(s), len(s), _ptr(cav), len(cav),
+                                            _ptr(rows), _ptr(counts), _ptr(walks))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        out = {"u": rows[:, 0], "p": rows[:, 1], "grad_u": rows[:, 2:5], "grad_p": rows[:, 5:8], "cross": rows[:, 8],
+               "cross_se": rows[:, 9], "steps": counts[:, 0], "caps": counts[:, 1]}
+        if samples:
+            out["samples"] = walks
+        return out
 
     def validate(self, sites, radius_cap, value_cap, site_ids=None, cavities=None, **kw):
         """Certified fresh samples (minimum_benefit.hpp cert_walk) at each site:

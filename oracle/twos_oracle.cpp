@@ -350,6 +350,10 @@ double term_value(const Term &t, const Vec3 &x) {
       const Vec3 d{x.x - t.c[0], x.y - t.c[1], x.z - t.c[2]};
       return dot(d, d) <= t.w[0] * t.w[0] ? t.amp : 0.0;
     }
+    case 6: {  // amp * sum_k w_k (x_k - c_k)^2
+      const double a = x.x - t.c[0], b = x.y - t.c[1], c = x.z - t.c[2];
+      return t.amp * (t.w[0] * (a * a) + t.w[1] * (b * b) + t.w[2] * (c * c));
+    }
     default:
       return 0.0;
   }
@@ -525,6 +529,9 @@ struct oracle_params {
   int32_t threads;
   Term source[8];
   Term adjoint[8];
+  int32_t n_boundary;  // Dirichlet data of u on the mesh (gradient form)
+  int32_t pad;
+  Term boundary[8];
 };
 
 struct oracle_site {
@@ -1412,6 +1419,182 @@ int oracle_validate(const oracle_mesh *om, const oracle_params *o, double radius
       steps[slot] = static_cast<uint32_t>(c.steps);
       flags[slot] = static_cast<uint8_t>((c.capped ? 1 : 0) | (c.clipped ? 2 : 0) | (c.contained ? 0 : 4));
     }
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+// ================================================================ gradient form
+// The GPU's gradient form (twos_estimate_gradient) in the counter stream:
+// paired walks whose first ball gives the gradient samples
+//   grad U = (3/R) (U - u0) w + R (1 - t^3) f(x + t R w') w'
+// (likewise grad P with the adjoint source), plus Dirichlet data g of u at
+// the exit point on the mesh.  No reference counterpart: this is the plain
+// method's Neumann-cavity estimator.
+
+namespace {
+
+struct GradWalk {
+  double u = 0.0, p = 0.0, gu[3] = {0, 0, 0}, gp[3] = {0, 0, 0};
+  uint32_t steps = 0;
+  bool cap = false, failed = false;
+};
+
+GradWalk grad_walk(const Mesh &m, const oracle_params &o, const double *cav, uint32_t ncav, Vec3 y, uint64_t site,
+                   uint32_t sample) {
+  GradWalk out;
+  CounterStream cs;
+  counter_key(o.seed, o.stream, cs.k0, cs.k1);
+  cs.walk = sample;
+  cs.site = static_cast<uint32_t>(site);
+  cs.repeat = o.repeat;
+  double r0 = 0.0, u0 = 0.0, p0 = 0.0;
+  Vec3 w0, su, sp;
+  for (int k = 0; k < o.max_steps; ++k) {
+    const Closest c = closest_point(m, y, o.query_radius, nullptr);
+    if (!std::isfinite(c.distance)) out.failed = true;
+    double r = c.distance;
+    bool cav_nearer = false;
+    for (uint32_t i = 0; i < ncav; ++i) {
+      const Vec3 cc{cav[3 * i], cav[3 * i + 1], cav[3 * i + 2]};
+      const double dc = norm(y - cc) - o.cavity_radius;
+      r = std::min(r, dc);
+      if (dc < c.distance) cav_nearer = true;
+    }
+    if (!(r > o.epsilon)) {
+      // Exit: Dirichlet data at the nearest mesh point (the walk's position
+      // when it stops at its first query, as the device does).
+      if (o.n_boundary > 0 && !cav_nearer) out.u += source_value(o.boundary, o.n_boundary, k == 0 ? y : c.point);
+      break;
+    }
+    double a0, a1;
+    cs.uniforms(static_cast<uint32_t>(k), 0, a0, a1);
+    Vec3 a = y;
+    if (o.green) {
+      double g0, g1, b0, b1, b2, spare;
+      cs.uniforms(static_cast<uint32_t>(k), 1, g0, g1);
+      cs.uniforms(static_cast<uint32_t>(k), 2, b0, b1);
+      cs.uniforms(static_cast<uint32_t>(k), 3, b2, spare);
+      a = y + direction_from(g0, g1) * (r * median3(b0, b1, b2));
+    }
+    const double w = r * r / 6.0;
+    const double du = w * source_value(o.source, o.n_source, a), dp = w * source_value(o.adjoint, o.n_adjoint, a);
+    out.u += du;
+    out.p += dp;
+    const Vec3 dir = direction_from(a0, a1);
+    if (k == 0) {
+      double t, b0, b1, spare;
+      cs.uniforms(0, 4, t, b0);
+      cs.uniforms(0, 5, b1, spare);
+      const Vec3 wp = direction_from(b0, b1);
+      const Vec3 z = y + wp * (t * r);
+      const double wt = r * (1.0 - t * t * t);
+      const double fs = wt * source_value(o.source, o.n_source, z);
+      const double fq = wt * source_value(o.adjoint, o.n_adjoint, z);
+      su = wp * fs;
+      sp = wp * fq;
+      r0 = r;
+      u0 = du;
+      p0 = dp;
+      w0 = dir;
+    }
+    y = y + dir * r;
+    ++out.steps;
+    if (k + 1 == o.max_steps) out.cap = true;
+  }
+  if (r0 > 0.0) {
+    const double kf = 3.0 / r0, cu = kf * (out.u - u0), cp = kf * (out.p - p0);
+    const Vec3 gu = w0 * cu + su, gp = w0 * cp + sp;
+    out.gu[0] = gu.x;
+    out.gu[1] = gu.y;
+    out.gu[2] = gu.z;
+    out.gp[0] = gp.x;
+    out.gp[1] = gp.y;
+    out.gp[2] = gp.z;
+  }
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per-site gradient rows (GRADIENT layout: u, p, grad_u[3], grad_p[3],
+// cross, cross_se as doubles; steps, caps as uint64 in a separate array),
+// and optionally the per-walk samples (u, p, grad_u, grad_p: 8 doubles).
+int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, const double *sites, uint32_t n_sites,
+                             const double *cav, uint32_t ncav, double *rows, uint64_t *counts, double *walks) {
+  std::atomic<int> failed{0};
+  const int N = o->walks;
+#ifdef _OPENMP
+  if (o->threads > 0) omp_set_num_threads(o->threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int64_t s = 0; s < static_cast<int64_t>(n_sites); ++s) {
+    const Vec3 x{sites[3 * s], sites[3 * s + 1], sites[3 * s + 2]};
+    std::vector<GradWalk> W(N);
+    for (int j = 0; j < N; ++j) {
+      W[j] = grad_walk(om->m, *o, cav, ncav, x, static_cast<uint64_t>(s), static_cast<uint32_t>(j));
+      if (W[j].failed) failed = 1;
+    }
+    double su = 0, sp = 0, sgu[3] = {0, 0, 0}, sgp[3] = {0, 0, 0}, sdot = 0;
+    uint64_t steps = 0, caps = 0;
+    for (const GradWalk &g : W) {
+      su += g.u;
+      sp += g.p;
+      double d = 0;
+      for (int k = 0; k < 3; ++k) {
+        sgu[k] += g.gu[k];
+        sgp[k] += g.gp[k];
+        d += g.gu[k] * g.gp[k];
+      }
+      sdot += d;
+      steps += g.steps;
+      caps += g.cap;
+    }
+    const double n = N;
+    const double cross = (sgu[0] * sgp[0] + sgu[1] * sgp[1] + sgu[2] * sgp[2] - sdot) / (n * (n - 1.0));
+    std::vector<double> leave(N);
+    double mean = 0;
+    for (int j = 0; j < N; ++j) {
+      const GradWalk &g = W[j];
+      double d = 0, c = 0;
+      for (int k = 0; k < 3; ++k) {
+        d += g.gu[k] * g.gp[k];
+        c += (sgu[k] - g.gu[k]) * (sgp[k] - g.gp[k]);
+      }
+      leave[j] = (c - (sdot - d)) / ((n - 1.0) * (n - 2.0));
+      mean += leave[j];
+    }
+    mean /= n;
+    double spread = 0;
+    for (double v : leave) spread += (v - mean) * (v - mean);
+    double *row = rows + 10 * s;
+    row[0] = su / n;
+    row[1] = sp / n;
+    for (int k = 0; k < 3; ++k) {
+      row[2 + k] = sgu[k] / n;
+      row[5 + k] = sgp[k] / n;
+    }
+    row[8] = cross;
+    row[9] = N > 2 ? std::sqrt((n - 1.0) / n * spread) : 0.0;
+    counts[2 * s] = steps;
+    counts[2 * s + 1] = caps;
+    if (walks)
+      for (int j = 0; j < N; ++j) {
+        double *w = walks + (static_cast<size_t>(s) * N + j) * 8;
+        w[0] = W[j].u;
+        w[1] = W[j].p;
+        for (int k = 0; k < 3; ++k) {
+          w[2 + k] = W[j].gu[k];
+          w[5 + k] = W[j].gp[k];
+        }
+      }
+  }
+  if (failed) {
+    g_error = "closest-point query failed";
+    return 1;
   }
   return 0;
 }

@@ -1,0 +1,117 @@
+"""The gradient form (twos_estimate_gradient): first-ball gradient samples,
+Dirichlet boundary data and the cross-index gradient product behind the
+Neumann-cavity topological derivative of the plain method (
+unit-sphere icosphere L4, g = x0^2 - x1^2 + 0.5 x2, adjoint source the mean
+over r < 0.5, 64 sites uniform in r < 0.9 from seed 0, 1024 walks, eps 1e-4,
+FP64).  The reference has no Neumann cavity, so the checks are the oracle
+(counter stream) and the analytic fields: u = g (harmonic), grad u =
+(2 x0, -2 x1, 0.5), p radial with grad p = -x/(3|B|) inside r < 0.5 and
+-x/(4 pi r^3) outside, and D_T = (3/2) grad u . grad p - q(x) u(x).
+
+Tolerances
+* FP64 form vs the oracle in the shared counter stream: steps identical,
+  rows to rtol 1e-9 (sincospi against cos/sin).
+* Analytic: the cross statistic's z = (estimate - grad u . grad p) / SE
+  within 4.5 everywhere, |z| < 3 for >= 95 % of sites, |mean z| < 0.6; u
+  within 0.03 of g on average (Monte Carlo at 1024 walks plus the inscribed
+  polyhedron).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tb(lib_built):
+    import twos_b200
+    return twos_b200
+
+
+def c1_setup(tb):
+    V, F = tb.geometry.icosphere(4)
+    rng = np.random.default_rng(0)
+    d = rng.normal(size=(64, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    sites = d * (0.9 * rng.random(64) ** (1 / 3))[:, None]
+    boundary = tb.sources.quadratic((1.0, -1.0, 0.0)) + tb.sources.linear(0.5, 2)
+    q = tb.sources.ball_mean_density((0.0, 0.0, 0.0), 0.5)
+    return V, F, sites, boundary, q
+
+
+def analytic(sites):
+    x0, x1, x2 = sites.T
+    g = x0 ** 2 - x1 ** 2 + 0.5 * x2
+    grad_g = np.c_[2 * x0, -2 * x1, 0.5 * np.ones(len(sites))]
+    r = np.linalg.norm(sites, axis=1)
+    a = 0.5
+    c = 1.0 / (4.0 / 3.0 * np.pi * a ** 3)
+    grad_p = np.where(r[:, None] < a, -c * sites / 3.0, -sites / (4.0 * np.pi * r[:, None] ** 3))
+    q = np.where(r < a, c, 0.0)
+    return g, grad_g, grad_p, q
+
+
+def _oracle_terms(oracle_mod, terms):
+    return [oracle_mod.term(t.kind, t.amp, t.axis, t.offset, t.div, tuple(t.c), tuple(t.w)) for t in terms]
+
+
+def test_gradient_fp64_equals_oracle(tb, oracle_mod):
+    V, F, sites, boundary, q = c1_setup(tb)
+    V3, F3 = tb.geometry.icosphere(3)
+    s = sites[:12]
+    holes = np.array([[0.3, 0.3, 0.0]])
+    cfg = tb.Config(walks=64, mode="paired", precision="fp64", seed=17, epsilon=1e-4, max_steps=4096, green=True,
+                    source=tb.sources.constant(0.5), adjoint=q, boundary=boundary, cavity_radius=0.08)
+    with tb.Mesh(V3, F3) as mesh:
+        rows, summ = mesh.estimate_gradient(s, cfg, cavities=holes)
+    o = oracle_mod.OracleMesh(V3, F3).estimate_gradient(
+        s, cavities=holes, rng=oracle_mod.RNG_COUNTER, mode=1, walks=64, seed=17, epsilon=1e-4, max_steps=4096,
+        green=True, cavity_radius=0.08, source=_oracle_terms(oracle_mod, cfg.source),
+        adjoint=_oracle_terms(oracle_mod, q), boundary=_oracle_terms(oracle_mod, boundary))
+    np.testing.assert_array_equal(rows["steps"], o["steps"])
+    for k in ("u", "p", "grad_u", "grad_p", "cross", "cross_se"):
+        np.testing.assert_allclose(rows[k], o[k], rtol=1e-9, atol=1e-12, err_msg=k)
+    assert summ["launches"] == 3
+
+
+def test_config1_neumann_topological_derivative(tb):
+    V, F, sites, boundary, q = c1_setup(tb)
+    cfg = tb.Config(walks=1024, mode="paired", precision="fp64", seed=5, epsilon=1e-4, max_steps=4096, green=True,
+                    source=[], adjoint=q, boundary=boundary)
+    with tb.Mesh(V, F) as mesh:
+        rows, summ = mesh.estimate_gradient(sites, cfg)
+    g, grad_g, grad_p, qx = analytic(sites)
+    assert summ["caps"] == 0
+    assert np.mean(np.abs(rows["u"] - g)) < 0.03
+    exact = np.sum(grad_g * grad_p, axis=1)
+    z = (rows["cross"] - exact) / rows["cross_se"]
+    assert np.max(np.abs(z)) < 4.5, np.max(np.abs(z))
+    assert np.mean(np.abs(z) < 3.0) >= 0.95
+    assert abs(np.mean(z)) < 0.6
+    # The topological derivative assembled from the estimates.
+    td = 1.5 * rows["cross"] - qx * rows["u"]
+    td_exact = 1.5 * exact - qx * g
+    assert np.corrcoef(td, td_exact)[0, 1] > 0.9
+
+
+def test_gradient_mixed_shares_samples(tb):
+    V, F, sites, boundary, q = c1_setup(tb)
+    base = dict(walks=512, mode="paired", seed=9, epsilon=1e-4, max_steps=4096, green=True, source=[], adjoint=q,
+                boundary=boundary)
+    with tb.Mesh(V, F) as mesh:
+        r64, _ = mesh.estimate_gradient(sites[:32], tb.Config(precision="fp64", **base))
+        r32, _ = mesh.estimate_gradient(sites[:32], tb.Config(precision="mixed", **base))
+    se = np.sqrt(r64["cross_se"] ** 2 + r32["cross_se"] ** 2)
+    assert np.all(np.abs(r64["cross"] - r32["cross"]) <= 2.0 * se + 1e-12)
+
+
+def test_gradient_usage_errors(tb):
+    V, F, sites, boundary, q = c1_setup(tb)
+    with tb.Mesh(V, F) as mesh:
+        with pytest.raises(tb.TwosError, match="paired"):
+            mesh.estimate_gradient(sites[:2], tb.Config(walks=8, mode="compliance", boundary=boundary))
+        with pytest.raises(tb.TwosError, match="centre or the Green"):
+            mesh.estimate_gradient(sites[:2], tb.Config(walks=8, mode="paired", green="exact",
+                                                        adjoint=tb.sources.constant(1.0)))
+        with pytest.raises(tb.TwosError, match="Dirichlet boundary data"):
+            mesh.estimate(sites[:2], tb.Config(walks=8, boundary=boundary))

@@ -412,6 +412,10 @@ template <typename T> __device__ __forceinline__ T term_value(const TermT<T> &t,
       const T dd = d.x * d.x + d.y * d.y + d.z * d.z;
       return dd <= t.w[0] * t.w[0] ? t.amp : T(0);
     }
+    case TWOS_TERM_QUAD: {
+      const T a = x.x - t.c[0], b = x.y - t.c[1], c = x.z - t.c[2];
+      return t.amp * (t.w[0] * (a * a) + t.w[1] * (b * b) + t.w[2] * (c * c));
+    }
     default:
       return T(0);
   }
@@ -532,6 +536,8 @@ template <typename T, int MODE, int SRC, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
+  constexpr bool GRAD = MODE == kModeGradient;
+  constexpr bool PAIRED = MODE == TWOS_MODE_PAIRED || GRAD;
   // Dynamic shared memory: the traversal stacks (kStack entries per thread,
   // column-major so a warp's accesses hit distinct banks), then the tables.
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -573,6 +579,10 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
   uint32_t job = 0, site = 0, walk = 0, steps = 0;
   Vec<T> pos{T(0), T(0), T(0)};
   T u = T(0), pv = T(0);
+  // Gradient mode: first-ball radius, direction and payoff increments, and
+  // the ball source terms of grad U / grad P.
+  T g_r0 = T(0), g_u0 = T(0), g_p0 = T(0);
+  Vec<T> g_w0{T(0), T(0), T(0)}, g_su{T(0), T(0), T(0)}, g_sp{T(0), T(0), T(0)};
   // Query state.
   T best2 = T(0);
   int node = 0, sp = 0;
@@ -613,6 +623,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           pv = T(0);
           steps = 0;
           tri_ok = false;
+          if (GRAD) g_r0 = T(0);
           if (!skip && (J.flags & kJobSkipCavitySites)) {
             const T R = to_T<T>(J.cavity_radius);
             for (uint32_t c = 0; c < J.n_cav; ++c) {
@@ -623,7 +634,9 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           }
           if (skip) {
             if (MODE != kModeBoundary) static_cast<T *>(L.u_out)[wid] = T(0);
-            if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+            if (PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+            if (GRAD)
+              for (int k = 0; k < 6; ++k) static_cast<T *>(L.grad_out)[6ull * wid + k] = T(0);
             if (MODE == kModeBoundary) L.hits[wid].cavity = -2;
             L.steps_out[wid] = 0u;
           } else if (L.site_best2 && MODE != kModeBoundary) {
@@ -659,6 +672,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
       const T R = to_T<T>(J.cavity_radius);
       const T dmesh = d;
       int hit_cav = -1;
+      bool cav_nearer = false;  // gradient mode: the exit is on a cavity
       for (uint32_t c = 0; c < J.n_cav; ++c) {
         const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
         const Vec<T> dv = sub(pos, cc);
@@ -672,6 +686,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           }
         } else {
           d = dc < d ? dc : d;
+          if (GRAD && dc < dmesh) cav_nearer = true;
         }
       }
       // The mixed form shrinks the radius by the FP32 distance error bound;
@@ -693,13 +708,38 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
         }
         if (EXACT) {
           u = exact_source(u, s_terms, J.src_begin, J.n_src, pos, r, err);
-          if (MODE == TWOS_MODE_PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
+          if (PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
         } else {
           const T w = r * r / T(6);
-          if (MODE != kModeBoundary) u = u + w * source_value(s_terms, J.src_begin, J.n_src, a);
-          if (MODE == TWOS_MODE_PAIRED) pv = pv + w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+          if (MODE != kModeBoundary) {
+            const T du = w * source_value(s_terms, J.src_begin, J.n_src, a);
+            u = u + du;
+            if (GRAD && steps == 0) g_u0 = du;
+          }
+          if (PAIRED) {
+            const T dp = w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+            pv = pv + dp;
+            if (GRAD && steps == 0) g_p0 = dp;
+          }
         }
         const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
+        if (GRAD && steps == 0) {
+          // First ball: the sphere term's radius and direction, and one draw
+          // (blocks 4-5) for the ball source term of the gradient,
+          // R (1 - t^3) f(x + t R w') w' with t ~ U(0,1), w' uniform.
+          const Philox4 q4 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 4u);
+          const Philox4 q5 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 5u);
+          const T t = uniform<T>(q4.x, q4.y);
+          const Vec<T> wp = direction<T>(uniform<T>(q4.z, q4.w), uniform<T>(q5.x, q5.y));
+          const Vec<T> z = add_scaled(pos, wp, t * r);
+          const T wt = r * (T(1) - t * t * t);
+          const T fs = wt * source_value(s_terms, J.src_begin, J.n_src, z);
+          const T fq = wt * source_value(s_terms, J.adj_begin, J.n_adj, z);
+          g_su = {wp.x * fs, wp.y * fs, wp.z * fs};
+          g_sp = {wp.x * fq, wp.y * fq, wp.z * fq};
+          g_r0 = r;
+          g_w0 = dir;
+        }
         pos = add_scaled(pos, dir, r);
         ++steps;
         if (static_cast<int>(steps) >= J.max_steps) {
@@ -744,9 +784,34 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
           h.normal[2] = static_cast<double>(nrm.z);
           L.hits[wid] = h;
         } else {
+          if (GRAD) {
+            // Dirichlet data of u at the exit point on the mesh.
+            if (!cap && found && J.n_bnd > 0 && !cav_nearer) {
+              Vec<T> q = pos;
+              if (tri_ok) {
+                Vec<T> ta, tb, tc;
+                load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+                q = tri_closest(pos, ta, tb, tc);
+              }
+              u = u + source_value(s_terms, J.bnd_begin, J.n_bnd, q);
+            }
+            T *go = static_cast<T *>(L.grad_out) + 6ull * wid;
+            if (g_r0 > T(0)) {
+              const T k = T(3) / g_r0;
+              const T cu = k * (u - g_u0), cp = k * (pv - g_p0);
+              go[0] = g_w0.x * cu + g_su.x;
+              go[1] = g_w0.y * cu + g_su.y;
+              go[2] = g_w0.z * cu + g_su.z;
+              go[3] = g_w0.x * cp + g_sp.x;
+              go[4] = g_w0.y * cp + g_sp.y;
+              go[5] = g_w0.z * cp + g_sp.z;
+            } else {
+              for (int k = 0; k < 6; ++k) go[k] = T(0);
+            }
+          }
           static_cast<T *>(L.u_out)[wid] = u;
         }
-        if (MODE == TWOS_MODE_PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
+        if (PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
         L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
         phase = kIdle;
       } else {
@@ -923,6 +988,7 @@ template <int BLOCK> static const void *select_wos_block(int precision, int mode
 #define TWOS_PICK(T)                                                                 \
   if (mode == TWOS_MODE_COMPLIANCE) return select_src<T, TWOS_MODE_COMPLIANCE, BLOCK>(src); \
   if (mode == TWOS_MODE_PAIRED) return select_src<T, TWOS_MODE_PAIRED, BLOCK>(src);         \
+  if (mode == kModeGradient) return select_src<T, kModeGradient, BLOCK>(src);               \
   return select_src<T, TWOS_MODE_HOT, BLOCK>(src);
   if (precision == TWOS_PREC_MIXED) {
     TWOS_PICK(float)
@@ -1097,6 +1163,111 @@ __global__ void __launch_bounds__(256) finalize_kernel(const FinalizeLaunch F) {
       }
     }
   }
+}
+
+// Gradient mode: one warp per site (warp_sum: a fixed xor-tree order).  Pass 1: sums of u, p, grad u, grad p
+// and grad u . grad p; pass 2: the leave-one-out cross statistics and their
+// mean; pass 3: the jackknife variance.  FP64 throughout.
+template <typename V> __global__ void __launch_bounds__(256) grad_finalize_kernel(const GradFinalizeLaunch F) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  const V *u = static_cast<const V *>(F.u), *p = static_cast<const V *>(F.p), *g = static_cast<const V *>(F.grad);
+  const uint32_t N = F.walks;
+  const double n = static_cast<double>(N);
+  for (uint64_t site = warp; site < F.n_sites; site += nwarps) {
+    const uint64_t base = site * N;
+    double su = 0, sp = 0, sgu[3] = {0, 0, 0}, sgp[3] = {0, 0, 0}, sdot = 0;
+    unsigned long long steps = 0, caps = 0;
+    for (uint32_t w = lane; w < N; w += 32) {
+      const uint64_t i = base + w;
+      su += static_cast<double>(u[i]);
+      sp += static_cast<double>(p[i]);
+      double d = 0;
+      for (int k = 0; k < 3; ++k) {
+        const double a = static_cast<double>(g[6 * i + k]), b = static_cast<double>(g[6 * i + 3 + k]);
+        sgu[k] += a;
+        sgp[k] += b;
+        d += a * b;
+      }
+      sdot += d;
+      const uint32_t st = F.steps[i];
+      steps += st & 0x7fffffffu;
+      caps += st >> 31;
+    }
+    su = warp_sum(su);
+    sp = warp_sum(sp);
+    for (int k = 0; k < 3; ++k) {
+      sgu[k] = warp_sum(sgu[k]);
+      sgp[k] = warp_sum(sgp[k]);
+    }
+    sdot = warp_sum(sdot);
+    const double den = n * (n - 1.0);
+    const double cross = (sgu[0] * sgp[0] + sgu[1] * sgp[1] + sgu[2] * sgp[2] - sdot) / den;
+    // Leave-one-out: ((S_u - g_i).(S_p - h_i) - (S_dot - g_i.h_i)) / ((N-1)(N-2)).
+    const double den1 = (n - 1.0) * (n - 2.0);
+    double s1 = 0, s2 = 0;
+    if (N > 2) {
+      for (uint32_t w = lane; w < N; w += 32) {
+        const uint64_t i = base + w;
+        double a[3], b[3], d = 0;
+        for (int k = 0; k < 3; ++k) {
+          a[k] = static_cast<double>(g[6 * i + k]);
+          b[k] = static_cast<double>(g[6 * i + 3 + k]);
+          d += a[k] * b[k];
+        }
+        const double c = ((sgu[0] - a[0]) * (sgp[0] - b[0]) + (sgu[1] - a[1]) * (sgp[1] - b[1]) +
+                          (sgu[2] - a[2]) * (sgp[2] - b[2]) - (sdot - d)) / den1;
+        s1 += c;
+      }
+      s1 = warp_sum(s1);
+      const double mean = s1 / n;
+      for (uint32_t w = lane; w < N; w += 32) {
+        const uint64_t i = base + w;
+        double a[3], b[3], d = 0;
+        for (int k = 0; k < 3; ++k) {
+          a[k] = static_cast<double>(g[6 * i + k]);
+          b[k] = static_cast<double>(g[6 * i + 3 + k]);
+          d += a[k] * b[k];
+        }
+        const double c = ((sgu[0] - a[0]) * (sgp[0] - b[0]) + (sgu[1] - a[1]) * (sgp[1] - b[1]) +
+                          (sgu[2] - a[2]) * (sgp[2] - b[2]) - (sdot - d)) / den1;
+        s2 += (c - mean) * (c - mean);
+      }
+      s2 = warp_sum(s2);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      steps += __shfl_xor_sync(0xffffffffu, steps, o);
+      caps += __shfl_xor_sync(0xffffffffu, caps, o);
+    }
+    if (lane == 0) {
+      twos_gradient_result r;
+      r.u = su / n;
+      r.p = sp / n;
+      for (int k = 0; k < 3; ++k) {
+        r.grad_u[k] = sgu[k] / n;
+        r.grad_p[k] = sgp[k] / n;
+      }
+      r.cross = cross;
+      r.cross_se = N > 2 ? sqrt((n - 1.0) / n * s2) : 0.0;
+      r.steps = steps;
+      r.caps = caps;
+      F.out[site] = r;
+      atomicAdd(&F.totals[0], steps);
+      atomicAdd(&F.totals[1], caps);
+    }
+  }
+}
+
+cudaError_t launch_grad_finalize(int precision, const GradFinalizeLaunch &F, cudaStream_t s) {
+  if (F.n_sites == 0) return cudaSuccess;
+  const int grid = static_cast<int>(std::min<uint64_t>((static_cast<uint64_t>(F.n_sites) * 32 + 255) / 256,
+                                                       148ull * 16));
+  if (precision == TWOS_PREC_MIXED)
+    grad_finalize_kernel<float><<<grid, 256, 0, s>>>(F);
+  else
+    grad_finalize_kernel<double><<<grid, 256, 0, s>>>(F);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cudaStream_t s) {

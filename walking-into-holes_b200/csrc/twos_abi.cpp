@@ -145,7 +145,7 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
   return TWOS_OK;
 }
 
-int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav) {
+int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav, bool allow_boundary) {
   if (!r) return fail(TWOS_ERR_USAGE, "null request");
   if (r->mode < 0 || r->mode > 2) return fail(TWOS_ERR_USAGE, "invalid mode");
   if (r->precision != TWOS_PREC_FP64 && r->precision != TWOS_PREC_MIXED)
@@ -159,7 +159,7 @@ int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav) {
     return fail(TWOS_ERR_USAGE, "too many source terms");
   for (int i = 0; i < r->n_source + r->n_adjoint; ++i) {
     const twos_source_term &t = i < r->n_source ? r->source[i] : r->adjoint[i - r->n_source];
-    if (t.kind < TWOS_TERM_CONST || t.kind > TWOS_TERM_BALL) return fail(TWOS_ERR_USAGE, "unknown source term");
+    if (t.kind < TWOS_TERM_CONST || t.kind > TWOS_TERM_QUAD) return fail(TWOS_ERR_USAGE, "unknown source term");
     if (t.kind == TWOS_TERM_LINEAR && (t.axis < 0 || t.axis > 2)) return fail(TWOS_ERR_USAGE, "bad term axis");
     if (r->green == TWOS_SOURCE_EXACT && t.kind != TWOS_TERM_CONST && t.kind != TWOS_TERM_LINEAR &&
         t.kind != TWOS_TERM_BUMP)
@@ -167,6 +167,14 @@ int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav) {
   }
   if (r->green < TWOS_SOURCE_CENTER || r->green > TWOS_SOURCE_EXACT)
     return fail(TWOS_ERR_USAGE, "invalid source integration mode");
+  if (r->n_boundary > TWOS_MAX_TERMS) return fail(TWOS_ERR_USAGE, "too many boundary terms");
+  if (r->n_boundary && !allow_boundary)
+    return fail(TWOS_ERR_USAGE, "Dirichlet boundary data is taken by twos_estimate_gradient");
+  for (uint32_t i = 0; i < r->n_boundary; ++i) {
+    const twos_source_term &t = r->boundary[i];
+    if (t.kind < TWOS_TERM_CONST || t.kind > TWOS_TERM_QUAD) return fail(TWOS_ERR_USAGE, "unknown boundary term");
+    if (t.kind == TWOS_TERM_LINEAR && (t.axis < 0 || t.axis > 2)) return fail(TWOS_ERR_USAGE, "bad term axis");
+  }
   if (n_cav > 4096) return fail(TWOS_ERR_USAGE, "at most 4096 cavities per request");
   (void)n_sites;
   return TWOS_OK;
@@ -183,6 +191,7 @@ TermDev frame_term(const twos_source_term &t, const double c[3]) {
     case TWOS_TERM_GAUSS:
     case TWOS_TERM_BUMP:
     case TWOS_TERM_BALL:
+    case TWOS_TERM_QUAD:
       for (int a = 0; a < 3; ++a) d.c[a] = t.c[a] - c[a];
       break;
     case TWOS_TERM_BOX:
@@ -239,6 +248,9 @@ JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint3
   J.cav_begin = cav_begin;
   J.n_cav = n_cav;
   J.site_rank = site_rank;
+  J.bnd_begin = static_cast<uint32_t>(terms.size());
+  J.n_bnd = r->n_boundary;
+  for (uint32_t i = 0; i < r->n_boundary; ++i) terms.push_back(frame_term(r->boundary[i], frame));
   return J;
 }
 
@@ -257,11 +269,13 @@ struct JobSpec {
 // on `owner`'s stream; sites and rows are device arrays indexed by
 // JobSpec::site_begin.  All jobs share mode, precision and the Green flag.
 void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const double *d_sites, twos_site_result *d_out,
-                RunOut &ro) {
+                RunOut &ro, twos_gradient_result *d_grad = nullptr) {
   const twos_request *r0 = specs.front().r;
   const bool mixed = r0->precision == TWOS_PREC_MIXED;
-  const int mode = r0->mode;
-  const bool paired = mode == TWOS_MODE_PAIRED;
+  // d_grad selects the gradient form (paired walks with first-ball gradient
+  // samples, finalized into twos_gradient_result rows).
+  const int mode = d_grad ? kModeGradient : r0->mode;
+  const bool paired = mode == TWOS_MODE_PAIRED || mode == kModeGradient;
   const int green = r0->green;
   std::vector<JobDesc> jobs;
   std::vector<GeoDesc> geos;
@@ -295,6 +309,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   m->u.reserve(walk_total * vbytes);
   if (paired) m->p.reserve(walk_total * vbytes);
   m->steps.reserve(walk_total * sizeof(uint32_t));
+  if (d_grad) m->grad.reserve(walk_total * 6 * vbytes);
   m->first.reserve(static_cast<size_t>(site_total) * sizeof(double));
   check(cudaMemcpyAsync(m->jobs.ptr, jobs.data(), jobs.size() * sizeof(JobDesc), cudaMemcpyHostToDevice, m->stream),
         "upload jobs");
@@ -330,6 +345,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
+  L.grad_out = d_grad ? m->grad.ptr : nullptr;
   const int block = m->block;
   const int per_sm = wos_max_blocks_per_sm(r0->precision, mode, green, block, L);
   if (per_sm <= 0) throw std::runtime_error("WoS kernel cannot be resident on this device");
@@ -347,7 +363,21 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   check(launch_site_prepass(r0->precision, L, m->stream), "site pre-pass");
   check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
   check(cudaEventRecord(m->evw, m->stream), "event");
-  check(launch_finalize(r0->precision, mode, F, m->stream), "finalize launch");
+  if (d_grad) {
+    // One job per launch in the gradient form: its rows start at the job's site_begin.
+    GradFinalizeLaunch G{};
+    G.n_sites = site_total;
+    G.walks = static_cast<uint32_t>(r0->walks);
+    G.u = L.u_out;
+    G.p = L.p_out;
+    G.grad = L.grad_out;
+    G.steps = L.steps_out;
+    G.out = d_grad + specs.front().site_begin;
+    G.totals = m->totals.as<unsigned long long>();
+    check(launch_grad_finalize(r0->precision, G, m->stream), "gradient finalize launch");
+  } else {
+    check(launch_finalize(r0->precision, mode, F, m->stream), "finalize launch");
+  }
   check(cudaEventRecord(m->ev1, m->stream), "event");
   check(cudaEventSynchronize(m->ev1), "WoS kernels");
   float ms = 0.f, msw = 0.f;
@@ -1052,6 +1082,50 @@ int twos_validate(twos_mesh *m, const twos_request *r, const twos_validate_param
   if (tot[0])
     return fail(TWOS_ERR_RUNTIME, "sample containment guard failed; validation record must be rejected");
   return TWOS_OK;
+}
+
+int twos_estimate_gradient(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,
+                           const double *cavities, uint32_t n_cav, twos_gradient_result *out,
+                           twos_summary *summary) {
+  if (!m || !r) return fail(TWOS_ERR_USAGE, "null mesh or request");
+  if (int rc = validate_request(r, n_sites, n_cav, true)) return rc;
+  if (r->mode != TWOS_MODE_PAIRED) return fail(TWOS_ERR_USAGE, "the gradient form takes a paired request");
+  if (r->green == TWOS_SOURCE_EXACT)
+    return fail(TWOS_ERR_USAGE, "the gradient form takes the centre or the Green-point source rule");
+  if (r->walks < 3) return fail(TWOS_ERR_USAGE, "the gradient form needs at least 3 walks per site");
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  if (!sites || !out || (n_cav && !cavities)) return fail(TWOS_ERR_USAGE, "null buffer");
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
+  DevBuf rows;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    rows.reserve(static_cast<size_t>(n_sites) * sizeof(twos_gradient_result));
+    const size_t walks = static_cast<size_t>(r->walks);
+    const size_t chunk =
+        std::max<size_t>(1, std::min<size_t>(n_sites, std::max<size_t>(1, m->max_launch_walks / walks)));
+    begin_totals(m);
+    for (size_t first = 0; first < n_sites; first += chunk) {
+      const uint32_t count = static_cast<uint32_t>(std::min<size_t>(chunk, n_sites - first));
+      JobSpec js{m, r, count, static_cast<uint32_t>(first), r->site_offset + static_cast<uint32_t>(first), cavities,
+                 n_cav};
+      run_launch(m, {js}, m->sites.as<double>(), nullptr, ro, rows.as<twos_gradient_result>());
+    }
+    check(cudaMemcpyAsync(out, rows.ptr, static_cast<size_t>(n_sites) * sizeof(twos_gradient_result),
+                          cudaMemcpyDeviceToHost, m->stream),
+          "download rows");
+    end_totals(m, ro);
+  } catch (const std::exception &e) {
+    rows.release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  rows.release();
+  return finish(ro, n_sites, r, summary, seconds_since(t0), static_cast<uint64_t>(n_sites) * 24,
+                static_cast<uint64_t>(n_sites) * sizeof(twos_gradient_result));
 }
 
 int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device) {

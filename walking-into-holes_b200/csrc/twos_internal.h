@@ -120,6 +120,7 @@ struct JobDesc {
   uint32_t src_begin, n_src, adj_begin, n_adj;
   uint32_t cav_begin, n_cav;
   uint32_t site_rank;    // sites of the launch's earlier jobs (finalize lookup)
+  uint32_t bnd_begin, n_bnd;  // Dirichlet data of u on the mesh (term range)
   uint32_t pad;
 };
 constexpr uint32_t kJobGreen = 1u;
@@ -169,11 +170,17 @@ struct WosLaunch {
   const double *walk_start;
   // Boundary mode (kModeBoundary): per-walk boundary hit of the terminal step.
   struct HitRec *hits;
+  // Gradient mode (kModeGradient): per-walk grad U and grad P, 6 values of
+  // the walk type per walk.
+  void *grad_out;
 };
 
 // Walk-to-boundary mode of the walk kernel (walk_to_boundary,
 // wih_twos.cpp:725-740): no payoff; each walk records its terminal hit.
 constexpr int kModeBoundary = 3;
+// Paired walks that also return first-ball gradient samples
+// (twos_estimate_gradient).
+constexpr int kModeGradient = 4;
 
 // Boundary hit of a walk's terminal step (closest_boundary, wih_twos.cpp:
 // 602-626), original coordinates.  cavity = -1 for the mesh, -2 when the
@@ -198,6 +205,16 @@ struct FinalizeLaunch {
   const uint32_t *steps;
   twos_site_result *out;
 };
+
+// Gradient-mode finalize: one warp per site over u, p, grad u, grad p.
+struct GradFinalizeLaunch {
+  uint32_t n_sites, walks;
+  const void *u, *p, *grad;     // per walk (float or double); grad 6 per walk
+  const uint32_t *steps;
+  twos_gradient_result *out;
+  unsigned long long *totals;   // [0] += steps, [1] += caps
+};
+cudaError_t launch_grad_finalize(int precision, const GradFinalizeLaunch &F, cudaStream_t s);
 
 // Differential WoS pass over one chunk of sites (diffwos.cuh).
 constexpr uint32_t kDiffCavity = 1u, kDiffNearSeam = 2u, kDiffSegmentUnsafe = 4u, kDiffUnsafe = 8u;

@@ -36,7 +36,7 @@ struct DevBuf {
   template <typename T> T *as() const { return static_cast<T *>(ptr); }
 };
 
-int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav);
+int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav, bool allow_boundary = false);
 JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint32_t site_begin,
                  uint32_t site_offset, uint32_t geo, uint64_t walk_begin, uint32_t site_rank, uint32_t cav_begin,
                  uint32_t n_cav, std::vector<TermDev> &terms);
@@ -60,7 +60,7 @@ struct twos_mesh {
   twos::GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
   // Scratch, grown on demand.
-  twos::DevBuf jobs, geos, terms, cavities, sites, out, u, p, steps, first, counter, totals, points, dist, closest,
+  twos::DevBuf jobs, geos, terms, cavities, sites, out, u, p, grad, steps, first, counter, totals, points, dist, closest,
       topk;
   size_t max_launch_walks = size_t(1) << 30;
   int block = 128;         // walk-kernel threads per block

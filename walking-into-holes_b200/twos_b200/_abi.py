@@ -17,7 +17,7 @@ OK, ERR_RUNTIME, ERR_USAGE = 0, 1, 2
 MODE_COMPLIANCE, MODE_PAIRED, MODE_HOT = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 SOURCE_CENTER, SOURCE_GREEN, SOURCE_EXACT = 0, 1, 2
-TERM_CONST, TERM_LINEAR, TERM_GAUSS, TERM_BUMP, TERM_BOX, TERM_BALL = range(6)
+TERM_CONST, TERM_LINEAR, TERM_GAUSS, TERM_BUMP, TERM_BOX, TERM_BALL, TERM_QUAD = range(7)
 MAX_TERMS = 8
 DEVERR_QUERY, DEVERR_STACK, DEVERR_ITER, DEVERR_CONFIG = 1, 2, 4, 8
 
@@ -26,7 +26,7 @@ EXPORTED = [
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
-    "twos_ball_green_integral", "twos_validate",
+    "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient",
 ]
 
 
@@ -45,8 +45,8 @@ class Request(ctypes.Structure):
         ("seed", ctypes.c_uint64), ("repeat", ctypes.c_uint32), ("stream", ctypes.c_uint32),
         ("epsilon", ctypes.c_double), ("cavity_radius", ctypes.c_double), ("query_radius", ctypes.c_double),
         ("green", ctypes.c_int32), ("n_source", ctypes.c_int32), ("n_adjoint", ctypes.c_int32),
-        ("skip_cavity_sites", ctypes.c_int32), ("site_offset", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
-        ("source", SourceTerm * MAX_TERMS), ("adjoint", SourceTerm * MAX_TERMS),
+        ("skip_cavity_sites", ctypes.c_int32), ("site_offset", ctypes.c_uint32), ("n_boundary", ctypes.c_uint32),
+        ("source", SourceTerm * MAX_TERMS), ("adjoint", SourceTerm * MAX_TERMS), ("boundary", SourceTerm * MAX_TERMS),
     ]
 
 
@@ -104,6 +104,9 @@ class DesignStep(ctypes.Structure):
 class ValidateParams(ctypes.Structure):
     _fields_ = [("radius_cap", ctypes.c_double), ("value_cap", ctypes.c_double)]
 
+
+GRADIENT_DTYPE = [("u", "f8"), ("p", "f8"), ("grad_u", "f8", (3,)), ("grad_p", "f8", (3,)), ("cross", "f8"),
+                  ("cross_se", "f8"), ("steps", "u8"), ("caps", "u8")]
 
 VALIDATE_MAX_STAGES = 5
 CERT_SAMPLE_DTYPE = [("value", "f8"), ("steps", "u4"), ("capped", "u1"), ("clipped", "u1"), ("contained", "u1"),
@@ -164,6 +167,7 @@ def load(path: Path | str | None = None):
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
     L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
+    L.twos_estimate_gradient.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_validate.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ValidateParams), vp, u32, vp, u32, vp,
                                 vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,

@@ -54,6 +54,7 @@ class Config:
     adjoint: list = field(default_factory=list)
     skip_cavity_sites: bool | None = None
     site_offset: int = 0
+    boundary: list = field(default_factory=list)  # Dirichlet data of u (gradient form)
 
     def to_request(self) -> Request:
         r = Request()
@@ -80,6 +81,11 @@ class Config:
             skip = r.mode != MODE_COMPLIANCE
         r.skip_cavity_sites = int(bool(skip))
         r.site_offset = int(self.site_offset)
+        if len(self.boundary) > _abi.MAX_TERMS:
+            raise ValueError("too many boundary terms")
+        r.n_boundary = len(self.boundary)
+        for i, t in enumerate(self.boundary):
+            r.boundary[i] = t
         return r
 
 
@@ -249,6 +255,21 @@ class Mesh:
                 raise TwosError(rc, msg)
             out["error"] = msg
         return rows, stats, out
+
+    def estimate_gradient(self, sites, config: Config, cavities=None):
+        """Gradient samples and the cross-index gradient product
+        (twos_estimate_gradient): rows of GRADIENT_DTYPE and the summary.
+        config must be paired; config.boundary holds the primal's Dirichlet
+        data on the mesh."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
+        rows = np.zeros(len(s), dtype=_abi.GRADIENT_DTYPE)
+        req = config.to_request()
+        summ = Summary()
+        check(_abi.load().twos_estimate_gradient(self._h, ctypes.byref(req), _ptr(s), len(s),
+                                                 _ptr(cav) if len(cav) else None, len(cav), _ptr(rows),
+                                                 ctypes.byref(summ)))
+        return rows, _summary_dict(summ)
 
     def validate(self, sites, config: Config, cavities=None, radius_cap: float = 0.1, value_cap: float = 0.1,
                  strict: bool = True):

@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import math
 
-from ._abi import (SourceTerm, TERM_BALL, TERM_BOX, TERM_BUMP, TERM_CONST, TERM_GAUSS, TERM_LINEAR)
+from ._abi import (SourceTerm, TERM_BALL, TERM_BOX, TERM_BUMP, TERM_CONST, TERM_GAUSS, TERM_LINEAR, TERM_QUAD)
 
 
 def term(kind, amp=1.0, axis=0, offset=0.0, div=1.0, c=(0.0, 0.0, 0.0), w=(1.0, 1.0, 1.0)) -> SourceTerm:
@@ -92,3 +92,14 @@ def load_study_config(path):
     if not heat:
         raise ValueError(f"{path}: missing compact heat sources")
     return tuple(values[:4]), study_heat(heat)
+
+
+def quadratic(weights, amp=1.0, center=(0.0, 0.0, 0.0)):
+    """amp * sum_k weights_k (x_k - c_k)^2 (harmonic when the weights sum to
+    zero), e.g. boundary data x0^2 - x1^2 = quadratic((1, -1, 0))."""
+    return [term(TERM_QUAD, amp, c=center, w=tuple(weights))]
+
+
+def linear(slope, axis, offset=0.0):
+    """slope * (x[axis] + offset)."""
+    return [term(TERM_LINEAR, slope, axis=axis, offset=offset)]
