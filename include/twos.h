@@ -408,6 +408,35 @@ int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const d
                            const double *cavities, uint32_t n_cavities, twos_gradient_result *out,
                            twos_summary *summary);
 
+/* Array-RQMC and matched Monte Carlo (benchmarks/critical_baselines/
+ * sampling.py:49-88, the reference's 2D study, here in 3D on the mesh).  Each
+ * site's request->walks walks (a power of two, 32..1024) advance in lockstep,
+ * one CUDA block per (site, batch).  ARRAY: at every step the active walks
+ * are ordered by the 3D Hilbert index of their position (10 bits per axis in
+ * the mesh's bounding box; finished walks last) and the walk of rank i takes
+ * the i-th point of a randomly shifted rank-1 lattice (i/n, g i/n) mod 1 (Ho
+ * and Owen's Array-RQMC with the reference's Korobov generators g); the two
+ * coordinates give the step direction.  MC: independent uniforms.  A walk's
+ * payoff is request->source at each ball centre times r^2/6 plus u_boundary
+ * (primal) or p_boundary (adjoint) at its exit point on the mesh.  The
+ * cross-fitting unit is a whole batch (an independent randomization):
+ * batch_u/batch_p [batches][n_sites] are the batch means and
+ * td[site] = -(sum a sum b - sum ab) / (R (R - 1)) over the R batches
+ * (crossfit, sampling.py:84-86).  Capped walks are an error (sampling.py:
+ * 73-74).  No reference counterpart in the compiled backend. */
+enum { TWOS_RQMC_MC = 0, TWOS_RQMC_ARRAY = 1 };
+
+typedef struct twos_rqmc_params {
+  int32_t method;    /* TWOS_RQMC_* */
+  uint32_t batches;  /* >= 2 */
+  uint32_t n_u_boundary, n_p_boundary;
+  twos_source_term u_boundary[TWOS_MAX_TERMS];
+  twos_source_term p_boundary[TWOS_MAX_TERMS];
+} twos_rqmc_params;
+
+int twos_rqmc(twos_mesh *mesh, const twos_request *request, const twos_rqmc_params *params, const double *sites,
+              uint32_t n_sites, double *batch_u, double *batch_p, double *td, twos_summary *summary);
+
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid
  * out [site][walk].  Host buffers.  Used by parity tests. */

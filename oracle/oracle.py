@@ -102,6 +102,12 @@ def lib():
             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p]
         L.oracle_exact_bump_green.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_hilbert_key.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        L.oracle_hilbert_key.restype = ctypes.c_uint32
+        L.oracle_rqmc.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_estimate_gradient.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
             ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
@@ -299,6 +305,26 @@ class OracleMesh:
         if rc:
             raise RuntimeError(lib().oracle_last_error().decode())
         return out, stats, totals
+
+    def rqmc(self, sites, method, batches, generator, u_boundary, p_boundary, **kw):
+        """The GPU's lockstep Array-RQMC (method 1) / MC (method 0) in the
+        counter stream: (batch_u, batch_p [batches, n_sites], steps, caps)."""
+        p = self._params(**kw)
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        lo = np.ascontiguousarray(self.vertices.min(0))
+        hi = np.ascontiguousarray(self.vertices.max(0))
+        ub = (Term * max(1, len(u_boundary)))(*u_boundary)
+        pb = (Term * max(1, len(p_boundary)))(*p_boundary)
+        bu = np.zeros((batches, len(s)))
+        bp = np.zeros((batches, len(s)))
+        tot = np.zeros(2, dtype=np.uint64)
+        rc = lib().oracle_rqmc(self.handle, ctypes.byref(p), int(method), int(batches), int(generator), _ptr(lo),
+                               _ptr(hi), ctypes.cast(ub, ctypes.c_void_p), len(u_boundary),
+                               ctypes.cast(pb, ctypes.c_void_p), len(p_boundary), _ptr(s), len(s), _ptr(bu), _ptr(bp),
+                               _ptr(tot))
+        if rc:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return bu, bp, int(tot[0]), int(tot[1])
 
     def estimate_gradient(self, sites, cavities=None, samples=False, **kw):
         """The GPU gradient form in the counter stream (rng must be the counter

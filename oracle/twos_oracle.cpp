@@ -1600,3 +1600,153 @@ int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, cons
 }
 
 }  // extern "C"
+
+// ================================================================ Array-RQMC
+// The GPU's lockstep Array-RQMC / matched MC walks (twos_rqmc) in FP64 and
+// the counter stream: per (site, batch), each step answers every active
+// walk's query, stops walks within epsilon (boundary data at the exit),
+// orders active walks by the 3D Hilbert key of their position (finished
+// walks last, ties by walk index) and gives the walk of rank i the shifted
+// lattice point ((i/n + U1) mod 1, (g i/n + U2) mod 1) -- the 3D form of
+// benchmarks/critical_baselines/sampling.py:49-76.
+
+namespace {
+
+// Skilling's transpose method for the Hilbert index (AIP Conf. Proc. 707,
+// 2004), 3 axes x 10 bits, axis 0 most significant.
+uint32_t oracle_hilbert3(uint32_t x, uint32_t y, uint32_t z) {
+  uint32_t X[3] = {x, y, z};
+  for (uint32_t Q = 1u << 9; Q > 1u; Q >>= 1) {
+    const uint32_t P = Q - 1u;
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < 3; ++i) X[i] ^= X[i - 1];
+  uint32_t t = 0;
+  for (uint32_t Q = 1u << 9; Q > 1u; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1u;
+  for (int i = 0; i < 3; ++i) X[i] ^= t;
+  uint32_t h = 0;
+  for (int bit = 9; bit >= 0; --bit)
+    for (int i = 0; i < 3; ++i) h = (h << 1) | ((X[i] >> bit) & 1u);
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t oracle_hilbert_key(uint32_t x, uint32_t y, uint32_t z) { return oracle_hilbert3(x, y, z); }
+
+// batch_u, batch_p: [batches][n_sites]; steps, caps summed.  method 0 MC, 1 ARRAY.
+int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint32_t batches, uint32_t generator,
+                const double *bbox_lo, const double *bbox_hi, const Term *ub, int n_ub, const Term *pb, int n_pb,
+                const double *sites, uint32_t n_sites, double *batch_u, double *batch_p, uint64_t *totals) {
+  const Mesh &m = om->m;
+  const uint32_t n = static_cast<uint32_t>(o->walks);
+  uint32_t k0, k1;
+  counter_key(o->seed, o->stream, k0, k1);
+  std::atomic<uint64_t> tsteps{0}, tcaps{0};
+  std::atomic<int> failed{0};
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int64_t job = 0; job < static_cast<int64_t>(n_sites) * batches; ++job) {
+    const uint32_t site = static_cast<uint32_t>(job % n_sites), batch = static_cast<uint32_t>(job / n_sites);
+    const uint32_t ctr3 = (batch << 16) | (o->repeat << 3);
+    std::vector<Vec3> pos(n, Vec3{sites[3 * site], sites[3 * site + 1], sites[3 * site + 2]});
+    std::vector<char> active(n, 1);
+    std::vector<double> r(n, 0.0);
+    double vu = 0.0, vp = 0.0;
+    uint64_t steps = 0, caps = 0;
+    std::vector<uint32_t> stepc(n, 0);
+    for (int k = 0; k < o->max_steps; ++k) {
+      bool any = false;
+      for (uint32_t i = 0; i < n; ++i) {
+        if (!active[i]) continue;
+        const Closest c = closest_point(m, pos[i], std::numeric_limits<double>::infinity(), nullptr);
+        if (!std::isfinite(c.distance)) {
+          failed = 1;
+          active[i] = 0;
+          continue;
+        }
+        r[i] = c.distance;
+        if (!(r[i] > o->epsilon)) {
+          if (n_ub) vu += source_value(ub, n_ub, c.point);
+          if (n_pb) vp += source_value(pb, n_pb, c.point);
+          active[i] = 0;
+        }
+        any = any || active[i];
+      }
+      if (!any) break;
+      std::vector<double> u1(n), u2(n);
+      if (method == 1) {
+        std::vector<std::pair<uint64_t, uint32_t>> keys(n);
+        for (uint32_t i = 0; i < n; ++i) {
+          uint32_t key = 0xffffffffu;
+          if (active[i]) {
+            uint32_t q[3];
+            for (int a = 0; a < 3; ++a) {
+              const double f = (coord(pos[i], a) - bbox_lo[a]) * (1.0 / std::max(bbox_hi[a] - bbox_lo[a], 1e-300)) *
+                               1024.0;
+              q[a] = static_cast<uint32_t>(std::min(std::max(f, 0.0), 1023.0));
+            }
+            key = oracle_hilbert3(q[0], q[1], q[2]);
+          }
+          keys[i] = {(static_cast<uint64_t>(key) << 32) | i, i};
+        }
+        std::sort(keys.begin(), keys.end());
+        uint32_t sh[4];
+        Philox::block(k0, k1, static_cast<uint32_t>(k), 0xffffffffu, site, ctr3 | 6u, sh);
+        const double U1 = u53(sh[0], sh[1]), U2 = u53(sh[2], sh[3]);
+        for (uint32_t rank = 0; rank < n; ++rank) {
+          const uint32_t i = keys[rank].second;
+          // Korobov point (i/n, a i/n, a^2 i/n): the rank orders, the rest step.
+          const uint64_t g2 = (static_cast<uint64_t>(generator) * generator) % n;
+          double a1 = static_cast<double>((static_cast<uint64_t>(generator) * rank) % n) / n + U1;
+          double a2 = static_cast<double>((g2 * rank) % n) / n + U2;
+          u1[i] = a1 - std::floor(a1);
+          u2[i] = a2 - std::floor(a2);
+        }
+      } else {
+        for (uint32_t i = 0; i < n; ++i) {
+          uint32_t q[4];
+          Philox::block(k0, k1, static_cast<uint32_t>(k), i, site, ctr3, q);
+          u1[i] = u53(q[0], q[1]);
+          u2[i] = u53(q[2], q[3]);
+        }
+      }
+      for (uint32_t i = 0; i < n; ++i) {
+        if (!active[i]) continue;
+        if (o->n_source) vu += r[i] * r[i] / 6.0 * source_value(o->source, o->n_source, pos[i]);
+        pos[i] = pos[i] + direction_from(u1[i], u2[i]) * r[i];
+        ++stepc[i];
+        if (static_cast<int>(stepc[i]) >= o->max_steps) {
+          active[i] = 0;
+          ++caps;
+        }
+      }
+    }
+    for (uint32_t i = 0; i < n; ++i) steps += stepc[i];
+    batch_u[static_cast<size_t>(batch) * n_sites + site] = vu / n;
+    batch_p[static_cast<size_t>(batch) * n_sites + site] = vp / n;
+    tsteps += steps;
+    tcaps += caps;
+  }
+  totals[0] = tsteps;
+  totals[1] = tcaps;
+  if (failed) {
+    g_error = "closest-point query failed";
+    return 1;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,71 @@
+"""Array-RQMC and matched Monte Carlo on the GPU (twos_rqmc) against the
+oracle's restatement and the exact harmonic fields (the 3D form of
+benchmarks/critical_baselines/sampling.py).
+
+Tolerances
+* FP64 form vs the oracle in the shared counter stream: total steps equal;
+  batch means to rtol 1e-10.
+* The batch cross-fit against -u p (exact): Array-RQMC's mean-square error
+  below half of matched Monte Carlo's, both in FP64 and in the mixed form.
+"""
+import numpy as np
+import pytest
+
+from test_rqmc_cpu import HARMONIC, fields, grid_sites, terms
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tb(lib_built):
+    import twos_b200
+    return twos_b200
+
+
+@pytest.mark.parametrize("method", ["mc", "array"])
+def test_rqmc_fp64_equals_oracle(tb, oracle_mod, method):
+    V, F = tb.geometry.icosphere(3)
+    sites = grid_sites(3)
+    ub, pb = terms(tb.sources.term, HARMONIC["u"]), terms(tb.sources.term, HARMONIC["p"])
+    cfg = tb.Config(walks=64, precision="fp64", seed=7, epsilon=1e-5, max_steps=4096, source=tb.sources.constant(0.3))
+    with tb.Mesh(V, F) as mesh:
+        bu, bp, td, summ = mesh.rqmc(sites, cfg, ub, pb, method=method, batches=3)
+    obu, obp, steps, caps = oracle_mod.OracleMesh(V, F).rqmc(
+        sites, {"mc": 0, "array": 1}[method], 3, 5, terms(oracle_mod.term, HARMONIC["u"]),
+        terms(oracle_mod.term, HARMONIC["p"]), rng=oracle_mod.RNG_COUNTER, walks=64, seed=7, epsilon=1e-5,
+        max_steps=4096, source=[oracle_mod.term(oracle_mod.TERM_CONST, 0.3)])
+    assert summ["steps"] == steps and summ["caps"] == caps == 0
+    np.testing.assert_allclose(bu, obu, rtol=1e-10)
+    np.testing.assert_allclose(bp, obp, rtol=1e-10)
+    R = 3
+    np.testing.assert_allclose(td, -(bu.sum(0) * bp.sum(0) - (bu * bp).sum(0)) / (R * (R - 1)), rtol=1e-14)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_array_rqmc_beats_mc(tb, precision):
+    V, F = tb.geometry.icosphere(4)
+    sites = grid_sites(5)
+    u, p = fields(sites)
+    exact = -u * p
+    ub, pb = terms(tb.sources.term, HARMONIC["u"]), terms(tb.sources.term, HARMONIC["p"])
+    mse = {}
+    with tb.Mesh(V, F) as mesh:
+        for method in ("mc", "array"):
+            errs = []
+            for rep in range(16):
+                cfg = tb.Config(walks=256, precision=precision, seed=1000 + rep, epsilon=1e-5, max_steps=4096,
+                                source=[])
+                _, _, td, summ = mesh.rqmc(sites, cfg, ub, pb, method=method, batches=4)
+                assert summ["caps"] == 0
+                errs.append(np.mean((td - exact) ** 2))
+            mse[method] = np.mean(errs)
+    assert mse["array"] < 0.5 * mse["mc"], mse
+
+
+def test_rqmc_usage_errors(tb):
+    V, F = tb.geometry.icosphere(2)
+    with tb.Mesh(V, F) as mesh:
+        with pytest.raises(tb.TwosError, match="power of two"):
+            mesh.rqmc(np.zeros((1, 3)), tb.Config(walks=100), [], [])
+        with pytest.raises(tb.TwosError, match="2 batches"):
+            mesh.rqmc(np.zeros((1, 3)), tb.Config(walks=64), [], [], batches=1)

@@ -1474,3 +1474,6 @@ cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *in
 
 // Certified validation kernels (use the stream, direction and nearest<double> above).
 #include "validate.cuh"
+
+// Array-RQMC / matched MC lockstep walks (use nearest<T>, the stream and warp sums above).
+#include "rqmc.cuh"

@@ -1,0 +1,205 @@
+// Array-RQMC and matched Monte Carlo walks (twos_rqmc): the 3D counterpart
+// of the reference's sampling study (benchmarks/critical_baselines/
+// sampling.py:49-88: Ho and Owen's Array-RQMC, shifted Korobov lattice,
+// Hilbert ordering, converged paths last).
+//
+// One block per (site, batch), one thread per walk; all walks of the block
+// take their steps together.  At each step a thread answers its walk's
+// closest-point query (nearest<T>, stack in local memory); walks within
+// epsilon stop and add the boundary data at their exit point; then, in
+// ARRAY mode, the block sorts (Hilbert key, thread) pairs with a bitonic
+// network in shared memory and the walk of rank i takes the Korobov lattice
+// point (i/n, a i/n, a^2 i/n) mod 1 -- the first coordinate is consumed by
+// the ordering, the other two, shifted by one random (U1, U2) per (site,
+// batch, step), give the direction as in the walk kernel; in MC mode every
+// walk draws its own uniforms.
+//
+// Included at the end of kernels.cu.
+#pragma once
+
+namespace twos {
+
+namespace {
+
+// Hilbert index of a point of the 1024^3 grid: Skilling's transpose method
+// ("Programming the Hilbert curve", AIP Conf. Proc. 707, 2004): undo the
+// excess work of the reflected Gray code per bit plane, Gray-encode, then
+// interleave the transposed bits (axis 0 most significant).
+__host__ __device__ inline uint32_t hilbert3(uint32_t x, uint32_t y, uint32_t z) {
+  uint32_t X[3] = {x, y, z};
+  constexpr int kBits = 10;
+  for (uint32_t Q = 1u << (kBits - 1); Q > 1u; Q >>= 1) {
+    const uint32_t P = Q - 1u;
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < 3; ++i) X[i] ^= X[i - 1];
+  uint32_t t = 0;
+  for (uint32_t Q = 1u << (kBits - 1); Q > 1u; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1u;
+  for (int i = 0; i < 3; ++i) X[i] ^= t;
+  uint32_t h = 0;
+  for (int bit = kBits - 1; bit >= 0; --bit)
+    for (int i = 0; i < 3; ++i) h = (h << 1) | ((X[i] >> bit) & 1u);
+  return h;
+}
+
+template <typename T> __device__ __forceinline__ TermT<T> to_termT(const TermDev &d) {
+  TermT<T> t;
+  t.kind = d.kind;
+  t.axis = d.axis;
+  t.amp = to_T<T>(d.amp);
+  t.offset = to_T<T>(d.offset);
+  t.div = to_T<T>(d.div);
+  for (int k = 0; k < 3; ++k) {
+    t.c[k] = to_T<T>(d.c[k]);
+    t.w[k] = to_T<T>(d.w[k]);
+  }
+  return t;
+}
+
+}  // namespace
+
+template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const RqmcLaunch R) {
+  extern __shared__ unsigned long long s_keys[];  // [walks] (key << 32 | thread), then ranks
+  uint32_t *s_rank = reinterpret_cast<uint32_t *>(s_keys + R.walks);
+  __shared__ TermT<T> s_terms[3 * TWOS_MAX_TERMS];
+  __shared__ double s_red[32][2];
+  const uint32_t n_terms = R.n_src + R.n_ub + R.n_pb;
+  for (uint32_t i = threadIdx.x; i < n_terms; i += blockDim.x) s_terms[i] = to_termT<T>(R.terms[i]);
+  __syncthreads();
+  const uint32_t site = blockIdx.x % R.n_sites, batch = blockIdx.x / R.n_sites;
+  const uint32_t tid = threadIdx.x, n = R.walks;
+  const GeoDesc G = *R.geo;
+  Vec<T> pos = to_frame<T>(R.sites + 3ull * site, G);
+  bool active = true, cap = false;
+  uint32_t steps = 0, err = 0;
+  double vu = 0.0, vp = 0.0;
+  uint2 lstack[kStack];
+  const uint32_t ctr3 = (batch << 16) | (R.repeat << 3);
+  for (int k = 0; k < R.max_steps; ++k) {
+    T r = T(0);
+    if (active) {
+      T best2 = static_cast<T>(CUDART_INF);
+      uint32_t tri = 0;
+      if (!nearest<T>(geo_nodes<T>(G), geo_tris<T>(G), G.max_iter, pos, best2, tri, lstack, 1, err)) {
+        err |= TWOS_DEVERR_QUERY;
+        active = false;
+      } else {
+        const T d = sqrt(best2);
+        r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
+        if (!(r > static_cast<T>(R.epsilon))) {
+          Vec<T> a, b, c;
+          load_tri(geo_tris<T>(G), tri, a, b, c);
+          const Vec<T> q = tri_closest(pos, a, b, c);
+          if (R.n_ub) vu += static_cast<double>(source_value(s_terms, R.n_src, R.n_ub, q));
+          if (R.n_pb) vp += static_cast<double>(source_value(s_terms, R.n_src + R.n_ub, R.n_pb, q));
+          active = false;
+        }
+      }
+    }
+    if (!__syncthreads_or(active)) break;
+    T u1, u2;
+    if (R.method == TWOS_RQMC_ARRAY) {
+      uint32_t key = 0xffffffffu;
+      if (active) {
+        uint32_t qc[3];
+        const T pc[3] = {pos.x, pos.y, pos.z};
+        for (int a = 0; a < 3; ++a) {
+          const double f = (static_cast<double>(pc[a]) - R.lo[a]) * R.inv_extent[a] * 1024.0;
+          qc[a] = static_cast<uint32_t>(fmin(fmax(f, 0.0), 1023.0));
+        }
+        key = hilbert3(qc[0], qc[1], qc[2]);
+      }
+      s_keys[tid] = (static_cast<unsigned long long>(key) << 32) | tid;
+      __syncthreads();
+      for (uint32_t kk = 2; kk <= n; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+          const uint32_t ixj = tid ^ j;
+          if (ixj > tid) {
+            const unsigned long long a = s_keys[tid], b = s_keys[ixj];
+            const bool ascending = (tid & kk) == 0;
+            if ((a > b) == ascending) {
+              s_keys[tid] = b;
+              s_keys[ixj] = a;
+            }
+          }
+          __syncthreads();
+        }
+      }
+      s_rank[static_cast<uint32_t>(s_keys[tid] & 0xffffffffu)] = tid;
+      __syncthreads();
+      const uint32_t rank = s_rank[tid];
+      const Philox4 sh = philox(R.k0, R.k1, static_cast<uint32_t>(k), 0xffffffffu, site, ctr3 | 6u);
+      const double U1 = uniform<double>(sh.x, sh.y), U2 = uniform<double>(sh.z, sh.w);
+      // Korobov point (i/n, a i/n, a^2 i/n) mod 1: its first coordinate is
+      // the sorted rank itself; the other two drive the step.
+      double a1 = static_cast<double>((static_cast<uint64_t>(R.generator) * rank) % n) / n + U1;
+      double a2 = static_cast<double>((static_cast<uint64_t>(R.generator2) * rank) % n) / n + U2;
+      a1 -= floor(a1);
+      a2 -= floor(a2);
+      u1 = static_cast<T>(a1);
+      u2 = static_cast<T>(a2);
+    } else {
+      const Philox4 q = philox(R.k0, R.k1, static_cast<uint32_t>(k), tid, site, ctr3);
+      u1 = uniform<T>(q.x, q.y);
+      u2 = uniform<T>(q.z, q.w);
+    }
+    if (active) {
+      if (R.n_src) vu += static_cast<double>(r * r / T(6) * source_value(s_terms, 0, R.n_src, pos));
+      const Vec<T> dir = direction<T>(u1, u2);
+      pos = add_scaled(pos, dir, r);
+      ++steps;
+      if (static_cast<int>(steps) >= R.max_steps) {
+        cap = true;
+        active = false;
+      }
+    }
+    __syncthreads();
+  }
+  // Block sums in a fixed order: warp xor trees, then warp 0 over the warps.
+  double su = warp_sum(vu), sp = warp_sum(vp);
+  const uint32_t warp = tid >> 5, lane = tid & 31u;
+  if (lane == 0) {
+    s_red[warp][0] = su;
+    s_red[warp][1] = sp;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double tu = 0.0, tp = 0.0;
+    for (uint32_t w = 0; w < (n + 31) / 32; ++w) {
+      tu += s_red[w][0];
+      tp += s_red[w][1];
+    }
+    R.batch_u[static_cast<size_t>(batch) * R.n_sites + site] = tu / n;
+    R.batch_p[static_cast<size_t>(batch) * R.n_sites + site] = tp / n;
+  }
+  const unsigned long long st = warp_sum_u64(steps), cp = warp_sum_u64(cap ? 1ull : 0ull);
+  if (lane == 0) {
+    if (st) atomicAdd(&R.totals[0], st);
+    if (cp) atomicAdd(&R.totals[1], cp);
+  }
+  if (err) atomicOr(R.error, err);
+}
+
+cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s) {
+  const uint64_t blocks = static_cast<uint64_t>(R.n_sites) * R.batches;
+  if (blocks == 0) return cudaSuccess;
+  if (blocks > 0x7fffffffull || R.walks < 32 || R.walks > 1024 || (R.walks & (R.walks - 1)))
+    return cudaErrorInvalidValue;
+  const size_t dyn = R.walks * (sizeof(unsigned long long) + sizeof(uint32_t));
+  if (precision == TWOS_PREC_MIXED)
+    rqmc_kernel<float><<<static_cast<unsigned>(blocks), R.walks, dyn, s>>>(R);
+  else
+    rqmc_kernel<double><<<static_cast<unsigned>(blocks), R.walks, dyn, s>>>(R);
+  return cudaGetLastError();
+}
+
+}  // namespace twos

@@ -1128,6 +1128,111 @@ int twos_estimate_gradient(twos_mesh *m, const twos_request *r, const double *si
                 static_cast<uint64_t>(n_sites) * sizeof(twos_gradient_result));
 }
 
+int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, const double *sites, uint32_t n_sites,
+              double *batch_u, double *batch_p, double *td, twos_summary *summary) {
+  if (!m || !r || !rp) return fail(TWOS_ERR_USAGE, "null mesh, request or parameters");
+  if (int rc = validate_request(r, n_sites, 0)) return rc;
+  // Korobov generators a of the 3D lattice (i/n, a i/n, a^2 i/n): for each n
+  // the odd a with the largest minimum toroidal distance between lattice
+  // points (the reference's table, sampling.py:16, serves its 2D (1, a)
+  // lattice).
+  uint32_t generator = 0;
+  switch (r->walks) {
+    case 32: generator = 3; break;
+    case 64: generator = 5; break;
+    case 128: generator = 5; break;
+    case 256: generator = 13; break;
+    case 512: generator = 101; break;
+    case 1024: generator = 35; break;
+    default: return fail(TWOS_ERR_USAGE, "RQMC walks must be a power of two from 32 to 1024");
+  }
+  if (rp->method != TWOS_RQMC_MC && rp->method != TWOS_RQMC_ARRAY) return fail(TWOS_ERR_USAGE, "invalid RQMC method");
+  if (rp->batches < 2) return fail(TWOS_ERR_USAGE, "RQMC needs at least 2 batches");
+  if (rp->n_u_boundary > TWOS_MAX_TERMS || rp->n_p_boundary > TWOS_MAX_TERMS)
+    return fail(TWOS_ERR_USAGE, "too many boundary terms");
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
+  if (!sites || !batch_u || !batch_p || !td) return fail(TWOS_ERR_USAGE, "null buffer");
+  const auto t0 = std::chrono::steady_clock::now();
+  const bool mixed = r->precision == TWOS_PREC_MIXED;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const double *frame = mixed ? m->center : zero;
+  std::vector<TermDev> terms;
+  for (int i = 0; i < r->n_source; ++i) terms.push_back(frame_term(r->source[i], frame));
+  for (uint32_t i = 0; i < rp->n_u_boundary; ++i) terms.push_back(frame_term(rp->u_boundary[i], frame));
+  for (uint32_t i = 0; i < rp->n_p_boundary; ++i) terms.push_back(frame_term(rp->p_boundary[i], frame));
+  if (terms.empty()) terms.push_back(TermDev{});
+  const size_t nb = static_cast<size_t>(rp->batches) * n_sites;
+  RunOut ro;
+  DevBuf dterms, du, dp;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    dterms.reserve(terms.size() * sizeof(TermDev));
+    check(cudaMemcpyAsync(dterms.ptr, terms.data(), terms.size() * sizeof(TermDev), cudaMemcpyHostToDevice, m->stream),
+          "upload terms");
+    du.reserve(nb * sizeof(double));
+    dp.reserve(nb * sizeof(double));
+    begin_totals(m);
+    RqmcLaunch R{};
+    R.geo = m->geo.as<GeoDesc>();
+    R.sites = m->sites.as<double>();
+    R.n_sites = n_sites;
+    R.walks = static_cast<uint32_t>(r->walks);
+    R.batches = rp->batches;
+    R.method = rp->method;
+    R.generator = generator;
+    R.generator2 = static_cast<uint32_t>((static_cast<uint64_t>(generator) * generator) % R.walks);
+    R.terms = dterms.as<TermDev>();
+    R.n_src = static_cast<uint32_t>(r->n_source);
+    R.n_ub = rp->n_u_boundary;
+    R.n_pb = rp->n_p_boundary;
+    counter_key(r->seed, r->stream, R.k0, R.k1);
+    R.repeat = r->repeat;
+    R.max_steps = r->max_steps;
+    R.epsilon = r->epsilon;
+    for (int a = 0; a < 3; ++a) {
+      R.lo[a] = m->bmin[a] - frame[a];
+      R.inv_extent[a] = 1.0 / std::max(m->bmax[a] - m->bmin[a], 1e-300);
+    }
+    R.batch_u = du.as<double>();
+    R.batch_p = dp.as<double>();
+    R.totals = m->totals.as<unsigned long long>();
+    R.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    check(cudaEventRecord(m->ev0, m->stream), "event");
+    check(launch_rqmc(r->precision, R, m->stream), "RQMC launch");
+    check(cudaEventRecord(m->ev1, m->stream), "event");
+    ro.launches = 1;
+    check(cudaMemcpyAsync(batch_u, du.ptr, nb * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
+    check(cudaMemcpyAsync(batch_p, dp.ptr, nb * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
+    end_totals(m, ro);
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
+    ro.kernel_seconds = ro.walk_seconds = ms / 1e3;
+  } catch (const std::exception &e) {
+    for (DevBuf *b : {&dterms, &du, &dp}) b->release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  for (DevBuf *b : {&dterms, &du, &dp}) b->release();
+  // Cross-fitting over batches (crossfit, sampling.py:84-86).
+  const double R = rp->batches;
+  for (uint32_t s = 0; s < n_sites; ++s) {
+    double sa = 0.0, sb = 0.0, sab = 0.0;
+    for (uint32_t b = 0; b < rp->batches; ++b) {
+      const double a = batch_u[static_cast<size_t>(b) * n_sites + s], c = batch_p[static_cast<size_t>(b) * n_sites + s];
+      sa += a;
+      sb += c;
+      sab += a * c;
+    }
+    td[s] = -(sa * sb - sab) / (R * (R - 1.0));
+  }
+  twos_request rr = *r;
+  rr.walks = r->walks * static_cast<int>(rp->batches);
+  return finish(ro, n_sites, &rr, summary, seconds_since(t0), static_cast<uint64_t>(n_sites) * 24, nb * 16);
+}
+
 int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device) {
   if (n == 0) return TWOS_OK;
   if (!cases || !out) return fail(TWOS_ERR_USAGE, "null buffer");

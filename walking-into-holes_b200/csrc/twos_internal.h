@@ -206,6 +206,27 @@ struct FinalizeLaunch {
   twos_site_result *out;
 };
 
+// Array-RQMC / matched MC lockstep walks (rqmc.cuh): one block per
+// (site, batch), blockDim = walks.
+struct RqmcLaunch {
+  const GeoDesc *geo;
+  const double *sites;
+  uint32_t n_sites, walks, batches;
+  int method;                  // TWOS_RQMC_*
+  uint32_t generator;          // Korobov generator a for `walks`
+  uint32_t generator2;         // a^2 mod walks
+  const TermDev *terms;        // [src | u boundary | p boundary]
+  uint32_t n_src, n_ub, n_pb;
+  uint32_t k0, k1, repeat;
+  int max_steps;
+  double epsilon;
+  double lo[3], inv_extent[3];  // Hilbert quantization box (geometry frame of T)
+  double *batch_u, *batch_p;   // [batches][n_sites]
+  unsigned long long *totals;  // [0] steps, [1] caps
+  uint32_t *error;
+};
+cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s);
+
 // Gradient-mode finalize: one warp per site over u, p, grad u, grad p.
 struct GradFinalizeLaunch {
   uint32_t n_sites, walks;

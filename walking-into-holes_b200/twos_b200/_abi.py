@@ -26,8 +26,9 @@ EXPORTED = [
     "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
-    "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient",
+    "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc",
 ]
+RQMC_MC, RQMC_ARRAY = 0, 1
 
 
 class SourceTerm(ctypes.Structure):
@@ -101,6 +102,12 @@ class DesignStep(ctypes.Structure):
     ]
 
 
+class RqmcParams(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("batches", ctypes.c_uint32), ("n_u_boundary", ctypes.c_uint32),
+                ("n_p_boundary", ctypes.c_uint32), ("u_boundary", SourceTerm * MAX_TERMS),
+                ("p_boundary", SourceTerm * MAX_TERMS)]
+
+
 class ValidateParams(ctypes.Structure):
     _fields_ = [("radius_cap", ctypes.c_double), ("value_cap", ctypes.c_double)]
 
@@ -167,7 +174,9 @@ def load(path: Path | str | None = None):
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
     L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
-    L.twos_estimate_gradient.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
+    L.twos_rqmc.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(RqmcParams), vp, u32, vp, vp, vp,
+                            ctypes.POINTER(Summary)]
+    L.twos_estimate_gradient.argtypes =[vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_validate.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ValidateParams), vp, u32, vp, u32, vp,
                                 vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,

@@ -256,6 +256,28 @@ class Mesh:
             out["error"] = msg
         return rows, stats, out
 
+    def rqmc(self, sites, config: Config, u_boundary, p_boundary, method: str = "array", batches: int = 4):
+        """Array-RQMC or matched MC (twos_rqmc): returns (batch_u, batch_p
+        [batches, n_sites], td [n_sites], summary), td the batch cross-fit
+        -(sum a sum b - sum ab)/(R(R-1)) of sampling.py:84-86."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        p = _abi.RqmcParams()
+        p.method = {"mc": _abi.RQMC_MC, "array": _abi.RQMC_ARRAY}[method]
+        p.batches = int(batches)
+        p.n_u_boundary, p.n_p_boundary = len(u_boundary), len(p_boundary)
+        for i, t in enumerate(u_boundary):
+            p.u_boundary[i] = t
+        for i, t in enumerate(p_boundary):
+            p.p_boundary[i] = t
+        bu = np.zeros((batches, len(s)))
+        bp = np.zeros((batches, len(s)))
+        td = np.zeros(len(s))
+        req = config.to_request()
+        summ = Summary()
+        check(_abi.load().twos_rqmc(self._h, ctypes.byref(req), ctypes.byref(p), _ptr(s), len(s), _ptr(bu), _ptr(bp),
+                                    _ptr(td), ctypes.byref(summ)))
+        return bu, bp, td, _summary_dict(summ)
+
     def estimate_gradient(self, sites, config: Config, cavities=None):
         """Gradient samples and the cross-index gradient product
         (twos_estimate_gradient): rows of GRADIENT_DTYPE and the summary.
