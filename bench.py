@@ -79,6 +79,10 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--workload", choices=["noise-sphere", "housing"], default="noise-sphere",
+                    help="housing: the BASELINE config-4 epsilon sweep (a separate JSON line)")
+    ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
+    ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
     return ap.parse_args(argv)
 
 
@@ -415,8 +419,59 @@ def run_reference(args):
     }
 
 
+def run_housing_box(args):
+    """BASELINE config 4 (not the headline line): box 4 x 2 x 1 minus 6
+    through-cylinders of radius 0.15 (centres from seed 34), 529,608
+    triangles; f = 1 on x0 < 1, adjoint q = 1_{x0 > 3} / |{x0 > 3}|; paired
+    walks with a Green point per step; mixed form at eps in {1e-3, 1e-4,
+    1e-5}: site-estimates/s over `--sites` sites x `--walks` walks, and the
+    error of the cross-index TD against the FP64 form with 16x the walks on
+    the first `--ref-sites` sites (RMS error, and its ratio to the mixed
+    form's own standard error)."""
+    import torch
+    import twos_b200 as tb
+    from twos_b200 import geometry, sources
+    V, F, centres = geometry.box_minus_cylinders(0.0115, 34)
+    big = 1e30
+    f = sources.box_indicator((-big, -big, -big), (1.0, big, big))
+    vol = geometry.box_region_volume(centres, 0.15, 3.0, right=True)
+    q = sources.box_indicator((3.0, -big, -big), (big, big, big), amp=1.0 / vol)
+    sites = geometry.box_interior_points(args.sites, centres, 0.15, seed=35)
+    mesh = tb.Mesh(V, F)
+    n = len(sites)
+    d_sites = torch.from_numpy(np.ascontiguousarray(sites)).cuda()
+    d_out = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    rows = []
+    for eps in (1e-3, 1e-4, 1e-5):
+        base = dict(mode="paired", seed=SEED, epsilon=eps, max_steps=1 << 16, green=True, source=f, adjoint=q)
+        cfg = tb.Config(walks=args.walks, precision="mixed", **base)
+        mesh.estimate_device(d_sites, min(n, 16384), d_out, cfg)  # warm-up on a prefix
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        summ = mesh.estimate_device(d_sites, n, d_out, cfg)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        est = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        m = args.ref_sites
+        ref, _ = mesh.estimate(sites[:m], tb.Config(walks=16 * args.walks, precision="fp64", **dict(base, seed=SEED + 1)))
+        err = est["score"][:m] - ref["score"]
+        ok = est["score_se"][:m] > 0  # sites where some walk pair saw both sources
+        rows.append({"epsilon": eps, "site_estimates_per_s": n / dt, "seconds": dt,
+                     "mean_steps_per_walk": summ["steps"] / summ["paths"],
+                     "td_rms_error_vs_fp64_16x": float(np.sqrt(np.mean(err ** 2))),
+                     "td_rms_error_over_se": float(np.sqrt(np.mean((err[ok] / est["score_se"][:m][ok]) ** 2))),
+                     "td_rms": float(np.sqrt(np.mean(ref["score"] ** 2)))})
+    mesh.close()
+    return {"workload": "housing-like box minus cylinders (BASELINE config 4)", "triangles": int(len(F)),
+            "sites": n, "walks": args.walks, "reference": f"FP64 form, {16 * args.walks} walks, {args.ref_sites} sites",
+            "dtype": "f32 query/position, f64 accumulation", "data": "synthetic", "per_epsilon": rows}
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.workload == "housing":
+        print(json.dumps(run_housing_box(args)), flush=True)
+        return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)
