@@ -101,8 +101,14 @@ __device__ __forceinline__ double dot3(const Vec<double> &a, const Vec<double> &
 template <typename T> __device__ __forceinline__ Vec<T> sub(const Vec<T> &a, const Vec<T> &b) {
   return {a.x - b.x, a.y - b.y, a.z - b.z};
 }
+// a*b + c: one fused multiply-add in FP32 (the mixed form's arithmetic);
+// separately rounded in FP64, so the plain form keeps the host's operations
+// (the library is built without contraction).
+template <typename T> __device__ __forceinline__ T mad_t(T a, T b, T c) { return a * b + c; }
+template <> __device__ __forceinline__ float mad_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
 template <typename T> __device__ __forceinline__ Vec<T> add_scaled(const Vec<T> &a, const Vec<T> &d, T s) {
-  return {a.x + d.x * s, a.y + d.y * s, a.z + d.z * s};
+  return {mad_t(d.x, s, a.x), mad_t(d.y, s, a.y), mad_t(d.z, s, a.z)};
 }
 
 // Squared distance from p to the closest point of triangle (a, b, c):
@@ -121,7 +127,7 @@ __device__ __forceinline__ Vec<T> tri_closest(const Vec<T> &p, const Vec<T> &a, 
     if (d3 >= T(0) && d4 <= d3) {
       q = b;
     } else {
-      const T vc = d1 * d4 - d3 * d2;
+      const T vc = mad_t(d1, d4, -(d3 * d2));
       if (vc <= T(0) && d1 >= T(0) && d3 <= T(0)) {
         const T v = d1 / (d1 - d3);
         q = add_scaled(a, ab, v);
@@ -131,12 +137,12 @@ __device__ __forceinline__ Vec<T> tri_closest(const Vec<T> &p, const Vec<T> &a, 
         if (d6 >= T(0) && d5 <= d6) {
           q = c;
         } else {
-          const T vb = d5 * d2 - d1 * d6;
+          const T vb = mad_t(d5, d2, -(d1 * d6));
           if (vb <= T(0) && d2 >= T(0) && d6 <= T(0)) {
             const T w = d2 / (d2 - d6);
             q = add_scaled(a, ac, w);
           } else {
-            const T va = d3 * d6 - d5 * d4;
+            const T va = mad_t(d3, d6, -(d5 * d4));
             if (va <= T(0) && (d4 - d3) >= T(0) && (d5 - d6) >= T(0)) {
               const T w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
               q = add_scaled(b, sub(c, b), w);
@@ -845,11 +851,15 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
     // unit per iteration -- triangle tests or node tests/pops -- whichever
     // more of its traversing lanes need, so each iteration executes one code
     // path instead of the union of both.
-    const bool want_tri = phase == kTraverse && tri_cur < tri_end;
-    const unsigned vt = __ballot_sync(full, want_tri);
-    const unsigned vn = __ballot_sync(full, phase == kTraverse && !want_tri);
-    const bool tri_turn = __popc(vt) >= __popc(vn);
-    if (phase == kTraverse && (!L.vote || want_tri == tri_turn)) {
+    bool take = phase == kTraverse;
+    if (L.vote) {  // warp-uniform; the ballots cost nothing when it is off
+      const bool want_tri = phase == kTraverse && tri_cur < tri_end;
+      const unsigned vt = __ballot_sync(full, want_tri);
+      const unsigned vn = __ballot_sync(full, phase == kTraverse && !want_tri);
+      const bool tri_turn = __popc(vt) >= __popc(vn);
+      take = take && want_tri == tri_turn;
+    }
+    if (take) {
       const GeoDesc &G = s_geos[s_jobs[job].geo];
       if (++iter > G.max_iter) {
         err |= TWOS_DEVERR_ITER;
