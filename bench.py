@@ -79,8 +79,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["noise-sphere", "housing"], default="noise-sphere",
-                    help="housing: the BASELINE config-4 epsilon sweep (a separate JSON line)")
+    ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch"], default="noise-sphere",
+                    help="housing: the BASELINE config-4 epsilon sweep; batch: config 3 (separate JSON lines)")
     ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
     ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
     return ap.parse_args(argv)
@@ -467,10 +467,65 @@ def run_housing_box(args):
             "dtype": "f32 query/position, f64 accumulation", "data": "synthetic", "per_epsilon": rows}
 
 
+def run_batch(args):
+    """BASELINE config 3 (not the headline line): 32 noise-displaced
+    icospheres (seeds 2-33, subdivision levels uniform in 3..7), site counts
+    log-uniform in [100, 50000] (uniform in the ball r < 0.5, kept when
+    inside), walks per site log-uniform in [256, 8192]; compliance, f = 1,
+    eps = 1e-4, mixed form.  Times all 32 jobs in one persistent launch
+    (twos_estimate_batch: one device work queue over every job) against one
+    twos_estimate call per job, and reports the autotuner's pick for the
+    largest job."""
+    import torch  # noqa: F401  (initialises the device the library shares)
+    import twos_b200 as tb
+    from twos_b200 import autotune, geometry, sources
+    rng = np.random.default_rng(3)
+    meshes, sites, cfgs, info = [], [], [], []
+    for j in range(32):
+        level = int(rng.integers(3, 8))
+        V, F = geometry.noise_sphere(level, 2 + j)
+        m = tb.Mesh(V, F)
+        n = int(round(np.exp(rng.uniform(np.log(100), np.log(50000)))))
+        w = int(round(np.exp(rng.uniform(np.log(256), np.log(8192)))))
+        pts = geometry.uniform_ball(2 * n, 0.5, seed=100 + j)
+        pts = pts[m.inside(pts)][:n]
+        meshes.append(m)
+        sites.append(pts)
+        cfgs.append(tb.Config(walks=w, precision="mixed", seed=SEED + j, epsilon=EPSILON, max_steps=MAX_STEPS,
+                              source=sources.constant(1.0)))
+        info.append({"level": level, "triangles": int(len(F)), "sites": int(len(pts)), "walks": w})
+    total_sites = sum(len(s) for s in sites)
+    total_walks = sum(len(s) * c.walks for s, c in zip(sites, cfgs))
+    tb.estimate_batch(meshes, sites, cfgs)  # warm-up
+    t0 = time.perf_counter()
+    _, summ = tb.estimate_batch(meshes, sites, cfgs)
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for m, s, c in zip(meshes, sites, cfgs):
+        m.estimate(s, c)
+    t_seq = time.perf_counter() - t0
+    big = int(np.argmax([len(s) * c.walks for s, c in zip(sites, cfgs)]))
+    best, table = autotune.autotune(meshes[big], sites[big], cfgs[big])
+    for m in meshes:
+        m.close()
+    return {"workload": "32 uneven noise spheres in one launch (BASELINE config 3)", "jobs": info,
+            "sites": total_sites, "walks": int(total_walks), "dtype": "f32 query/position, f64 accumulation",
+            "data": "synthetic",
+            "batched": {"seconds": t_batch, "site_estimates_per_s": total_sites / t_batch,
+                        "walks_per_s": total_walks / t_batch, "launches": summ["launches"]},
+            "one_call_per_job": {"seconds": t_seq, "site_estimates_per_s": total_sites / t_seq,
+                                 "walks_per_s": total_walks / t_seq},
+            "autotune_largest_job": {"pick": best,
+                                     "seconds_per_query": {json.dumps(t): s for t, s in table}}}
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.workload == "housing":
         print(json.dumps(run_housing_box(args)), flush=True)
+        return
+    if args.workload == "batch":
+        print(json.dumps(run_batch(args)), flush=True)
         return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
