@@ -79,7 +79,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch"], default="noise-sphere",
+    ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design"], default="noise-sphere",
                     help="housing: the BASELINE config-4 epsilon sweep; batch: config 3 (separate JSON lines)")
     ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
     ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
@@ -519,8 +519,52 @@ def run_batch(args):
                                      "seconds_per_query": {json.dumps(t): s for t, s in table}}}
 
 
+def run_design(args):
+    """BASELINE config 5 (not the headline line): the design loop captured as
+    a CUDA graph on the config-1 geometry (unit icosphere L4).  Each of 20
+    iterations scouts 100,000 candidates (uniform in r < 0.85) with 2,048
+    walks, takes the top 64, validates them with 4,096 fresh walks (stream
+    1), takes the best lower bound score - 1.96 SE and inserts a ball cavity
+    of radius 0.03 when it clears the threshold; compliance, f = 1, eps 1e-4.
+    Reports iterations/s of the mixed and the FP64 form and whether their
+    chosen candidates and accept decisions agree under shared samples."""
+    import torch  # noqa: F401
+    import twos_b200 as tb
+    from twos_b200 import geometry, sources
+    V, F = geometry.icosphere(4)
+    cand = geometry.uniform_ball(100_000, 0.85, seed=5)
+    kw = dict(iterations=20, shortlist=64, cavity_radius=0.03, z=1.96, accept_threshold=0.02,
+              outer_clearance=0.02, pair_gap=0.01)
+    out = {"workload": "design loop as a CUDA graph (BASELINE config 5)", "candidates": len(cand), **kw,
+           "scout_walks": 2048, "validate_walks": 4096, "data": "synthetic"}
+    hist = {}
+    with tb.Mesh(V, F) as mesh:
+        for prec in ("mixed", "fp64"):
+            scout = tb.Config(walks=2048, precision=prec, seed=SEED, stream=0, epsilon=EPSILON, max_steps=MAX_STEPS,
+                              source=sources.constant(1.0))
+            val = tb.Config(walks=4096, precision=prec, seed=SEED, stream=1, epsilon=EPSILON, max_steps=MAX_STEPS,
+                            source=sources.constant(1.0))
+            mesh.design_loop(cand, scout, val, **dict(kw, iterations=1))  # warm-up and graph capture path
+            t0 = time.perf_counter()
+            h, cav, summ = mesh.design_loop(cand, scout, val, **kw)
+            dt = time.perf_counter() - t0
+            hist[prec] = h
+            out[prec] = {"seconds": dt, "iterations_per_s": kw["iterations"] / dt, "accepted": int(h["accepted"].sum()),
+                         "launches": summ["launches"]}
+    out["decisions_identical"] = bool(np.array_equal(hist["mixed"]["chosen"], hist["fp64"]["chosen"]) and
+                                      np.array_equal(hist["mixed"]["accepted"], hist["fp64"]["accepted"]))
+    for prec in ("mixed", "fp64"):
+        out[f"chosen_{prec}"] = hist[prec]["chosen"].tolist()
+        out[f"accepted_{prec}"] = hist[prec]["accepted"].tolist()
+        out[f"lower_{prec}"] = hist[prec]["lower"].tolist()
+    return out
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.workload == "design":
+        print(json.dumps(run_design(args)), flush=True)
+        return
     if args.workload == "housing":
         print(json.dumps(run_housing_box(args)), flush=True)
         return
