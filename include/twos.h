@@ -408,23 +408,30 @@ int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const d
                            const double *cavities, uint32_t n_cavities, twos_gradient_result *out,
                            twos_summary *summary);
 
-/* Array-RQMC and matched Monte Carlo (benchmarks/critical_baselines/
- * sampling.py:49-88, the reference's 2D study, here in 3D on the mesh).  Each
- * site's request->walks walks (a power of two, 32..1024) advance in lockstep,
- * one CUDA block per (site, batch).  ARRAY: at every step the active walks
- * are ordered by the 3D Hilbert index of their position (10 bits per axis in
- * the mesh's bounding box; finished walks last) and the walk of rank i takes
- * the i-th point of a randomly shifted rank-1 lattice (i/n, g i/n) mod 1 (Ho
- * and Owen's Array-RQMC with the reference's Korobov generators g); the two
- * coordinates give the step direction.  MC: independent uniforms.  A walk's
- * payoff is request->source at each ball centre times r^2/6 plus u_boundary
- * (primal) or p_boundary (adjoint) at its exit point on the mesh.  The
- * cross-fitting unit is a whole batch (an independent randomization):
+/* Array-RQMC, matched Monte Carlo and neighbour reuse (benchmarks/
+ * critical_baselines/sampling.py:49-110, the reference's 2D study, here in
+ * 3D on the mesh).  Each site's request->walks walks (a power of two,
+ * 32..1024) advance in lockstep, one CUDA block per (site, batch).  ARRAY: at
+ * every step the active walks are ordered by the 3D Hilbert index of their
+ * position (10 bits per axis in the mesh's bounding box; finished walks last)
+ * and the walk of rank i takes the 3D Korobov lattice point
+ * (i/n, g i/n, g^2 i/n) mod 1 shifted by one random (U1, U2) per (site,
+ * batch, step) (Ho and Owen's Array-RQMC; the first coordinate is the
+ * ordering, the other two give the step direction; g maximises the lattice's
+ * minimum distance).  MC: independent uniforms.  NEIGHBOUR: the MC walks,
+ * then each site's batch mean pools the walks of every site y whose first
+ * ball B(y, r_y) contains it, each walk reweighted by the Poisson kernel
+ * ratio r_y (r_y^2 - |x-y|^2) / |x - z|^3 (z the walk's first step point)
+ * and each site y weighted by (1-a)^4 / (1+a)^2, a = |x-y| / r_y (reused_means,
+ * sampling.py:76-88, in 3D; harmonic problems only: no request->source).
+ * A walk's payoff is request->source at each ball centre times r^2/6 plus
+ * u_boundary (primal) or p_boundary (adjoint) at its exit point on the mesh.
+ * The cross-fitting unit is a whole batch (an independent randomization):
  * batch_u/batch_p [batches][n_sites] are the batch means and
  * td[site] = -(sum a sum b - sum ab) / (R (R - 1)) over the R batches
- * (crossfit, sampling.py:84-86).  Capped walks are an error (sampling.py:
- * 73-74).  No reference counterpart in the compiled backend. */
-enum { TWOS_RQMC_MC = 0, TWOS_RQMC_ARRAY = 1 };
+ * (crossfit, sampling.py:90-92).  Capped walks are an error (sampling.py:
+ * 72-73).  No reference counterpart in the compiled backend. */
+enum { TWOS_RQMC_MC = 0, TWOS_RQMC_ARRAY = 1, TWOS_RQMC_NEIGHBOUR = 2 };
 
 typedef struct twos_rqmc_params {
   int32_t method;    /* TWOS_RQMC_* */
@@ -432,6 +439,12 @@ typedef struct twos_rqmc_params {
   uint32_t n_u_boundary, n_p_boundary;
   twos_source_term u_boundary[TWOS_MAX_TERMS];
   twos_source_term p_boundary[TWOS_MAX_TERMS];
+  /* Optional per-walk record (host buffers, each may be NULL):
+   * walk_first [batches][n_sites][walks][3] the first step's point,
+   * walk_u / walk_p [batches][n_sites][walks] each walk's payoffs, and
+   * site_radius [n_sites] the first ball's radius at each site (the record
+   * reused_means takes, sampling.py:49-88). */
+  double *walk_first, *walk_u, *walk_p, *site_radius;
 } twos_rqmc_params;
 
 int twos_rqmc(twos_mesh *mesh, const twos_request *request, const twos_rqmc_params *params, const double *sites,

@@ -107,7 +107,11 @@ def lib():
         L.oracle_rqmc.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
-            ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_neighbour_means.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32] + \
+            [ctypes.c_void_p] * 6
+        L.oracle_neighbour_means.restype = None
         L.oracle_estimate_gradient.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
             ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
@@ -306,25 +310,36 @@ class OracleMesh:
             raise RuntimeError(lib().oracle_last_error().decode())
         return out, stats, totals
 
-    def rqmc(self, sites, method, batches, generator, u_boundary, p_boundary, **kw):
-        """The GPU's lockstep Array-RQMC (method 1) / MC (method 0) in the
-        counter stream: (batch_u, batch_p [batches, n_sites], steps, caps)."""
+    def rqmc(self, sites, method, batches, generator, u_boundary, p_boundary, record=False, **kw):
+        """The GPU's lockstep Array-RQMC (method 1) / MC (method 0) / MC with
+        neighbour reuse (method 2) in the counter stream: (batch_u, batch_p
+        [batches, n_sites], steps, caps), plus the per-walk record dict
+        (walk_first, walk_u, walk_p, site_radius) when record is true."""
         p = self._params(**kw)
         s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
         lo = np.ascontiguousarray(self.vertices.min(0))
         hi = np.ascontiguousarray(self.vertices.max(0))
         ub = (Term * max(1, len(u_boundary)))(*u_boundary)
         pb = (Term * max(1, len(p_boundary)))(*p_boundary)
-        bu = np.zeros((batches, len(s)))
-        bp = np.zeros((batches, len(s)))
+        n, w = len(s), p.walks
+        bu = np.zeros((batches, n))
+        bp = np.zeros((batches, n))
         tot = np.zeros(2, dtype=np.uint64)
-        rc = lib().oracle_rqmc(self.handle, ctypes.byref(p), int(method), int(batches), int(generator), _ptr(lo),
-                               _ptr(hi), ctypes.cast(ub, ctypes.c_void_p), len(u_boundary),
-                               ctypes.cast(pb, ctypes.c_void_p), len(p_boundary), _ptr(s), len(s), _ptr(bu), _ptr(bp),
-                               _ptr(tot))
+        rec = {"walk_first": np.zeros((batches, n, w, 3)), "walk_u": np.zeros((batches, n, w)),
+               "walk_p": np.zeros((batches, n, w)), "site_radius": np.zeros(n)}
+        keep = record or method == 2
+        rc = lib().oracle_rqmc(self.handle, ctypes.byref(p), 1 if method == 1 else 0, int(batches), int(generator),
+                               _ptr(lo), _ptr(hi), ctypes.cast(ub, ctypes.c_void_p), len(u_boundary),
+                               ctypes.cast(pb, ctypes.c_void_p), len(p_boundary), _ptr(s), n, _ptr(bu), _ptr(bp),
+                               _ptr(tot), *[_ptr(rec[k]) if keep else None for k in
+                                            ("walk_first", "walk_u", "walk_p", "site_radius")])
         if rc:
             raise RuntimeError(lib().oracle_last_error().decode())
-        return bu, bp, int(tot[0]), int(tot[1])
+        if method == 2:
+            lib().oracle_neighbour_means(_ptr(s), n, int(batches), w, _ptr(rec["walk_first"]), _ptr(rec["walk_u"]),
+                                         _ptr(rec["walk_p"]), _ptr(rec["site_radius"]), _ptr(bu), _ptr(bp))
+        out = (bu, bp, int(tot[0]), int(tot[1]))
+        return out + (rec,) if record else out
 
     def estimate_gradient(self, sites, cavities=None, samples=False, **kw):
         """The GPU gradient form in the counter stream (rng must be the counter

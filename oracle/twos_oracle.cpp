@@ -1606,9 +1606,11 @@ int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, cons
 // the counter stream: per (site, batch), each step answers every active
 // walk's query, stops walks within epsilon (boundary data at the exit),
 // orders active walks by the 3D Hilbert key of their position (finished
-// walks last, ties by walk index) and gives the walk of rank i the shifted
-// lattice point ((i/n + U1) mod 1, (g i/n + U2) mod 1) -- the 3D form of
-// benchmarks/critical_baselines/sampling.py:49-76.
+// walks last, ties by walk index) and gives the walk of rank i the 3D
+// Korobov point (i/n, g i/n, g^2 i/n) whose last two coordinates, shifted by
+// (U1, U2) mod 1, drive the step -- the 3D form of
+// benchmarks/critical_baselines/sampling.py:49-74.  oracle_neighbour_means
+// is reused_means (sampling.py:76-88) in 3D.
 
 namespace {
 
@@ -1646,9 +1648,13 @@ extern "C" {
 uint32_t oracle_hilbert_key(uint32_t x, uint32_t y, uint32_t z) { return oracle_hilbert3(x, y, z); }
 
 // batch_u, batch_p: [batches][n_sites]; steps, caps summed.  method 0 MC, 1 ARRAY.
+// Optional record (each may be null): walk_first [batches][n_sites][walks][3]
+// the point after the first step, walk_u / walk_p [batches][n_sites][walks]
+// each walk's payoffs, site_radius [n_sites] the first ball's radius.
 int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint32_t batches, uint32_t generator,
                 const double *bbox_lo, const double *bbox_hi, const Term *ub, int n_ub, const Term *pb, int n_pb,
-                const double *sites, uint32_t n_sites, double *batch_u, double *batch_p, uint64_t *totals) {
+                const double *sites, uint32_t n_sites, double *batch_u, double *batch_p, uint64_t *totals,
+                double *walk_first, double *walk_u, double *walk_p, double *site_radius) {
   const Mesh &m = om->m;
   const uint32_t n = static_cast<uint32_t>(o->walks);
   uint32_t k0, k1;
@@ -1664,8 +1670,9 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
     std::vector<Vec3> pos(n, Vec3{sites[3 * site], sites[3 * site + 1], sites[3 * site + 2]});
     std::vector<char> active(n, 1);
     std::vector<double> r(n, 0.0);
-    double vu = 0.0, vp = 0.0;
+    std::vector<double> vu(n, 0.0), vp(n, 0.0);
     uint64_t steps = 0, caps = 0;
+    const size_t wbase = (static_cast<size_t>(batch) * n_sites + site) * n;
     std::vector<uint32_t> stepc(n, 0);
     for (int k = 0; k < o->max_steps; ++k) {
       bool any = false;
@@ -1679,8 +1686,8 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
         }
         r[i] = c.distance;
         if (!(r[i] > o->epsilon)) {
-          if (n_ub) vu += source_value(ub, n_ub, c.point);
-          if (n_pb) vp += source_value(pb, n_pb, c.point);
+          if (n_ub) vu[i] += source_value(ub, n_ub, c.point);
+          if (n_pb) vp[i] += source_value(pb, n_pb, c.point);
           active[i] = 0;
         }
         any = any || active[i];
@@ -1725,8 +1732,14 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
       }
       for (uint32_t i = 0; i < n; ++i) {
         if (!active[i]) continue;
-        if (o->n_source) vu += r[i] * r[i] / 6.0 * source_value(o->source, o->n_source, pos[i]);
+        if (o->n_source) vu[i] += r[i] * r[i] / 6.0 * source_value(o->source, o->n_source, pos[i]);
         pos[i] = pos[i] + direction_from(u1[i], u2[i]) * r[i];
+        if (k == 0 && walk_first) {
+          walk_first[3 * (wbase + i)] = pos[i].x;
+          walk_first[3 * (wbase + i) + 1] = pos[i].y;
+          walk_first[3 * (wbase + i) + 2] = pos[i].z;
+        }
+        if (k == 0 && site_radius && batch == 0 && i == 0) site_radius[site] = r[i];
         ++stepc[i];
         if (static_cast<int>(stepc[i]) >= o->max_steps) {
           active[i] = 0;
@@ -1734,9 +1747,16 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
         }
       }
     }
-    for (uint32_t i = 0; i < n; ++i) steps += stepc[i];
-    batch_u[static_cast<size_t>(batch) * n_sites + site] = vu / n;
-    batch_p[static_cast<size_t>(batch) * n_sites + site] = vp / n;
+    double su = 0.0, sp = 0.0;
+    for (uint32_t i = 0; i < n; ++i) {
+      steps += stepc[i];
+      su += vu[i];
+      sp += vp[i];
+      if (walk_u) walk_u[wbase + i] = vu[i];
+      if (walk_p) walk_p[wbase + i] = vp[i];
+    }
+    batch_u[static_cast<size_t>(batch) * n_sites + site] = su / n;
+    batch_p[static_cast<size_t>(batch) * n_sites + site] = sp / n;
     tsteps += steps;
     tcaps += caps;
   }
@@ -1747,6 +1767,45 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
     return 1;
   }
   return 0;
+}
+
+// reused_means (sampling.py:76-88) in 3D over the record of oracle_rqmc:
+// site x pools the walks started at every site y with a = |x - y| / r_y <
+// 1 - 1e-12, walk j weighted by the Poisson kernel ratio of B(y, r_y),
+// r_y (r_y^2 - |x - y|^2) / |x - z_j|^3, site y by (1 - a)^4 / (1 + a)^2.
+// A site with no such y keeps its plain mean (batch_u/batch_p in, out).
+void oracle_neighbour_means(const double *sites, uint32_t n_sites, uint32_t batches, uint32_t walks,
+                            const double *walk_first, const double *walk_u, const double *walk_p,
+                            const double *site_radius, double *batch_u, double *batch_p) {
+  for (uint32_t b = 0; b < batches; ++b)
+    for (uint32_t x = 0; x < n_sites; ++x) {
+      const Vec3 X{sites[3 * x], sites[3 * x + 1], sites[3 * x + 2]};
+      double wsum = 0.0, su = 0.0, sp = 0.0;
+      for (uint32_t y = 0; y < n_sites; ++y) {
+        const double ry = site_radius[y];
+        const Vec3 Y{sites[3 * y], sites[3 * y + 1], sites[3 * y + 2]};
+        const double rho2 = dot(X - Y, X - Y);
+        const double a = std::sqrt(rho2) / ry;
+        if (!(a < 1.0 - 1e-12)) continue;
+        const double w = std::pow(1.0 - a, 4) / ((1.0 + a) * (1.0 + a));
+        double mu = 0.0, mp = 0.0;
+        const size_t base = (static_cast<size_t>(b) * n_sites + y) * walks;
+        for (uint32_t j = 0; j < walks; ++j) {
+          const Vec3 Z{walk_first[3 * (base + j)], walk_first[3 * (base + j) + 1], walk_first[3 * (base + j) + 2]};
+          const double d = std::sqrt(dot(X - Z, X - Z));
+          const double K = ry * (ry * ry - rho2) / (d * d * d);
+          mu += K * walk_u[base + j];
+          mp += K * walk_p[base + j];
+        }
+        wsum += w;
+        su += w * mu / walks;
+        sp += w * mp / walks;
+      }
+      if (wsum > 0.0) {
+        batch_u[static_cast<size_t>(b) * n_sites + x] = su / wsum;
+        batch_p[static_cast<size_t>(b) * n_sites + x] = sp / wsum;
+      }
+    }
 }
 
 }  // extern "C"

@@ -12,7 +12,9 @@
 // point (i/n, a i/n, a^2 i/n) mod 1 -- the first coordinate is consumed by
 // the ordering, the other two, shifted by one random (U1, U2) per (site,
 // batch, step), give the direction as in the walk kernel; in MC mode every
-// walk draws its own uniforms.
+// walk draws its own uniforms.  NEIGHBOUR mode runs the MC walks with the
+// per-walk record on (first step point, payoffs, first radius) and then
+// rqmc_reuse_kernel pools the neighbours' walks into each site's batch mean.
 //
 // Included at the end of kernels.cu.
 #pragma once
@@ -156,6 +158,14 @@ template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const 
       if (R.n_src) vu += static_cast<double>(r * r / T(6) * source_value(s_terms, 0, R.n_src, pos));
       const Vec<T> dir = direction<T>(u1, u2);
       pos = add_scaled(pos, dir, r);
+      if (k == 0 && R.walk_first) {
+        const size_t w = (static_cast<size_t>(batch) * R.n_sites + site) * n + tid;
+        const bool f32 = sizeof(T) == 4;
+        R.walk_first[3 * w] = static_cast<double>(pos.x) + (f32 ? G.center[0] : 0.0);
+        R.walk_first[3 * w + 1] = static_cast<double>(pos.y) + (f32 ? G.center[1] : 0.0);
+        R.walk_first[3 * w + 2] = static_cast<double>(pos.z) + (f32 ? G.center[2] : 0.0);
+        if (tid == 0 && batch == 0 && R.site_radius) R.site_radius[site] = static_cast<double>(r);
+      }
       ++steps;
       if (static_cast<int>(steps) >= R.max_steps) {
         cap = true;
@@ -163,6 +173,11 @@ template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const 
       }
     }
     __syncthreads();
+  }
+  if (R.walk_u) {
+    const size_t w = (static_cast<size_t>(batch) * R.n_sites + site) * n + tid;
+    R.walk_u[w] = vu;
+    R.walk_p[w] = vp;
   }
   // Block sums in a fixed order: warp xor trees, then warp 0 over the warps.
   double su = warp_sum(vu), sp = warp_sum(vp);
@@ -189,16 +204,80 @@ template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const 
   if (err) atomicOr(R.error, err);
 }
 
+// Neighbour reuse (reused_means, sampling.py:76-88, in 3D): block (site x,
+// batch b) pools the walks of batch b started at every site y whose first
+// ball B(y, r_y) holds x, a = |x - y| / r_y < 1 - 1e-12.  A walk whose first
+// step landed at z carries the Poisson kernel ratio of the ball,
+// P(x, z) / P(y, z) = r_y (r_y^2 - |x - y|^2) / |x - z|^3, and site y the
+// weight (1 - a)^4 / (1 + a)^2 -- the inverse square of that ratio's bound
+// (1 + a) / (1 - a)^2, as the reference's 2D weight (1 - a)^4 / (1 - a^2)^2
+// is for the 2D ratio's bound (1 + a) / (1 - a).  The batch mean of x becomes
+// sum_y w_y mean_j(K_yj v_yj) / sum_y w_y; a site with no such y (its walks
+// stopped at once, r = 0) keeps its plain mean.  Each thread sums its walks
+// over all y in a fixed order, then the block sums in a fixed order.
+__global__ void __launch_bounds__(256) rqmc_reuse_kernel(const RqmcLaunch R) {
+  __shared__ double s_red[8][2];
+  const uint32_t x = blockIdx.x % R.n_sites, b = blockIdx.x / R.n_sites;
+  const uint32_t tid = threadIdx.x, n = R.walks;
+  const double x0 = R.sites[3ull * x], x1 = R.sites[3ull * x + 1], x2 = R.sites[3ull * x + 2];
+  double au = 0.0, ap = 0.0, wsum = 0.0;
+  for (uint32_t y = 0; y < R.n_sites; ++y) {
+    const double ry = R.site_radius[y];
+    const double e0 = x0 - R.sites[3ull * y], e1 = x1 - R.sites[3ull * y + 1], e2 = x2 - R.sites[3ull * y + 2];
+    const double rho2 = e0 * e0 + e1 * e1 + e2 * e2;
+    const double a = sqrt(rho2) / ry;
+    if (!(a < 1.0 - 1e-12)) continue;
+    const double w = (1.0 - a) * (1.0 - a) * (1.0 - a) * (1.0 - a) / ((1.0 + a) * (1.0 + a));
+    wsum += w;
+    const double c = w * ry * (ry * ry - rho2) / n;
+    const size_t base = (static_cast<size_t>(b) * R.n_sites + y) * n;
+    for (uint32_t j = tid; j < n; j += blockDim.x) {
+      const double *z = R.walk_first + 3 * (base + j);
+      const double d0 = x0 - z[0], d1 = x1 - z[1], d2 = x2 - z[2];
+      const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+      const double K = c / (dist2 * sqrt(dist2));
+      au += K * R.walk_u[base + j];
+      ap += K * R.walk_p[base + j];
+    }
+  }
+  double su = warp_sum(au), sp = warp_sum(ap);
+  const uint32_t warp = tid >> 5, lane = tid & 31u;
+  if (lane == 0) {
+    s_red[warp][0] = su;
+    s_red[warp][1] = sp;
+  }
+  __syncthreads();
+  if (tid == 0 && wsum > 0.0) {
+    double tu = 0.0, tp = 0.0;
+    for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+      tu += s_red[w][0];
+      tp += s_red[w][1];
+    }
+    R.batch_u[static_cast<size_t>(b) * R.n_sites + x] = tu / wsum;
+    R.batch_p[static_cast<size_t>(b) * R.n_sites + x] = tp / wsum;
+  }
+}
+
 cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s) {
   const uint64_t blocks = static_cast<uint64_t>(R.n_sites) * R.batches;
   if (blocks == 0) return cudaSuccess;
   if (blocks > 0x7fffffffull || R.walks < 32 || R.walks > 1024 || (R.walks & (R.walks - 1)))
     return cudaErrorInvalidValue;
+  if ((R.walk_u == nullptr) != (R.walk_p == nullptr)) return cudaErrorInvalidValue;
   const size_t dyn = R.walks * (sizeof(unsigned long long) + sizeof(uint32_t));
   if (precision == TWOS_PREC_MIXED)
     rqmc_kernel<float><<<static_cast<unsigned>(blocks), R.walks, dyn, s>>>(R);
   else
     rqmc_kernel<double><<<static_cast<unsigned>(blocks), R.walks, dyn, s>>>(R);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rqmc_reuse(const RqmcLaunch &R, cudaStream_t s) {
+  const uint64_t blocks = static_cast<uint64_t>(R.n_sites) * R.batches;
+  if (blocks == 0) return cudaSuccess;
+  if (blocks > 0x7fffffffull || !R.walk_first || !R.walk_u || !R.walk_p || !R.site_radius)
+    return cudaErrorInvalidValue;
+  rqmc_reuse_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(R);
   return cudaGetLastError();
 }
 

@@ -1146,7 +1146,13 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
     case 1024: generator = 35; break;
     default: return fail(TWOS_ERR_USAGE, "RQMC walks must be a power of two from 32 to 1024");
   }
-  if (rp->method != TWOS_RQMC_MC && rp->method != TWOS_RQMC_ARRAY) return fail(TWOS_ERR_USAGE, "invalid RQMC method");
+  if (rp->method != TWOS_RQMC_MC && rp->method != TWOS_RQMC_ARRAY && rp->method != TWOS_RQMC_NEIGHBOUR)
+    return fail(TWOS_ERR_USAGE, "invalid RQMC method");
+  // The Poisson kernel reweights a walk's exit value only: a source's path
+  // integral depends on where the walk started (sampling.py runs the
+  // neighbour estimator on the harmonic problem alone).
+  if (rp->method == TWOS_RQMC_NEIGHBOUR && r->n_source)
+    return fail(TWOS_ERR_USAGE, "neighbour reuse needs a harmonic problem (no source terms)");
   if (rp->batches < 2) return fail(TWOS_ERR_USAGE, "RQMC needs at least 2 batches");
   if (rp->n_u_boundary > TWOS_MAX_TERMS || rp->n_p_boundary > TWOS_MAX_TERMS)
     return fail(TWOS_ERR_USAGE, "too many boundary terms");
@@ -1162,8 +1168,11 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
   for (uint32_t i = 0; i < rp->n_p_boundary; ++i) terms.push_back(frame_term(rp->p_boundary[i], frame));
   if (terms.empty()) terms.push_back(TermDev{});
   const size_t nb = static_cast<size_t>(rp->batches) * n_sites;
+  const size_t nw = nb * static_cast<size_t>(r->walks);
+  const bool reuse = rp->method == TWOS_RQMC_NEIGHBOUR;
+  const bool rec_first = reuse || rp->walk_first || rp->site_radius, rec_walk = reuse || rp->walk_u || rp->walk_p;
   RunOut ro;
-  DevBuf dterms, du, dp;
+  DevBuf dterms, du, dp, dfirst, dwu, dwp, drad;
   try {
     check(cudaSetDevice(m->device), "cudaSetDevice");
     m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
@@ -1175,6 +1184,16 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
           "upload terms");
     du.reserve(nb * sizeof(double));
     dp.reserve(nb * sizeof(double));
+    if (rec_first) {
+      dfirst.reserve(nw * 3 * sizeof(double));
+      drad.reserve(static_cast<size_t>(n_sites) * sizeof(double));
+      check(cudaMemsetAsync(dfirst.ptr, 0, nw * 3 * sizeof(double), m->stream), "memset");
+      check(cudaMemsetAsync(drad.ptr, 0, static_cast<size_t>(n_sites) * sizeof(double), m->stream), "memset");
+    }
+    if (rec_walk) {
+      dwu.reserve(nw * sizeof(double));
+      dwp.reserve(nw * sizeof(double));
+    }
     begin_totals(m);
     RqmcLaunch R{};
     R.geo = m->geo.as<GeoDesc>();
@@ -1199,24 +1218,41 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
     }
     R.batch_u = du.as<double>();
     R.batch_p = dp.as<double>();
+    R.walk_first = rec_first ? dfirst.as<double>() : nullptr;
+    R.site_radius = rec_first ? drad.as<double>() : nullptr;
+    R.walk_u = rec_walk ? dwu.as<double>() : nullptr;
+    R.walk_p = rec_walk ? dwp.as<double>() : nullptr;
     R.totals = m->totals.as<unsigned long long>();
     R.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
     check(cudaEventRecord(m->ev0, m->stream), "event");
     check(launch_rqmc(r->precision, R, m->stream), "RQMC launch");
-    check(cudaEventRecord(m->ev1, m->stream), "event");
     ro.launches = 1;
+    if (reuse) {
+      check(launch_rqmc_reuse(R, m->stream), "neighbour reuse launch");
+      ro.launches = 2;
+    }
+    check(cudaEventRecord(m->ev1, m->stream), "event");
     check(cudaMemcpyAsync(batch_u, du.ptr, nb * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
     check(cudaMemcpyAsync(batch_p, dp.ptr, nb * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
+    const std::pair<double *, DevBuf *> records[] = {
+        {rp->walk_first, &dfirst}, {rp->walk_u, &dwu}, {rp->walk_p, &dwp}, {rp->site_radius, &drad}};
+    const size_t record_bytes[] = {nw * 3 * sizeof(double), nw * sizeof(double), nw * sizeof(double),
+                                   static_cast<size_t>(n_sites) * sizeof(double)};
+    for (int i = 0; i < 4; ++i)
+      if (records[i].first)
+        check(cudaMemcpyAsync(records[i].first, records[i].second->ptr, record_bytes[i], cudaMemcpyDeviceToHost,
+                              m->stream),
+              "download");
     end_totals(m, ro);
     float ms = 0.f;
     check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
     ro.kernel_seconds = ro.walk_seconds = ms / 1e3;
   } catch (const std::exception &e) {
-    for (DevBuf *b : {&dterms, &du, &dp}) b->release();
+    for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad}) b->release();
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
-  for (DevBuf *b : {&dterms, &du, &dp}) b->release();
-  // Cross-fitting over batches (crossfit, sampling.py:84-86).
+  for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad}) b->release();
+  // Cross-fitting over batches (crossfit, sampling.py:90-92).
   const double R = rp->batches;
   for (uint32_t s = 0; s < n_sites; ++s) {
     double sa = 0.0, sb = 0.0, sab = 0.0;
@@ -1230,7 +1266,10 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
   }
   twos_request rr = *r;
   rr.walks = r->walks * static_cast<int>(rp->batches);
-  return finish(ro, n_sites, &rr, summary, seconds_since(t0), static_cast<uint64_t>(n_sites) * 24, nb * 16);
+  const uint64_t record_d2h = (rp->walk_first ? nw * 24 : 0) + (rp->walk_u ? nw * 8 : 0) + (rp->walk_p ? nw * 8 : 0) +
+                              (rp->site_radius ? static_cast<uint64_t>(n_sites) * 8 : 0);
+  return finish(ro, n_sites, &rr, summary, seconds_since(t0), static_cast<uint64_t>(n_sites) * 24,
+                nb * 16 + record_d2h);
 }
 
 int twos_ball_green_integral(const double *cases, uint32_t n, double *out, int device) {

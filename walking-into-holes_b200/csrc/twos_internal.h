@@ -222,10 +222,14 @@ struct RqmcLaunch {
   double epsilon;
   double lo[3], inv_extent[3];  // Hilbert quantization box (geometry frame of T)
   double *batch_u, *batch_p;   // [batches][n_sites]
+  double *walk_first;          // optional [batches][n_sites][walks][3] (original coordinates)
+  double *walk_u, *walk_p;     // optional [batches][n_sites][walks]
+  double *site_radius;         // optional [n_sites]
   unsigned long long *totals;  // [0] steps, [1] caps
   uint32_t *error;
 };
 cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s);
+cudaError_t launch_rqmc_reuse(const RqmcLaunch &R, cudaStream_t s);
 
 // Gradient-mode finalize: one warp per site over u, p, grad u, grad p.
 struct GradFinalizeLaunch {

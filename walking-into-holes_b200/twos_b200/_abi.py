@@ -28,7 +28,7 @@ EXPORTED = [
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
     "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc",
 ]
-RQMC_MC, RQMC_ARRAY = 0, 1
+RQMC_MC, RQMC_ARRAY, RQMC_NEIGHBOUR = 0, 1, 2
 
 
 class SourceTerm(ctypes.Structure):
@@ -105,7 +105,8 @@ class DesignStep(ctypes.Structure):
 class RqmcParams(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("batches", ctypes.c_uint32), ("n_u_boundary", ctypes.c_uint32),
                 ("n_p_boundary", ctypes.c_uint32), ("u_boundary", SourceTerm * MAX_TERMS),
-                ("p_boundary", SourceTerm * MAX_TERMS)]
+                ("p_boundary", SourceTerm * MAX_TERMS), ("walk_first", ctypes.c_void_p),
+                ("walk_u", ctypes.c_void_p), ("walk_p", ctypes.c_void_p), ("site_radius", ctypes.c_void_p)]
 
 
 class ValidateParams(ctypes.Structure):

@@ -256,13 +256,19 @@ class Mesh:
             out["error"] = msg
         return rows, stats, out
 
-    def rqmc(self, sites, config: Config, u_boundary, p_boundary, method: str = "array", batches: int = 4):
-        """Array-RQMC or matched MC (twos_rqmc): returns (batch_u, batch_p
-        [batches, n_sites], td [n_sites], summary), td the batch cross-fit
-        -(sum a sum b - sum ab)/(R(R-1)) of sampling.py:84-86."""
+    def rqmc(self, sites, config: Config, u_boundary, p_boundary, method: str = "array", batches: int = 4,
+             record: bool = False):
+        """Array-RQMC, matched MC or neighbour reuse (twos_rqmc; the methods
+        'array', 'mc' and 'neighbors' of sampling.py:118-132): returns
+        (batch_u, batch_p [batches, n_sites], td [n_sites], summary), td the
+        batch cross-fit -(sum a sum b - sum ab)/(R(R-1)) of sampling.py:90-92.
+        With record=True the summary also holds the per-walk record:
+        walk_first [batches, n_sites, walks, 3], walk_u / walk_p
+        [batches, n_sites, walks] and site_radius [n_sites]."""
         s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
         p = _abi.RqmcParams()
-        p.method = {"mc": _abi.RQMC_MC, "array": _abi.RQMC_ARRAY}[method]
+        p.method = {"mc": _abi.RQMC_MC, "array": _abi.RQMC_ARRAY, "neighbors": _abi.RQMC_NEIGHBOUR,
+                    "neighbours": _abi.RQMC_NEIGHBOUR}[method]
         p.batches = int(batches)
         p.n_u_boundary, p.n_p_boundary = len(u_boundary), len(p_boundary)
         for i, t in enumerate(u_boundary):
@@ -272,11 +278,21 @@ class Mesh:
         bu = np.zeros((batches, len(s)))
         bp = np.zeros((batches, len(s)))
         td = np.zeros(len(s))
+        rec = None
+        if record:
+            w = int(config.walks)
+            rec = {"walk_first": np.zeros((batches, len(s), w, 3)), "walk_u": np.zeros((batches, len(s), w)),
+                   "walk_p": np.zeros((batches, len(s), w)), "site_radius": np.zeros(len(s))}
+            for k, v in rec.items():
+                setattr(p, k, v.ctypes.data)
         req = config.to_request()
         summ = Summary()
         check(_abi.load().twos_rqmc(self._h, ctypes.byref(req), ctypes.byref(p), _ptr(s), len(s), _ptr(bu), _ptr(bp),
                                     _ptr(td), ctypes.byref(summ)))
-        return bu, bp, td, _summary_dict(summ)
+        out = _summary_dict(summ)
+        if rec is not None:
+            out.update(rec)
+        return bu, bp, td, out
 
     def estimate_gradient(self, sites, config: Config, cavities=None):
         """Gradient samples and the cross-index gradient product
