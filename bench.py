@@ -78,6 +78,8 @@ def parse_args(argv=None):
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ablation", action="store_true",
+                    help="skip the one-step mixed-form run with the distance grid off")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design"], default="noise-sphere",
                     help="housing: the BASELINE config-4 epsilon sweep; batch: config 3 (separate JSON lines)")
@@ -306,7 +308,20 @@ def run_ours(args):
         h64 = float(np.median(1.96 * rows64["score_se"]))
         fp64 = {"rate": world * n * len(ms64) / (t64 / 1e3), "ms_per_step": t64 / len(ms64), "steps": len(ms64),
                 "h_median": h64, "walk_seconds": float(np.mean([s["walk_seconds"] for s in s64]))}
+    no_grid = None
+    if not args.no_ablation:
+        mesh.set_tuning(grid_threshold=0)
+        t_ng, ms_ng, s_ng = timed(tb.Config(precision="mixed", **base), 1, 1)
+        rows_ng = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        mesh.set_tuning()
+        no_grid = {"rate_unscaled": world * n / (t_ng / 1e3), "ms_per_step": t_ng,
+                   "h_median": float(np.median(1.96 * rows_ng["score_se"])),
+                   "walk_seconds": s_ng[0]["walk_seconds"], "steps_per_walk": s_ng[0]["steps"] / s_ng[0]["paths"]}
     h_ref = fp64["h_median"] if fp64 else h_mixed
+    if no_grid:
+        no_grid["rate"] = no_grid["rate_unscaled"] * (no_grid["h_median"] / h_ref) ** 2
+        if fp64:
+            no_grid["over_fp64"] = no_grid["rate"] / fp64["rate"]
     scale = (h_mixed / h_ref) ** 2
     rate_mixed = world * n * args.steps / (t_mixed / 1e3)
     value = rate_mixed * scale
@@ -315,6 +330,8 @@ def run_ours(args):
     out = None
     if rank == 0:
         queries = np.mean([s["queries"] for s in s_mixed])
+        grid_steps = np.mean([s["grid_steps"] for s in s_mixed])
+        steps = np.mean([s["steps"] for s in s_mixed])
         walk_s = float(np.mean([s["walk_seconds"] for s in s_mixed]))
         nodes = np.mean([s["node_tests"] for s in s_mixed])
         planes = np.mean([s["plane_tests"] for s in s_mixed])
@@ -322,22 +339,29 @@ def run_ours(args):
         # Bytes the walk kernel must fetch: 96 B per node visit (two child
         # boxes + normal slabs + child words), 32 B per triangle plane test
         # (plane slab + first vertex), 32 B more per full closest-point test
-        # (the other two vertices), counted on the device.
-        fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris
+        # (the other two vertices), counted on the device; one 32 B sector
+        # per distance-grid lookup (one after every step).
+        grid_lookups = steps if info["grid_dims"][0] else 0.0
+        fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris + 32.0 * grid_lookups
+        bvh_queries = queries - grid_steps
         peak, peak_kind = measured_peaks()
         ach = fetched / walk_s / 1e9
         l2 = l2_copy_gbs(stream)
-        canon = CANONICAL_BYTES_PER_QUERY * queries / walk_s / 1e9
+        canon = CANONICAL_BYTES_PER_QUERY * bvh_queries / walk_s / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "traffic": dram_traffic_per_launch(n * args.walks),
                 "traffic_source": "profiles/wos_kernel_noise_sphere_L7.md (ncu, full workload, 12.72 B/walk)",
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "bytes_per_query": float(fetched / queries),
-                "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test",
-                "queries_per_launch": float(queries), "walk_kernel_seconds": walk_s,
-                "queries_per_second": float(queries / walk_s),
-                "node_tests_per_query": float(nodes / queries), "plane_tests_per_query": float(planes / queries),
-                "triangle_tests_per_query": float(tris / queries),
+                "bytes_per_walk": float(fetched / (n * args.walks)),
+                "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test"
+                                    " + 32 B/distance-grid lookup (one per step)",
+                "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),
+                "bvh_queries_per_launch": float(bvh_queries), "walk_kernel_seconds": walk_s,
+                "bvh_queries_per_second": float(bvh_queries / walk_s),
+                "steps_per_walk": float(steps / (n * args.walks)),
+                "node_tests_per_bvh_query": float(nodes / bvh_queries),
+                "plane_tests_per_bvh_query": float(planes / bvh_queries),
+                "triangle_tests_per_bvh_query": float(tris / bvh_queries),
                 "l2": {"peak": l2, "frac": ach / l2, "peak_source": "in-run copy of a 24 MiB L2-resident buffer"},
                 "canonical": {"bytes_per_query": CANONICAL_BYTES_PER_QUERY, "source": CANONICAL_SOURCE,
                               "effective_gbs": canon,
@@ -363,6 +387,7 @@ def run_ours(args):
                    "rate_mixed_unscaled": rate_mixed},
             "fp64_form": fp64,
             "mixed_over_fp64": (value / fp64["rate"]) if fp64 else None,
+            "mixed_without_grid": no_grid,
             "e2e": {"value": rate_e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
                     "d2h_bytes_per_step": int(n * 56), "ms_per_step": t_e2e / args.steps},
             "roofline": roof,

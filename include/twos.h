@@ -168,6 +168,8 @@ typedef struct twos_summary {
   uint64_t node_tests;     /* BVH node fetches (two child bounds each) */
   uint64_t plane_tests;    /* triangle plane-slab tests */
   uint64_t triangle_tests; /* full closest-point-on-triangle tests */
+  uint64_t grid_steps;     /* steps whose radius came from the distance-bound
+                              grid instead of a closest-point query (mixed form) */
 } twos_summary;
 
 /* Device-side error bits (set by kernels, never by a trap). */
@@ -192,8 +194,11 @@ typedef struct twos_mesh_info {
   double bounds_max[3];
   double center[3];
   double mixed_delta;         /* FP32 distance error bound used by TWOS_PREC_MIXED */
-  double build_seconds;       /* host BVH build + upload */
-  uint64_t device_bytes;      /* BVH + triangle bytes resident on the device */
+  double build_seconds;       /* host BVH build + upload + distance grid */
+  uint64_t device_bytes;      /* BVH + triangle + grid bytes resident on the device */
+  uint32_t grid_dims[3];      /* distance-bound grid vertices per axis (0: no grid) */
+  uint32_t grid_pad;
+  double grid_spacing;        /* its spacing h */
 } twos_mesh_info;
 
 /* Library version and the message of the last failed call on this thread. */
@@ -201,7 +206,16 @@ int twos_abi_version(void);
 const char *twos_last_error(void);
 
 /* Build a session from an in-memory triangle mesh: host BVH build, upload of
- * the FP32 and FP64 layouts to `device`.  Replaces EmbreeMesh's constructor
+ * the FP32 and FP64 layouts to `device`, and the distance-bound grid of the
+ * mixed form: a uniform grid over the padded bounding box (about 64 vertices
+ * per triangle, at most 2^24; environment TWOS_GRID_VERTICES overrides, 0
+ * builds none) holding at each vertex v a lower bound of the distance from v
+ * to the surface (the FP32 distance minus twice the mixed form's error bound,
+ * rounded down to 1/128 of the spacing h, 16 bits).  The distance function
+ * is 1-Lipschitz, so D(v) - |x - v| bounds the distance at any x from below:
+ * a mixed-form step may take that as its ball radius -- the ball still lies in
+ * the domain, so the walk stays an unbiased walk-on-spheres -- and skip the
+ * closest-point query.  Replaces EmbreeMesh's constructor
  * (wih_twos.cpp:298-325; rtcCommitScene is the BVH build). */
 int twos_mesh_open(const double *vertices, uint64_t n_vertices, const uint32_t *faces,
                    uint64_t n_faces, int device, twos_mesh **out);
@@ -227,12 +241,17 @@ int twos_mesh_set_stream(twos_mesh *mesh, void *stream);
  *                   are idle (1..32)
  *   step_threshold: a warp takes its batched walk step once this many lanes
  *                   have finished their closest-point query (1..32)
- *   blocks_per_sm:  resident blocks per SM, 0 = as many as fit */
+ *   blocks_per_sm:  resident blocks per SM, 0 = as many as fit
+ *   grid_threshold: see below */
 typedef struct twos_tuning {
   int32_t block;
   int32_t refill;
   int32_t step_threshold;
   int32_t blocks_per_sm;
+  float grid_threshold;  /* mixed form: a step takes its radius from the
+                            distance-bound grid when the bound is at least
+                            this many grid spacings (>= 0.25); 0 = every step
+                            queries the BVH.  Default 0.5. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);
@@ -243,6 +262,13 @@ int twos_mesh_get_tuning(const twos_mesh *mesh, twos_tuning *tuning);
  * 416-430).  `closest` may be NULL.  Host buffers. */
 int twos_closest_point(twos_mesh *mesh, int precision, const double *points, uint64_t n,
                        double query_radius, double *distance, double *closest);
+
+/* The mixed form's distance-grid lower bound at each point (the radius a
+ * grid step would take before the threshold test: D(v) - |x - v| at the
+ * nearest grid vertex v), NaN outside the grid or when the session has none.
+ * Never above the distance to the surface.  Host buffers.  No reference
+ * counterpart. */
+int twos_mesh_distance_bound(twos_mesh *mesh, const double *points, uint64_t n, double *bound);
 
 /* Per-site TWoS estimates for n_sites sites (the OpenMP site loop of
  * wih_twos.cpp:1825-1841 with evaluate_site 674-717, or the paired loop of

@@ -5,9 +5,13 @@ validation -> lower-bound argmax -> accept/insert, captured as a CUDA graph.
   samples: identical chosen candidates, accept decisions and cavities (bit
   exact); scores to rtol 1e-9.
 * Graph replay vs plain launches: identical histories.
-* Mixed vs FP64 form under shared samples: identical decisions wherever the
-  FP64 lower bounds of the best two shortlist entries differ by more than the
-  mixed form's perturbation.
+* Mixed vs FP64 form under shared samples, distance grid off (the FP32 query
+  alone only perturbs the FP64 path by its rounding): identical decisions
+  wherever the FP64 lower bounds of the best two shortlist entries differ by
+  more than the mixed form's perturbation.
+* Mixed form with the distance grid (its walks take other radii, so its
+  samples are no longer the FP64 ones): the first iteration's chosen lower
+  bound agrees with the FP64 one within 4 combined standard errors.
 """
 import numpy as np
 import pytest
@@ -74,6 +78,7 @@ def test_graph_replay_equals_plain_launches(tb):
 def test_mixed_decisions_match_fp64(tb):
     V, F, cand = _setup(tb)
     with tb.Mesh(V, F) as mesh:
+        mesh.set_tuning(grid_threshold=0)
         h64, c64, _ = mesh.design_loop(cand, *_configs(tb, "fp64"), **KW)
         h32, c32, _ = mesh.design_loop(cand, *_configs(tb, "mixed"), **KW)
     for it in range(KW["iterations"]):
@@ -83,3 +88,13 @@ def test_mixed_decisions_match_fp64(tb):
             break
         assert h64["accepted"][it] == h32["accepted"][it]
     assert h64["chosen"][0] == h32["chosen"][0]
+
+
+def test_mixed_grid_design_loop_agrees_with_fp64(tb):
+    V, F, cand = _setup(tb)
+    with tb.Mesh(V, F) as mesh:
+        h64, _, _ = mesh.design_loop(cand, *_configs(tb, "fp64"), **KW)
+        h32, _, summ = mesh.design_loop(cand, *_configs(tb, "mixed"), **KW)
+    assert summ["grid_steps"] > 0 and summ["caps"] == 0
+    se = np.hypot(h64["score_se"][0], h32["score_se"][0])
+    assert abs(h64["lower"][0] - h32["lower"][0]) < 4 * se

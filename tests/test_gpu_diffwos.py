@@ -125,7 +125,12 @@ def test_mixed_shares_samples_with_fp64(tb, branch_mesh):
     off = float(a["--diff-offset"])
     r64, s64, _ = branch_mesh.diffwos(pts, cfg, holes, diff_offset=off, enclosure_fallback=True)
     cfg.precision = "mixed"
-    r32, s32, summ = branch_mesh.diffwos(pts, cfg, holes, diff_offset=off, enclosure_fallback=True)
+    # Distance grid off: the FP32 query alone keeps the FP64 form's paths.
+    branch_mesh.set_tuning(grid_threshold=0)
+    try:
+        r32, s32, summ = branch_mesh.diffwos(pts, cfg, holes, diff_offset=off, enclosure_fallback=True)
+    finally:
+        branch_mesh.set_tuning()
     assert summ["launches"] == 4
     # Most walks take the same path; the termination counts nearly agree.
     t64, t32 = s64["cavity_terminations"].sum(), s32["cavity_terminations"].sum()
@@ -135,6 +140,14 @@ def test_mixed_shares_samples_with_fp64(tb, branch_mesh):
         s = np.sqrt(g64[..., se] ** 2 + g32[..., se] ** 2)
         diff = np.abs(g64[..., mean] - g32[..., mean])
         assert np.all(diff <= 2.0 * s + 1e-12), np.max(diff / np.maximum(s, 1e-300))
+    # With the grid (the default) the mixed walks are other samples of the same
+    # estimator: agreement within the combined Monte Carlo error.
+    rg, _, _ = branch_mesh.diffwos(pts, cfg, holes, diff_offset=off, enclosure_fallback=True)
+    gg = _flat(rg)
+    for mean, se in [(0, 3), (1, 4), (2, 5), (6, 7)]:
+        s = np.sqrt(g64[..., se] ** 2 + gg[..., se] ** 2)
+        diff = np.abs(g64[..., mean] - gg[..., mean])
+        assert np.all(diff <= 4.5 * s + 1e-12), np.max(diff / np.maximum(s, 1e-300))
 
 
 def test_unsafe_offsets_are_reported(tb, oracle_mod):

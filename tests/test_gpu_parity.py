@@ -149,14 +149,19 @@ def test_sites_inside_cavities_give_zero_rows(tb, housing_mesh):
 
 # ---------------------------------------------------------------- mixed form
 def test_mixed_shares_samples_with_fp64(tb, bunny_mesh, eval_points):
+    # Distance grid off: the FP32 query alone keeps the FP64 form's paths.
     sites = eval_points[:64]
     base = dict(walks=256, mode="compliance", seed=11, epsilon=5e-4, source=tb.sources.affine(0.65))
-    g64 = bunny_mesh.walk_samples(sites, tb.Config(precision="fp64", **base))
-    g32 = bunny_mesh.walk_samples(sites, tb.Config(precision="mixed", **base))
-    same = np.mean(g64["steps"] == g32["steps"])
-    assert same > 0.5, same
-    e64, _ = bunny_mesh.estimate(sites, tb.Config(precision="fp64", **base))
-    e32, _ = bunny_mesh.estimate(sites, tb.Config(precision="mixed", **base))
+    bunny_mesh.set_tuning(grid_threshold=0)
+    try:
+        g64 = bunny_mesh.walk_samples(sites, tb.Config(precision="fp64", **base))
+        g32 = bunny_mesh.walk_samples(sites, tb.Config(precision="mixed", **base))
+        same = np.mean(g64["steps"] == g32["steps"])
+        assert same > 0.5, same
+        e64, _ = bunny_mesh.estimate(sites, tb.Config(precision="fp64", **base))
+        e32, _ = bunny_mesh.estimate(sites, tb.Config(precision="mixed", **base))
+    finally:
+        bunny_mesh.set_tuning()
     z = (e32["score"] - e64["score"]) / np.sqrt(e32["score_se"] ** 2 + e64["score_se"] ** 2)
     assert np.max(np.abs(z)) < 3.0
 
@@ -170,6 +175,14 @@ def test_reference_field_within_combined_error(tb, oracle_mod, precision, eval_p
         cfg = tb.Config(walks=2048, precision=precision, seed=12345, epsilon=5e-4, max_steps=512,
                         source=tb.sources.affine(0.65))
         est, summ = mesh.estimate(eval_points, cfg)
+        if precision == "mixed":
+            # The distance grid (on by default in the mixed form) takes shorter
+            # steps far from the surface; the step count of the reference's
+            # algorithm is the grid-off run's.
+            assert summ["grid_steps"] > 0 and summ["steps"] / summ["paths"] > 17.7199
+            mesh.set_tuning(grid_threshold=0)
+            _, summ = mesh.estimate(eval_points, cfg)
+            assert summ["grid_steps"] == 0
     z = (est["score"] - ref["score"].values) / np.sqrt(est["score_se"] ** 2 + ref["score_se"].values ** 2)
     assert np.max(np.abs(z)) < 4.5, np.max(np.abs(z))
     assert np.mean(np.abs(z) < 3.0) >= 0.95

@@ -272,7 +272,7 @@ __device__ __forceinline__ void load_tri(const TriD *__restrict__ tris, uint32_t
 // full closest-point test only when the bound is below best.  Returns true
 // when the triangle is strictly closer (best2 updated); `full` counts full tests.
 __device__ __forceinline__ bool tri_test(const TriF *__restrict__ tris, uint32_t i, const Vec<float> &p, float &best2,
-                                         unsigned long long &full) {
+                                         uint32_t &full) {
   float4 P, A;
   ldg32(&tris[i].plane, P, A);
   const float s = __fmaf_rn(P.x, p.x, __fmaf_rn(P.y, p.y, P.z * p.z));
@@ -289,7 +289,7 @@ __device__ __forceinline__ bool tri_test(const TriF *__restrict__ tris, uint32_t
   return false;
 }
 __device__ __forceinline__ bool tri_test(const TriD *__restrict__ tris, uint32_t i, const Vec<double> &p,
-                                         double &best2, unsigned long long &full) {
+                                         double &best2, uint32_t &full) {
   if (!(tri_plane_gap2(tris, i, p) < best2)) return false;
   ++full;
   Vec<double> a, b, c;
@@ -359,7 +359,7 @@ __device__ bool nearest(const typename Layout<T>::Node *__restrict__ nodes,
       const uint32_t enc = ~static_cast<uint32_t>(node);
       const uint32_t first = enc >> 3, count = enc & 7u;
       for (uint32_t i = 0; i < count; ++i) {
-        unsigned long long full = 0;
+        uint32_t full = 0;
         if (tri_test(tris, first + i, p, best2, full)) {
           best_tri = first + i;
           found = true;
@@ -498,6 +498,34 @@ template <typename T> __device__ __forceinline__ const typename Layout<T>::Tri *
 template <> __device__ __forceinline__ const TriF *geo_tris<float>(const GeoDesc &g) { return g.tris_f; }
 template <> __device__ __forceinline__ const TriD *geo_tris<double>(const GeoDesc &g) { return g.tris_d; }
 
+// Distance-grid vertex (i, j, k) in the FP32 frame, rounded the same way in
+// the grid build and in the walk step.
+__device__ __forceinline__ Vec<float> grid_vertex(const GeoDesc &g, uint32_t i, uint32_t j, uint32_t k) {
+  return {__fadd_rn(g.grid_lo[0], __fmul_rn(static_cast<float>(i), g.grid_h)),
+          __fadd_rn(g.grid_lo[1], __fmul_rn(static_cast<float>(j), g.grid_h)),
+          __fadd_rn(g.grid_lo[2], __fmul_rn(static_cast<float>(k), g.grid_h))};
+}
+
+// The grid's lower bound of the mesh distance at `p` (FP32 frame): D(v) -
+// |p - v| at the nearest vertex v (the distance is 1-Lipschitz).  False when
+// p lies outside the grid (or is NaN).
+__device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p, float &bound) {
+  const float fx = (p.x - g.grid_lo[0]) * g.grid_inv_h;
+  const float fy = (p.y - g.grid_lo[1]) * g.grid_inv_h;
+  const float fz = (p.z - g.grid_lo[2]) * g.grid_inv_h;
+  if (!(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx <= static_cast<float>(g.grid_n[0] - 1) &&
+        fy <= static_cast<float>(g.grid_n[1] - 1) && fz <= static_cast<float>(g.grid_n[2] - 1)))
+    return false;
+  const uint32_t i = static_cast<uint32_t>(__float2int_rn(fx));
+  const uint32_t j = static_cast<uint32_t>(__float2int_rn(fy));
+  const uint32_t k = static_cast<uint32_t>(__float2int_rn(fz));
+  const Vec<float> v = grid_vertex(g, i, j, k);
+  const Vec<float> dv = sub(p, v);
+  bound = static_cast<float>(__ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k)) * g.grid_q -
+          sqrtf(dot3(dv, dv));
+  return true;
+}
+
 __device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, uint64_t wid) {
   uint32_t lo = 0, hi = n - 1;
   while (lo < hi) {
@@ -538,8 +566,18 @@ enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
 // in the mixed form, FP64 in the plain form).  SRC: TWOS_SOURCE_* (a
 // template argument, so the exact-integral code of TWOS_SOURCE_EXACT adds no
 // registers to the other forms).
+// Residency: the FP32 form with the centre-point source fits 64 registers, so
+// 1024 threads (8 blocks of 128) stay resident per SM; the others take up to
+// 80 (768 threads, 6 blocks of 128).
+template <typename T, int MODE, int SRC>
+constexpr int wos_min_blocks(int block) {
+  return sizeof(T) == 4 && SRC == TWOS_SOURCE_CENTER && MODE != kModeGradient ? 1024 / block
+         : block >= 768                                                      ? 1
+                                                                              : 768 / block;
+}
+
 template <typename T, int MODE, int SRC, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_kernel(const WosLaunch L) {
+__global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
   constexpr bool GRAD = MODE == kModeGradient;
@@ -576,7 +614,9 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
   const unsigned full = 0xffffffffu;
   uint2 *stack = s_stack + threadIdx.x;
   uint32_t err = 0;
-  unsigned long long c_nodes = 0, c_planes = 0, c_tris = 0;
+  // Per-thread traversal counters (32-bit: a thread's share of one launch
+  // stays far below 2^32), summed in 64 bits at the end.
+  uint32_t c_nodes = 0, c_planes = 0, c_tris = 0, c_grid = 0;
 
   int phase = kIdle;
   bool exhausted = false;  // warp-uniform
@@ -823,22 +863,42 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
       } else {
         best2 = static_cast<T>(J.query_radius2);
         found = false;
-        if (L.warm && tri_ok) {
-          Vec<T> ta, tb, tc;
-          load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
-          ++c_tris;
-          const T w2 = tri_dist2(pos, ta, tb, tc);
-          if (w2 < best2) {
-            best2 = w2;
+        bool from_grid = false;
+        if constexpr (sizeof(T) == 4) {
+          // Distance-bound grid: D(v) - |x - v| at the nearest vertex v bounds
+          // the mesh distance from below; a bound of at least grid_tau
+          // spacings is the next ball's radius and no query is needed.
+          float bound;
+          // A grid step never ends a walk: the bound must clear the
+          // termination shell with room to spare.
+          if (L.grid_tau > 0.f && G.grid && grid_bound(G, pos, bound) && bound >= L.grid_tau * G.grid_h &&
+              bound > 2.f * (static_cast<float>(J.epsilon) + G.delta) && bound * bound < best2) {
+            best2 = bound * bound;
             found = true;
+            from_grid = true;
+            ++c_grid;
           }
         }
-        node = 0;
-        sp = 0;
-        have = true;
-        tri_cur = tri_end = 0;
-        iter = 0;
-        phase = kTraverse;
+        if (from_grid) {
+          phase = kStep;
+        } else {
+          if (L.warm && tri_ok) {
+            Vec<T> ta, tb, tc;
+            load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+            ++c_tris;
+            const T w2 = tri_dist2(pos, ta, tb, tc);
+            if (w2 < best2) {
+              best2 = w2;
+              found = true;
+            }
+          }
+          node = 0;
+          sp = 0;
+          have = true;
+          tri_cur = tri_end = 0;
+          iter = 0;
+          phase = kTraverse;
+        }
       }
     }
 
@@ -928,16 +988,19 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 768 ? 1 : 768 / BLOCK)) wos_k
   }
   if (err) atomicOr(L.error, err);
   if (L.counters) {
+    unsigned long long n_nodes = c_nodes, n_planes = c_planes, n_tris = c_tris, n_grid = c_grid;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      c_nodes += __shfl_xor_sync(full, c_nodes, o);
-      c_planes += __shfl_xor_sync(full, c_planes, o);
-      c_tris += __shfl_xor_sync(full, c_tris, o);
+      n_nodes += __shfl_xor_sync(full, n_nodes, o);
+      n_planes += __shfl_xor_sync(full, n_planes, o);
+      n_tris += __shfl_xor_sync(full, n_tris, o);
+      if (sizeof(T) == 4) n_grid += __shfl_xor_sync(full, n_grid, o);
     }
     if (lane == 0) {
-      atomicAdd(&L.counters[0], c_nodes);
-      atomicAdd(&L.counters[1], c_planes);
-      atomicAdd(&L.counters[2], c_tris);
+      atomicAdd(&L.counters[0], n_nodes);
+      atomicAdd(&L.counters[1], n_planes);
+      atomicAdd(&L.counters[2], n_tris);
+      if (n_grid) atomicAdd(&L.counters[3], n_grid);
     }
   }
 }
@@ -1366,6 +1429,65 @@ cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *
     closest_kernel<float><<<grid, block, 0, s>>>(geo_dev, pts, n, query_radius2, dist, closest, error);
   else
     closest_kernel<double><<<grid, block, 0, s>>>(geo_dev, pts, n, query_radius2, dist, closest, error);
+  return cudaGetLastError();
+}
+
+// ================================================================ distance-bound grid
+// One thread per grid vertex: its FP32 closest-point distance, less `margin`,
+// rounded down to a multiple of grid_q and saturated at 65535 multiples.  A
+// vertex whose query fails keeps 0 (a bound no step uses).
+__global__ void __launch_bounds__(kWosBlock) grid_build_kernel(const GeoDesc *geo, double margin, uint16_t *out,
+                                                               uint32_t *error) {
+  __shared__ uint2 s_stack[kStack * kWosBlock];
+  __shared__ GeoDesc G;
+  if (threadIdx.x == 0) G = *geo;
+  __syncthreads();
+  uint32_t err = 0;
+  uint2 *stack = s_stack + threadIdx.x;
+  const uint64_t n = static_cast<uint64_t>(G.grid_n[0]) * G.grid_n[1] * G.grid_n[2];
+  for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < n;
+       v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t gk = static_cast<uint32_t>(v % G.grid_n[2]);
+    const uint64_t ij = v / G.grid_n[2];
+    const uint32_t gj = static_cast<uint32_t>(ij % G.grid_n[1]), gi = static_cast<uint32_t>(ij / G.grid_n[1]);
+    const Vec<float> p = grid_vertex(G, gi, gj, gk);
+    float best2 = CUDART_INF_F;
+    uint32_t tri = 0;
+    uint16_t q = 0;
+    if (nearest<float>(geo_nodes<float>(G), geo_tris<float>(G), G.max_iter, p, best2, tri, stack, kWosBlock, err)) {
+      const double m = floor((static_cast<double>(sqrtf(best2)) - margin) / static_cast<double>(G.grid_q));
+      q = m <= 0.0 ? 0 : m >= 65535.0 ? 65535 : static_cast<uint16_t>(m);
+    }
+    out[v] = q;
+  }
+  if (err) atomicOr(error, err);
+}
+
+// The grid's lower bound at each point (original coordinates), NaN where the
+// point lies outside the grid or the geometry has none.
+__global__ void __launch_bounds__(256) grid_bound_kernel(const GeoDesc *geo, const double *pts, uint64_t n,
+                                                         double *out) {
+  const GeoDesc G = *geo;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    float b = 0.f;
+    out[i] = G.grid && grid_bound(G, to_frame<float>(pts + 3 * i, G), b) ? static_cast<double>(b) : CUDART_NAN;
+  }
+}
+
+cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_t n, double *out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int grid = static_cast<int>(std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+  grid_bound_kernel<<<grid, 256, 0, s>>>(geo_dev, pts, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_build(const GeoDesc *geo_dev, uint64_t n, double margin, uint16_t *out, uint32_t *error,
+                              cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int block = kWosBlock;
+  const int grid = static_cast<int>(std::min<uint64_t>((n + block - 1) / block, 148ull * 32));
+  grid_build_kernel<<<grid, block, 0, s>>>(geo_dev, margin, out, error);
   return cudaGetLastError();
 }
 

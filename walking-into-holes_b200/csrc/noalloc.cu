@@ -150,6 +150,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.step_threshold = m->step_threshold;
     L.vote = m->vote;
     L.warm = m->warm;
+    L.grid_tau = m->grid_tau;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;
@@ -190,6 +191,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     s.node_tests = tot[3];
     s.plane_tests = tot[4];
     s.triangle_tests = tot[5];
+    s.grid_steps = tot[6];
   } catch (const std::exception &e) {
     return fail(TWOS_ERR_RUNTIME, e.what());
   }

@@ -53,6 +53,54 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Sizes and fills the mixed form's distance-bound grid of a session whose
+// BVH is on the device and whose geo_host describes it (m->geo allocated).
+// About 64 vertices per triangle (environment TWOS_GRID_VERTICES overrides;
+// 0 builds none), at most 2^24, over the bounding box padded by one spacing.
+// Values are FP32 distances less 2 delta (the mixed form's own error bound,
+// covering the FP32 query and the vertex placement), in steps of h/128.
+void build_distance_grid(twos_mesh *m, size_t n_tris) {
+  GeoDesc &g = m->geo_host;
+  g.grid = nullptr;
+  uint64_t target = std::min<uint64_t>(std::max<uint64_t>(64ull * n_tris, 4096ull), 1ull << 24);
+  if (const char *e = std::getenv("TWOS_GRID_VERTICES"))
+    target = std::min<uint64_t>(std::strtoull(e, nullptr, 10), 1ull << 24);
+  double ext[3], emax = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    ext[a] = m->bmax[a] - m->bmin[a];
+    emax = std::max(emax, ext[a]);
+  }
+  if (target < 64 || !(emax > 0.0)) return;
+  double vol = 1.0;
+  for (int a = 0; a < 3; ++a) vol *= std::max(ext[a], 1e-3 * emax);
+  double h = std::cbrt(vol / static_cast<double>(target));
+  uint64_t n[3];
+  for (int it = 0;; ++it) {
+    for (int a = 0; a < 3; ++a) n[a] = static_cast<uint64_t>(std::ceil(ext[a] / h)) + 3;
+    const uint64_t total = n[0] * n[1] * n[2];
+    if ((total <= target + target / 2 && total <= (1ull << 24)) || it > 200) break;
+    h *= 1.03;
+  }
+  if (n[0] * n[1] * n[2] > (1ull << 24)) return;
+  for (int a = 0; a < 3; ++a) {
+    g.grid_lo[a] = static_cast<float>(m->bmin[a] - h - m->center[a]);
+    g.grid_n[a] = static_cast<uint32_t>(n[a]);
+  }
+  g.grid_h = static_cast<float>(h);
+  g.grid_inv_h = 1.0f / g.grid_h;
+  g.grid_q = g.grid_h / 128.0f;
+  const uint64_t count = n[0] * n[1] * n[2];
+  check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
+  m->grid.reserve(count * sizeof(uint16_t));
+  uint32_t *err = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+  check(cudaMemset(err, 0, sizeof(uint32_t)), "memset");
+  check(launch_grid_build(m->geo.as<GeoDesc>(), count, 2.0 * m->delta, m->grid.as<uint16_t>(), err, nullptr),
+        "grid build");
+  check(cudaDeviceSynchronize(), "grid build");
+  g.grid = m->grid.as<uint16_t>();
+  m->resident_bytes += count * sizeof(uint16_t);
+}
+
 int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, twos_mesh **out) {
   if (!out) return fail(TWOS_ERR_USAGE, "null output pointer");
   *out = nullptr;
@@ -124,9 +172,10 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     g.max_iter = static_cast<uint32_t>(
         std::min<uint64_t>(2ull * (m->bvh.nodes.size() + m->faces.size() / 3) + 16, 0xffffffffull));
     m->geo.reserve(sizeof(GeoDesc));
-    check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
     m->counter.reserve(16);
     m->totals.reserve(64);
+    build_distance_grid(m.get(), tf.size());
+    check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
     m->build_seconds = seconds_since(t0);
     if (const char *e = std::getenv("TWOS_MAX_LAUNCH_WALKS")) m->max_launch_walks = std::strtoull(e, nullptr, 10);
     if (const char *e = std::getenv("TWOS_REFILL")) m->refill = std::max(1, std::atoi(e));
@@ -212,7 +261,7 @@ struct RunOut {
   uint32_t launches = 0;
   uint32_t error_flags = 0;
   uint64_t steps = 0, caps = 0;
-  uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0;
+  uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0, grid_steps = 0;
 };
 
 // The device descriptor of one job; its source terms are appended to `terms`
@@ -342,6 +391,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.step_threshold = m->step_threshold;
   L.vote = m->vote;
   L.warm = m->warm;
+  L.grid_tau = m->grid_tau;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -406,6 +456,7 @@ void end_totals(twos_mesh *m, RunOut &ro) {
   ro.node_tests = tot[3];
   ro.plane_tests = tot[4];
   ro.triangle_tests = tot[5];
+  ro.grid_steps = tot[6];
 }
 
 // Runs the estimator over device-resident sites into device-resident rows,
@@ -444,6 +495,7 @@ int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summa
     summary->node_tests = ro.node_tests;
     summary->plane_tests = ro.plane_tests;
     summary->triangle_tests = ro.triangle_tests;
+    summary->grid_steps = ro.grid_steps;
   }
   if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
   if (ro.error_flags & TWOS_DEVERR_STACK) return fail(TWOS_ERR_RUNTIME, "BVH traversal stack bound exceeded");
@@ -508,12 +560,14 @@ int twos_mesh_set_stream(twos_mesh *m, void *stream) {
 int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if (!m || !t) return fail(TWOS_ERR_USAGE, "null argument");
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
-      t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0)
+      t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
+      !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.25f && t->grid_threshold <= 1e6f)))
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
   m->step_threshold = t->step_threshold;
   m->blocks_per_sm = t->blocks_per_sm;
+  m->grid_tau = t->grid_threshold;
   return TWOS_OK;
 }
 
@@ -523,6 +577,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->refill = m->refill;
   t->step_threshold = m->step_threshold;
   t->blocks_per_sm = m->blocks_per_sm;
+  t->grid_threshold = m->grid_tau;
   return TWOS_OK;
 }
 
@@ -541,6 +596,9 @@ int twos_mesh_get_info(const twos_mesh *m, twos_mesh_info *info) {
   info->mixed_delta = m->delta;
   info->build_seconds = m->build_seconds;
   info->device_bytes = m->resident_bytes;
+  for (int a = 0; a < 3; ++a) info->grid_dims[a] = m->geo_host.grid ? m->geo_host.grid_n[a] : 0u;
+  info->grid_pad = 0;
+  info->grid_spacing = m->geo_host.grid ? static_cast<double>(m->geo_host.grid_h) : 0.0;
   return TWOS_OK;
 }
 
@@ -571,6 +629,25 @@ int twos_closest_point(twos_mesh *m, int precision, const double *points, uint64
     check(cudaMemcpyAsync(&e, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, m->stream), "download");
     check(cudaStreamSynchronize(m->stream), "closest kernel");
     if (e & (TWOS_DEVERR_STACK | TWOS_DEVERR_ITER)) return fail(TWOS_ERR_RUNTIME, "BVH traversal bound exceeded");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  return TWOS_OK;
+}
+
+int twos_mesh_distance_bound(twos_mesh *m, const double *points, uint64_t n, double *bound) {
+  if (!m || (n && (!points || !bound))) return fail(TWOS_ERR_USAGE, "null argument");
+  if (n == 0) return TWOS_OK;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    m->points.reserve(n * 3 * sizeof(double));
+    m->dist.reserve(n * sizeof(double));
+    check(cudaMemcpyAsync(m->points.ptr, points, n * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream),
+          "upload points");
+    check(launch_grid_bound(m->geo.as<GeoDesc>(), m->points.as<double>(), n, m->dist.as<double>(), m->stream),
+          "grid bound launch");
+    check(cudaMemcpyAsync(bound, m->dist.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download");
+    check(cudaStreamSynchronize(m->stream), "grid bound");
   } catch (const std::exception &e) {
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
@@ -810,6 +887,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.step_threshold = m->step_threshold;
     Ls.vote = m->vote;
     Ls.warm = m->warm;
+    Ls.grid_tau = m->grid_tau;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -1377,6 +1455,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.step_threshold = m->step_threshold;
         L.vote = m->vote;
         L.warm = m->warm;
+        L.grid_tau = m->grid_tau;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;

@@ -100,6 +100,14 @@ struct GeoDesc {
   double center[3];   // FP32 frame origin (mixed form)
   float delta;        // FP32 distance error bound (mixed form)
   uint32_t max_iter;  // traversal iteration bound (node + leaf visits)
+  // Distance-bound grid of the mixed form (null: none).  Vertex (i, j, k)
+  // sits at grid_lo + (i, j, k) * grid_h in the FP32 frame and holds, at
+  // grid[(i * n1 + j) * n2 + k] * grid_q, a lower bound of its distance to
+  // the surface.
+  const uint16_t *grid;
+  float grid_lo[3];
+  float grid_h, grid_inv_h, grid_q;
+  uint32_t grid_n[3];
 };
 
 // One job = one geometry x a contiguous range of sites with one request.
@@ -152,7 +160,8 @@ struct WosLaunch {
   uint32_t *steps_out;          // per-walk steps | cap << 31
   int refill;                   // refill a warp once this many lanes are idle
   int step_threshold;           // step a warp's walks once this many queries are done
-  unsigned long long *counters; // [0] node tests, [1] triangle plane tests, [2] full triangle tests
+  unsigned long long *counters; // [0] node tests, [1] triangle plane tests, [2] full triangle tests,
+                                // [3] grid steps
   // Squared mesh distance at each launch site (index site_rank + site), from
   // the pre-pass; every walk of a site starts from the same point, so its
   // first query is answered from here (-1 when nothing is within range).
@@ -173,6 +182,9 @@ struct WosLaunch {
   // Gradient mode (kModeGradient): per-walk grad U and grad P, 6 values of
   // the walk type per walk.
   void *grad_out;
+  // Mixed form: a step whose grid bound is at least grid_tau spacings takes
+  // it as the ball radius instead of querying the BVH (0: never).
+  float grid_tau;
 };
 
 // Walk-to-boundary mode of the walk kernel (walk_to_boundary,
@@ -332,6 +344,13 @@ cudaError_t launch_validate(const ValidateLaunch &V, cudaStream_t s);
 cudaError_t launch_ball_green(const double *cases, uint32_t n, double *out, uint32_t *error, cudaStream_t s);
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
                            double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s);
+// Fills a geometry's distance-bound grid (n = vertices of the grid described
+// in *geo_dev; its `grid` pointer is not read).
+cudaError_t launch_grid_build(const GeoDesc *geo_dev, uint64_t n, double margin, uint16_t *out, uint32_t *error,
+                              cudaStream_t s);
+// The walk step's grid bound at each point (original coordinates); NaN
+// outside the grid.
+cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_t n, double *out, cudaStream_t s);
 cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *index, void *scratch,
                         size_t scratch_bytes, cudaStream_t s);
 size_t topk_scratch_bytes(uint32_t n, uint32_t k);

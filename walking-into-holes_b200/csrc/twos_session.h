@@ -56,6 +56,7 @@ struct twos_mesh {
   cudaStream_t own_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
   twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
+  twos::DevBuf grid;  // distance-bound grid (uint16 per vertex), may be empty
   twos::DevBuf geo;  // one GeoDesc
   twos::GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
@@ -69,4 +70,5 @@ struct twos_mesh {
   int blocks_per_sm = 0;   // 0: as many as fit
   int vote = 0;            // 1: one kind of traversal unit per warp iteration
   int warm = 1;            // 1: seed each step's query with the previous nearest triangle
+  float grid_tau = 0.5f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
 };

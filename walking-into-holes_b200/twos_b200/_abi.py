@@ -23,7 +23,8 @@ DEVERR_QUERY, DEVERR_STACK, DEVERR_ITER, DEVERR_CONFIG = 1, 2, 4, 8
 
 EXPORTED = [
     "twos_abi_version", "twos_last_error", "twos_mesh_open", "twos_mesh_open_ply", "twos_mesh_close",
-    "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_estimate", "twos_estimate_device",
+    "twos_mesh_get_info", "twos_mesh_set_stream", "twos_closest_point", "twos_mesh_distance_bound", "twos_estimate",
+    "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
     "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc",
@@ -67,6 +68,7 @@ class Summary(ctypes.Structure):
         ("queries", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("launches", ctypes.c_uint32), ("error_flags", ctypes.c_uint32),
         ("node_tests", ctypes.c_uint64), ("plane_tests", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
+        ("grid_steps", ctypes.c_uint64),
     ]
 
 
@@ -77,12 +79,13 @@ class MeshInfo(ctypes.Structure):
         ("bounds_min", ctypes.c_double * 3), ("bounds_max", ctypes.c_double * 3),
         ("center", ctypes.c_double * 3), ("mixed_delta", ctypes.c_double),
         ("build_seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
+        ("grid_dims", ctypes.c_uint32 * 3), ("grid_pad", ctypes.c_uint32), ("grid_spacing", ctypes.c_double),
     ]
 
 
 class Tuning(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("refill", ctypes.c_int32), ("step_threshold", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("grid_threshold", ctypes.c_float)]
 
 
 class DesignParams(ctypes.Structure):
@@ -164,6 +167,7 @@ def load(path: Path | str | None = None):
     L.twos_mesh_get_info.argtypes = [vp, ctypes.POINTER(MeshInfo)]
     L.twos_mesh_set_stream.argtypes = [vp, vp]
     L.twos_closest_point.argtypes = [vp, i32, vp, u64, dbl, vp, vp]
+    L.twos_mesh_distance_bound.argtypes = [vp, vp, u64, vp]
     L.twos_estimate.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_estimate_device.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, ctypes.POINTER(Summary)]
     L.twos_mesh_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]

@@ -7,9 +7,12 @@ the workload's own request with fewer walks) for every candidate setting of
 * queue-refill threshold: idle lanes before a warp refills from the queue;
 * step threshold: finished queries before a warp takes its batched step;
 * resident blocks per SM (occupancy cap);
+* the mixed form's distance-grid threshold (grid spacings a bound must reach
+  before a step skips its closest-point query);
 
-and leaves the fastest (walk-kernel device time per closest-point query) set
-on the mesh.  Results can be cached in a JSON file keyed by the mesh's size and
+and leaves the fastest (walk-kernel device time per walk: every setting runs
+the same walks, and only the grid threshold changes how many steps they
+take) set on the mesh.  Results can be cached in a JSON file keyed by the mesh's size and
 the request's precision/mode, so a service tunes once per geometry class.
 """
 from __future__ import annotations
@@ -26,6 +29,7 @@ DEFAULT_GRID = {
     "refill": (1, 4),
     "step_threshold": (1, 4),
     "blocks_per_sm": (0,),
+    "grid_threshold": (0.25, 0.5, 1.0),
 }
 
 
@@ -37,7 +41,7 @@ def _key(mesh, config) -> str:
 def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, repeats=2, seed=0,
              cache: str | Path | None = None, cavities=None):
     """Pick the fastest launch tuning for `config` on `mesh`; returns
-    (best tuning dict, list of (tuning, seconds per query))."""
+    (best tuning dict, list of (tuning, seconds per walk))."""
     key = _key(mesh, config)
     if cache is not None and Path(cache).exists():
         table = json.loads(Path(cache).read_text())
@@ -59,7 +63,7 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
             calib.repeat = 5000 + r
             _, s = mesh.estimate(pick, calib, cavities=cavities)
             if r:  # the first run is a warm-up
-                times.append(s["walk_seconds"] / max(1, s["queries"]))
+                times.append(s["walk_seconds"] / max(1, s["paths"]))
         results.append((tuning, float(np.median(times))))
     best = min(results, key=lambda t: t[1])[0]
     mesh.set_tuning(**best)

@@ -130,15 +130,18 @@ class Mesh:
         handle = getattr(stream, "cuda_stream", stream)
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
-    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0):
-        t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm))
+    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.5):
+        """Walk-kernel launch tuning; grid_threshold is the mixed form's
+        distance-grid bound (in grid spacings) above which a step skips its
+        closest-point query, 0 to query every step."""
+        t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _abi.Tuning()
         check(_abi.load().twos_mesh_get_tuning(self._h, ctypes.byref(t)))
         return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
-                "blocks_per_sm": t.blocks_per_sm}
+                "blocks_per_sm": t.blocks_per_sm, "grid_threshold": t.grid_threshold}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
@@ -146,7 +149,7 @@ class Mesh:
         return {"vertices": i.vertices, "faces": i.faces, "bvh_nodes": i.bvh_nodes, "bvh_depth": i.bvh_depth,
                 "device": i.device, "bounds_min": list(i.bounds_min), "bounds_max": list(i.bounds_max),
                 "center": list(i.center), "mixed_delta": i.mixed_delta, "build_seconds": i.build_seconds,
-                "device_bytes": i.device_bytes}
+                "device_bytes": i.device_bytes, "grid_dims": list(i.grid_dims), "grid_spacing": i.grid_spacing}
 
     # ------------------------------------------------------------------ queries
     def closest_point(self, points, precision="fp64", query_radius=0.0, with_points=True):
@@ -157,6 +160,14 @@ class Mesh:
         check(_abi.load().twos_closest_point(self._h, PRECISIONS[precision], _ptr(pts), n, float(query_radius),
                                              _ptr(dist), _ptr(closest)))
         return (dist, closest) if with_points else dist
+
+    def distance_bound(self, points):
+        """The mixed form's distance-grid lower bound at each point
+        (twos_mesh_distance_bound); NaN outside the grid."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(len(pts))
+        check(_abi.load().twos_mesh_distance_bound(self._h, _ptr(pts), len(pts), _ptr(out)))
+        return out
 
     def inside(self, points):
         pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
