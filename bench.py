@@ -55,11 +55,12 @@ CANONICAL_SOURCE = "oracle/canonical_bytes.py --sites 96 --walks 64"
 
 def dram_traffic_per_launch(walks: int) -> float:
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one walk-
-    kernel launch, from one ncu capture of the full workload: 1.47 GB read +
-    4.92 GB written for 502,403,072 walks, 12.72 B per walk.  The traffic is
-    the per-walk samples and the lines they evict; the BVH itself (31 MB)
-    stays in L2, so it scales with the walks of the launch."""
-    return 12.72 * walks
+    kernel launch, from one ncu capture of the full workload: 2.83 GB read +
+    4.33 GB written for 502,403,072 walks, 14.25 B per walk.  The traffic is
+    the per-walk samples and the lines they evict; the BVH (31 MB) and the
+    distance grid (32 MB) stay in L2, so it scales with the walks of the
+    launch."""
+    return 14.25 * walks
 
 
 EPSILON = 1e-4
@@ -350,7 +351,7 @@ def run_ours(args):
         canon = CANONICAL_BYTES_PER_QUERY * bvh_queries / walk_s / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "traffic": dram_traffic_per_launch(n * args.walks),
-                "traffic_source": "profiles/wos_kernel_noise_sphere_L7.md (ncu, full workload, 12.72 B/walk)",
+                "traffic_source": "profiles/wos_kernel_noise_sphere_L7.md (ncu, full workload, 14.25 B/walk)",
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "bytes_per_walk": float(fetched / (n * args.walks)),
                 "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test"
