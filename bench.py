@@ -452,8 +452,8 @@ def run_housing_box(args):
     walks with a Green point per step; mixed form at eps in {1e-3, 1e-4,
     1e-5}: site-estimates/s over `--sites` sites x `--walks` walks, and the
     error of the cross-index TD against the FP64 form with 16x the walks on
-    the first `--ref-sites` sites (RMS error, and its ratio to the mixed
-    form's own standard error)."""
+    the first `--ref-sites` sites (RMS error, and z = error / combined
+    standard error), also with the distance grid off."""
     import torch
     import twos_b200 as tb
     from twos_b200 import geometry, sources
@@ -480,12 +480,27 @@ def run_housing_box(args):
         est = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
         m = args.ref_sites
         ref, _ = mesh.estimate(sites[:m], tb.Config(walks=16 * args.walks, precision="fp64", **dict(base, seed=SEED + 1)))
-        err = est["score"][:m] - ref["score"]
-        ok = est["score_se"][:m] > 0  # sites where some walk pair saw both sources
+        # The same sites in the mixed form with the distance grid off: the
+        # grid's share of the error, if any.
+        mesh.set_tuning(grid_threshold=0)
+        off, _ = mesh.estimate(sites[:m], cfg)
+        mesh.set_tuning()
+
+        def errors(e):
+            err = e["score"] - ref["score"]
+            comb = np.hypot(e["score_se"], ref["score_se"])
+            ok = comb > 0  # sites where some walk pair saw both sources
+            z = err[ok] / comb[ok]
+            return float(np.sqrt(np.mean(err ** 2))), float(np.median(np.abs(z))), float(np.mean(np.abs(z) < 3))
+
+        rms, zmed, z3 = errors(est[:m])
+        rms_off, zmed_off, z3_off = errors(off)
         rows.append({"epsilon": eps, "site_estimates_per_s": n / dt, "seconds": dt,
                      "mean_steps_per_walk": summ["steps"] / summ["paths"],
-                     "td_rms_error_vs_fp64_16x": float(np.sqrt(np.mean(err ** 2))),
-                     "td_rms_error_over_se": float(np.sqrt(np.mean((err[ok] / est["score_se"][:m][ok]) ** 2))),
+                     "grid_steps_share": summ["grid_steps"] / max(1, summ["steps"]),
+                     "td_rms_error_vs_fp64_16x": rms, "td_median_abs_z": zmed, "td_share_abs_z_below_3": z3,
+                     "grid_off": {"td_rms_error_vs_fp64_16x": rms_off, "td_median_abs_z": zmed_off,
+                                  "td_share_abs_z_below_3": z3_off},
                      "td_rms": float(np.sqrt(np.mean(ref["score"] ** 2)))})
     mesh.close()
     return {"workload": "housing-like box minus cylinders (BASELINE config 4)", "triangles": int(len(F)),

@@ -539,15 +539,23 @@ __device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, ui
 }
 
 // Dynamic shared memory: the launch's job, geometry and term tables.
+// Job and geometry descriptors are copied to shared memory when they take at
+// most kTableSmem bytes, which keeps 8 blocks of 128 threads (with their
+// traversal stacks) resident per SM; a launch with more jobs reads them from
+// global memory (through L1) instead of giving up resident blocks.
+constexpr uint32_t kTableSmem = 2048;
 struct SmemPlan {
   uint32_t geo_offset, term_offset, bytes;
+  bool tables;  // jobs and geometries in shared memory
 };
 template <typename T> __host__ __device__ inline SmemPlan smem_plan(uint32_t n_jobs, uint32_t n_geos, uint32_t n_terms) {
   SmemPlan p;
   const uint32_t jobs = n_jobs * static_cast<uint32_t>(sizeof(JobDesc));
-  p.geo_offset = (jobs + 15u) & ~15u;
-  const uint32_t geos = p.geo_offset + n_geos * static_cast<uint32_t>(sizeof(GeoDesc));
-  p.term_offset = (geos + 15u) & ~15u;
+  const uint32_t geo_offset = (jobs + 15u) & ~15u;
+  const uint32_t geos = geo_offset + n_geos * static_cast<uint32_t>(sizeof(GeoDesc));
+  p.tables = geos <= kTableSmem;
+  p.geo_offset = p.tables ? geo_offset : 0u;
+  p.term_offset = p.tables ? (geos + 15u) & ~15u : 0u;
   p.bytes = p.term_offset + n_terms * static_cast<uint32_t>(sizeof(TermT<T>));
   return p;
 }
@@ -588,12 +596,16 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
   uint2 *s_stack = reinterpret_cast<uint2 *>(s_dyn);
   unsigned char *s_tab = s_dyn + kStack * BLOCK * sizeof(uint2);
   const SmemPlan plan = smem_plan<T>(L.n_jobs, L.n_geos, L.n_terms);
-  JobDesc *s_jobs = reinterpret_cast<JobDesc *>(s_tab);
-  GeoDesc *s_geos = reinterpret_cast<GeoDesc *>(s_tab + plan.geo_offset);
+  const JobDesc *s_jobs = plan.tables ? reinterpret_cast<const JobDesc *>(s_tab) : L.jobs;
+  const GeoDesc *s_geos = plan.tables ? reinterpret_cast<const GeoDesc *>(s_tab + plan.geo_offset) : L.geos;
   TermT<T> *s_terms = reinterpret_cast<TermT<T> *>(s_tab + plan.term_offset);
 
-  for (uint32_t i = threadIdx.x; i < L.n_jobs; i += blockDim.x) s_jobs[i] = L.jobs[i];
-  for (uint32_t i = threadIdx.x; i < L.n_geos; i += blockDim.x) s_geos[i] = L.geos[i];
+  if (plan.tables) {
+    JobDesc *tj = reinterpret_cast<JobDesc *>(s_tab);
+    GeoDesc *tg = reinterpret_cast<GeoDesc *>(s_tab + plan.geo_offset);
+    for (uint32_t i = threadIdx.x; i < L.n_jobs; i += blockDim.x) tj[i] = L.jobs[i];
+    for (uint32_t i = threadIdx.x; i < L.n_geos; i += blockDim.x) tg[i] = L.geos[i];
+  }
   for (uint32_t i = threadIdx.x; i < L.n_terms; i += blockDim.x) {
     const TermDev &d = L.terms[i];
     TermT<T> t;
