@@ -251,7 +251,10 @@ typedef struct twos_tuning {
   float grid_threshold;  /* mixed form: a step takes its radius from the
                             distance-bound grid when the bound is at least
                             this many grid spacings (>= 0.25); 0 = every step
-                            queries the BVH.  Default 0.5. */
+                            queries the BVH.  Default 0.25. */
+  int32_t units;         /* traversal units (node visits or triangle tests) a
+                            lane runs back to back before its warp returns to
+                            the refill and step ballots (1..64).  Default 8. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);

@@ -1,6 +1,8 @@
 """Launch tuning (twos_mesh_set_tuning) and the autotuner: results are a pure
 function of the request and the samples, so every block size, refill
-threshold, step threshold and occupancy cap gives bit-identical rows."""
+threshold, step threshold, occupancy cap and traversal-unit count gives
+bit-identical rows (the distance-grid threshold changes the walks' radii and
+is held fixed)."""
 import numpy as np
 import pytest
 
@@ -22,16 +24,22 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
                                          (256, 4, 16, 1)]:
             mesh.set_tuning(block=block, refill=refill, step_threshold=step, blocks_per_sm=bps)
             assert mesh.get_tuning() == {"block": block, "refill": refill, "step_threshold": step,
-                                         "blocks_per_sm": bps, "grid_threshold": 0.5}
+                                         "blocks_per_sm": bps, "grid_threshold": 0.25, "units": 8}
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {block} {refill} {step} {bps}")
+        for units in (1, 3, 64):
+            mesh.set_tuning(units=units)
+            out, _ = mesh.estimate(eval_points, cfg)
+            for k in ("u", "score", "score_se", "steps"):
+                np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} units={units}")
 
 
 def test_invalid_tuning_is_usage_error(tb, bunny1000):
     with tb.Mesh(*bunny1000) as mesh:
         for bad in [dict(block=96), dict(refill=0), dict(step_threshold=33), dict(blocks_per_sm=-1),
-                    dict(grid_threshold=0.2), dict(grid_threshold=-1.0), dict(grid_threshold=float("nan"))]:
+                    dict(grid_threshold=0.2), dict(grid_threshold=-1.0), dict(grid_threshold=float("nan")),
+                    dict(units=0), dict(units=65)]:
             with pytest.raises(tb.TwosError) as e:
                 mesh.set_tuning(**bad)
             assert e.value.code == 2

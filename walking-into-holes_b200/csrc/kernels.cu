@@ -632,6 +632,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
 
   int phase = kIdle;
   bool exhausted = false;  // warp-uniform
+  const int units = L.units > 0 ? L.units : 1;
   // Walk state.
   uint64_t wid = 0;
   uint32_t job = 0, site = 0, walk = 0, steps = 0;
@@ -933,67 +934,72 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
     }
     if (take) {
       const GeoDesc &G = s_geos[s_jobs[job].geo];
-      if (++iter > G.max_iter) {
-        err |= TWOS_DEVERR_ITER;
-        found = false;
-        phase = kStep;
-      } else if (tri_cur < tri_end) {
-        const typename Layout<T>::Tri *tris = geo_tris<T>(G);
-        ++c_planes;
-        if (tri_test(tris, tri_cur, pos, best2, c_tris)) {
-          found = true;
-          best_tri = tri_cur;
-          tri_ok = true;
-        }
-        ++tri_cur;
-      } else {
-        // Pop the next entry still closer than the current best.
-        while (!have && sp > 0) {
-          --sp;
-          const uint2 e = stack[sp * BLOCK];
-          if (static_cast<T>(__uint_as_float(e.y)) < best2) {
-            node = static_cast<int>(e.x);
-            have = true;
-          }
-        }
-        if (!have) {
+      // Up to `units` units back to back before the warp returns to the
+      // refill and step ballots: the loop overhead is paid once per batch.
+#pragma unroll 1
+      for (int unit = 0; unit < units && phase == kTraverse; ++unit) {
+        if (++iter > G.max_iter) {
+          err |= TWOS_DEVERR_ITER;
+          found = false;
           phase = kStep;
-        } else if (node >= 0) {
-          ++c_nodes;
-          T dl, dr;
-          int cl, cr;
-          node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
-          const bool vl = dl < best2, vr = dr < best2;
-          if (vl && vr) {
-            if (dr < dl) {
-              const T td = dl;
-              dl = dr;
-              dr = td;
-              const int tc = cl;
-              cl = cr;
-              cr = tc;
+        } else if (tri_cur < tri_end) {
+          const typename Layout<T>::Tri *tris = geo_tris<T>(G);
+          ++c_planes;
+          if (tri_test(tris, tri_cur, pos, best2, c_tris)) {
+            found = true;
+            best_tri = tri_cur;
+            tri_ok = true;
+          }
+          ++tri_cur;
+        } else {
+          // Pop the next entry still closer than the current best.
+          while (!have && sp > 0) {
+            --sp;
+            const uint2 e = stack[sp * BLOCK];
+            if (static_cast<T>(__uint_as_float(e.y)) < best2) {
+              node = static_cast<int>(e.x);
+              have = true;
             }
-            if (sp >= kStack) {
-              err |= TWOS_DEVERR_STACK;
-              found = false;
-              phase = kStep;
-            } else {
-              stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
-              ++sp;
+          }
+          if (!have) {
+            phase = kStep;
+          } else if (node >= 0) {
+            ++c_nodes;
+            T dl, dr;
+            int cl, cr;
+            node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
+            const bool vl = dl < best2, vr = dr < best2;
+            if (vl && vr) {
+              if (dr < dl) {
+                const T td = dl;
+                dl = dr;
+                dr = td;
+                const int tc = cl;
+                cl = cr;
+                cr = tc;
+              }
+              if (sp >= kStack) {
+                err |= TWOS_DEVERR_STACK;
+                found = false;
+                phase = kStep;
+              } else {
+                stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+                ++sp;
+                node = cl;
+              }
+            } else if (vl) {
               node = cl;
+            } else if (vr) {
+              node = cr;
+            } else {
+              have = false;
             }
-          } else if (vl) {
-            node = cl;
-          } else if (vr) {
-            node = cr;
           } else {
+            const uint32_t enc = ~static_cast<uint32_t>(node);
+            tri_cur = enc >> 3;
+            tri_end = tri_cur + (enc & 7u);
             have = false;
           }
-        } else {
-          const uint32_t enc = ~static_cast<uint32_t>(node);
-          tri_cur = enc >> 3;
-          tri_end = tri_cur + (enc & 7u);
-          have = false;
         }
       }
     }

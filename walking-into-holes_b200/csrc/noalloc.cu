@@ -151,6 +151,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.vote = m->vote;
     L.warm = m->warm;
     L.grid_tau = m->grid_tau;
+    L.units = m->units;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;

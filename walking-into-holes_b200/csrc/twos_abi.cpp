@@ -183,6 +183,7 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_BLOCKS_PER_SM")) m->blocks_per_sm = std::max(0, std::atoi(e));
     if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
+    if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
     if (const char *e = std::getenv("TWOS_BLOCK")) {
       const int b = std::atoi(e);
       if (b == 128 || b == 256 || b == 512) m->block = b;
@@ -392,6 +393,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.vote = m->vote;
   L.warm = m->warm;
   L.grid_tau = m->grid_tau;
+  L.units = m->units;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -561,13 +563,15 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if (!m || !t) return fail(TWOS_ERR_USAGE, "null argument");
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
-      !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.25f && t->grid_threshold <= 1e6f)))
+      !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.25f && t->grid_threshold <= 1e6f)) ||
+      t->units < 1 || t->units > 64)
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
   m->step_threshold = t->step_threshold;
   m->blocks_per_sm = t->blocks_per_sm;
   m->grid_tau = t->grid_threshold;
+  m->units = t->units;
   return TWOS_OK;
 }
 
@@ -578,6 +582,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->step_threshold = m->step_threshold;
   t->blocks_per_sm = m->blocks_per_sm;
   t->grid_threshold = m->grid_tau;
+  t->units = m->units;
   return TWOS_OK;
 }
 
@@ -888,6 +893,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.vote = m->vote;
     Ls.warm = m->warm;
     Ls.grid_tau = m->grid_tau;
+    Ls.units = m->units;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -1456,6 +1462,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.vote = m->vote;
         L.warm = m->warm;
         L.grid_tau = m->grid_tau;
+        L.units = m->units;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;

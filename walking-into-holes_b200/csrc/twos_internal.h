@@ -185,6 +185,9 @@ struct WosLaunch {
   // Mixed form: a step whose grid bound is at least grid_tau spacings takes
   // it as the ball radius instead of querying the BVH (0: never).
   float grid_tau;
+  // Traversal units (node visits / triangle tests) a lane runs back to back
+  // per iteration of the warp loop (>= 1).
+  int units;
 };
 
 // Walk-to-boundary mode of the walk kernel (walk_to_boundary,

@@ -9,6 +9,7 @@ the workload's own request with fewer walks) for every candidate setting of
 * resident blocks per SM (occupancy cap);
 * the mixed form's distance-grid threshold (grid spacings a bound must reach
   before a step skips its closest-point query);
+* traversal units a lane runs per iteration of the warp loop;
 
 and leaves the fastest (walk-kernel device time per walk: every setting runs
 the same walks, and only the grid threshold changes how many steps they
@@ -29,7 +30,8 @@ DEFAULT_GRID = {
     "refill": (1, 4),
     "step_threshold": (1, 4),
     "blocks_per_sm": (0,),
-    "grid_threshold": (0.25, 0.5, 1.0),
+    "grid_threshold": (0.25, 0.5),
+    "units": (4, 8, 16),
 }
 
 

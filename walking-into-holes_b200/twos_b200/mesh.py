@@ -130,18 +130,20 @@ class Mesh:
         handle = getattr(stream, "cuda_stream", stream)
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
-    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.5):
+    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.25, units=8):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
-        closest-point query, 0 to query every step."""
-        t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold))
+        closest-point query, 0 to query every step; units is the number of
+        traversal units a lane runs per warp-loop iteration."""
+        t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold),
+                        int(units))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _abi.Tuning()
         check(_abi.load().twos_mesh_get_tuning(self._h, ctypes.byref(t)))
         return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
-                "blocks_per_sm": t.blocks_per_sm, "grid_threshold": t.grid_threshold}
+                "blocks_per_sm": t.blocks_per_sm, "grid_threshold": t.grid_threshold, "units": t.units}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
