@@ -79,6 +79,7 @@ def parse_args(argv=None):
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the session's default launch tuning")
     ap.add_argument("--no-ablation", action="store_true",
                     help="skip the one-step mixed-form run with the distance grid off")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -288,6 +289,13 @@ def run_ours(args):
         total = max_over_ranks(total, dist, "cuda")
         return total, ms, summs
 
+    tuning = mesh.get_tuning()
+    if not args.no_autotune:
+        # The product's autotuner on a calibration subset, before any timing:
+        # every rank tunes its own session the same way.
+        from twos_b200.autotune import autotune
+        tuning, _ = autotune(mesh, sites, tb.Config(precision="mixed", **base), calib_sites=4096, calib_walks=128,
+                             repeats=2, seed=rank)
     clocks = ClockSampler(local)
     clocks.start()
     cfg_mixed = tb.Config(precision="mixed", **base)
@@ -311,10 +319,10 @@ def run_ours(args):
                 "h_median": h64, "walk_seconds": float(np.mean([s["walk_seconds"] for s in s64]))}
     no_grid = None
     if not args.no_ablation:
-        mesh.set_tuning(grid_threshold=0)
+        mesh.set_tuning(**dict(tuning, grid_threshold=0))
         t_ng, ms_ng, s_ng = timed(tb.Config(precision="mixed", **base), 1, 1)
         rows_ng = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
-        mesh.set_tuning()
+        mesh.set_tuning(**tuning)
         no_grid = {"rate_unscaled": world * n / (t_ng / 1e3), "ms_per_step": t_ng,
                    "h_median": float(np.median(1.96 * rows_ng["score_se"])),
                    "walk_seconds": s_ng[0]["walk_seconds"], "steps_per_walk": s_ng[0]["steps"] / s_ng[0]["paths"]}
@@ -383,7 +391,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "sites": int(n), "walks": args.walks, "epsilon": EPSILON,
                        "max_steps": MAX_STEPS, "mesh_triangles": int(info["faces"]),
                        "bvh_nodes": int(info["bvh_nodes"]), "mixed_delta": info["mixed_delta"],
-                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                       "tuning": tuning},
             "ci": {"h_mixed_median": h_mixed, "h_fp64_median": h_ref, "scale": scale,
                    "rate_mixed_unscaled": rate_mixed},
             "fp64_form": fp64,
