@@ -84,7 +84,7 @@ def parse_args(argv=None):
                     help="skip the one-step mixed-form run with the distance grid off")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design"], default="noise-sphere",
-                    help="housing: the BASELINE config-4 epsilon sweep; batch: config 3 (separate JSON lines)")
+                    help="housing: the box-minus-cylinders epsilon sweep; batch: 32 uneven meshes in one launch; design: the graph-captured design loop (separate JSON lines)")
     ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
     ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
     return ap.parse_args(argv)
@@ -455,7 +455,7 @@ def run_reference(args):
 
 
 def run_housing_box(args):
-    """BASELINE config 4 (not the headline line): box 4 x 2 x 1 minus 6
+    """Housing-like workload (not the headline line): box 4 x 2 x 1 minus 6
     through-cylinders of radius 0.15 (centres from seed 34), 529,608
     triangles; f = 1 on x0 < 1, adjoint q = 1_{x0 > 3} / |{x0 > 3}|; paired
     walks with a Green point per step; mixed form at eps in {1e-3, 1e-4,
@@ -512,13 +512,13 @@ def run_housing_box(args):
                                   "td_share_abs_z_below_3": z3_off},
                      "td_rms": float(np.sqrt(np.mean(ref["score"] ** 2)))})
     mesh.close()
-    return {"workload": "housing-like box minus cylinders (BASELINE config 4)", "triangles": int(len(F)),
+    return {"workload": "housing-like box 4x2x1 minus 6 cylinders, 529,608 triangles, 1M sites", "triangles": int(len(F)),
             "sites": n, "walks": args.walks, "reference": f"FP64 form, {16 * args.walks} walks, {args.ref_sites} sites",
             "dtype": "f32 query/position, f64 accumulation", "data": "synthetic", "per_epsilon": rows}
 
 
 def run_batch(args):
-    """BASELINE config 3 (not the headline line): 32 noise-displaced
+    """Batched uneven workload (not the headline line): 32 noise-displaced
     icospheres (seeds 2-33, subdivision levels uniform in 3..7), site counts
     log-uniform in [100, 50000] (uniform in the ball r < 0.5, kept when
     inside), walks per site log-uniform in [256, 8192]; compliance, f = 1,
@@ -558,7 +558,7 @@ def run_batch(args):
     best, table = autotune.autotune(meshes[big], sites[big], cfgs[big])
     for m in meshes:
         m.close()
-    return {"workload": "32 uneven noise spheres in one launch (BASELINE config 3)", "jobs": info,
+    return {"workload": "32 uneven noise spheres (levels 3-7) in one launch", "jobs": info,
             "sites": total_sites, "walks": int(total_walks), "dtype": "f32 query/position, f64 accumulation",
             "data": "synthetic",
             "batched": {"seconds": t_batch, "site_estimates_per_s": total_sites / t_batch,
@@ -570,8 +570,8 @@ def run_batch(args):
 
 
 def run_design(args):
-    """BASELINE config 5 (not the headline line): the design loop captured as
-    a CUDA graph on the config-1 geometry (unit icosphere L4).  Each of 20
+    """Design-loop workload (not the headline line): the design loop captured as
+    a CUDA graph on the unit icosphere L4.  Each of 20
     iterations scouts 100,000 candidates (uniform in r < 0.85) with 2,048
     walks, takes the top 64, validates them with 4,096 fresh walks (stream
     1), takes the best lower bound score - 1.96 SE and inserts a ball cavity
@@ -585,7 +585,7 @@ def run_design(args):
     cand = geometry.uniform_ball(100_000, 0.85, seed=5)
     kw = dict(iterations=20, shortlist=64, cavity_radius=0.03, z=1.96, accept_threshold=0.02,
               outer_clearance=0.02, pair_gap=0.01)
-    out = {"workload": "design loop as a CUDA graph (BASELINE config 5)", "candidates": len(cand), **kw,
+    out = {"workload": "design loop as a CUDA graph: 20 iterations on the unit icosphere L4, 100k candidates", "candidates": len(cand), **kw,
            "scout_walks": 2048, "validate_walks": 4096, "data": "synthetic"}
     hist = {}
     with tb.Mesh(V, F) as mesh:

@@ -410,7 +410,7 @@ int twos_diffwos(twos_mesh *mesh, const twos_request *request, double diff_offse
                  twos_diff_result *out, twos_diff_stats *stats, twos_summary *summary);
 
 /* Gradient estimates and the cross-index gradient product (the Neumann-
- * cavity topological derivative of the plain method, BASELINE config 1; no
+ * cavity topological derivative of the plain method on the unit sphere; no
  * reference counterpart: the reference implements only Dirichlet cavities,
  * paper/sections/03_problem.tex:153).  A paired request (source = the
  * primal's f, adjoint = the adjoint's source q, boundary = the primal's

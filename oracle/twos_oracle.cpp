@@ -1431,7 +1431,7 @@ int oracle_validate(const oracle_mesh *om, const oracle_params *o, double radius
 //   grad U = (3/R) (U - u0) w + R (1 - t^3) f(x + t R w') w'
 // (likewise grad P with the adjoint source), plus Dirichlet data g of u at
 // the exit point on the mesh.  No reference counterpart: this is the plain
-// method's Neumann-cavity estimator.
+// method's Neumann-cavity estimator (unit sphere, harmonic Dirichlet data).
 
 namespace {
 

@@ -1,7 +1,7 @@
 """The gradient form (twos_estimate_gradient): first-ball gradient samples,
 Dirichlet boundary data and the cross-index gradient product behind the
-Neumann-cavity topological derivative of the plain method (
-unit-sphere icosphere L4, g = x0^2 - x1^2 + 0.5 x2, adjoint source the mean
+Neumann-cavity topological derivative of the plain method (the unit-sphere
+workload: icosphere L4, g = x0^2 - x1^2 + 0.5 x2, adjoint source the mean
 over r < 0.5, 64 sites uniform in r < 0.9 from seed 0, 1024 walks, eps 1e-4,
 FP64).  The reference has no Neumann cavity, so the checks are the oracle
 (counter stream) and the analytic fields: u = g (harmonic), grad u =

@@ -1,4 +1,4 @@
-"""BASELINE config 4's geometry and sources at test size: the box 4 x 2 x 1
+"""The housing-like workload's geometry and sources at test size: the box 4 x 2 x 1
 minus six through-cylinders (builder-written mesher, seed 34), f = 1 on
 x0 < 1, adjoint q = 1_{x0 > 3} / |{x0 > 3}| with a Green point per step.
 

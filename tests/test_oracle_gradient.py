@@ -1,5 +1,6 @@
 """The oracle's gradient form against the analytic fields of the plain
-method (see tests/test_gpu_gradient.py for the fields).
+method (the unit-sphere workload; see tests/test_gpu_gradient.py for the
+fields).
 No reference output exists for a Neumann cavity (the reference implements
 only Dirichlet cavities), so this pins the restatement to the analytic
 u = g, grad u . grad p and their standard errors."""
