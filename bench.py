@@ -348,10 +348,11 @@ def run_ours(args):
         # Bytes the walk kernel must fetch: 96 B per node visit (two child
         # boxes + normal slabs + child words), 32 B per triangle plane test
         # (plane slab + first vertex), 32 B more per full closest-point test
-        # (the other two vertices), counted on the device; one 32 B sector
-        # per distance-grid lookup (one after every step).
+        # (the other two vertices), counted on the device; four 32 B sectors
+        # per distance-grid lookup (the cell's eight corners lie in four
+        # (i, j) rows; one lookup after every step).
         grid_lookups = steps if info["grid_dims"][0] else 0.0
-        fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris + 32.0 * grid_lookups
+        fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris + 128.0 * grid_lookups
         bvh_queries = queries - grid_steps
         peak, peak_kind = measured_peaks()
         ach = fetched / walk_s / 1e9
@@ -363,7 +364,7 @@ def run_ours(args):
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "bytes_per_walk": float(fetched / (n * args.walks)),
                 "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test"
-                                    " + 32 B/distance-grid lookup (one per step)",
+                                    " + 128 B/distance-grid lookup (one per step)",
                 "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),
                 "bvh_queries_per_launch": float(bvh_queries), "walk_kernel_seconds": walk_s,
                 "bvh_queries_per_second": float(bvh_queries / walk_s),

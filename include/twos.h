@@ -250,8 +250,8 @@ typedef struct twos_tuning {
   int32_t blocks_per_sm;
   float grid_threshold;  /* mixed form: a step takes its radius from the
                             distance-bound grid when the bound is at least
-                            this many grid spacings (>= 0.25); 0 = every step
-                            queries the BVH.  Default 0.25. */
+                            this many grid spacings (>= 0.1); 0 = every step
+                            queries the BVH.  Default 0.1. */
   int32_t units;         /* traversal units (node visits or triangle tests) a
                             lane runs back to back before its warp returns to
                             the refill and step ballots (1..64).  Default 8. */
@@ -267,8 +267,9 @@ int twos_closest_point(twos_mesh *mesh, int precision, const double *points, uin
                        double query_radius, double *distance, double *closest);
 
 /* The mixed form's distance-grid lower bound at each point (the radius a
- * grid step would take before the threshold test: D(v) - |x - v| at the
- * nearest grid vertex v), NaN outside the grid or when the session has none.
+ * grid step would take before the threshold test: the largest D(v) - |x - v|
+ * over the corners v of x's grid cell), NaN outside the grid or when the
+ * session has none.
  * Never above the distance to the surface.  Host buffers.  No reference
  * counterpart. */
 int twos_mesh_distance_bound(twos_mesh *mesh, const double *points, uint64_t n, double *bound);

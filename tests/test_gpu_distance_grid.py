@@ -3,9 +3,10 @@ step when the bound clears grid_threshold spacings).
 
 * The bound never exceeds the FP64 distance to the surface (inside, outside
   and near the surface), and is tight: at least d - sqrt(3) h - 3 delta - h/128
-  at every point inside the grid (the nearest vertex is within sqrt(3) h / 2,
-  the distance is 1-Lipschitz, the stored value is the FP32 distance less
-  2 delta rounded down to h/128).
+  at every point inside the grid (the bound is the best of the cell's eight
+  corners, the nearest of which is within sqrt(3) h / 2; the distance is
+  1-Lipschitz; the stored value is the FP32 distance less 2 delta rounded
+  down to h/128).
 * The grid is sized from the triangle count (64 vertices per triangle, at
   most 2^24) and TWOS_GRID_VERTICES=0 builds none.
 * Walks with grid steps estimate the same field: on the unit ball the mixed

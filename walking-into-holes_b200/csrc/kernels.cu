@@ -506,9 +506,10 @@ __device__ __forceinline__ Vec<float> grid_vertex(const GeoDesc &g, uint32_t i, 
           __fadd_rn(g.grid_lo[2], __fmul_rn(static_cast<float>(k), g.grid_h))};
 }
 
-// The grid's lower bound of the mesh distance at `p` (FP32 frame): D(v) -
-// |p - v| at the nearest vertex v (the distance is 1-Lipschitz).  False when
-// p lies outside the grid (or is NaN).
+// The grid's lower bound of the mesh distance at `p` (FP32 frame): the
+// largest D(v) - |p - v| over the eight corners v of p's cell (the distance
+// is 1-Lipschitz, so each is a bound).  False when p lies outside the grid
+// (or is NaN).
 __device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p, float &bound) {
   const float fx = (p.x - g.grid_lo[0]) * g.grid_inv_h;
   const float fy = (p.y - g.grid_lo[1]) * g.grid_inv_h;
@@ -516,13 +517,23 @@ __device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p
   if (!(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx <= static_cast<float>(g.grid_n[0] - 1) &&
         fy <= static_cast<float>(g.grid_n[1] - 1) && fz <= static_cast<float>(g.grid_n[2] - 1)))
     return false;
-  const uint32_t i = static_cast<uint32_t>(__float2int_rn(fx));
-  const uint32_t j = static_cast<uint32_t>(__float2int_rn(fy));
-  const uint32_t k = static_cast<uint32_t>(__float2int_rn(fz));
-  const Vec<float> v = grid_vertex(g, i, j, k);
-  const Vec<float> dv = sub(p, v);
-  bound = static_cast<float>(__ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k)) * g.grid_q -
-          sqrtf(dot3(dv, dv));
+  // The cell's lower corner (clamped so the cell lies inside the grid), then
+  // the best of its eight corners' bounds.
+  const uint32_t i0 = min(static_cast<uint32_t>(fx), g.grid_n[0] - 2);
+  const uint32_t j0 = min(static_cast<uint32_t>(fy), g.grid_n[1] - 2);
+  const uint32_t k0 = min(static_cast<uint32_t>(fz), g.grid_n[2] - 2);
+  float best = -CUDART_INF_F;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const uint32_t i = i0 + (c >> 2), j = j0 + ((c >> 1) & 1), k = k0 + (c & 1);
+    const Vec<float> v = grid_vertex(g, i, j, k);
+    const Vec<float> dv = sub(p, v);
+    const float b =
+        static_cast<float>(__ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k)) * g.grid_q -
+        sqrtf(dot3(dv, dv));
+    best = fmaxf(best, b);
+  }
+  bound = best;
   return true;
 }
 

@@ -563,7 +563,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if (!m || !t) return fail(TWOS_ERR_USAGE, "null argument");
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
-      !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.25f && t->grid_threshold <= 1e6f)) ||
+      !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
       t->units < 1 || t->units > 64)
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;

@@ -70,6 +70,6 @@ struct twos_mesh {
   int blocks_per_sm = 0;   // 0: as many as fit
   int vote = 0;            // 1: one kind of traversal unit per warp iteration
   int warm = 1;            // 1: seed each step's query with the previous nearest triangle
-  float grid_tau = 0.25f;  // mixed-form grid steps need a bound of this many spacings; 0 = off
+  float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
 };

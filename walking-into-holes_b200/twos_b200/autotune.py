@@ -30,7 +30,7 @@ DEFAULT_GRID = {
     "refill": (1, 4),
     "step_threshold": (1, 4),
     "blocks_per_sm": (0,),
-    "grid_threshold": (0.25, 0.5),
+    "grid_threshold": (0.1, 0.25),
     "units": (4, 8, 16),
 }
 

@@ -130,7 +130,7 @@ class Mesh:
         handle = getattr(stream, "cuda_stream", stream)
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
-    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.25, units=8):
+    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
         closest-point query, 0 to query every step; units is the number of
@@ -143,7 +143,9 @@ class Mesh:
         t = _abi.Tuning()
         check(_abi.load().twos_mesh_get_tuning(self._h, ctypes.byref(t)))
         return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
-                "blocks_per_sm": t.blocks_per_sm, "grid_threshold": t.grid_threshold, "units": t.units}
+                "blocks_per_sm": t.blocks_per_sm,
+                # The ABI keeps a float; report the shortest decimal that rounds to it (0.1, not 0.10000000149).
+                "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
