@@ -32,7 +32,7 @@ void write_field(const std::string &path, const std::vector<double> &points,
 
 void write_summary(const std::string &path, const twos_mesh_info &info, size_t n_cavities, const Options &o,
                    size_t site_count, const std::vector<double> &times, const std::vector<double> &kernel_times,
-                   uint64_t total_steps, uint64_t total_limits) {
+                   uint64_t total_steps, uint64_t total_limits, uint64_t grid_steps) {
   const double runtime = median(times);
   const double paths = static_cast<double>(site_count) * o.walks;
   std::ofstream out(path);
@@ -66,6 +66,7 @@ void write_summary(const std::string &path, const twos_mesh_info &info, size_t n
       << "  \"gpu_bvh_nodes\": " << info.bvh_nodes << ",\n"
       << "  \"gpu_bvh_depth\": " << info.bvh_depth << ",\n"
       << "  \"gpu_mixed_delta\": " << info.mixed_delta << ",\n"
+      << "  \"gpu_grid_steps\": " << grid_steps << ",\n"
       << "  \"timings_seconds\": [";
   for (size_t i = 0; i < times.size(); ++i) {
     if (i) out << ", ";
@@ -237,7 +238,7 @@ int run(const Options &o) {
   twos_request r = base_request(o);
   std::vector<double> times, kernel_times;
   std::vector<twos_site_result> retained(n);
-  uint64_t retained_steps = 0, retained_limits = 0;
+  uint64_t retained_steps = 0, retained_limits = 0, retained_grid_steps = 0;
   for (int repeat = 0; repeat < o.repeats; ++repeat) {
     std::vector<twos_site_result> results(n);
     r.repeat = static_cast<uint32_t>(repeat);
@@ -254,6 +255,7 @@ int run(const Options &o) {
       retained = std::move(results);
       retained_steps = s.steps;
       retained_limits = s.caps;
+      retained_grid_steps = s.grid_steps;
     }
   }
   if (retained_limits != 0) throw std::runtime_error("one or more paths hit --max-steps");
@@ -261,7 +263,7 @@ int run(const Options &o) {
   if (!o.trace_path.empty() && o.trace_sites > 0)
     std::cerr << "warning: --trace-output is not written by the TWoS B200 backend\n";
   write_summary(o.summary_path, info, cavities.size() / 3, o, n, times, kernel_times, retained_steps,
-                retained_limits);
+                retained_limits, retained_grid_steps);
   std::cout << "TWoS B200: " << n << " sites x " << o.walks << " walks, median " << median(times) << " s, "
             << std::fixed << std::setprecision(0) << (static_cast<double>(n) * o.walks / median(times))
             << " paths/s\n";
