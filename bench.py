@@ -83,8 +83,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-ablation", action="store_true",
                     help="skip the one-step mixed-form run with the distance grid off")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design"], default="noise-sphere",
-                    help="housing: the box-minus-cylinders epsilon sweep; batch: 32 uneven meshes in one launch; design: the graph-captured design loop (separate JSON lines)")
+    ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design", "unit-sphere"],
+                    default="noise-sphere",
+                    help="housing: the box-minus-cylinders epsilon sweep; batch: 32 uneven meshes in one launch; design: the graph-captured design loop; unit-sphere: the plain method's Neumann-cavity TD (separate JSON lines)")
     ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
     ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
     return ap.parse_args(argv)
@@ -611,6 +612,84 @@ def run_design(args):
     return out
 
 
+def run_unit_sphere(args):
+    """Plain-method workload (not the headline line): the unit sphere as an
+    icosphere L4 (5,120 triangles), Dirichlet data g = x0^2 - x1^2 + 0.5 x2,
+    adjoint source the mean over r < 0.5, 64 sites uniform in r < 0.9 (seed
+    0), 1,024 paired walks per site with a Green point, eps = 1e-4, FP64 (the
+    mixed form beside it).  The gradient form's cross-index product and the
+    Neumann-cavity TD D_T = 3/2 grad u . grad p - q u against the analytic
+    fields, GPU site-estimates/s through twos_estimate_gradient (host
+    buffers), and the oracle's restatement of the same form on the host
+    cores (counter stream, OpenMP) on the same 64 sites."""
+    import twos_b200 as tb
+    V, F = tb.geometry.icosphere(4)
+    rng = np.random.default_rng(0)
+    d = rng.normal(size=(64, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    sites = d * (0.9 * rng.random(64) ** (1 / 3))[:, None]
+    boundary = tb.sources.quadratic((1.0, -1.0, 0.0)) + tb.sources.linear(0.5, 2)
+    q = tb.sources.ball_mean_density((0.0, 0.0, 0.0), 0.5)
+    x0, x1, x2 = sites.T
+    g = x0 ** 2 - x1 ** 2 + 0.5 * x2
+    grad_g = np.c_[2 * x0, -2 * x1, 0.5 * np.ones(len(sites))]
+    r = np.linalg.norm(sites, axis=1)
+    c = 1.0 / (4.0 / 3.0 * np.pi * 0.5 ** 3)
+    grad_p = np.where(r[:, None] < 0.5, -c * sites / 3.0, -sites / (4.0 * np.pi * r[:, None] ** 3))
+    qx = np.where(r < 0.5, c, 0.0)
+    cross_exact = np.sum(grad_g * grad_p, axis=1)
+    td_exact = 1.5 * cross_exact - qx * g
+    base = dict(walks=1024, mode="paired", seed=SEED, epsilon=1e-4, max_steps=4096, green=True, source=[],
+                adjoint=q, boundary=boundary)
+    out = {"workload": "unit sphere (icosphere L4, 5,120 triangles), Neumann-cavity TD, 64 sites x 1,024 walks",
+           "data": "synthetic", "steps": args.steps, "warmup": args.warmup}
+    with tb.Mesh(V, F) as mesh:
+        for prec in ("fp64", "mixed"):
+            cfg = tb.Config(precision=prec, **base)
+            for w in range(args.warmup):
+                cfg.repeat = 1000 + w
+                mesh.estimate_gradient(sites, cfg)
+            times, ktimes = [], []
+            for k in range(args.steps):
+                cfg.repeat = k
+                t0 = time.perf_counter()
+                rows, summ = mesh.estimate_gradient(sites, cfg)
+                times.append(time.perf_counter() - t0)
+                ktimes.append(summ["kernel_seconds"])
+            z = (rows["cross"] - cross_exact) / rows["cross_se"]
+            td = 1.5 * rows["cross"] - qx * rows["u"]
+            out[prec] = {"site_estimates_per_s": len(sites) / float(np.median(times)),
+                         "seconds": float(np.median(times)), "kernel_seconds": float(np.median(ktimes)),
+                         "steps_per_walk": summ["steps"] / summ["paths"], "grid_steps": summ["grid_steps"],
+                         "cross_max_abs_z": float(np.max(np.abs(z))), "cross_share_abs_z_below_3":
+                         float(np.mean(np.abs(z) < 3)), "cross_mean_z": float(np.mean(z)),
+                         "u_mean_abs_error": float(np.mean(np.abs(rows["u"] - g))),
+                         "td_rms_error": float(np.sqrt(np.mean((td - td_exact) ** 2))),
+                         "td_rms": float(np.sqrt(np.mean(td_exact ** 2)))}
+    if not args.no_cpu:
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle
+        oracle.build()
+        threads = oracle.default_threads()
+        om = oracle.OracleMesh(V, F)
+
+        def terms(ts):
+            return [oracle.term(t.kind, t.amp, t.axis, t.offset, t.div, tuple(t.c), tuple(t.w)) for t in ts]
+
+        sub = sites
+        t0 = time.perf_counter()
+        om.estimate_gradient(sub, rng=oracle.RNG_COUNTER, mode=1, walks=1024, seed=SEED, epsilon=1e-4,
+                             max_steps=4096, green=True, source=[], adjoint=terms(q), boundary=terms(boundary),
+                             threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(sub) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{len(sub)} sites x 1024 walks, oracle restatement of the gradient "
+                                         f"form (counter stream), OpenMP {threads} threads, {dt:.1f} s"}
+        out["fp64_over_cpu"] = out["fp64"]["site_estimates_per_s"] / out["cpu_baseline"]["value"]
+    out["mixed_over_fp64"] = out["mixed"]["site_estimates_per_s"] / out["fp64"]["site_estimates_per_s"]
+    return out
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.workload == "design":
@@ -621,6 +700,9 @@ def main(argv=None):
         return
     if args.workload == "batch":
         print(json.dumps(run_batch(args)), flush=True)
+        return
+    if args.workload == "unit-sphere":
+        print(json.dumps(run_unit_sphere(args)), flush=True)
         return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:

@@ -99,6 +99,8 @@ def test_gradient_mixed_shares_samples(tb):
     base = dict(walks=512, mode="paired", seed=9, epsilon=1e-4, max_steps=4096, green=True, source=[], adjoint=q,
                 boundary=boundary)
     with tb.Mesh(V, F) as mesh:
+        # Distance grid off: the FP32 query alone keeps the FP64 form's paths.
+        mesh.set_tuning(grid_threshold=0)
         r64, _ = mesh.estimate_gradient(sites[:32], tb.Config(precision="fp64", **base))
         r32, _ = mesh.estimate_gradient(sites[:32], tb.Config(precision="mixed", **base))
     se = np.sqrt(r64["cross_se"] ** 2 + r32["cross_se"] ** 2)
