@@ -5,6 +5,8 @@ layouts, and the executables keep the reference's usage/runtime exit codes
 without touching a GPU.
 """
 import ctypes
+
+import numpy as np
 import re
 import subprocess
 
@@ -34,12 +36,24 @@ def test_abi_version_and_layouts(lib_built, tmp_path):
     L = _abi.load()
     assert L.twos_abi_version() == 1
     structs = {"twos_source_term": _abi.SourceTerm, "twos_request": _abi.Request,
-               "twos_site_result": _abi.SiteResult, "twos_summary": _abi.Summary, "twos_mesh_info": _abi.MeshInfo}
+               "twos_site_result": _abi.SiteResult, "twos_summary": _abi.Summary, "twos_mesh_info": _abi.MeshInfo,
+               "twos_tuning": _abi.Tuning, "twos_design_params": _abi.DesignParams,
+               "twos_design_step": _abi.DesignStep, "twos_rqmc_params": _abi.RqmcParams,
+               "twos_validate_params": _abi.ValidateParams}
+    # Result rows read as numpy structured arrays: field offsets and sizes.
+    dtypes = {"twos_site_result": _abi.SITE_DTYPE, "twos_gradient_result": _abi.GRADIENT_DTYPE,
+              "twos_diff_result": _abi.DIFF_DTYPE, "twos_diff_stats": _abi.DIFF_STATS_DTYPE,
+              "twos_cert_sample": _abi.CERT_SAMPLE_DTYPE, "twos_validate_stage": _abi.VALIDATE_STAGE_DTYPE,
+              "twos_design_step": _abi.DESIGN_DTYPE}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "twos.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for fname, _ in cls._fields_:
             lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    for cname, dt in dtypes.items():
+        lines.append(f'printf("np.{cname} %zu\\n", sizeof({cname}));')
+        for f in dt:
+            lines.append(f'printf("np.{cname}.{f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
     lines.append("return 0; }")
     src = tmp_path / "layout.c"
     src.write_text("\n".join(lines))
@@ -51,6 +65,13 @@ def test_abi_version_and_layouts(lib_built, tmp_path):
         assert int(got[cname]) == ctypes.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, (cname, fname)
+    for cname, dt in dtypes.items():
+        d = np.dtype(dt, align=True)
+        # The package builds these dtypes unaligned, so they must need no padding.
+        assert np.dtype(dt).itemsize == d.itemsize, cname
+        assert int(got[f"np.{cname}"]) == d.itemsize, cname
+        for f in dt:
+            assert int(got[f"np.{cname}.{f[0]}"]) == d.fields[f[0]][1], (cname, f[0])
 
 
 def test_request_validation_without_gpu(lib_built):
