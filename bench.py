@@ -393,6 +393,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "sites": int(n), "walks": args.walks, "epsilon": EPSILON,
                        "max_steps": MAX_STEPS, "mesh_triangles": int(info["faces"]),
                        "bvh_nodes": int(info["bvh_nodes"]), "mixed_delta": info["mixed_delta"],
+                       "distance_grid": {"dims": info["grid_dims"], "spacing": info["grid_spacing"],
+                                         "build_seconds_with_bvh": info["build_seconds"]},
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "tuning": tuning},
             "ci": {"h_mixed_median": h_mixed, "h_fp64_median": h_ref, "scale": scale,

@@ -207,8 +207,8 @@ const char *twos_last_error(void);
 
 /* Build a session from an in-memory triangle mesh: host BVH build, upload of
  * the FP32 and FP64 layouts to `device`, and the distance-bound grid of the
- * mixed form: a uniform grid over the padded bounding box (about 64 vertices
- * per triangle, at most 2^24; environment TWOS_GRID_VERTICES overrides, 0
+ * mixed form: a uniform grid over the padded bounding box (about 128 vertices
+ * per triangle, at most 2^25; environment TWOS_GRID_VERTICES sets it, up to 2^26; 0
  * builds none) holding at each vertex v a lower bound of the distance from v
  * to the surface (the FP32 distance minus twice the mixed form's error bound,
  * rounded down to 1/128 of the spacing h, 16 bits).  The distance function

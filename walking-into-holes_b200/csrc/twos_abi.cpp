@@ -55,16 +55,18 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 
 // Sizes and fills the mixed form's distance-bound grid of a session whose
 // BVH is on the device and whose geo_host describes it (m->geo allocated).
-// About 64 vertices per triangle (environment TWOS_GRID_VERTICES overrides;
-// 0 builds none), at most 2^24, over the bounding box padded by one spacing.
+// About 128 vertices per triangle, at most 2^25, over the bounding box padded
+// by one spacing (environment TWOS_GRID_VERTICES sets the count, up to 2^26;
+// 0 builds none).
 // Values are FP32 distances less 2 delta (the mixed form's own error bound,
 // covering the FP32 query and the vertex placement), in steps of h/128.
 void build_distance_grid(twos_mesh *m, size_t n_tris) {
   GeoDesc &g = m->geo_host;
   g.grid = nullptr;
-  uint64_t target = std::min<uint64_t>(std::max<uint64_t>(64ull * n_tris, 4096ull), 1ull << 24);
+  uint64_t target = std::min<uint64_t>(std::max<uint64_t>(128ull * n_tris, 4096ull), 1ull << 25);
   if (const char *e = std::getenv("TWOS_GRID_VERTICES"))
-    target = std::min<uint64_t>(std::strtoull(e, nullptr, 10), 1ull << 24);
+    target = std::min<uint64_t>(std::strtoull(e, nullptr, 10), 1ull << 26);
+  const uint64_t cap = std::max<uint64_t>(target, 1ull << 25);
   double ext[3], emax = 0.0;
   for (int a = 0; a < 3; ++a) {
     ext[a] = m->bmax[a] - m->bmin[a];
@@ -78,10 +80,10 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
   for (int it = 0;; ++it) {
     for (int a = 0; a < 3; ++a) n[a] = static_cast<uint64_t>(std::ceil(ext[a] / h)) + 3;
     const uint64_t total = n[0] * n[1] * n[2];
-    if ((total <= target + target / 2 && total <= (1ull << 24)) || it > 200) break;
+    if ((total <= target + target / 2 && total <= cap) || it > 200) break;
     h *= 1.03;
   }
-  if (n[0] * n[1] * n[2] > (1ull << 24)) return;
+  if (n[0] * n[1] * n[2] > cap) return;
   for (int a = 0; a < 3; ++a) {
     g.grid_lo[a] = static_cast<float>(m->bmin[a] - h - m->center[a]);
     g.grid_n[a] = static_cast<uint32_t>(n[a]);
