@@ -16,6 +16,10 @@
 //                    warp-shuffle reductions in a fixed order (wih_twos.cpp:
 //                    691-715; adjoint.cpp:36-41).
 //   closest_kernel   batched closest point (tests and the queries/s figure).
+//   grid_build_kernel / grid_bound_kernel
+//                    the mixed form's distance-bound grid: one FP32 closest-
+//                    point query per grid vertex at mesh open, and the bound
+//                    a walk step would use at given points.
 //   topk kernels     block-local bitonic top-k then a merge block.
 //
 // Compiled with -fmad=false: FP64 arithmetic is evaluated exactly as written
@@ -574,15 +578,18 @@ template <typename T> __host__ __device__ inline SmemPlan smem_plan(uint32_t n_j
 enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
 
 // Persistent walk-on-spheres kernel as a per-lane state machine.  Each loop
-// iteration every lane does at most one unit of work: one BVH node test or
-// one triangle test of its current closest-point query.  A lane whose query
+// iteration every traversing lane runs up to `units` units of work back to
+// back -- BVH node tests or triangle tests of its current closest-point query
+// -- and stops early when its query ends.  A lane whose query
 // has finished waits in kStep until at least `step_threshold` lanes of its
 // warp are ready (or no lane is still traversing); those lanes then take
 // their walk step together and start their next query, and lanes whose walk
 // ended refill from the work queue once `refill` lanes are idle.  So lanes
 // never wait for the slowest traversal of the warp, only for the batched
-// step.  MODE: TWOS_MODE_*; the per-walk value type is T (FP32 accumulation
-// in the mixed form, FP64 in the plain form).  SRC: TWOS_SOURCE_* (a
+// step.  In the mixed form a step first tries the geometry's distance-bound
+// grid and skips the query when the grid's bound is large enough.  MODE:
+// TWOS_MODE_*; the per-walk value type is T (FP32 accumulation in the mixed
+// form, FP64 in the plain form).  SRC: TWOS_SOURCE_* (a
 // template argument, so the exact-integral code of TWOS_SOURCE_EXACT adds no
 // registers to the other forms).
 // Residency: the FP32 form with the centre-point source fits 64 registers, so
