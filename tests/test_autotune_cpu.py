@@ -1,0 +1,73 @@
+"""The autotuner's host logic without a GPU: a stand-in mesh answers each
+calibration estimate with a walk-kernel time that depends on the tuning, so
+the sweep, the warm-up rule, the objective (seconds per walk, since the grid
+threshold changes the step count but not the walks) and the JSON cache can be
+checked exactly."""
+import json
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from twos_b200.autotune import DEFAULT_GRID, autotune
+
+
+@dataclass
+class Cfg:
+    walks: int = 512
+    precision: str = "mixed"
+    mode: str = "compliance"
+    green: bool = False
+    repeat: int = 0
+
+
+@dataclass
+class FakeMesh:
+    tuning: dict = field(default_factory=dict)
+    calls: list = field(default_factory=list)
+
+    def info(self):
+        return {"faces": 1234}
+
+    def set_tuning(self, **t):
+        self.tuning = dict(t)
+
+    def get_tuning(self):
+        return dict(self.tuning)
+
+    def estimate(self, sites, cfg, cavities=None):
+        t = self.tuning
+        self.calls.append((dict(t), cfg.walks, cfg.repeat, len(sites)))
+        paths = len(sites) * cfg.walks
+        # Fastest at block 256, step threshold 4, 8 units, grid 0.1; a low grid
+        # threshold adds steps (queries) but fewer seconds per walk.
+        per_walk = (1.0 + 0.1 * abs(t["block"] - 256) / 128 + 0.05 * (t["step_threshold"] != 4)
+                    + 0.02 * abs(t["units"] - 8) / 4 + 0.3 * t["grid_threshold"] + 0.01 * (t["refill"] != 1))
+        steps = paths * (30 if t["grid_threshold"] < 0.2 else 25)
+        if cfg.repeat == 5000:  # the warm-up run is slow and must be ignored
+            per_walk *= 100
+        return None, {"walk_seconds": per_walk * paths * 1e-9, "paths": paths, "queries": steps + paths}
+
+
+def test_autotune_sweeps_every_setting_and_picks_the_fastest(tmp_path):
+    mesh = FakeMesh()
+    sites = np.random.default_rng(0).normal(size=(10_000, 3))
+    cache = tmp_path / "tuning.json"
+    best, results = autotune(mesh, sites, Cfg(), calib_sites=100, calib_walks=64, repeats=2, cache=cache)
+    assert len(results) == np.prod([len(v) for v in DEFAULT_GRID.values()])
+    assert best == {"block": 256, "refill": 1, "step_threshold": 4, "blocks_per_sm": 0, "grid_threshold": 0.1,
+                    "units": 8}
+    assert mesh.get_tuning() == best
+    # Calibration: a seeded subset of the sites, the request's walks capped, one warm-up plus two timed runs.
+    assert all(n == 100 and w == 64 for _, w, _, n in mesh.calls)
+    assert len(mesh.calls) == 3 * len(results)
+    # Cached by mesh size and request shape; a second call reads the cache and runs nothing.
+    table = json.loads(cache.read_text())
+    assert list(table.values()) == [best]
+    mesh2 = FakeMesh()
+    again, cached = autotune(mesh2, sites, Cfg(), cache=cache)
+    assert again == best and cached == [] and mesh2.calls == [] and mesh2.get_tuning() == best
+    # Another precision is another key.
+    mesh3 = FakeMesh()
+    _, res3 = autotune(mesh3, sites, Cfg(precision="fp64"), calib_sites=50, calib_walks=32, repeats=1,
+                       cache=cache)
+    assert res3 and len(json.loads(cache.read_text())) == 2
