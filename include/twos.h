@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define TWOS_ABI_VERSION 1
+#define TWOS_ABI_VERSION 2
 
 enum { TWOS_OK = 0, TWOS_ERR_RUNTIME = 1, TWOS_ERR_USAGE = 2 };
 
@@ -295,27 +295,30 @@ int twos_estimate_device(twos_mesh *mesh, const twos_request *request, const dou
  *
  * Some callers must not call cudaMalloc: code running while a framework owns
  * the device memory pool (a raw cudaMalloc bypasses its allocator and
- * fragments memory it manages), code on paths that must not synchronise the
- * device (cudaMalloc/cudaFree may), and services with a fixed memory budget.
- * This entry point allocates nothing: every per-call device buffer (launch
- * tables, cavities, first-query distances, queue counter, totals and the
- * per-walk samples) is carved out of one static device array of
- * TWOS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
- * the process exits.  The mesh session (opened earlier with twos_mesh_open*),
- * the sites (d_sites, 3 doubles each) and the result rows (d_out) belong to
- * the caller.
+ * fragments memory it manages), and services with a fixed device-memory
+ * budget that must not grow per request.  This entry point allocates nothing:
+ * every per-call device buffer (launch tables, cavities, first-query
+ * distances, queue counter, totals and the per-walk samples) is carved out of
+ * one static device array of TWOS_NOALLOC_SCRATCH_BYTES (16 MiB) that every
+ * GPU loading the library holds until the process exits.  The mesh session
+ * (opened earlier with twos_mesh_open*), the sites (d_sites, 3 doubles each)
+ * and the result rows (d_out) belong to the caller.
  *
- * Limit: the scratch holds the per-walk samples of one call, so
- * n_sites * walks may be at most about 4 M in mixed compliance mode (8 bytes
- * per walk), 1.3 M in FP64 paired mode (20 bytes per walk); larger requests
- * are rejected with TWOS_ERR_USAGE and a message giving the bytes needed.
- * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share
- * the one array and it keeps the previous call's contents (the call clears
- * what must start at zero): calls that overlap on the GPU, from different
- * threads, streams or sessions, race on it and must be serialised by the
- * caller.  Work runs on the session's stream and the call returns after it
- * completes.  Results equal twos_estimate_device's. */
+ * Limit: the scratch holds the per-walk samples of one call (a value per walk
+ * for u, another for p in paired mode, 4 bytes of step count), so
+ * n_sites * walks may be at most about 2.0 M in mixed compliance mode
+ * (8 bytes per walk), 1.39 M in mixed paired or FP64 compliance mode (12) and
+ * 0.83 M in FP64 paired mode (20), less a few KB of tables and 8 bytes per
+ * site; larger requests are rejected with TWOS_ERR_USAGE and a message giving
+ * the bytes needed.  The first call on a device looks up the array's device
+ * address (once per device); make that first call before any stream capture.
+ * All calls share the one array and it keeps the previous call's contents
+ * (the call clears what must start at zero): calls that overlap on the GPU,
+ * from different threads, streams or sessions, race on it and must be
+ * serialised by the caller.  Work runs on the session's stream and the call
+ * returns after that stream has completed it.  Rows equal
+ * twos_estimate_device's, and errors and the summary are reported the same
+ * way (h2d_bytes and d2h_bytes are 0). */
 #define TWOS_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int twos_estimate_noalloc(twos_mesh *mesh, const twos_request *request, const double *d_sites,
                           uint32_t n_sites, const double *cavities, uint32_t n_cavities,
@@ -425,14 +428,17 @@ int twos_diffwos(twos_mesh *mesh, const twos_request *request, double diff_offse
  * cross = sum_{i != j} grad U_i . grad P_j / (N (N-1)) estimates
  * grad u . grad p without the i = j bias, with its leave-one-out jackknife
  * SE.  For a small Neumann sphere at x the topological derivative of
- * J = int q u is D_T = (3/2) grad u . grad p - q(x) u(x) (the dipole of a
- * Neumann sphere in a uniform field, 3D polarization 3/2). */
+ * J = int q u is D_T = (3/2) grad u . grad p - q(x) u(x) - f(x) p(x) (the
+ * dipole of a Neumann sphere in a uniform field, 3D polarization 3/2, plus
+ * the removed volume); u_se and p_se with cross_se bound the standard error
+ * of an assembled D_T. */
 typedef struct twos_gradient_result {
   double u, p;
   double grad_u[3], grad_p[3];
   double cross, cross_se;
   uint64_t steps, caps;
-} twos_gradient_result; /* 96 bytes */
+  double u_se, p_se; /* standard errors of the means u and p */
+} twos_gradient_result; /* 112 bytes */
 
 int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const double *sites, uint32_t n_sites,
                            const double *cavities, uint32_t n_cavities, twos_gradient_result *out,
@@ -479,6 +485,21 @@ typedef struct twos_rqmc_params {
 
 int twos_rqmc(twos_mesh *mesh, const twos_request *request, const twos_rqmc_params *params, const double *sites,
               uint32_t n_sites, double *batch_u, double *batch_p, double *td, twos_summary *summary);
+
+/* The estimator's per-site reduction on caller-supplied per-walk samples:
+ * u and p (p may be NULL outside paired mode) [n_sites][walks] as doubles,
+ * steps (may be NULL) with bit 31 set on a cap, out one row per site -- all
+ * host buffers.  The rows are what twos_estimate writes for walks with these
+ * payoffs: compliance the U-statistic (S^2 - S2)/(N(N-1)) with its
+ * leave-one-out jackknife SE (evaluate_site, wih_twos.cpp:686-715, and
+ * crossfit_square, stanford_bunny/run_bunny_benchmark.py:257-269); paired
+ * (S_u S_p - S_up)/(N(N-1)), i.e. minus crossfit_product of
+ * experiments/run_controlled_experiments.py:79-87, with the same jackknife;
+ * hot the mean.  With TWOS_PREC_MIXED the samples are rounded to float
+ * first, as the mixed walk kernel stores them.  `mesh` supplies the device
+ * and stream.  Used to check the device reduction on identical inputs. */
+int twos_finalize_samples(twos_mesh *mesh, int precision, int mode, const double *u, const double *p,
+                          const uint32_t *steps, uint32_t n_sites, uint32_t walks, twos_site_result *out);
 
 /* Per-walk samples (the `values` vector of wih_twos.cpp:678-690): u and p
  * (p may be NULL) as doubles, steps per walk with bit 31 set on a cap, laid

@@ -343,14 +343,14 @@ class OracleMesh:
 
     def estimate_gradient(self, sites, cavities=None, samples=False, **kw):
         """The GPU gradient form in the counter stream (rng must be the counter
-        stream): rows (u, p, grad_u, grad_p, cross, cross_se), steps/caps, and
+        stream): rows (u, p, grad_u, grad_p, cross, cross_se, u_se, p_se), steps/caps, and
         optionally the per-walk samples [n, walks, 8]."""
         p = self._params(**kw)
         if p.rng != RNG_COUNTER:
             raise ValueError("the gradient form is defined in the counter stream")
         s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
         cav = np.zeros((0, 3)) if cavities is None else np.ascontiguousarray(cavities, dtype=np.float64).reshape(-1, 3)
-        rows = np.zeros((len(s), 10))
+        rows = np.zeros((len(s), 12))
         counts = np.zeros((len(s), 2), dtype=np.uint64)
         walks = np.zeros((len(s), p.walks, 8)) if samples else None
         rc = lib().oracle_estimate_gradient(self.handle, ctypes.byref(p), _ptr(s), len(s), _ptr(cav), len(cav),
@@ -358,7 +358,8 @@ class OracleMesh:
         if rc:
             raise RuntimeError(lib().oracle_last_error().decode())
         out = {"u": rows[:, 0], "p": rows[:, 1], "grad_u": rows[:, 2:5], "grad_p": rows[:, 5:8], "cross": rows[:, 8],
-               "cross_se": rows[:, 9], "steps": counts[:, 0], "caps": counts[:, 1]}
+               "cross_se": rows[:, 9], "u_se": rows[:, 10], "p_se": rows[:, 11], "steps": counts[:, 0],
+               "caps": counts[:, 1]}
         if samples:
             out["samples"] = walks
         return out
@@ -491,11 +492,60 @@ def crossfit_square(samples):
 
 
 def crossfit_product(a, b):
-    """experiments/run_controlled_experiments.py:79-87: the off-diagonal mean of a_i b_j."""
+    """experiments/run_controlled_experiments.py:79-87: minus the off-diagonal
+    mean of a_i b_j along the last axis (the reference's sign: an estimate of
+    -E[A]E[B], the TD of a compliance-type objective)."""
     a = np.asarray(a, dtype=float)
     b = np.asarray(b, dtype=float)
     n = a.shape[-1]
-    return (a.sum(axis=-1) * b.sum(axis=-1) - np.sum(a * b, axis=-1)) / (n * (n - 1))
+    if n < 2:
+        raise ValueError("cross-fitting requires at least two pairs")
+    return -(np.sum(a, axis=-1) * np.sum(b, axis=-1) - np.sum(a * b, axis=-1)) / (n * (n - 1))
+
+
+CROSSFIT_SEED = 20260912  # run_controlled_experiments.py:34 (SEED); the experiment takes spawn index 2 (:800-801)
+
+
+def crossfit_experiment_draws(correlation, rng, n=32, replicates=30000, mu=(0.8, 0.65), sigma=(0.5, 0.6)):
+    """One correlation of run_crossfit_experiment (run_controlled_experiments.py:250-271):
+    the paired samples a, b and the independent b' [replicates, n], drawn in the
+    reference's order (z1, z2, z3 standard normals)."""
+    z1 = rng.standard_normal(size=(replicates, n))
+    z2 = rng.standard_normal(size=(replicates, n))
+    z3 = rng.standard_normal(size=(replicates, n))
+    a = mu[0] + sigma[0] * z1
+    b = mu[1] + sigma[1] * (correlation * z1 + np.sqrt(1.0 - correlation * correlation) * z2)
+    b_independent = mu[1] + sigma[1] * z3
+    return a, b, b_independent
+
+
+def crossfit_experiment(estimator=None, n=32, replicates=30000):
+    """run_crossfit_experiment (run_controlled_experiments.py:250-321): for each
+    correlation in linspace(-0.9, 0.9, 10), the four estimators' mean and bias
+    against true_td = -mu_a mu_b.  `estimator(a, b)` replaces the cross-fit
+    estimator (crossfit_product by default), so a device reduction can be
+    dropped into the same seeded experiment.  Rows as dicts keyed like the
+    reference's crossfit_bias.csv."""
+    estimator = estimator or crossfit_product
+    rng = np.random.default_rng(np.random.SeedSequence(CROSSFIT_SEED).spawn(5)[2])
+    mu_a, mu_b = 0.8, 0.65
+    true_td = -mu_a * mu_b
+    rows = []
+    for correlation in np.linspace(-0.9, 0.9, 10):
+        a, b, bi = crossfit_experiment_draws(correlation, rng, n, replicates)
+        estimates = {
+            "Same-seed product": -np.mean(a * b, axis=1),
+            "Product of means": -np.mean(a, axis=1) * np.mean(b, axis=1),
+            "Cross-fit TWoS": estimator(a, b),
+            "Independent batches": -np.mean(a, axis=1) * np.mean(bi, axis=1),
+        }
+        for method, values in estimates.items():
+            err = values - true_td
+            rows.append({"method": method, "correlation": float(correlation), "true_td": true_td,
+                         "mean_estimate": float(np.mean(values)), "bias": float(np.mean(err)),
+                         "bias_se": float(np.std(err, ddof=1) / np.sqrt(replicates)),
+                         "rmse": float(np.sqrt(np.mean(err * err)))})
+    return rows
 
 
 def cross_jackknife_se(a, b):

@@ -1520,8 +1520,8 @@ GradWalk grad_walk(const Mesh &m, const oracle_params &o, const double *cav, uin
 
 extern "C" {
 
-// Per-site gradient rows (GRADIENT layout: u, p, grad_u[3], grad_p[3],
-// cross, cross_se as doubles; steps, caps as uint64 in a separate array),
+// Per-site gradient rows (u, p, grad_u[3], grad_p[3], cross, cross_se,
+// u_se, p_se as doubles; steps, caps as uint64 in a separate array),
 // and optionally the per-walk samples (u, p, grad_u, grad_p: 8 doubles).
 int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, const double *sites, uint32_t n_sites,
                              const double *cav, uint32_t ncav, double *rows, uint64_t *counts, double *walks) {
@@ -1570,7 +1570,12 @@ int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, cons
     mean /= n;
     double spread = 0;
     for (double v : leave) spread += (v - mean) * (v - mean);
-    double *row = rows + 10 * s;
+    double vu = 0, vp = 0;
+    for (const GradWalk &g : W) {
+      vu += (g.u - su / n) * (g.u - su / n);
+      vp += (g.p - sp / n) * (g.p - sp / n);
+    }
+    double *row = rows + 12 * s;
     row[0] = su / n;
     row[1] = sp / n;
     for (int k = 0; k < 3; ++k) {
@@ -1579,6 +1584,8 @@ int oracle_estimate_gradient(const oracle_mesh *om, const oracle_params *o, cons
     }
     row[8] = cross;
     row[9] = N > 2 ? std::sqrt((n - 1.0) / n * spread) : 0.0;
+    row[10] = N > 1 ? std::sqrt(vu / (n * (n - 1.0))) : 0.0;
+    row[11] = N > 1 ? std::sqrt(vp / (n * (n - 1.0))) : 0.0;
     counts[2 * s] = steps;
     counts[2 * s + 1] = caps;
     if (walks)

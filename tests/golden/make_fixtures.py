@@ -116,6 +116,18 @@ def main(reference: Path) -> None:
         keep["has_cavities"] = bool(dict(zip(argv[0::2], argv[1::2])).get("--cavities"))
         (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
     minimum_benefit(reference, out)
+    controlled_experiments(reference, out)
+
+
+def controlled_experiments(reference: Path, out: Path) -> None:
+    """The seeded cross-fit bias experiment of experiments/
+    run_controlled_experiments.py:250-321 (its tracked per-correlation rows
+    and the summary's claims), which pins the statistics the device
+    reduction computes."""
+    dst = out / "controlled_experiments"
+    dst.mkdir(exist_ok=True)
+    shutil.copyfile(reference / "experiments/output/crossfit_bias.csv", dst / "crossfit_bias.csv")
+    shutil.copyfile(reference / "experiments/output/summary.json", dst / "summary.json")
 
 
 def minimum_benefit(reference: Path, out: Path) -> None:

@@ -34,7 +34,7 @@ def test_abi_version_and_layouts(lib_built, tmp_path):
     """Every ctypes field offset and struct size equals the C header's."""
     from twos_b200 import _abi
     L = _abi.load()
-    assert L.twos_abi_version() == 1
+    assert L.twos_abi_version() == _abi.ABI_VERSION == 2
     structs = {"twos_source_term": _abi.SourceTerm, "twos_request": _abi.Request,
                "twos_site_result": _abi.SiteResult, "twos_summary": _abi.Summary, "twos_mesh_info": _abi.MeshInfo,
                "twos_tuning": _abi.Tuning, "twos_design_params": _abi.DesignParams,

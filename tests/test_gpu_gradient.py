@@ -14,7 +14,10 @@ Tolerances
 * Analytic: the cross statistic's z = (estimate - grad u . grad p) / SE
   within 4.5 everywhere, |z| < 3 for >= 95 % of sites, |mean z| < 0.6; u
   within 0.03 of g on average (Monte Carlo at 1024 walks plus the inscribed
-  polyhedron).
+  polyhedron); the assembled TD's z against the analytic TD (SE bounded by
+  1.5 cross_se + q u_se) within 4.5, >= 95 % within 3, RMS below 1.5.  On
+  these samples a polarization of 1 or 3, or a flipped sign of q u, gives
+  an RMS z above 2 and max |z| above 4.7 (the oracle, same counter stream).
 """
 import numpy as np
 import pytest
@@ -69,7 +72,7 @@ def test_gradient_fp64_equals_oracle(tb, oracle_mod):
         green=True, cavity_radius=0.08, source=_oracle_terms(oracle_mod, cfg.source),
         adjoint=_oracle_terms(oracle_mod, q), boundary=_oracle_terms(oracle_mod, boundary))
     np.testing.assert_array_equal(rows["steps"], o["steps"])
-    for k in ("u", "p", "grad_u", "grad_p", "cross", "cross_se"):
+    for k in ("u", "p", "grad_u", "grad_p", "cross", "cross_se", "u_se", "p_se"):
         np.testing.assert_allclose(rows[k], o[k], rtol=1e-9, atol=1e-12, err_msg=k)
     assert summ["launches"] == 3
 
@@ -88,10 +91,16 @@ def test_config1_neumann_topological_derivative(tb):
     assert np.max(np.abs(z)) < 4.5, np.max(np.abs(z))
     assert np.mean(np.abs(z) < 3.0) >= 0.95
     assert abs(np.mean(z)) < 0.6
-    # The topological derivative assembled from the estimates.
+    # The Neumann-cavity TD assembled from the estimates (the formula is
+    # checked exactly on a finite hole in tests/test_neumann_hole_cpu.py),
+    # against the analytic TD; its standard error is bounded by the sum of
+    # the parts' (|cov| <= product of the standard deviations).
     td = 1.5 * rows["cross"] - qx * rows["u"]
     td_exact = 1.5 * exact - qx * g
-    assert np.corrcoef(td, td_exact)[0, 1] > 0.9
+    zt = (td - td_exact) / (1.5 * rows["cross_se"] + np.abs(qx) * rows["u_se"])
+    assert np.max(np.abs(zt)) < 4.5, np.max(np.abs(zt))
+    assert np.mean(np.abs(zt) < 3.0) >= 0.95
+    assert np.sqrt(np.mean(zt ** 2)) < 1.5
 
 
 def test_gradient_mixed_shares_samples(tb):

@@ -1345,6 +1345,16 @@ template <typename V> __global__ void __launch_bounds__(256) grad_finalize_kerne
       }
       s2 = warp_sum(s2);
     }
+    // Standard errors of the means of u and p (two-pass sample variance).
+    const double mu = su / n, mp = sp / n;
+    double vu = 0, vp = 0;
+    for (uint32_t w = lane; w < N; w += 32) {
+      const double du = static_cast<double>(u[base + w]) - mu, dp = static_cast<double>(p[base + w]) - mp;
+      vu += du * du;
+      vp += dp * dp;
+    }
+    vu = warp_sum(vu);
+    vp = warp_sum(vp);
     for (int o = 16; o > 0; o >>= 1) {
       steps += __shfl_xor_sync(0xffffffffu, steps, o);
       caps += __shfl_xor_sync(0xffffffffu, caps, o);
@@ -1361,6 +1371,8 @@ template <typename V> __global__ void __launch_bounds__(256) grad_finalize_kerne
       r.cross_se = N > 2 ? sqrt((n - 1.0) / n * s2) : 0.0;
       r.steps = steps;
       r.caps = caps;
+      r.u_se = N > 1 ? sqrt(vu / (n * (n - 1.0))) : 0.0;
+      r.p_se = N > 1 ? sqrt(vp / (n * (n - 1.0))) : 0.0;
       F.out[site] = r;
       atomicAdd(&F.totals[0], steps);
       atomicAdd(&F.totals[1], caps);

@@ -1,9 +1,8 @@
 // twos_estimate_noalloc: the device-buffer estimator without any device
 // allocation, for callers that cannot call cudaMalloc -- code that runs while
-// a framework owns the device memory pool (its allocator would be bypassed or
-// fragmented by a raw cudaMalloc), code on a path that must not synchronise
-// the device (cudaMalloc/cudaFree may), and long-running services with a
-// fixed memory budget.
+// a framework owns the device memory pool (a raw cudaMalloc bypasses its
+// allocator and fragments memory it manages), and long-running services with
+// a fixed device-memory budget that must not grow per request.
 //
 // All per-call device scratch of an estimate -- the launch's job, geometry and
 // term tables, the cavities, the per-site first-query distances, the work-
@@ -11,10 +10,13 @@
 // carved out of one file-scope static device array of kNoallocScratchBytes
 // (16 MiB).  Every GPU that loads the library holds this array until the
 // process exits.  The caller passes the sites and the result rows (device
-// memory) and a mesh session opened earlier.
+// memory) and a mesh session opened earlier.  The call returns after the work
+// on the session's stream has completed, and reports errors and its summary
+// through the same mapping as twos_estimate_device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <limits>
 #include <mutex>
@@ -92,10 +94,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
                                      twos_summary *summary) {
   if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
   if (int rc = validate_request(r, n_sites, n_cavities)) return rc;
-  if (n_sites == 0) {
-    if (summary) std::memset(summary, 0, sizeof(*summary));
-    return TWOS_OK;
-  }
+  if (n_sites == 0) return finish(RunOut{}, 0, r, summary, 0.0, 0, 0);
   if (!d_sites || !d_out || (n_cavities && !cavities)) return fail(TWOS_ERR_USAGE, "null buffer");
   const bool mixed = r->precision == TWOS_PREC_MIXED;
   const bool paired = r->mode == TWOS_MODE_PAIRED;
@@ -111,7 +110,8 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
                                     std::to_string(kNoallocScratchBytes / per_walk) +
                                     " walks per call at this mode and precision)");
   }
-  twos_summary s{};
+  const auto t0 = std::chrono::steady_clock::now();
+  RunOut ro;
   try {
     check(cudaSetDevice(m->device), "cudaSetDevice");
     unsigned char *base = static_cast<unsigned char *>(scratch_address(m->device));
@@ -180,25 +180,19 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     float ms = 0.f, msw = 0.f;
     check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
     check(cudaEventElapsedTime(&msw, m->ev0, m->evw), "event time");
-    s.kernel_seconds = ms * 1e-3;
-    s.walk_seconds = msw * 1e-3;
-    s.total_seconds = s.kernel_seconds;
-    s.paths = walks_total;
-    s.steps = tot[0];
-    s.caps = tot[1];
-    s.queries = tot[0] + walks_total;
-    s.launches = 3;
-    std::memcpy(&s.error_flags, &tot[2], sizeof(uint32_t));
-    s.node_tests = tot[3];
-    s.plane_tests = tot[4];
-    s.triangle_tests = tot[5];
-    s.grid_steps = tot[6];
+    ro.kernel_seconds = ms * 1e-3;
+    ro.walk_seconds = msw * 1e-3;
+    ro.launches = 3;
+    ro.steps = tot[0];
+    ro.caps = tot[1];
+    std::memcpy(&ro.error_flags, &tot[2], sizeof(uint32_t));
+    ro.node_tests = tot[3];
+    ro.plane_tests = tot[4];
+    ro.triangle_tests = tot[5];
+    ro.grid_steps = tot[6];
   } catch (const std::exception &e) {
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
-  if (summary) *summary = s;
-  if (s.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
-  if (s.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
-  if (s.caps) return fail(TWOS_ERR_RUNTIME, "one or more paths hit --max-steps");
-  return TWOS_OK;
+  return finish(ro, n_sites, r, summary, std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(),
+                0, 0);
 }

@@ -258,15 +258,6 @@ TermDev frame_term(const twos_source_term &t, const double c[3]) {
   return d;
 }
 
-struct RunOut {
-  double kernel_seconds = 0.0;
-  double walk_seconds = 0.0;
-  uint32_t launches = 0;
-  uint32_t error_flags = 0;
-  uint64_t steps = 0, caps = 0;
-  uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0, grid_steps = 0;
-};
-
 // The device descriptor of one job; its source terms are appended to `terms`
 // in the job geometry's frame.
 JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint32_t site_begin,
@@ -1611,6 +1602,66 @@ int twos_walk_samples(twos_mesh *m, const twos_request *r, const double *sites, 
   }
   if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
   if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  return TWOS_OK;
+}
+
+int twos_finalize_samples(twos_mesh *m, int precision, int mode, const double *u, const double *p,
+                          const uint32_t *steps, uint32_t n_sites, uint32_t walks, twos_site_result *out) {
+  if (!m) return fail(TWOS_ERR_USAGE, "null mesh");
+  if (precision != TWOS_PREC_FP64 && precision != TWOS_PREC_MIXED) return fail(TWOS_ERR_USAGE, "invalid precision");
+  if (mode != TWOS_MODE_COMPLIANCE && mode != TWOS_MODE_PAIRED && mode != TWOS_MODE_HOT)
+    return fail(TWOS_ERR_USAGE, "invalid mode");
+  if (walks < 2) return fail(TWOS_ERR_USAGE, "walks must be at least 2");
+  if (n_sites == 0) return TWOS_OK;
+  const bool paired = mode == TWOS_MODE_PAIRED;
+  if (!u || !out || (paired && !p)) return fail(TWOS_ERR_USAGE, "null buffer");
+  const size_t total = static_cast<size_t>(n_sites) * walks;
+  if (total > m->max_launch_walks) return fail(TWOS_ERR_USAGE, "too many samples for one launch");
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    const bool mixed = precision == TWOS_PREC_MIXED;
+    const size_t vbytes = mixed ? sizeof(float) : sizeof(double);
+    m->u.reserve(total * vbytes);
+    if (paired) m->p.reserve(total * vbytes);
+    m->steps.reserve(total * sizeof(uint32_t));
+    m->out.reserve(static_cast<size_t>(n_sites) * sizeof(twos_site_result));
+    m->jobs.reserve(sizeof(JobDesc));
+    auto upload = [&](const double *src, DevBuf &dst) {
+      if (mixed) {
+        std::vector<float> tmp(src, src + total);
+        check(cudaMemcpy(dst.ptr, tmp.data(), total * sizeof(float), cudaMemcpyHostToDevice), "upload samples");
+      } else {
+        check(cudaMemcpy(dst.ptr, src, total * sizeof(double), cudaMemcpyHostToDevice), "upload samples");
+      }
+    };
+    upload(u, m->u);
+    if (paired) upload(p, m->p);
+    if (steps)
+      check(cudaMemcpy(m->steps.ptr, steps, total * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload steps");
+    else
+      check(cudaMemset(m->steps.ptr, 0, total * sizeof(uint32_t)), "memset");
+    JobDesc J{};
+    J.n_sites = n_sites;
+    J.walks = walks;
+    check(cudaMemcpy(m->jobs.ptr, &J, sizeof(JobDesc), cudaMemcpyHostToDevice), "upload job");
+    begin_totals(m);
+    FinalizeLaunch F{};
+    F.jobs = m->jobs.as<JobDesc>();
+    F.n_jobs = 1;
+    F.total_sites = n_sites;
+    F.totals = m->totals.as<unsigned long long>();
+    F.u = m->u.ptr;
+    F.p = paired ? m->p.ptr : m->u.ptr;
+    F.steps = m->steps.as<uint32_t>();
+    F.out = m->out.as<twos_site_result>();
+    check(launch_finalize(precision, mode, F, m->stream), "finalize launch");
+    check(cudaMemcpyAsync(out, m->out.ptr, static_cast<size_t>(n_sites) * sizeof(twos_site_result),
+                          cudaMemcpyDeviceToHost, m->stream),
+          "download results");
+    check(cudaStreamSynchronize(m->stream), "finalize");
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
   return TWOS_OK;
 }
 

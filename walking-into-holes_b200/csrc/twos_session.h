@@ -36,7 +36,21 @@ struct DevBuf {
   template <typename T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// What a group of launches reports back to the entry point that ran them.
+struct RunOut {
+  double kernel_seconds = 0.0;
+  double walk_seconds = 0.0;
+  uint32_t launches = 0;
+  uint32_t error_flags = 0;
+  uint64_t steps = 0, caps = 0;
+  uint64_t node_tests = 0, plane_tests = 0, triangle_tests = 0, grid_steps = 0;
+};
+
 int validate_request(const twos_request *r, uint32_t n_sites, uint32_t n_cav, bool allow_boundary = false);
+// Fills `summary` (when not NULL) from `ro` and maps device error bits and
+// step caps onto the ABI's return codes and last-error messages.
+int finish(const RunOut &ro, uint32_t n_sites, const twos_request *r, twos_summary *summary, double t_total,
+           uint64_t h2d, uint64_t d2h);
 JobDesc make_job(twos_mesh *mesh, const twos_request *r, uint32_t n_sites, uint32_t site_begin,
                  uint32_t site_offset, uint32_t geo, uint64_t walk_begin, uint32_t site_rank, uint32_t cav_begin,
                  uint32_t n_cav, std::vector<TermDev> &terms);

@@ -13,6 +13,7 @@ PKG_ROOT = Path(__file__).resolve().parent.parent
 LIB_PATH = PKG_ROOT / "_build" / "libtwos.so"
 BIN_DIR = PKG_ROOT / "_build"
 
+ABI_VERSION = 2  # TWOS_ABI_VERSION of include/twos.h
 OK, ERR_RUNTIME, ERR_USAGE = 0, 1, 2
 MODE_COMPLIANCE, MODE_PAIRED, MODE_HOT = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
@@ -27,7 +28,7 @@ EXPORTED = [
     "twos_estimate_device",
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
-    "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc",
+    "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc", "twos_finalize_samples",
 ]
 RQMC_MC, RQMC_ARRAY, RQMC_NEIGHBOUR = 0, 1, 2
 
@@ -117,7 +118,7 @@ class ValidateParams(ctypes.Structure):
 
 
 GRADIENT_DTYPE = [("u", "f8"), ("p", "f8"), ("grad_u", "f8", (3,)), ("grad_p", "f8", (3,)), ("cross", "f8"),
-                  ("cross_se", "f8"), ("steps", "u8"), ("caps", "u8")]
+                  ("cross_se", "f8"), ("steps", "u8"), ("caps", "u8"), ("u_se", "f8"), ("p_se", "f8")]
 
 VALIDATE_MAX_STAGES = 5
 CERT_SAMPLE_DTYPE = [("value", "f8"), ("steps", "u4"), ("capped", "u1"), ("clipped", "u1"), ("contained", "u1"),
@@ -178,6 +179,7 @@ def load(path: Path | str | None = None):
                                    ctypes.POINTER(DesignParams), vp, vp, ctypes.POINTER(u32), ctypes.POINTER(Summary)]
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
+    L.twos_finalize_samples.argtypes = [vp, i32, i32, vp, vp, vp, u32, u32, vp]
     L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
     L.twos_rqmc.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(RqmcParams), vp, u32, vp, vp, vp,
                             ctypes.POINTER(Summary)]
@@ -190,7 +192,7 @@ def load(path: Path | str | None = None):
     for name in EXPORTED:
         if name not in ("twos_mesh_close", "twos_last_error"):
             getattr(L, name).restype = ctypes.c_int
-    if L.twos_abi_version() != 1:
+    if L.twos_abi_version() != ABI_VERSION:
         raise RuntimeError("libtwos.so ABI version mismatch")
     _lib = L
     return L

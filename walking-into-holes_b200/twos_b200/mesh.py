@@ -243,6 +243,21 @@ class Mesh:
                                             _ptr(p), _ptr(st)))
         return {"u": u, "p": p, "steps": st & 0x7FFFFFFF, "caps": (st >> 31).astype(bool)}
 
+    def finalize_samples(self, u, p=None, steps=None, mode: str = "compliance", precision: str = "fp64"):
+        """The device's per-site reduction (twos_finalize_samples) of given
+        per-walk samples u, p [n_sites, walks]: rows of SITE_DTYPE, as
+        twos_estimate writes them for walks with these payoffs."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.ndim != 2:
+            raise ValueError("u must be [n_sites, walks]")
+        n, w = u.shape
+        pp = None if p is None else np.ascontiguousarray(p, dtype=np.float64).reshape(n, w)
+        st = None if steps is None else np.ascontiguousarray(steps, dtype=np.uint32).reshape(n, w)
+        out = np.zeros(n, dtype=SITE_DTYPE)
+        check(_abi.load().twos_finalize_samples(self._h, PRECISIONS[precision], MODES[mode], _ptr(u), _ptr(pp),
+                                                _ptr(st), n, w, _ptr(out)))
+        return out
+
     def diffwos(self, sites, config: Config, cavities, diff_offset: float = 0.02,
                 enclosure_fallback: bool = False, strict: bool = True):
         """Differential WoS (twos_diffwos): returns (rows [n_sites, n_cav] of
