@@ -66,9 +66,17 @@ class Site(ctypes.Structure):
     ]
 
 
+REFERENCE = Path("/root/reference")
+
+
 def build() -> Path:
-    """Compile the oracle with its Makefile (system g++, no FMA contraction)."""
+    """Compile the oracle with its Makefile (system g++, no FMA contraction),
+    and, where the reference's source tree is present, the reference's own
+    backend against the shim headers (oracle/_ref/wih_twos; elsewhere the
+    prebuilt binary is used as it is)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if (REFERENCE / "benchmarks/compiled_bunny/src/wih_twos.cpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REFERENCE={REFERENCE}"], check=True)
     return LIB_PATH
 
 
