@@ -8,7 +8,7 @@ include/twos.h); this package is the host side.
 """
 from ._abi import (MODE_COMPLIANCE, MODE_HOT, MODE_PAIRED, PREC_FP64, PREC_MIXED, SITE_DTYPE, TwosError, load)
 from .mesh import Config, Mesh, ball_green_integral, estimate_batch
-from . import sources, geometry
+from . import sources, geometry, shard
 
-__all__ = ["Config", "Mesh", "estimate_batch", "ball_green_integral", "TwosError", "load", "sources", "geometry", "SITE_DTYPE", "MODE_COMPLIANCE",
-           "MODE_PAIRED", "MODE_HOT", "PREC_FP64", "PREC_MIXED"]
+__all__ = ["Config", "Mesh", "estimate_batch", "ball_green_integral", "TwosError", "load", "sources",
+           "geometry", "shard", "SITE_DTYPE", "MODE_COMPLIANCE", "MODE_PAIRED", "MODE_HOT", "PREC_FP64", "PREC_MIXED"]
