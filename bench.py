@@ -5,7 +5,8 @@ Workload (one "step"): the compliance TWoS estimator over every interior
 site of the noise-displaced icosphere -- subdivision 7 (327,680 triangles),
 vertices scaled radially by 1 + 0.15 * (8 random real spherical harmonics of
 degree <= 6, seed 1), Poisson f = 1 with u = 0 on the surface, sites = the
-64^3 cell centres of the bounding box kept when inside the mesh (ray parity),
+64^3 cell centres of the bounding box inside the displaced sphere (kept when
+|x| < r(x/|x|) (1 - 2e-4), which keeps them inside the inscribed mesh too),
 4,096 walks per site, epsilon = 1e-4, max 1,024 steps.  Synthetic inputs,
 generated here from seeds.
 
@@ -16,13 +17,20 @@ e2e      the same metric through the host-buffer C-ABI call (twos_estimate):
          pinned host sites in, pinned host rows out, copies inside the timed
          region.
 fp64     the plain all-FP64 GPU form at the same N (the target comparison).
-cpu_baseline  the CPU oracle (the reference's algorithm and random stream,
-         OpenMP over all host cores) on a bounded random subset of the sites.
+accuracy mixed against FP64 per site (z of the TD difference over every
+         site), and on the unit ball (closed-form TD u^2 = ((1-|x|^2)/6)^2)
+         the ratio of the mixed form's RMS error to the FP64 form's.
+cpu_baseline  the reference's own compiled backend (wih_twos.cpp built
+         unchanged against the project's Embree/Eigen shims, oracle/_ref),
+         OpenMP over all host cores, on a fixed random subset of the sites.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--shard sites|replicas]
 
-For N > 1 (torchrun) every rank runs the full workload on its own GPU with
-its own seed (weak scaling, no data-path collective); time = max over ranks.
+For N > 1 (torchrun) the sites are split into contiguous blocks of equal
+predicted cost, one per rank, each keyed by its global site index (so the
+gathered rows equal a one-GPU run's), and the rows are gathered once; time
+= max over ranks.  --shard replicas runs the full workload on every rank
+with its own seed instead.
 """
 from __future__ import annotations
 
@@ -32,6 +40,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 from pathlib import Path
@@ -45,12 +54,27 @@ METRIC = "TD site-estimates/s at equal 95% CI: mixed vs FP64 GPU, vs host CPU"
 UNIT = "site-estimates/s"
 WORKLOAD = ("noise-displaced icosphere L7 (327,680 tris, SH seed 1), Poisson f=1 u=0, 64^3 grid clipped to "
             "interior, 4096 walks/site, eps=1e-4")
+L2_POLICY = "GPU arms: 256 MiB write between timed steps (L2 flush)"
 # Canonical algorithmic bytes per closest-point query on this workload:
 # 32 B per AABB test + 36 B per triangle test of the canonical binary SAH
 # traversal, counted at the workload's own walk positions by
 # `python oracle/canonical_bytes.py` (96 sites x 64 walks).
 CANONICAL_BYTES_PER_QUERY = 38530.8  # 546.3 AABB + 584.7 triangle tests per query
 CANONICAL_SOURCE = "oracle/canonical_bytes.py --sites 96 --walks 64"
+SITE_MARGIN = 2e-4  # relative radial margin inside the displaced sphere (the mesh's chords lie within 4.5e-5)
+REF_SUBSET = 1024   # fixed random subset of sites timed on the host cores
+REF_SUBSET_SEED = 1234
+
+# The walk kernel's counters from one `ncu --set full` capture of the medium
+# case (the command and the rest of the metrics are in the profiles folder's
+# summary of the walk kernel); they change only with the kernel.
+NCU_WALK_KERNEL = {
+    "case": "bench.py --walks 256 --grid 24 --steps 1 --warmup 1 --no-cpu --no-fp64 --no-ablation --no-autotune",
+    "lts__throughput_pct": 24.1,
+    "smsp__thread_inst_executed_per_inst_executed": 8.64,
+    "smsp__issue_active_pct": 67.5,
+    "sm__warps_active_pct": 48.2,
+}
 
 
 def dram_traffic_per_launch(walks: int) -> float:
@@ -58,7 +82,7 @@ def dram_traffic_per_launch(walks: int) -> float:
     kernel launch, from one ncu capture of the full workload: 2.83 GB read +
     4.33 GB written for 502,403,072 walks, 14.25 B per walk.  The traffic is
     the per-walk samples and the lines they evict; the BVH (31 MB) and the
-    distance grid (32 MB) stay in L2, so it scales with the walks of the
+    distance grid (64 MB) stay in L2, so it scales with the walks of the
     launch."""
     return 14.25 * walks
 
@@ -74,20 +98,26 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--shard", choices=["sites", "replicas"], default="sites",
+                    help="N > 1: split the sites over the ranks (default) or run a full replica per rank")
     ap.add_argument("--walks", type=int, default=4096)
     ap.add_argument("--grid", type=int, default=64)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the unit-ball error-ratio leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the session's default launch tuning")
     ap.add_argument("--no-ablation", action="store_true",
                     help="skip the one-step mixed-form run with the distance grid off")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sites", type=int, default=128,
+                    help="sites of the fixed subset timed on the host cores in this arm's cpu_baseline")
+    ap.add_argument("--ref-sites", type=int, default=REF_SUBSET,
+                    help="--impl reference: sites of the fixed subset (split over the steps)")
+    ap.add_argument("--housing-ref-sites", type=int, default=256, help="housing workload: FP64 reference sites")
     ap.add_argument("--workload", choices=["noise-sphere", "housing", "batch", "design", "unit-sphere"],
                     default="noise-sphere",
                     help="housing: the box-minus-cylinders epsilon sweep; batch: 32 uneven meshes in one launch; design: the graph-captured design loop; unit-sphere: the plain method's Neumann-cavity TD (separate JSON lines)")
     ap.add_argument("--sites", type=int, default=1_000_000, help="housing workload sites")
-    ap.add_argument("--ref-sites", type=int, default=256, help="housing workload FP64 reference sites")
     return ap.parse_args(argv)
 
 
@@ -99,9 +129,33 @@ def workload(grid_n):
     return V, F, grid
 
 
+def workload_sites(grid):
+    """Grid points inside the displaced sphere by the analytic radius with a
+    relative margin: the same sites for every arm, inside the mesh as well."""
+    from twos_b200 import geometry
+    r = np.linalg.norm(grid, axis=1)
+    keep = r > 1e-12
+    g = grid[keep]
+    rad = 1.0 + 0.15 * geometry.sh_field(g / r[keep][:, None], 1)
+    return g[r[keep] < rad * (1.0 - SITE_MARGIN)]
+
+
+def reference_subset(n: int, count: int) -> np.ndarray:
+    """Indices of the fixed random subset of sites timed on the host cores."""
+    rng = np.random.default_rng(REF_SUBSET_SEED)
+    return np.sort(rng.choice(n, size=min(n, count), replace=False))
+
+
 def source_terms():
     from twos_b200 import sources
     return sources.constant(1.0)
+
+
+def workload_config(n_sites: int, walks: int) -> dict:
+    """The workload keys both arms report identically."""
+    return {"workload": WORKLOAD, "sites": int(n_sites), "walks": int(walks), "epsilon": EPSILON,
+            "max_steps": MAX_STEPS, "mesh_triangles": 327680, "source": "f = 1, u = 0 on the surface",
+            "l2": L2_POLICY}
 
 
 # ---------------------------------------------------------------- clocks
@@ -164,30 +218,6 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def l2_copy_gbs(stream, mib: int = 24, reps: int = 50) -> float:
-    """Copy bandwidth (read + write bytes) of an L2-resident buffer pair,
-    best of five timed batches: the in-run L2 roof for kernels whose working
-    set fits the 126 MB L2."""
-    import torch
-    n = mib * 1024 * 1024 // 4
-    a = torch.ones(n, dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
-    best = 0.0
-    with torch.cuda.stream(stream):
-        for _ in range(3):
-            b.copy_(a)
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(reps):
-                b.copy_(a)
-            e1.record(stream)
-            e1.synchronize()
-            best = max(best, 2.0 * a.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9)
-    del a, b
-    return best
-
-
 # ---------------------------------------------------------------- ranks
 def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
     """Max of a per-rank time over all ranks (identity without a process group)."""
@@ -200,40 +230,95 @@ def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
 
 
 def replica_seed(rank: int) -> int:
-    """Each rank's replica of the workload draws an independent stream."""
+    """In the replica mode each rank's copy of the workload draws an independent stream."""
     return SEED + rank
 
 
-# ---------------------------------------------------------------- CPU oracle leg
-def cpu_leg(V, F, sites, walks, seconds, repeat=0, threads=None):
-    """Times the oracle (reference algorithm and mt19937_64 stream, OpenMP) on a
-    random subset of the sites sized for about `seconds` of work."""
+# ---------------------------------------------------------------- host CPU legs
+def cpu_reference_leg(V, F, sites, walks, threads=None, workdir=None, repeat_tag=0):
+    """Times the reference's own compiled backend (oracle/_ref/wih_twos, its
+    `--mode twos` compliance path with f = 1 + 0 * (y + 0.5) = 1) on `sites`
+    with every host thread: its own timed region (runtime_seconds_median of
+    its summary: the site loop, not the mesh load or BVH build).  Falls back
+    to the oracle port (the same algorithm and mt19937_64 stream) when the
+    binary is missing.  Returns the rate and the per-site half-widths."""
     sys.path.insert(0, str(REPO / "oracle"))
+    import ref_runner
+    threads = threads or ref_runner.host_threads()
+    if ref_runner.available():
+        wd = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="twos_ref_"))
+        ply = wd / "mesh.ply"
+        if not ply.exists():
+            ref_runner.write_ply(ply, V, F)
+        rows, summ, wall = ref_runner.run_compliance(ply, sites, walks=walks, seed=SEED + repeat_tag,
+                                                     epsilon=EPSILON, max_steps=MAX_STEPS, slope=0.0,
+                                                     threads=threads, repeats=1, workdir=wd)
+        seconds = float(summ["runtime_seconds_median"])
+        return {"sites": len(sites), "seconds": seconds, "wall": wall, "rate": len(sites) / seconds,
+                "threads": int(summ["threads"]), "h": 1.96 * rows["score_se"], "kind": "reference",
+                "engine": "reference wih_twos.cpp (unchanged) + project BVH shim in place of Embree 4",
+                "queries_per_second": float(summ["distance_queries_per_second"]),
+                "mean_steps": float(summ["mean_steps"])}
     import oracle
     oracle.build()
-    threads = threads or oracle.default_threads()
     om = oracle.OracleMesh(V, F)
-    kw = dict(walks=walks, seed=SEED, epsilon=EPSILON, max_steps=MAX_STEPS,
-              source=[oracle.term(oracle.TERM_CONST, 1.0)], weight_order=0, threads=threads, repeat=repeat)
-    rng = np.random.default_rng(1234 + repeat)
-    pilot = sites[rng.choice(len(sites), size=min(len(sites), threads), replace=False)]
     t = time.perf_counter()
-    om.estimate(pilot, **kw)
-    per_round = time.perf_counter() - t
-    rounds = max(1, int(seconds / max(per_round, 1e-3)))
-    count = min(len(sites), threads * rounds)
-    idx = rng.choice(len(sites), size=count, replace=False)
-    t = time.perf_counter()
-    est = om.estimate(sites[idx], site_ids=idx, **kw)
+    est = om.estimate(sites, walks=walks, seed=SEED + repeat_tag, epsilon=EPSILON, max_steps=MAX_STEPS,
+                      source=[oracle.term(oracle.TERM_CONST, 1.0)], weight_order=0, threads=threads)
     dt = time.perf_counter() - t
-    return {"sites": count, "seconds": dt, "rate": count / dt, "threads": threads,
-            "h_median": float(np.median(1.96 * est["score_se"]))}
+    return {"sites": len(sites), "seconds": dt, "wall": dt, "rate": len(sites) / dt, "threads": threads,
+            "h": 1.96 * est["score_se"], "kind": "port",
+            "engine": "oracle restatement of wih_twos.cpp (reference algorithm + mt19937_64 stream)"}
+
+
+def cpu_model() -> str:
+    sys.path.insert(0, str(REPO / "oracle"))
+    import ref_runner
+    return ref_runner.cpu_model()
+
+
+# ---------------------------------------------------------------- accuracy legs
+def unit_ball_error_ratio(tb, walks: int, n_sites: int = 4096):
+    """Compliance on the unit sphere (icosphere L7, f = 1, u = 0, eps 1e-4):
+    the closed-form TD is u^2 = ((1 - |x|^2)/6)^2 (the reference's
+    paper/sections/03_problem.tex:5).  RMS error of each form's estimate
+    against it over n_sites sites uniform in r < 0.9, and their ratio
+    (mixed / FP64).  The mixed form runs with its distance grid."""
+    V, F = tb.geometry.icosphere(7)
+    sites = tb.geometry.uniform_ball(n_sites, 0.9, seed=2)
+    exact = ((1.0 - np.sum(sites ** 2, axis=1)) / 6.0) ** 2
+    out = {"workload": f"unit sphere (icosphere L7), compliance f=1 u=0, {n_sites} sites in r<0.9 x {walks} walks, "
+                       "eps 1e-4, exact TD ((1-|x|^2)/6)^2"}
+    with tb.Mesh(V, F) as mesh:
+        for prec in ("fp64", "mixed"):
+            cfg = tb.Config(walks=walks, precision=prec, seed=SEED + 7, epsilon=EPSILON, max_steps=MAX_STEPS,
+                            source=source_terms())
+            rows, summ = mesh.estimate(sites, cfg)
+            err = rows["score"] - exact
+            z = err / rows["score_se"]
+            out[prec] = {"rms_error": float(np.sqrt(np.mean(err ** 2))), "mean_error": float(np.mean(err)),
+                         "median_abs_z": float(np.median(np.abs(z))),
+                         "share_abs_z_below_3": float(np.mean(np.abs(z) < 3)),
+                         "grid_steps_share": summ["grid_steps"] / max(1, summ["steps"])}
+    out["error_ratio"] = out["mixed"]["rms_error"] / out["fp64"]["rms_error"]
+    out["target"] = "<= 1.1"
+    return out
+
+
+def mixed_vs_fp64(rows_mixed, rows64):
+    """Per-site z of the mixed form's TD against the FP64 form's over the
+    same sites (independent samples: the grid changes the mixed radii)."""
+    z = (rows_mixed["score"] - rows64["score"]) / np.hypot(rows_mixed["score_se"], rows64["score_se"])
+    return {"sites": int(len(z)), "max_abs_z": float(np.max(np.abs(z))),
+            "share_abs_z_below_3": float(np.mean(np.abs(z) < 3)), "mean_z": float(np.mean(z)),
+            "median_abs_z": float(np.median(np.abs(z)))}
 
 
 # ---------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
     import twos_b200 as tb
+    from twos_b200 import shard
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -246,17 +331,32 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     V, F, grid = workload(args.grid)
+    sites_all = workload_sites(grid)
+    n_all = len(sites_all)
     mesh = tb.Mesh(V, F, device=local)
     info = mesh.info()
-    sites = grid[mesh.inside(grid)]
+    sharded = world > 1 and args.shard == "sites"
+    if sharded:
+        # Contiguous blocks of equal predicted cost; every rank computes the
+        # same split from the same distances.
+        d = mesh.closest_point(sites_all, precision="mixed", with_points=False)
+        bounds = shard.partition(shard.site_cost(d, args.walks, EPSILON), world)
+        lo, hi = int(bounds[rank]), int(bounds[rank + 1])
+        seed = SEED
+    else:
+        bounds = np.array([0, n_all])
+        lo, hi = 0, n_all
+        seed = replica_seed(rank) if world > 1 else SEED
+    sites = sites_all[lo:hi]
     n = len(sites)
+    counts = np.diff(bounds) if sharded else [n]
     stream = torch.cuda.Stream()
     mesh.set_stream(stream)
     d_sites = torch.tensor(sites, dtype=torch.float64, device="cuda")
-    d_out = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    d_out = torch.zeros((max(n, 1), 7), dtype=torch.float64, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
-    base = dict(walks=args.walks, mode="compliance", seed=replica_seed(rank), epsilon=EPSILON, max_steps=MAX_STEPS,
-                source=source_terms(), query_radius=4.0)
+    base = dict(walks=args.walks, mode="compliance", seed=seed, epsilon=EPSILON, max_steps=MAX_STEPS,
+                source=source_terms(), query_radius=4.0, site_offset=lo)
 
     def barrier():
         if dist is not None:
@@ -286,23 +386,26 @@ def run_ours(args):
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
         barrier()
-        total = sum(ms)
-        total = max_over_ranks(total, dist, "cuda")
+        total = max_over_ranks(sum(ms), dist, "cuda")
         return total, ms, summs
+
+    def rows_now():
+        local_rows = d_out[:n].cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        return shard.gather_rows(local_rows, counts, dist, "cuda") if sharded else local_rows
 
     tuning = mesh.get_tuning()
     if not args.no_autotune:
         # The product's autotuner on a calibration subset, before any timing:
         # every rank tunes its own session the same way.
         from twos_b200.autotune import autotune
-        tuning, _ = autotune(mesh, sites, tb.Config(precision="mixed", **base), calib_sites=4096, calib_walks=128,
-                             repeats=2, seed=rank)
+        tuning, _ = autotune(mesh, sites_all, tb.Config(precision="mixed", **dict(base, site_offset=0)),
+                             calib_sites=4096, calib_walks=128, repeats=2, seed=rank)
     clocks = ClockSampler(local)
     clocks.start()
     cfg_mixed = tb.Config(precision="mixed", **base)
     t_mixed, ms_mixed, s_mixed = timed(cfg_mixed, args.steps, args.warmup)
-    rows_mixed = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
     clock_info = clocks.stop()
+    rows_mixed = rows_now()
     h_mixed = float(np.median(1.96 * rows_mixed["score_se"]))
 
     # e2e: host-buffer entry point, pinned host memory, copies inside the timed region.
@@ -311,31 +414,34 @@ def run_ours(args):
     host = (h_sites.numpy(), h_out.numpy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1))
     t_e2e, ms_e2e, s_e2e = timed(tb.Config(precision="mixed", **base), args.steps, 1, host=host)
 
+    units = n_all if sharded else world * n_all
     fp64 = None
+    rows64 = None
     if not args.no_fp64:
         t64, ms64, s64 = timed(tb.Config(precision="fp64", **base), args.fp64_steps, 1)
-        rows64 = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        rows64 = rows_now()
         h64 = float(np.median(1.96 * rows64["score_se"]))
-        fp64 = {"rate": world * n * len(ms64) / (t64 / 1e3), "ms_per_step": t64 / len(ms64), "steps": len(ms64),
+        fp64 = {"rate": units * len(ms64) / (t64 / 1e3), "ms_per_step": t64 / len(ms64), "steps": len(ms64),
                 "h_median": h64, "walk_seconds": float(np.mean([s["walk_seconds"] for s in s64]))}
     no_grid = None
     if not args.no_ablation:
         mesh.set_tuning(**dict(tuning, grid_threshold=0))
         t_ng, ms_ng, s_ng = timed(tb.Config(precision="mixed", **base), 1, 1)
-        rows_ng = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
+        rows_ng = rows_now()
         mesh.set_tuning(**tuning)
-        no_grid = {"rate_unscaled": world * n / (t_ng / 1e3), "ms_per_step": t_ng,
+        no_grid = {"rate_unscaled": units / (t_ng / 1e3), "ms_per_step": t_ng,
                    "h_median": float(np.median(1.96 * rows_ng["score_se"])),
-                   "walk_seconds": s_ng[0]["walk_seconds"], "steps_per_walk": s_ng[0]["steps"] / s_ng[0]["paths"]}
+                   "walk_seconds": s_ng[0]["walk_seconds"],
+                   "steps_per_walk": s_ng[0]["steps"] / max(1, s_ng[0]["paths"])}
     h_ref = fp64["h_median"] if fp64 else h_mixed
     if no_grid:
         no_grid["rate"] = no_grid["rate_unscaled"] * (no_grid["h_median"] / h_ref) ** 2
         if fp64:
             no_grid["over_fp64"] = no_grid["rate"] / fp64["rate"]
     scale = (h_mixed / h_ref) ** 2
-    rate_mixed = world * n * args.steps / (t_mixed / 1e3)
+    rate_mixed = units * args.steps / (t_mixed / 1e3)
     value = rate_mixed * scale
-    rate_e2e = world * n * args.steps / (t_e2e / 1e3) * scale
+    rate_e2e = units * args.steps / (t_e2e / 1e3) * scale
 
     out = None
     if rank == 0:
@@ -346,6 +452,7 @@ def run_ours(args):
         nodes = np.mean([s["node_tests"] for s in s_mixed])
         planes = np.mean([s["plane_tests"] for s in s_mixed])
         tris = np.mean([s["triangle_tests"] for s in s_mixed])
+        walks_launch = n * args.walks
         # Bytes the walk kernel must fetch: 96 B per node visit (two child
         # boxes + normal slabs + child words), 32 B per triangle plane test
         # (plane slab + first vertex), 32 B more per full closest-point test
@@ -355,53 +462,69 @@ def run_ours(args):
         grid_lookups = steps if info["grid_dims"][0] else 0.0
         fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris + 128.0 * grid_lookups
         bvh_queries = queries - grid_steps
-        peak, peak_kind = measured_peaks()
+        hbm_peak, hbm_kind = measured_peaks()
+        l2_peak = tb.l2_read_gbs(local)
         ach = fetched / walk_s / 1e9
-        l2 = l2_copy_gbs(stream)
-        canon = CANONICAL_BYTES_PER_QUERY * bvh_queries / walk_s / 1e9
-        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": dram_traffic_per_launch(n * args.walks),
-                "traffic_source": "profiles/wos_kernel_noise_sphere_L7.md (ncu, full workload, 14.25 B/walk)",
-                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "bytes_per_walk": float(fetched / (n * args.walks)),
+        traffic = dram_traffic_per_launch(walks_launch)
+        roof = {"bound": "l2", "achieved": ach, "peak": l2_peak, "unit": "GB/s", "frac": ach / l2_peak,
+                "traffic": traffic,
+                "peak_source": "measured in this run: twos_l2_read_gbs, 32-byte loads from every SM over a "
+                               "64 MiB L2-resident buffer (the walk kernel's load form)",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-workload walk-kernel "
+                                  "launch, 14.25 B per walk (per-walk samples), scaled to this launch's walks",
+                "hbm": {"peak": hbm_peak, "peak_source": hbm_kind + " hbm_gbs",
+                        "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
+                "ncu_walk_kernel": NCU_WALK_KERNEL,
+                "bytes_per_walk": float(fetched / walks_launch),
                 "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test"
                                     " + 128 B/distance-grid lookup (one per step)",
                 "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),
                 "bvh_queries_per_launch": float(bvh_queries), "walk_kernel_seconds": walk_s,
                 "bvh_queries_per_second": float(bvh_queries / walk_s),
-                "steps_per_walk": float(steps / (n * args.walks)),
+                "steps_per_walk": float(steps / walks_launch),
                 "node_tests_per_bvh_query": float(nodes / bvh_queries),
                 "plane_tests_per_bvh_query": float(planes / bvh_queries),
                 "triangle_tests_per_bvh_query": float(tris / bvh_queries),
-                "l2": {"peak": l2, "frac": ach / l2, "peak_source": "in-run copy of a 24 MiB L2-resident buffer"},
                 "canonical": {"bytes_per_query": CANONICAL_BYTES_PER_QUERY, "source": CANONICAL_SOURCE,
-                              "effective_gbs": canon,
-                              "note": "binary-SAH reference traversal's bytes; ours fetches fewer per query"}}
+                              "effective_gbs": CANONICAL_BYTES_PER_QUERY * bvh_queries / walk_s / 1e9,
+                              "note": "bytes of a plain binary-SAH traversal per BVH query; this traversal "
+                                      "fetches ~18x fewer and the grid skips most queries, so it is not a roof"}}
+        accuracy = {}
+        if rows64 is not None:
+            accuracy["mixed_vs_fp64_z"] = mixed_vs_fp64(rows_mixed, rows64)
+        if not args.no_accuracy and world == 1:
+            accuracy["error_ratio_vs_oracle"] = unit_ball_error_ratio(tb, args.walks)
         cpu = None
         if not args.no_cpu and world == 1:
-            c = cpu_leg(V, F, sites, args.walks, args.cpu_seconds)
-            cpu = {"value": c["rate"] * (c["h_median"] / h_ref) ** 2, "unit": UNIT, "cores": c["threads"],
-                   "kind": "port",
-                   "sample": f"{c['sites']} random interior sites x {args.walks} walks, oracle (reference "
-                             f"algorithm + mt19937_64 stream), OpenMP {c['threads']} threads, {c['seconds']:.1f} s"}
+            idx = reference_subset(n_all, REF_SUBSET)[: args.cpu_sites]
+            c = cpu_reference_leg(V, F, sites_all[idx], args.walks)
+            h_cpu = float(np.median(c["h"]))
+            h_gpu = float(np.median(1.96 * rows64["score_se"][idx])) if rows64 is not None else h_cpu
+            cpu = {"value": c["rate"] * (h_cpu / h_gpu) ** 2, "unit": UNIT, "cores": c["threads"], "kind": c["kind"],
+                   "cpu_model": cpu_model(), "rate_unscaled": c["rate"],
+                   "sample": f"the first {c['sites']} sites of the fixed {REF_SUBSET}-site random subset (seed "
+                             f"{REF_SUBSET_SEED}) x {args.walks} walks, {c['engine']}, OpenMP {c['threads']} threads, "
+                             f"OMP_PROC_BIND=true, {c['seconds']:.1f} s in its timed site loop; scaled to the FP64 "
+                             "GPU form's half-width on the same sites"}
         launches = int(sum(s["launches"] for s in s_mixed))
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 query/position, f64 accumulation",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sites": int(n), "walks": args.walks, "epsilon": EPSILON,
-                       "max_steps": MAX_STEPS, "mesh_triangles": int(info["faces"]),
-                       "bvh_nodes": int(info["bvh_nodes"]), "mixed_delta": info["mixed_delta"],
-                       "distance_grid": {"dims": info["grid_dims"], "spacing": info["grid_spacing"],
-                                         "build_seconds_with_bvh": info["build_seconds"]},
-                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                       "tuning": tuning},
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "f32 query/position, f64 accumulation", "data": "synthetic",
+            "config": workload_config(n_all, args.walks),
+            "parallelism": (f"sites sharded over {world} GPUs (contiguous equal-cost blocks, one row gather)"
+                            if sharded else (f"replicas x{world}" if world > 1 else "1 GPU")),
+            "implementation": {"bvh_nodes": int(info["bvh_nodes"]), "mixed_delta": info["mixed_delta"],
+                               "distance_grid": {"dims": info["grid_dims"], "spacing": info["grid_spacing"],
+                                                 "build_seconds_with_bvh": info["build_seconds"]},
+                               "tuning": tuning},
             "ci": {"h_mixed_median": h_mixed, "h_fp64_median": h_ref, "scale": scale,
                    "rate_mixed_unscaled": rate_mixed},
             "fp64_form": fp64,
             "mixed_over_fp64": (value / fp64["rate"]) if fp64 else None,
             "mixed_without_grid": no_grid,
+            "accuracy": accuracy,
             "e2e": {"value": rate_e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
                     "d2h_bytes_per_step": int(n * 56), "ms_per_step": t_e2e / args.steps},
             "roofline": roof,
@@ -419,41 +542,43 @@ def run_ours(args):
 
 
 def run_reference(args):
-    """The reference's algorithm on the host cores: the oracle (restatement of
-    wih_twos.cpp's compliance walk with its mt19937_64 stream), OpenMP over all
-    threads, each step a bounded random sample of the workload's sites."""
+    """The reference's own compiled backend on the host cores: wih_twos.cpp
+    built unchanged (oracle/_ref/wih_twos, with the project's shim headers in
+    place of Embree 4 and Eigen), OpenMP over every host thread with
+    OMP_PROC_BIND=true, on the same workload and sites.  The fixed
+    --ref-sites random subset is split over the K timed steps (one process
+    per step, its own timed site loop); warm-up steps run 4 sites each."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     V, F, grid = workload(args.grid)
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle
-    oracle.build()
-    # Interior sites by the oracle's exact distance + ray parity is not needed:
-    # the star-shaped surface gives the interior test directly.
-    from twos_b200 import geometry
-    r = np.linalg.norm(grid, axis=1)
-    keep = r > 1e-12
-    g = grid[keep]
-    rad = 1.0 + 0.15 * geometry.sh_field(g / r[keep][:, None], 1)
-    sites = g[r[keep] < rad]
-    per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
+    sites_all = workload_sites(grid)
+    idx = reference_subset(len(sites_all), args.ref_sites)
+    wd = Path(tempfile.mkdtemp(prefix="twos_ref_"))
     for w in range(args.warmup):
-        cpu_leg(V, F, sites, args.walks, per_step / 4, repeat=100 + w)
-    runs = [cpu_leg(V, F, sites, args.walks, per_step, repeat=k) for k in range(args.steps)]
+        cpu_reference_leg(V, F, sites_all[idx[4 * w: 4 * w + 4]], args.walks, workdir=wd, repeat_tag=100 + w)
+    chunks = np.array_split(idx, max(1, args.steps))
+    runs = [cpu_reference_leg(V, F, sites_all[c], args.walks, workdir=wd) for c in chunks if len(c)]
     total_sites = sum(c["sites"] for c in runs)
     total_s = sum(c["seconds"] for c in runs)
     value = total_sites / total_s
     threads = runs[0]["threads"]
+    h = np.concatenate([c["h"] for c in runs])
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / max(1, len(runs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "walks": args.walks, "epsilon": EPSILON, "max_steps": MAX_STEPS,
-                   "parallelism": f"OpenMP x{threads} host threads"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{total_sites} random interior sites over {args.steps} steps x {args.walks} "
-                                   "walks (oracle: reference algorithm + mt19937_64 stream)"},
+        "config": workload_config(len(sites_all), args.walks),
+        "parallelism": f"OpenMP x{threads} host threads",
+        "ci": {"h_median": float(np.median(h)),
+               "scale": 1.0, "note": "the reference is the FP64 algorithm at the same N: its half-width is the "
+                                     "FP64 GPU form's, so the equal-CI scale is 1"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": runs[0]["kind"],
+                         "cpu_model": cpu_model(),
+                         "sample": f"fixed {total_sites}-site random subset (seed {REF_SUBSET_SEED}) of the "
+                                   f"{len(sites_all)} sites over {len(runs)} steps x {args.walks} walks, "
+                                   f"{runs[0]['engine']}, OMP_PROC_BIND=true; rate = sites / the reference's own "
+                                   "timed site loop"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -465,7 +590,7 @@ def run_housing_box(args):
     walks with a Green point per step; mixed form at eps in {1e-3, 1e-4,
     1e-5}: site-estimates/s over `--sites` sites x `--walks` walks, and the
     error of the cross-index TD against the FP64 form with 16x the walks on
-    the first `--ref-sites` sites (RMS error, and z = error / combined
+    the first `--housing-ref-sites` sites (RMS error, and z = error / combined
     standard error), also with the distance grid off."""
     import torch
     import twos_b200 as tb
@@ -491,7 +616,7 @@ def run_housing_box(args):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         est = d_out.cpu().numpy().copy().view(np.dtype(tb.SITE_DTYPE)).reshape(-1)
-        m = args.ref_sites
+        m = args.housing_ref_sites
         ref, _ = mesh.estimate(sites[:m], tb.Config(walks=16 * args.walks, precision="fp64", **dict(base, seed=SEED + 1)))
         # The same sites in the mixed form with the distance grid off: the
         # grid's share of the error, if any.
@@ -517,7 +642,7 @@ def run_housing_box(args):
                      "td_rms": float(np.sqrt(np.mean(ref["score"] ** 2)))})
     mesh.close()
     return {"workload": "housing-like box 4x2x1 minus 6 cylinders, 529,608 triangles, 1M sites", "triangles": int(len(F)),
-            "sites": n, "walks": args.walks, "reference": f"FP64 form, {16 * args.walks} walks, {args.ref_sites} sites",
+            "sites": n, "walks": args.walks, "reference": f"FP64 form, {16 * args.walks} walks, {args.housing_ref_sites} sites",
             "dtype": "f32 query/position, f64 accumulation", "data": "synthetic", "per_epsilon": rows}
 
 
@@ -580,8 +705,12 @@ def run_design(args):
     walks, takes the top 64, validates them with 4,096 fresh walks (stream
     1), takes the best lower bound score - 1.96 SE and inserts a ball cavity
     of radius 0.03 when it clears the threshold; compliance, f = 1, eps 1e-4.
-    Reports iterations/s of the mixed and the FP64 form and whether their
-    chosen candidates and accept decisions agree under shared samples."""
+    Reports iterations/s of the mixed and the FP64 form, whether their
+    chosen candidates and accept decisions agree, and -- since the scout's
+    distance grid lets the two forms choose different (near-tied)
+    candidates -- whether the FP64 form, validating the mixed form's own
+    choice with the same samples (the validation stage runs without the
+    grid), reaches the same accept bit at every iteration."""
     import torch  # noqa: F401
     import twos_b200 as tb
     from twos_b200 import geometry, sources
@@ -603,8 +732,28 @@ def run_design(args):
             h, cav, summ = mesh.design_loop(cand, scout, val, **kw)
             dt = time.perf_counter() - t0
             hist[prec] = h
+            if prec == "mixed":
+                cav_mixed = cav
             out[prec] = {"seconds": dt, "iterations_per_s": kw["iterations"] / dt, "accepted": int(h["accepted"].sum()),
                          "launches": summ["launches"]}
+        # Replay each mixed-form validation in FP64 with the loop's keys:
+        # stream 1, repeat = iteration, site index = the choice's shortlist
+        # slot, the cavities present then.
+        h, cav = hist["mixed"], cav_mixed
+        same = []
+        for it in range(kw["iterations"]):
+            if h["chosen"][it] == 0xFFFFFFFF:
+                continue
+            val = tb.Config(walks=4096, precision="fp64", seed=SEED, stream=1, epsilon=EPSILON, max_steps=MAX_STEPS,
+                            source=sources.constant(1.0), repeat=it, site_offset=int(h["slot"][it]),
+                            cavity_radius=kw["cavity_radius"])
+            c = cav[: int(h["n_cavities"][it])]
+            r, _ = mesh.estimate(cand[int(h["chosen"][it])][None, :], val, cavities=c if len(c) else None)
+            lower64 = float(r["score"][0] - kw["z"] * r["score_se"][0])
+            same.append({"iteration": it, "lower_mixed": float(h["lower"][it]), "lower_fp64": lower64,
+                         "accept_mixed": bool(h["accepted"][it]), "accept_fp64": bool(lower64 > kw["accept_threshold"])})
+        out["accept_identical_given_chosen"] = all(s["accept_mixed"] == s["accept_fp64"] for s in same)
+        out["accept_replay"] = same
     out["decisions_identical"] = bool(np.array_equal(hist["mixed"]["chosen"], hist["fp64"]["chosen"]) and
                                       np.array_equal(hist["mixed"]["accepted"], hist["fp64"]["accepted"]))
     for prec in ("mixed", "fp64"):
@@ -660,6 +809,8 @@ def run_unit_sphere(args):
                 ktimes.append(summ["kernel_seconds"])
             z = (rows["cross"] - cross_exact) / rows["cross_se"]
             td = 1.5 * rows["cross"] - qx * rows["u"]
+            # The TD's standard error bounded by the parts' (|cov| <= sd sd).
+            zt = (td - td_exact) / (1.5 * rows["cross_se"] + np.abs(qx) * rows["u_se"])
             out[prec] = {"site_estimates_per_s": len(sites) / float(np.median(times)),
                          "seconds": float(np.median(times)), "kernel_seconds": float(np.median(ktimes)),
                          "steps_per_walk": summ["steps"] / summ["paths"], "grid_steps": summ["grid_steps"],
@@ -667,7 +818,9 @@ def run_unit_sphere(args):
                          float(np.mean(np.abs(z) < 3)), "cross_mean_z": float(np.mean(z)),
                          "u_mean_abs_error": float(np.mean(np.abs(rows["u"] - g))),
                          "td_rms_error": float(np.sqrt(np.mean((td - td_exact) ** 2))),
-                         "td_rms": float(np.sqrt(np.mean(td_exact ** 2)))}
+                         "td_rms": float(np.sqrt(np.mean(td_exact ** 2))),
+                         "td_max_abs_z": float(np.max(np.abs(zt))), "td_share_abs_z_below_3":
+                         float(np.mean(np.abs(zt) < 3)), "td_rms_z": float(np.sqrt(np.mean(zt ** 2)))}
     if not args.no_cpu:
         sys.path.insert(0, str(REPO / "oracle"))
         import oracle
@@ -689,6 +842,9 @@ def run_unit_sphere(args):
                                          f"form (counter stream), OpenMP {threads} threads, {dt:.1f} s"}
         out["fp64_over_cpu"] = out["fp64"]["site_estimates_per_s"] / out["cpu_baseline"]["value"]
     out["mixed_over_fp64"] = out["mixed"]["site_estimates_per_s"] / out["fp64"]["site_estimates_per_s"]
+    out["td_error_ratio_mixed_over_fp64"] = out["mixed"]["td_rms_error"] / out["fp64"]["td_rms_error"]
+    out["td_formula_check"] = ("D_T = 3/2 grad u . grad p - q u - f p, exact on a finite Neumann hole "
+                               "(tests/test_neumann_hole_cpu.py)")
     return out
 
 

@@ -255,6 +255,13 @@ typedef struct twos_tuning {
   int32_t units;         /* traversal units (node visits or triangle tests) a
                             lane runs back to back before its warp returns to
                             the refill and step ballots (1..64).  Default 8. */
+  int32_t chain;         /* mixed form: grid steps a lane may take back to back
+                            in one step phase before it rejoins its warp
+                            (1..64).  Default 1. */
+  int32_t entry;         /* mixed form: 1 lets a closest-point query whose
+                            initial bound is below one entry cell start at
+                            the entry-node table's node instead of the root
+                            (same result, fewer node visits); 0 = root. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);
@@ -329,7 +336,9 @@ int twos_estimate_noalloc(twos_mesh *mesh, const twos_request *request, const do
  * (may be NULL when n_cavities[j] == 0) and writes out[j].  All meshes must be
  * sessions on the same device; all requests must share mode, precision and the
  * Green-point flag.  Walks of every job share one device work queue, so a
- * batch of uneven meshes, site counts and walk counts keeps every SM busy.
+ * batch of uneven meshes, site counts and walk counts keeps every SM busy;
+ * the queue takes the jobs largest geometry, smallest, second largest, ...
+ * so two geometries that each fill much of the L2 are not in flight at once.
  * Results equal those of one twos_estimate call per job with the same
  * requests.  The work runs on meshes[0]'s stream; `summary` totals the batch.
  * Replaces a driver loop of one process call per geometry (e.g.
@@ -347,7 +356,12 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
  * when its surface distance is >= cavity_radius + outer_clearance and it is
  * at least 2 * cavity_radius + pair_gap from every cavity (feasible_mask,
  * run_bunny_benchmark.py:290-299).  Every decision is taken on the device;
- * with use_graph one iteration is captured as a CUDA graph and replayed. */
+ * with use_graph one iteration is captured as a CUDA graph and replayed.
+ * Iteration i keys its scout walks by (repeat i, candidate index) and its
+ * validation walks by (repeat i, shortlist slot); the validation stage runs
+ * without the mixed form's distance grid, so both precisions validate a
+ * candidate with the same samples.  history[i].slot and .n_cavities record
+ * what a replay of that validation needs. */
 typedef struct twos_design_params {
   uint32_t iterations;
   uint32_t shortlist;       /* <= 1024 */
@@ -367,6 +381,8 @@ typedef struct twos_design_step {
   double score;             /* validation estimate */
   double score_se;
   double lower;             /* score - z * score_se */
+  uint32_t slot;            /* the choice's shortlist slot: its validation walks' site index */
+  uint32_t n_cavities;      /* cavities present while it was validated */
 } twos_design_step;
 
 /* history[iterations]; cavities_out holds up to n_cavities + iterations
@@ -485,6 +501,23 @@ typedef struct twos_rqmc_params {
 
 int twos_rqmc(twos_mesh *mesh, const twos_request *request, const twos_rqmc_params *params, const double *sites,
               uint32_t n_sites, double *batch_u, double *batch_p, double *td, twos_summary *summary);
+
+/* Test hook for the mixed form's distance grid: runs the mixed compliance
+ * estimate of `request` (centre-point source, no cavities) over `sites` in a
+ * walk kernel that records every grid step -- the walk's position (original
+ * coordinates, the FP32 position exactly) and the bound it used as the
+ * ball's radius before the delta shrink -- keeping the first `capacity`
+ * records in points [capacity][3] and bounds [capacity]; *count is the total
+ * number of grid steps.  Host buffers.  No reference counterpart. */
+int twos_trace_grid_steps(twos_mesh *mesh, const twos_request *request, const double *sites, uint32_t n_sites,
+                          uint64_t capacity, double *points, double *bounds, uint64_t *count);
+
+/* Measured L2 read bandwidth of `device` in GB/s: the best of five timed
+ * launches that each stream a zeroed `bytes` buffer (an L2-resident size,
+ * e.g. 64 MiB) `passes` times with 32-byte vector loads from every SM, the
+ * walk kernel's load form.  The roofline denominator for kernels whose
+ * working set is L2-resident.  No reference counterpart (a measurement). */
+int twos_l2_read_gbs(int device, uint64_t bytes, uint32_t passes, double *gbs);
 
 /* The estimator's per-site reduction on caller-supplied per-walk samples:
  * u and p (p may be NULL outside paired mode) [n_sites][walks] as doubles,

@@ -17,7 +17,7 @@ from conftest import GOLDEN, PKG, REPO
 
 def _declared():
     text = (REPO / "include" / "twos.h").read_text()
-    return sorted(set(re.findall(r"\b(twos_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(twos_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol(lib_built):

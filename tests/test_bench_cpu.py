@@ -1,5 +1,7 @@
 """bench.py's reference arm on the host cores (no GPU): one JSON line with the
-contract's keys, the reference arm's marker and a bounded CPU sample."""
+contract's keys, the reference arm's marker, a bounded CPU sample of the
+reference's own compiled backend (oracle/_ref/wih_twos; the oracle port when
+it is not built), and the same workload keys as the GPU arm reports."""
 import contextlib
 import io
 import json
@@ -7,9 +9,10 @@ import json
 
 def test_reference_arm_prints_the_contract_line(lib_built):
     import bench
+    import ref_runner
     buf = io.StringIO()
     with contextlib.redirect_stdout(buf):
-        bench.main(["--impl", "reference", "--steps", "1", "--warmup", "0", "--walks", "64", "--cpu-seconds", "1"])
+        bench.main(["--impl", "reference", "--steps", "2", "--warmup", "1", "--walks", "64", "--ref-sites", "6"])
     lines = [l for l in buf.getvalue().splitlines() if l.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
@@ -17,7 +20,16 @@ def test_reference_arm_prints_the_contract_line(lib_built):
               "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
-    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1
-    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 2
+    assert d["cpu_baseline"]["kind"] == ("reference" if ref_runner.available() else "port")
+    assert d["cpu_baseline"]["cores"] >= 1 and d["cpu_baseline"]["cpu_model"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
-    assert "workload" in d["config"]
+    V, F, grid = bench.workload(64)
+    assert d["config"] == bench.workload_config(len(bench.workload_sites(grid)), 64)
+
+
+def test_reference_subset_is_fixed():
+    import bench
+    a = bench.reference_subset(122000, 1024)
+    assert len(a) == 1024 and len(set(a.tolist())) == 1024
+    assert (a == bench.reference_subset(122000, 1024)).all()

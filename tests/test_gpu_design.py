@@ -98,3 +98,41 @@ def test_mixed_grid_design_loop_agrees_with_fp64(tb):
     assert summ["grid_steps"] > 0 and summ["caps"] == 0
     se = np.hypot(h64["score_se"][0], h32["score_se"][0])
     assert abs(h64["lower"][0] - h32["lower"][0]) < 4 * se
+
+
+def _replay_validation(tb, mesh, cand, cav, h, it, precision):
+    """The validation estimate of iteration `it`'s chosen candidate, replayed
+    as a one-site estimate with the loop's keys: stream 1, repeat = it, site
+    index = the choice's shortlist slot, the cavities present then."""
+    _, val = _configs(tb, precision)
+    val.repeat = it
+    val.site_offset = int(h["slot"][it])
+    val.cavity_radius = KW["cavity_radius"]
+    c = cav[: int(h["n_cavities"][it])]
+    rows, _ = mesh.estimate(cand[int(h["chosen"][it])][None, :], val, cavities=c if len(c) else None)
+    return rows[0]
+
+
+def test_accept_decisions_identical_given_chosen(tb):
+    """The scout keeps the mixed form's distance grid, so the two forms may
+    choose different candidates; the validation stage runs without it, so
+    for the candidate the mixed loop chose, the FP64 form's validation of the
+    same candidate uses the same samples and reaches the same accept bit."""
+    V, F, cand = _setup(tb)
+    with tb.Mesh(V, F) as mesh:
+        h32, cav32, summ = mesh.design_loop(cand, *_configs(tb, "mixed"), **KW)
+        assert summ["grid_steps"] > 0
+        mesh.set_tuning(grid_threshold=0)
+        checked = 0
+        for it in range(KW["iterations"]):
+            if h32["chosen"][it] == 0xFFFFFFFF:
+                continue
+            same = _replay_validation(tb, mesh, cand, cav32, h32, it, "mixed")
+            assert same["score"] == h32["score"][it] and same["score_se"] == h32["score_se"][it]
+            r64 = _replay_validation(tb, mesh, cand, cav32, h32, it, "fp64")
+            lower64 = r64["score"] - KW["z"] * r64["score_se"]
+            assert abs(lower64 - h32["lower"][it]) < 1e-3 * abs(h32["lower"][it])
+            if abs(lower64 - KW["accept_threshold"]) > 1e-3 * KW["accept_threshold"]:
+                assert bool(lower64 > KW["accept_threshold"]) == bool(h32["accepted"][it])
+                checked += 1
+    assert checked >= KW["iterations"] - 1

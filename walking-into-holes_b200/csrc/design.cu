@@ -68,10 +68,13 @@ __global__ void design_select_kernel(const DesignLaunch D) {
   h.score = CUDART_NAN;
   h.score_se = CUDART_NAN;
   h.lower = CUDART_NAN;
+  h.slot = 0xffffffffu;
+  h.n_cavities = D.scout_job->n_cav;
   if (arg != 0xffffffffu) {
     const uint32_t c = D.shortlist[arg];
     const twos_site_result r = D.val_rows[arg];
     h.chosen = c;
+    h.slot = arg;
     h.scout_score = D.scout_rows[c].score;
     h.score = r.score;
     h.score_se = r.score_se;

@@ -14,6 +14,7 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include "twos_internal.h"
 
@@ -605,6 +606,89 @@ int inside_parity(const HostBvh &bvh, const std::vector<double> &v, const std::v
   }
   inside = (hits % 2u) == 1u;
   return 0;
+}
+
+
+// Entry nodes of the mixed form's query (see twos_internal.h).  Every cell
+// collects the leaf-order range [lo, hi] of the leaves whose box lies within
+// `radius` of the cell's box grown by `pad` (box-to-box distance, a lower
+// bound of every triangle's distance); the cell's entry is the deepest node
+// whose subtree covers that range.  Node subtrees cover contiguous
+// leaf-order ranges, so the descent from the root keeps the child that
+// contains the whole range.
+std::vector<int32_t> build_entry_table(const HostBvh &bvh, const double origin[3], double cell, const uint32_t dims[3],
+                                       double radius, double pad) {
+  const std::vector<Range> ranges = node_ranges(bvh);
+  const size_t count = static_cast<size_t>(dims[0]) * dims[1] * dims[2];
+  std::vector<int32_t> entry(count, 0);
+  if (bvh.nodes.empty() || count == 0) return entry;
+  const double r2 = radius * radius;
+  auto box_gap2 = [](const double *alo, const double *ahi, const double *blo, const double *bhi) {
+    double s = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double g = std::max(std::max(alo[a] - bhi[a], blo[a] - ahi[a]), 0.0);
+      s += g * g;
+    }
+    return s;
+  };
+  auto work = [&](uint32_t i_begin, uint32_t i_end) {
+    std::vector<int32_t> stack;
+    stack.reserve(256);
+    for (uint32_t i = i_begin; i < i_end; ++i)
+      for (uint32_t j = 0; j < dims[1]; ++j)
+        for (uint32_t k = 0; k < dims[2]; ++k) {
+          const uint32_t ijk[3] = {i, j, k};
+          double lo[3], hi[3];
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = origin[a] + cell * ijk[a] - pad;
+            hi[a] = origin[a] + cell * (ijk[a] + 1) + pad;
+          }
+          uint32_t mn = std::numeric_limits<uint32_t>::max(), mx = 0;
+          stack.clear();
+          stack.push_back(0);
+          while (!stack.empty()) {
+            const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(stack.back())];
+            stack.pop_back();
+            for (int c = 0; c < 2; ++c) {
+              if (!(nd.lo[c][0] <= nd.hi[c][0])) continue;  // empty child
+              if (box_gap2(lo, hi, nd.lo[c], nd.hi[c]) > r2) continue;
+              if (nd.child[c] >= 0) {
+                stack.push_back(nd.child[c]);
+              } else {
+                const Range rg = code_range(nd.child[c], ranges);
+                if (rg.end > rg.begin) {
+                  mn = std::min(mn, rg.begin);
+                  mx = std::max(mx, rg.end - 1);
+                }
+              }
+            }
+          }
+          int32_t ni = 0;
+          if (mn <= mx) {
+            for (bool deeper = true; deeper;) {
+              deeper = false;
+              const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(ni)];
+              for (int c = 0; c < 2; ++c) {
+                const int32_t code = nd.child[c];
+                if (code >= 0 && ranges[code].begin <= mn && mx < ranges[code].end) {
+                  ni = code;
+                  deeper = true;
+                  break;
+                }
+              }
+            }
+          }
+          entry[(static_cast<size_t>(i) * dims[1] + j) * dims[2] + k] = ni;
+        }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t threads = std::min<uint32_t>(hw, dims[0]);
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < threads; ++t)
+    pool.emplace_back(work, static_cast<uint32_t>(static_cast<uint64_t>(dims[0]) * t / threads),
+                      static_cast<uint32_t>(static_cast<uint64_t>(dims[0]) * (t + 1) / threads));
+  for (auto &th : pool) th.join();
+  return entry;
 }
 
 }  // namespace twos

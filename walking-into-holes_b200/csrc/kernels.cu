@@ -510,11 +510,16 @@ __device__ __forceinline__ Vec<float> grid_vertex(const GeoDesc &g, uint32_t i, 
           __fadd_rn(g.grid_lo[2], __fmul_rn(static_cast<float>(k), g.grid_h))};
 }
 
-// The grid's lower bound of the mesh distance at `p` (FP32 frame): the
+// The grid's bounds of the mesh distance at `p` (FP32 frame).  Lower: the
 // largest D(v) - |p - v| over the eight corners v of p's cell (the distance
-// is 1-Lipschitz, so each is a bound).  False when p lies outside the grid
-// (or is NaN).
-__device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p, float &bound) {
+// is 1-Lipschitz, so each is a bound).  Upper (before the FP32 allowance
+// the caller adds): the smallest (D(v) + 1) q + |p - v| over the corners
+// whose value is not saturated -- a vertex stores floor((d_FP32 - 2 delta)/q),
+// so its distance is below (D + 1) q + 3 delta.  `entry_at` is the index of
+// p's cell in the entry-node table (all ones without a table).  False when p
+// lies outside the grid (or is NaN).
+__device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &p, float &bound, float &upper,
+                                            uint32_t &entry_at) {
   const float fx = (p.x - g.grid_lo[0]) * g.grid_inv_h;
   const float fy = (p.y - g.grid_lo[1]) * g.grid_inv_h;
   const float fz = (p.z - g.grid_lo[2]) * g.grid_inv_h;
@@ -526,19 +531,29 @@ __device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p
   const uint32_t i0 = min(static_cast<uint32_t>(fx), g.grid_n[0] - 2);
   const uint32_t j0 = min(static_cast<uint32_t>(fy), g.grid_n[1] - 2);
   const uint32_t k0 = min(static_cast<uint32_t>(fz), g.grid_n[2] - 2);
-  float best = -CUDART_INF_F;
+  float best = -CUDART_INF_F, up = CUDART_INF_F;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const uint32_t i = i0 + (c >> 2), j = j0 + ((c >> 1) & 1), k = k0 + (c & 1);
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
-    const float b =
-        static_cast<float>(__ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k)) * g.grid_q -
-        sqrtf(dot3(dv, dv));
-    best = fmaxf(best, b);
+    const uint16_t raw = __ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k);
+    const float dist = sqrtf(dot3(dv, dv));
+    const float dq = static_cast<float>(raw) * g.grid_q;
+    best = fmaxf(best, dq - dist);
+    if (raw != 0xffffu) up = fminf(up, dq + g.grid_q + dist);
   }
   bound = best;
+  upper = up;
+  const uint32_t s = g.entry_shift;
+  entry_at = g.entry ? ((i0 >> s) * g.entry_n[1] + (j0 >> s)) * g.entry_n[2] + (k0 >> s) : 0xffffffffu;
   return true;
+}
+
+__device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p, float &bound) {
+  float upper;
+  uint32_t at;
+  return grid_bounds(g, p, bound, upper, at);
 }
 
 __device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, uint64_t wid) {
@@ -602,7 +617,7 @@ constexpr int wos_min_blocks(int block) {
                                                                               : 768 / block;
 }
 
-template <typename T, int MODE, int SRC, int BLOCK>
+template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false>
 __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
@@ -741,177 +756,212 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
     if (ready != 0u && (__popc(ready) >= L.step_threshold || trav == 0u) && phase == kStep) {
       const JobDesc &J = s_jobs[job];
       const GeoDesc &G = s_geos[J.geo];
-      T d = sqrt(best2);
-      if (!found) {
-        err |= TWOS_DEVERR_QUERY;
-        d = T(0);  // ends the walk; the call reports the failure
-      }
-      const T R = to_T<T>(J.cavity_radius);
-      const T dmesh = d;
-      int hit_cav = -1;
-      bool cav_nearer = false;  // gradient mode: the exit is on a cavity
-      for (uint32_t c = 0; c < J.n_cav; ++c) {
-        const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
-        const Vec<T> dv = sub(pos, cc);
-        const T len = sqrt(dot3(dv, dv));
-        const T dc = len - R;
-        if (MODE == kModeBoundary) {
-          // closest_boundary (wih_twos.cpp:612-624): the first strictly nearer cavity.
-          if (dc < d && len > T(0)) {
-            d = dc;
-            hit_cav = static_cast<int>(c);
-          }
-        } else {
-          d = dc < d ? dc : d;
-          if (GRAD && dc < dmesh) cav_nearer = true;
+      // Up to L.chain steps: a lane whose next radius comes from the grid
+      // takes that step at once instead of waiting for the warp's next batch.
+#pragma unroll 1
+      for (int link = 1;; ++link) {
+        T d = sqrt(best2);
+        if (!found) {
+          err |= TWOS_DEVERR_QUERY;
+          d = T(0);  // ends the walk; the call reports the failure
         }
-      }
-      // The mixed form shrinks the radius by the FP32 distance error bound;
-      // the FP64 form uses the distance itself (wih_twos.cpp:645-647).
-      const T r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
-      bool done = !(r > to_T<T>(J.epsilon));
-      bool cap = false;
-      if (!done) {
-        const uint32_t ctr3 = J.repeat << 3;
-        const Philox4 q0 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 0u);
-        Vec<T> a = pos;
-        if (GREEN) {
-          const Philox4 q1 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 1u);
-          const Philox4 q2 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 2u);
-          const Philox4 q3 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 3u);
-          const T beta = median3(uniform<T>(q2.x, q2.y), uniform<T>(q2.z, q2.w), uniform<T>(q3.x, q3.y));
-          const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
-          a = add_scaled(pos, g, r * beta);
-        }
-        if (EXACT) {
-          u = exact_source(u, s_terms, J.src_begin, J.n_src, pos, r, err);
-          if (PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
-        } else {
-          const T w = r * r / T(6);
-          if (MODE != kModeBoundary) {
-            const T du = w * source_value(s_terms, J.src_begin, J.n_src, a);
-            u = u + du;
-            if (GRAD && steps == 0) g_u0 = du;
-          }
-          if (PAIRED) {
-            const T dp = w * source_value(s_terms, J.adj_begin, J.n_adj, a);
-            pv = pv + dp;
-            if (GRAD && steps == 0) g_p0 = dp;
-          }
-        }
-        const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
-        if (GRAD && steps == 0) {
-          // First ball: the sphere term's radius and direction, and one draw
-          // (blocks 4-5) for the ball source term of the gradient,
-          // R (1 - t^3) f(x + t R w') w' with t ~ U(0,1), w' uniform.
-          const Philox4 q4 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 4u);
-          const Philox4 q5 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 5u);
-          const T t = uniform<T>(q4.x, q4.y);
-          const Vec<T> wp = direction<T>(uniform<T>(q4.z, q4.w), uniform<T>(q5.x, q5.y));
-          const Vec<T> z = add_scaled(pos, wp, t * r);
-          const T wt = r * (T(1) - t * t * t);
-          const T fs = wt * source_value(s_terms, J.src_begin, J.n_src, z);
-          const T fq = wt * source_value(s_terms, J.adj_begin, J.n_adj, z);
-          g_su = {wp.x * fs, wp.y * fs, wp.z * fs};
-          g_sp = {wp.x * fq, wp.y * fq, wp.z * fq};
-          g_r0 = r;
-          g_w0 = dir;
-        }
-        pos = add_scaled(pos, dir, r);
-        ++steps;
-        if (static_cast<int>(steps) >= J.max_steps) {
-          done = true;
-          cap = true;
-        }
-      }
-      if (done) {
-        if (MODE == kModeBoundary) {
-          HitRec h;
-          h.pad = 0;
-          Vec<T> q{T(0), T(0), T(0)}, nrm{T(0), T(0), T(0)};
-          if (cap || !found) {
-            h.cavity = -2;
-          } else if (hit_cav >= 0) {
-            // Point on the sphere along the radial direction; the domain
-            // excludes the sphere, so the outward normal points into it.
-            const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + hit_cav), G);
-            const Vec<T> dv = sub(pos, cc);
-            const T inv = T(1) / sqrt(dot3(dv, dv));
-            const Vec<T> dir{dv.x * inv, dv.y * inv, dv.z * inv};
-            q = add_scaled(cc, dir, R);
-            nrm = {dir.x * T(-1), dir.y * T(-1), dir.z * T(-1)};
-            h.cavity = hit_cav;
+        const T R = to_T<T>(J.cavity_radius);
+        const T dmesh = d;
+        int hit_cav = -1;
+        bool cav_nearer = false;  // gradient mode: the exit is on a cavity
+        for (uint32_t c = 0; c < J.n_cav; ++c) {
+          const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
+          const Vec<T> dv = sub(pos, cc);
+          const T len = sqrt(dot3(dv, dv));
+          const T dc = len - R;
+          if (MODE == kModeBoundary) {
+            // closest_boundary (wih_twos.cpp:612-624): the first strictly nearer cavity.
+            if (dc < d && len > T(0)) {
+              d = dc;
+              hit_cav = static_cast<int>(c);
+            }
           } else {
-            Vec<T> ta, tb, tc;
-            load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
-            q = tri_closest(pos, ta, tb, tc);
-            if (dmesh > T(0)) {
-              const T inv = T(1) / dmesh;
-              const Vec<T> dq = sub(q, pos);
-              nrm = {dq.x * inv, dq.y * inv, dq.z * inv};
-            }
-            h.cavity = -1;
+            d = dc < d ? dc : d;
+            if (GRAD && dc < dmesh) cav_nearer = true;
           }
-          const bool f32 = sizeof(T) == 4;
-          h.point[0] = static_cast<double>(q.x) + (f32 ? G.center[0] : 0.0);
-          h.point[1] = static_cast<double>(q.y) + (f32 ? G.center[1] : 0.0);
-          h.point[2] = static_cast<double>(q.z) + (f32 ? G.center[2] : 0.0);
-          h.normal[0] = static_cast<double>(nrm.x);
-          h.normal[1] = static_cast<double>(nrm.y);
-          h.normal[2] = static_cast<double>(nrm.z);
-          L.hits[wid] = h;
-        } else {
-          if (GRAD) {
-            // Dirichlet data of u at the exit point on the mesh.
-            if (!cap && found && J.n_bnd > 0 && !cav_nearer) {
-              Vec<T> q = pos;
-              if (tri_ok) {
-                Vec<T> ta, tb, tc;
-                load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
-                q = tri_closest(pos, ta, tb, tc);
-              }
-              u = u + source_value(s_terms, J.bnd_begin, J.n_bnd, q);
-            }
-            T *go = static_cast<T *>(L.grad_out) + 6ull * wid;
-            if (g_r0 > T(0)) {
-              const T k = T(3) / g_r0;
-              const T cu = k * (u - g_u0), cp = k * (pv - g_p0);
-              go[0] = g_w0.x * cu + g_su.x;
-              go[1] = g_w0.y * cu + g_su.y;
-              go[2] = g_w0.z * cu + g_su.z;
-              go[3] = g_w0.x * cp + g_sp.x;
-              go[4] = g_w0.y * cp + g_sp.y;
-              go[5] = g_w0.z * cp + g_sp.z;
-            } else {
-              for (int k = 0; k < 6; ++k) go[k] = T(0);
-            }
-          }
-          static_cast<T *>(L.u_out)[wid] = u;
         }
-        if (PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
-        L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
-        phase = kIdle;
-      } else {
+        // The mixed form shrinks the radius by the FP32 distance error bound;
+        // the FP64 form uses the distance itself (wih_twos.cpp:645-647).
+        const T r = sizeof(T) == 4 ? d - static_cast<T>(G.delta) : d;
+        bool done = !(r > to_T<T>(J.epsilon));
+        bool cap = false;
+        if (!done) {
+          const uint32_t ctr3 = J.repeat << 3;
+          const Philox4 q0 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 0u);
+          Vec<T> a = pos;
+          if (GREEN) {
+            const Philox4 q1 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 1u);
+            const Philox4 q2 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 2u);
+            const Philox4 q3 = philox(J.k0, J.k1, steps, walk, J.site_offset + site, ctr3 | 3u);
+            const T beta = median3(uniform<T>(q2.x, q2.y), uniform<T>(q2.z, q2.w), uniform<T>(q3.x, q3.y));
+            const Vec<T> g = direction<T>(uniform<T>(q1.x, q1.y), uniform<T>(q1.z, q1.w));
+            a = add_scaled(pos, g, r * beta);
+          }
+          if (EXACT) {
+            u = exact_source(u, s_terms, J.src_begin, J.n_src, pos, r, err);
+            if (PAIRED) pv = exact_source(pv, s_terms, J.adj_begin, J.n_adj, pos, r, err);
+          } else {
+            const T w = r * r / T(6);
+            if (MODE != kModeBoundary) {
+              const T du = w * source_value(s_terms, J.src_begin, J.n_src, a);
+              u = u + du;
+              if (GRAD && steps == 0) g_u0 = du;
+            }
+            if (PAIRED) {
+              const T dp = w * source_value(s_terms, J.adj_begin, J.n_adj, a);
+              pv = pv + dp;
+              if (GRAD && steps == 0) g_p0 = dp;
+            }
+          }
+          const Vec<T> dir = direction<T>(uniform<T>(q0.x, q0.y), uniform<T>(q0.z, q0.w));
+          if (GRAD && steps == 0) {
+            // First ball: the sphere term's radius and direction, and one draw
+            // (blocks 4-5) for the ball source term of the gradient,
+            // R (1 - t^3) f(x + t R w') w' with t ~ U(0,1), w' uniform.
+            const Philox4 q4 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 4u);
+            const Philox4 q5 = philox(J.k0, J.k1, 0u, walk, J.site_offset + site, ctr3 | 5u);
+            const T t = uniform<T>(q4.x, q4.y);
+            const Vec<T> wp = direction<T>(uniform<T>(q4.z, q4.w), uniform<T>(q5.x, q5.y));
+            const Vec<T> z = add_scaled(pos, wp, t * r);
+            const T wt = r * (T(1) - t * t * t);
+            const T fs = wt * source_value(s_terms, J.src_begin, J.n_src, z);
+            const T fq = wt * source_value(s_terms, J.adj_begin, J.n_adj, z);
+            g_su = {wp.x * fs, wp.y * fs, wp.z * fs};
+            g_sp = {wp.x * fq, wp.y * fq, wp.z * fq};
+            g_r0 = r;
+            g_w0 = dir;
+          }
+          pos = add_scaled(pos, dir, r);
+          ++steps;
+          if (static_cast<int>(steps) >= J.max_steps) {
+            done = true;
+            cap = true;
+          }
+        }
+        if (done) {
+          if (MODE == kModeBoundary) {
+            HitRec h;
+            h.pad = 0;
+            Vec<T> q{T(0), T(0), T(0)}, nrm{T(0), T(0), T(0)};
+            if (cap || !found) {
+              h.cavity = -2;
+            } else if (hit_cav >= 0) {
+              // Point on the sphere along the radial direction; the domain
+              // excludes the sphere, so the outward normal points into it.
+              const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + hit_cav), G);
+              const Vec<T> dv = sub(pos, cc);
+              const T inv = T(1) / sqrt(dot3(dv, dv));
+              const Vec<T> dir{dv.x * inv, dv.y * inv, dv.z * inv};
+              q = add_scaled(cc, dir, R);
+              nrm = {dir.x * T(-1), dir.y * T(-1), dir.z * T(-1)};
+              h.cavity = hit_cav;
+            } else {
+              Vec<T> ta, tb, tc;
+              load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+              q = tri_closest(pos, ta, tb, tc);
+              if (dmesh > T(0)) {
+                const T inv = T(1) / dmesh;
+                const Vec<T> dq = sub(q, pos);
+                nrm = {dq.x * inv, dq.y * inv, dq.z * inv};
+              }
+              h.cavity = -1;
+            }
+            const bool f32 = sizeof(T) == 4;
+            h.point[0] = static_cast<double>(q.x) + (f32 ? G.center[0] : 0.0);
+            h.point[1] = static_cast<double>(q.y) + (f32 ? G.center[1] : 0.0);
+            h.point[2] = static_cast<double>(q.z) + (f32 ? G.center[2] : 0.0);
+            h.normal[0] = static_cast<double>(nrm.x);
+            h.normal[1] = static_cast<double>(nrm.y);
+            h.normal[2] = static_cast<double>(nrm.z);
+            L.hits[wid] = h;
+          } else {
+            if (GRAD) {
+              // Dirichlet data of u at the exit point on the mesh.
+              if (!cap && found && J.n_bnd > 0 && !cav_nearer) {
+                Vec<T> q = pos;
+                if (tri_ok) {
+                  Vec<T> ta, tb, tc;
+                  load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+                  q = tri_closest(pos, ta, tb, tc);
+                }
+                u = u + source_value(s_terms, J.bnd_begin, J.n_bnd, q);
+              }
+              T *go = static_cast<T *>(L.grad_out) + 6ull * wid;
+              if (g_r0 > T(0)) {
+                const T k = T(3) / g_r0;
+                const T cu = k * (u - g_u0), cp = k * (pv - g_p0);
+                go[0] = g_w0.x * cu + g_su.x;
+                go[1] = g_w0.y * cu + g_su.y;
+                go[2] = g_w0.z * cu + g_su.z;
+                go[3] = g_w0.x * cp + g_sp.x;
+                go[4] = g_w0.y * cp + g_sp.y;
+                go[5] = g_w0.z * cp + g_sp.z;
+              } else {
+                for (int k = 0; k < 6; ++k) go[k] = T(0);
+              }
+            }
+            static_cast<T *>(L.u_out)[wid] = u;
+          }
+          if (PAIRED) static_cast<T *>(L.p_out)[wid] = pv;
+          L.steps_out[wid] = steps | (cap ? 0x80000000u : 0u);
+          phase = kIdle;
+          break;
+        }
         best2 = static_cast<T>(J.query_radius2);
         found = false;
-        bool from_grid = false;
+        node = 0;
         if constexpr (sizeof(T) == 4) {
-          // Distance-bound grid: D(v) - |x - v| at the nearest vertex v bounds
-          // the mesh distance from below; a bound of at least grid_tau
-          // spacings is the next ball's radius and no query is needed.
-          float bound;
-          // A grid step never ends a walk: the bound must clear the
-          // termination shell with room to spare.
-          if (L.grid_tau > 0.f && G.grid && grid_bound(G, pos, bound) && bound >= L.grid_tau * G.grid_h &&
+          // Distance-bound grid: D(v) - |x - v| over the corners v of x's cell
+          // bounds the mesh distance from below; a bound of at least grid_tau
+          // spacings is the next ball's radius and no query is needed.  A grid
+          // step never ends a walk: the bound must clear the termination
+          // shell with room to spare.
+          float bound, upper = CUDART_INF_F;
+          uint32_t entry_at = 0xffffffffu;
+          const bool in_grid = (L.grid_tau > 0.f || L.entry) && G.grid && grid_bounds(G, pos, bound, upper, entry_at);
+          if (in_grid && L.grid_tau > 0.f && bound >= L.grid_tau * G.grid_h &&
               bound > 2.f * (static_cast<float>(J.epsilon) + G.delta) && bound * bound < best2) {
             best2 = bound * bound;
             found = true;
-            from_grid = true;
             ++c_grid;
+            if constexpr (TRACE) {
+              const unsigned long long slot = atomicAdd(L.trace_count, 1ull);
+              if (slot < L.trace_cap) L.trace[slot] = make_float4(pos.x, pos.y, pos.z, bound);
+            }
+            // The next step at once while the chain allows, else with the
+            // warp's next batch.
+            if (link < L.chain) continue;
+            break;
           }
-        }
-        if (from_grid) {
-          phase = kStep;
+          if (!(in_grid && L.entry)) entry_at = 0xffffffffu;
+          if (L.warm && tri_ok) {
+            Vec<T> ta, tb, tc;
+            load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
+            ++c_tris;
+            const T w2 = tri_dist2(pos, ta, tb, tc);
+            if (w2 < best2) {
+              best2 = w2;
+              found = true;
+            }
+          }
+          // Entry node: with an initial bound b below one entry cell, every
+          // triangle outside the cell's entry subtree is farther than b (the
+          // table keeps every triangle within a cell size plus 4 delta), so
+          // the traversal starts there.  The grid's upper bound plus 6 delta
+          // (its 3 delta and the FP32 query's delta, with room) may serve as
+          // b before any triangle is found.
+          if (entry_at != 0xffffffffu) {
+            const float ubs = upper + 6.f * G.delta;
+            if (fminf(sqrtf(best2), ubs) < G.entry_radius) {
+              node = __ldg(G.entry + entry_at);
+              if (ubs * ubs < best2) best2 = ubs * ubs;
+            }
+          }
         } else {
           if (L.warm && tri_ok) {
             Vec<T> ta, tb, tc;
@@ -923,14 +973,14 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
               found = true;
             }
           }
-          node = 0;
-          sp = 0;
-          have = true;
-          tri_cur = tri_end = 0;
-          iter = 0;
-          phase = kTraverse;
         }
-      }
+        sp = 0;
+        have = true;
+        tri_cur = tri_end = 0;
+        iter = 0;
+        phase = kTraverse;
+        break;
+      }  // chain
     }
 
     if (__ballot_sync(full, phase != kIdle) == 0u) {
@@ -1124,6 +1174,21 @@ static uint32_t wos_dyn_smem(int precision, const WosLaunch &L, int block) {
   const uint32_t stack = static_cast<uint32_t>(kStack * block * sizeof(uint2));
   return stack + (precision == TWOS_PREC_MIXED ? smem_plan<float>(L.n_jobs, L.n_geos, L.n_terms).bytes
                                                : smem_plan<double>(L.n_jobs, L.n_geos, L.n_terms).bytes);
+}
+
+// The mixed compliance walk kernel (centre source, 128 threads) with a
+// record of every grid step's position and bound (L.trace): used by tests to
+// check each bound against the FP64 distance.
+cudaError_t launch_wos_traced(const WosLaunch &L, int grid, cudaStream_t s) {
+  if (L.n_jobs == 0 || L.n_geos == 0 || !L.trace || !L.trace_count) return cudaErrorInvalidValue;
+  const uint32_t dyn = wos_dyn_smem(TWOS_PREC_MIXED, L, kWosBlock);
+  const void *fn = reinterpret_cast<const void *>(&wos_kernel<float, TWOS_MODE_COMPLIANCE, TWOS_SOURCE_CENTER,
+                                                              kWosBlock, true>);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
+  if (e != cudaSuccess) return e;
+  WosLaunch copy = L;
+  void *args[] = {&copy};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(kWosBlock), args, dyn, s);
 }
 
 cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int grid, int block,
@@ -1409,6 +1474,32 @@ cudaError_t launch_finalize(int precision, int mode, const FinalizeLaunch &F, cu
                                       : reinterpret_cast<const void *>(&finalize_kernel<double, 2>);
   }
   return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+}
+
+// ================================================================ L2 read probe
+// Streams an L2-resident buffer with the walk kernel's load form (32-byte
+// read-only vector loads, one per lane, consecutive lanes on consecutive
+// sectors), `passes` times over.  The measured rate is the L2 read roof for a
+// working set that fits the L2 (the distance grid and the BVH of one mesh).
+__global__ void __launch_bounds__(256) l2_read_kernel(const float4 *__restrict__ buf, uint64_t n32, int passes,
+                                                      uint32_t *sink) {
+  float acc = 0.f;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (int p = 0; p < passes; ++p) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n32; i += stride) {
+      float4 a, b;
+      ldg32(buf + 2 * i, a, b);
+      acc += (a.x + a.y + a.z + a.w) + (b.x + b.y + b.z + b.w);
+    }
+  }
+  // The buffer holds zeros, so this store never happens; the compiler cannot
+  // know that and keeps every load.
+  if (acc != 0.f) sink[0] = __float_as_uint(acc);
+}
+
+cudaError_t launch_l2_read(const void *buf, uint64_t bytes, int passes, uint32_t *sink, int blocks, cudaStream_t s) {
+  l2_read_kernel<<<blocks, 256, 0, s>>>(static_cast<const float4 *>(buf), bytes / 32, passes, sink);
+  return cudaGetLastError();
 }
 
 // ================================================================ batched closest point

@@ -60,6 +60,8 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 // 0 builds none).
 // Values are FP32 distances less 2 delta (the mixed form's own error bound,
 // covering the FP32 query and the vertex placement), in steps of h/128.
+void build_entry_table(twos_mesh *m);
+
 void build_distance_grid(twos_mesh *m, size_t n_tris) {
   GeoDesc &g = m->geo_host;
   g.grid = nullptr;
@@ -99,8 +101,51 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
   check(launch_grid_build(m->geo.as<GeoDesc>(), count, 2.0 * m->delta, m->grid.as<uint16_t>(), err, nullptr),
         "grid build");
   check(cudaDeviceSynchronize(), "grid build");
+  uint32_t build_err = 0;
+  check(cudaMemcpy(&build_err, err, sizeof(uint32_t), cudaMemcpyDeviceToHost), "download");
+  if (build_err) {
+    // A vertex whose query overran its bounds holds 0: still a lower bound,
+    // but no upper bound, so the session runs without the grid.
+    m->grid.release();
+    return;
+  }
   g.grid = m->grid.as<uint16_t>();
   m->resident_bytes += count * sizeof(uint16_t);
+  build_entry_table(m);
+}
+
+// The entry-node table over the distance grid: cells of 2^s grid spacings
+// (4 spacings by default; TWOS_ENTRY_CELLS sets 1, 2, 4, 8 or 16, 0 builds
+// none), each with the node whose subtree holds every triangle within one
+// cell size (plus 4 delta) of the cell.  A query whose initial bound is below
+// one cell size starts there instead of at the root.
+void build_entry_table(twos_mesh *m) {
+  GeoDesc &g = m->geo_host;
+  g.entry = nullptr;
+  if (!g.grid) return;
+  uint32_t shift = 2;
+  if (const char *e = std::getenv("TWOS_ENTRY_CELLS")) {
+    const long c = std::strtol(e, nullptr, 10);
+    if (c <= 0) return;
+    shift = 0;
+    while (shift < 4 && (1L << (shift + 1)) <= c) ++shift;
+  }
+  const uint32_t c = 1u << shift;
+  const double h = static_cast<double>(g.grid_h);
+  double origin[3];
+  for (int a = 0; a < 3; ++a) {
+    origin[a] = static_cast<double>(g.grid_lo[a]) + m->center[a];
+    g.entry_n[a] = (g.grid_n[a] - 1 + c - 1) / c;
+  }
+  const double cell = c * h;
+  const std::vector<int32_t> table =
+      twos::build_entry_table(m->bvh, origin, cell, g.entry_n, cell + 4.0 * m->delta, 0.01 * h);
+  m->entry.reserve(table.size() * sizeof(int32_t));
+  check(cudaMemcpy(m->entry.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+  g.entry = m->entry.as<int32_t>();
+  g.entry_shift = shift;
+  g.entry_radius = static_cast<float>(cell);
+  m->resident_bytes += table.size() * sizeof(int32_t);
 }
 
 int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, twos_mesh **out) {
@@ -186,6 +231,8 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
+    if (const char *e = std::getenv("TWOS_CHAIN")) m->chain = std::min(64, std::max(1, std::atoi(e)));
+    if (const char *e = std::getenv("TWOS_ENTRY")) m->entry_start = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
       const int b = std::atoi(e);
       if (b == 128 || b == 256 || b == 512) m->block = b;
@@ -311,8 +358,15 @@ struct JobSpec {
 // Runs one persistent launch over a group of jobs (walk kernel + finalize)
 // on `owner`'s stream; sites and rows are device arrays indexed by
 // JobSpec::site_begin.  All jobs share mode, precision and the Green flag.
+// A device record of every grid step of a launch (tests).
+struct TraceOut {
+  float4 *rec;
+  unsigned long long *count;
+  uint32_t cap;
+};
+
 void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const double *d_sites, twos_site_result *d_out,
-                RunOut &ro, twos_gradient_result *d_grad = nullptr) {
+                RunOut &ro, twos_gradient_result *d_grad = nullptr, const TraceOut *trace = nullptr) {
   const twos_request *r0 = specs.front().r;
   const bool mixed = r0->precision == TWOS_PREC_MIXED;
   // d_grad selects the gradient form (paired walks with first-ball gradient
@@ -387,6 +441,8 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.warm = m->warm;
   L.grid_tau = m->grid_tau;
   L.units = m->units;
+  L.chain = m->chain;
+  L.entry = m->entry_start;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -406,7 +462,14 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   F.out = d_out;
   check(cudaEventRecord(m->ev0, m->stream), "event");
   check(launch_site_prepass(r0->precision, L, m->stream), "site pre-pass");
-  check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
+  if (trace) {
+    L.trace = trace->rec;
+    L.trace_count = trace->count;
+    L.trace_cap = trace->cap;
+    check(launch_wos_traced(L, per_sm * m->num_sms, m->stream), "traced WoS launch");
+  } else {
+    check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
+  }
   check(cudaEventRecord(m->evw, m->stream), "event");
   if (d_grad) {
     // One job per launch in the gradient form: its rows start at the job's site_begin.
@@ -535,7 +598,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
-                    &m->closest, &m->topk})
+                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -557,7 +620,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
-      t->units < 1 || t->units > 64)
+      t->units < 1 || t->units > 64 || t->chain < 1 || t->chain > 64 || (t->entry != 0 && t->entry != 1))
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -565,6 +628,8 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->blocks_per_sm = t->blocks_per_sm;
   m->grid_tau = t->grid_threshold;
   m->units = t->units;
+  m->chain = t->chain;
+  m->entry_start = t->entry;
   return TWOS_OK;
 }
 
@@ -576,6 +641,8 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->blocks_per_sm = m->blocks_per_sm;
   t->grid_threshold = m->grid_tau;
   t->units = m->units;
+  t->chain = m->chain;
+  t->entry = m->entry_start;
   return TWOS_OK;
 }
 
@@ -737,12 +804,34 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
               "upload sites");
       at += n_sites[j];
     }
+    // Queue order: the walks of consecutive jobs overlap in flight at each
+    // job boundary, so two geometries whose data fill much of the L2 should
+    // not follow each other.  Jobs go largest, smallest, second largest,
+    // second smallest, ... by the bytes their form reads (BVH and triangles,
+    // plus the distance grid and entry table in the mixed form).  Results do
+    // not depend on the order: every walk's samples are keyed by its own job.
+    const bool mixed = requests[0].precision == TWOS_PREC_MIXED;
+    auto footprint = [&](uint32_t j) {
+      const twos_mesh *mj = meshes[j];
+      return mixed ? mj->nodes_f.bytes + mj->tris_f.bytes + mj->grid.bytes + mj->entry.bytes
+                   : mj->nodes_d.bytes + mj->tris_d.bytes;
+    };
+    std::vector<uint32_t> by_size(n_jobs);
+    for (uint32_t j = 0; j < n_jobs; ++j) by_size[j] = j;
+    std::stable_sort(by_size.begin(), by_size.end(),
+                     [&](uint32_t a, uint32_t b) { return footprint(a) > footprint(b); });
+    std::vector<uint32_t> order;
+    for (uint32_t lo = 0, hi = n_jobs; lo < hi;) {
+      order.push_back(by_size[lo++]);
+      if (lo < hi) order.push_back(by_size[--hi]);
+    }
     // Group consecutive jobs into launches of at most max_launch_walks walks
     // (a single larger job runs alone).
     begin_totals(owner);
     std::vector<JobSpec> group;
     uint64_t group_walks = 0;
-    for (uint32_t j = 0; j <= n_jobs; ++j) {
+    for (uint32_t q = 0; q <= n_jobs; ++q) {
+      const uint32_t j = q < n_jobs ? order[q] : n_jobs;
       const uint64_t w = j < n_jobs ? static_cast<uint64_t>(n_sites[j]) * requests[j].walks : 0;
       if (!group.empty() && (j == n_jobs || group_walks + w > owner->max_launch_walks)) {
         run_launch(owner, group, owner->sites.as<double>(), owner->out.as<twos_site_result>(), ro);
@@ -887,12 +976,19 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.warm = m->warm;
     Ls.grid_tau = m->grid_tau;
     Ls.units = m->units;
+    Ls.chain = m->chain;
+    Ls.entry = m->entry_start;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
     Ls.site_best2 = m->first.ptr;
     Ls.total_sites = n;
     WosLaunch Lv = Ls;
+    // The validation stage decides acceptance; it runs without the mixed
+    // form's distance grid, so the mixed and FP64 forms validate a candidate
+    // with the same samples (the grid changes the walks' radii) and their
+    // accept decisions for the same candidate agree.  The scout keeps it.
+    Lv.grid_tau = 0.f;
     Lv.site_best2 = first_v.ptr;
     Lv.total_sites = k;
     Lv.jobs = jobs_v.as<JobDesc>();
@@ -1456,6 +1552,8 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.warm = m->warm;
         L.grid_tau = m->grid_tau;
         L.units = m->units;
+        L.chain = m->chain;
+        L.entry = m->entry_start;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;
@@ -1603,6 +1701,102 @@ int twos_walk_samples(twos_mesh *m, const twos_request *r, const double *sites, 
   if (ro.error_flags & TWOS_DEVERR_QUERY) return fail(TWOS_ERR_RUNTIME, "closest-point query failed");
   if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
   return TWOS_OK;
+}
+
+int twos_trace_grid_steps(twos_mesh *m, const twos_request *r, const double *sites, uint32_t n_sites,
+                          uint64_t capacity, double *points, double *bounds, uint64_t *count) {
+  if (!m || !count || (capacity && (!points || !bounds))) return fail(TWOS_ERR_USAGE, "null argument");
+  if (int rc = validate_request(r, n_sites, 0)) return rc;
+  if (r->precision != TWOS_PREC_MIXED || r->mode != TWOS_MODE_COMPLIANCE || r->green != TWOS_SOURCE_CENTER)
+    return fail(TWOS_ERR_USAGE, "the grid-step trace runs the mixed compliance form with the centre source");
+  if (capacity > 0xffffffffull) return fail(TWOS_ERR_USAGE, "trace capacity too large");
+  if (n_sites == 0) {
+    *count = 0;
+    return TWOS_OK;
+  }
+  if (!sites) return fail(TWOS_ERR_USAGE, "null buffer");
+  const size_t walks = static_cast<size_t>(n_sites) * static_cast<size_t>(r->walks);
+  if (walks > m->max_launch_walks) return fail(TWOS_ERR_USAGE, "too many walks for one traced launch");
+  RunOut ro;
+  DevBuf rec, cnt;
+  try {
+    check(cudaSetDevice(m->device), "cudaSetDevice");
+    rec.reserve(std::max<uint64_t>(capacity, 1) * sizeof(float4));
+    cnt.reserve(sizeof(unsigned long long));
+    check(cudaMemsetAsync(cnt.ptr, 0, sizeof(unsigned long long), m->stream), "memset");
+    m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
+    m->out.reserve(static_cast<size_t>(n_sites) * sizeof(twos_site_result));
+    check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
+                          cudaMemcpyHostToDevice, m->stream),
+          "upload sites");
+    begin_totals(m);
+    const TraceOut t{rec.as<float4>(), cnt.as<unsigned long long>(), static_cast<uint32_t>(capacity)};
+    JobSpec js{m, r, n_sites, 0, r->site_offset, nullptr, 0};
+    run_launch(m, {js}, m->sites.as<double>(), m->out.as<twos_site_result>(), ro, nullptr, &t);
+    end_totals(m, ro);
+    unsigned long long total = 0;
+    check(cudaMemcpy(&total, cnt.ptr, sizeof(total), cudaMemcpyDeviceToHost), "download count");
+    const uint64_t kept = std::min<uint64_t>(total, capacity);
+    std::vector<float4> host(kept);
+    if (kept) check(cudaMemcpy(host.data(), rec.ptr, kept * sizeof(float4), cudaMemcpyDeviceToHost), "download trace");
+    for (uint64_t i = 0; i < kept; ++i) {
+      // FP32 frame -> original coordinates (exact in FP64).
+      points[3 * i] = static_cast<double>(host[i].x) + m->center[0];
+      points[3 * i + 1] = static_cast<double>(host[i].y) + m->center[1];
+      points[3 * i + 2] = static_cast<double>(host[i].z) + m->center[2];
+      bounds[i] = static_cast<double>(host[i].w);
+    }
+    *count = total;
+  } catch (const std::exception &e) {
+    rec.release();
+    cnt.release();
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  rec.release();
+  cnt.release();
+  if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  return TWOS_OK;
+}
+
+int twos_l2_read_gbs(int device, uint64_t bytes, uint32_t passes, double *gbs) {
+  if (!gbs || bytes < 1024 || bytes % 32 || passes == 0) return fail(TWOS_ERR_USAGE, "invalid L2 probe arguments");
+  void *buf = nullptr;
+  uint32_t *sink = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = TWOS_OK;
+  try {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device attribute");
+    check(cudaMalloc(&buf, bytes), "cudaMalloc");
+    check(cudaMalloc(&sink, sizeof(uint32_t)), "cudaMalloc");
+    check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    check(cudaMemsetAsync(buf, 0, bytes, st), "memset");
+    const int blocks = 8 * sms;  // 2048 threads per SM
+    check(launch_l2_read(buf, bytes, 2, sink, blocks, st), "L2 probe");  // warm the L2
+    double best = 0.0;
+    for (int rep = 0; rep < 5; ++rep) {
+      check(cudaEventRecord(e0, st), "event");
+      check(launch_l2_read(buf, bytes, static_cast<int>(passes), sink, blocks, st), "L2 probe");
+      check(cudaEventRecord(e1, st), "event");
+      check(cudaEventSynchronize(e1), "L2 probe");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+      best = std::max(best, static_cast<double>(bytes) * passes / (ms * 1e-3) / 1e9);
+    }
+    *gbs = best;
+  } catch (const std::exception &e) {
+    rc = fail(TWOS_ERR_RUNTIME, e.what());
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  if (buf) cudaFree(buf);
+  if (sink) cudaFree(sink);
+  return rc;
 }
 
 int twos_finalize_samples(twos_mesh *m, int precision, int mode, const double *u, const double *p,

@@ -81,6 +81,16 @@ void pack_bvh_f32(const HostBvh &bvh, const std::vector<double> &vertices, const
 void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
                   std::vector<NodeD> &nodes, std::vector<TriD> &tris);
 
+// Entry-node table of the mixed form's closest-point query: for each cell of
+// a uniform grid (cell size `cell`, `dims` cells from `origin`, original
+// coordinates), the deepest BVH node whose subtree holds every triangle
+// within `radius` of the cell grown by `pad` (0, the root, when none is).
+// A query at a point of the cell whose initial bound is below `radius`
+// (less the FP32 error) may start its traversal there: every triangle
+// outside that subtree is farther than the bound.
+std::vector<int32_t> build_entry_table(const HostBvh &bvh, const double origin[3], double cell, const uint32_t dims[3],
+                                       double radius, double pad);
+
 // Host ray-parity membership over the host BVH (EmbreeMesh::inside).
 int inside_parity(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
                   const double p[3], bool &inside, std::string &err);
@@ -108,6 +118,15 @@ struct GeoDesc {
   float grid_lo[3];
   float grid_h, grid_inv_h, grid_q;
   uint32_t grid_n[3];
+  // Entry-node table of the mixed form (null: none): entry[(I * e1 + J) * e2
+  // + K] is the BVH node a query may start from at a point of grid cell
+  // (i, j, k), (I, J, K) = (i, j, k) >> entry_shift, when its initial bound
+  // is below entry_radius (every triangle outside that node's subtree is
+  // farther).
+  const int32_t *entry;
+  uint32_t entry_shift;  // an entry cell spans 2^entry_shift grid cells per axis
+  uint32_t entry_n[3];
+  float entry_radius;
 };
 
 // One job = one geometry x a contiguous range of sites with one request.
@@ -188,6 +207,15 @@ struct WosLaunch {
   // Traversal units (node visits / triangle tests) a lane runs back to back
   // per iteration of the warp loop (>= 1).
   int units;
+  // Mixed form: grid steps a lane may take back to back in one step phase
+  // (>= 1), and whether a query may start at the entry-node table's node.
+  int chain;
+  int entry;
+  // Optional record of every grid step (tests): position in the FP32 frame
+  // and the bound used, at most trace_cap records; trace_count counts all.
+  float4 *trace;
+  unsigned long long *trace_count;
+  uint32_t trace_cap;
 };
 
 // Walk-to-boundary mode of the walk kernel (walk_to_boundary,
@@ -288,6 +316,7 @@ struct DesignStep {
   uint32_t chosen;
   uint32_t accepted;
   double scout_score, score, score_se, lower;
+  uint32_t slot, n_cavities;
 };
 static_assert(sizeof(DesignStep) == sizeof(twos_design_step), "design step layout");
 
@@ -318,6 +347,7 @@ cudaError_t launch_design_select(const DesignLaunch &D, cudaStream_t s);
 cudaError_t launch_design_mask(const DesignLaunch &D, cudaStream_t s);
 
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
+cudaError_t launch_wos_traced(const WosLaunch &L, int grid, cudaStream_t s);
 cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int grid, int block,
                        cudaStream_t s);
 int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L);
@@ -345,6 +375,8 @@ cudaError_t launch_validate(const ValidateLaunch &V, cudaStream_t s);
 
 // Exact ball integrals of bump sources: cases[4i..4i+3] = (d, r, R, A).
 cudaError_t launch_ball_green(const double *cases, uint32_t n, double *out, uint32_t *error, cudaStream_t s);
+// L2 read probe: `passes` sweeps of 32-byte loads over `bytes` of buf.
+cudaError_t launch_l2_read(const void *buf, uint64_t bytes, int passes, uint32_t *sink, int blocks, cudaStream_t s);
 cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *pts, uint64_t n,
                            double query_radius2, double *dist, double *closest, uint32_t *error, cudaStream_t s);
 // Fills a geometry's distance-bound grid (n = vertices of the grid described

@@ -70,7 +70,8 @@ struct twos_mesh {
   cudaStream_t own_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
   twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
-  twos::DevBuf grid;  // distance-bound grid (uint16 per vertex), may be empty
+  twos::DevBuf grid;   // distance-bound grid (uint16 per vertex), may be empty
+  twos::DevBuf entry;  // entry-node table of the mixed form's queries, may be empty
   twos::DevBuf geo;  // one GeoDesc
   twos::GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
@@ -86,4 +87,6 @@ struct twos_mesh {
   int warm = 1;            // 1: seed each step's query with the previous nearest triangle
   float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
+  int chain = 1;           // grid steps a lane may take back to back in one step phase
+  int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
 };

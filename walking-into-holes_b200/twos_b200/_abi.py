@@ -29,6 +29,7 @@ EXPORTED = [
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
     "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc", "twos_finalize_samples",
+    "twos_l2_read_gbs", "twos_trace_grid_steps",
 ]
 RQMC_MC, RQMC_ARRAY, RQMC_NEIGHBOUR = 0, 1, 2
 
@@ -86,7 +87,8 @@ class MeshInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("refill", ctypes.c_int32), ("step_threshold", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("grid_threshold", ctypes.c_float), ("units", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("grid_threshold", ctypes.c_float), ("units", ctypes.c_int32),
+                ("chain", ctypes.c_int32), ("entry", ctypes.c_int32)]
 
 
 class DesignParams(ctypes.Structure):
@@ -102,7 +104,7 @@ class DesignStep(ctypes.Structure):
     _fields_ = [
         ("chosen", ctypes.c_uint32), ("accepted", ctypes.c_uint32),
         ("scout_score", ctypes.c_double), ("score", ctypes.c_double), ("score_se", ctypes.c_double),
-        ("lower", ctypes.c_double),
+        ("lower", ctypes.c_double), ("slot", ctypes.c_uint32), ("n_cavities", ctypes.c_uint32),
     ]
 
 
@@ -132,7 +134,7 @@ DIFF_STATS_DTYPE = [("outer_steps", "u8"), ("nested_steps", "u8"), ("cavity_term
                     ("near_seam", "u8"), ("segment_unsafe", "u8"), ("unsafe_offset", "u8"), ("limits", "u8")]
 
 DESIGN_DTYPE = [("chosen", "u4"), ("accepted", "u4"), ("scout_score", "f8"), ("score", "f8"),
-                ("score_se", "f8"), ("lower", "f8")]
+                ("score_se", "f8"), ("lower", "f8"), ("slot", "u4"), ("n_cavities", "u4")]
 
 assert ctypes.sizeof(SourceTerm) == 80
 assert ctypes.sizeof(SiteResult) == 56
@@ -180,6 +182,8 @@ def load(path: Path | str | None = None):
     L.twos_walk_samples.argtypes = [vp, ctypes.POINTER(Request), vp, u32, vp, u32, vp, vp, vp]
     L.twos_inside.argtypes = [vp, vp, u64, vp]
     L.twos_finalize_samples.argtypes = [vp, i32, i32, vp, vp, vp, u32, u32, vp]
+    L.twos_l2_read_gbs.argtypes = [i32, u64, u32, ctypes.POINTER(ctypes.c_double)]
+    L.twos_trace_grid_steps.argtypes = [vp, ctypes.POINTER(Request), vp, u32, u64, vp, vp, ctypes.POINTER(u64)]
     L.twos_ball_green_integral.argtypes = [vp, u32, vp, i32]
     L.twos_rqmc.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(RqmcParams), vp, u32, vp, vp, vp,
                             ctypes.POINTER(Summary)]

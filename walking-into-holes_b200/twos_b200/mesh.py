@@ -130,13 +130,16 @@ class Mesh:
         handle = getattr(stream, "cuda_stream", stream)
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
-    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8):
+    def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8,
+                   chain=1, entry=1):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
         closest-point query, 0 to query every step; units is the number of
-        traversal units a lane runs per warp-loop iteration."""
+        traversal units a lane runs per warp-loop iteration; chain the grid
+        steps a lane may take back to back; entry 1 starts qualifying
+        mixed-form queries at the entry-node table's node."""
         t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold),
-                        int(units))
+                        int(units), int(chain), int(entry))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -145,7 +148,8 @@ class Mesh:
         return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
                 "blocks_per_sm": t.blocks_per_sm,
                 # The ABI keeps a float; report the shortest decimal that rounds to it (0.1, not 0.10000000149).
-                "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units}
+                "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units, "chain": t.chain,
+                "entry": t.entry}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
@@ -242,6 +246,19 @@ class Mesh:
         check(_abi.load().twos_walk_samples(self._h, ctypes.byref(req), _ptr(s), n, _ptr(cav), len(cav), _ptr(u),
                                             _ptr(p), _ptr(st)))
         return {"u": u, "p": p, "steps": st & 0x7FFFFFFF, "caps": (st >> 31).astype(bool)}
+
+    def trace_grid_steps(self, sites, config: Config, capacity: int = 1 << 22):
+        """Every grid step of a mixed compliance estimate (twos_trace_grid_steps):
+        (points [k][3] in original coordinates, bounds [k], total grid steps)."""
+        s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        pts = np.zeros((capacity, 3))
+        bnd = np.zeros(capacity)
+        cnt = ctypes.c_uint64()
+        req = config.to_request()
+        check(_abi.load().twos_trace_grid_steps(self._h, ctypes.byref(req), _ptr(s), len(s), int(capacity), _ptr(pts),
+                                                _ptr(bnd), ctypes.byref(cnt)))
+        k = min(int(cnt.value), capacity)
+        return pts[:k], bnd[:k], int(cnt.value)
 
     def finalize_samples(self, u, p=None, steps=None, mode: str = "compliance", precision: str = "fp64"):
         """The device's per-site reduction (twos_finalize_samples) of given
@@ -384,6 +401,14 @@ def ball_green_integral(cases, device: int = 0):
     out = np.zeros(len(c))
     check(_abi.load().twos_ball_green_integral(_ptr(c), len(c), _ptr(out), int(device)))
     return out
+
+
+def l2_read_gbs(device: int = 0, mib: int = 64, passes: int = 20) -> float:
+    """Measured L2 read bandwidth of the device in GB/s (twos_l2_read_gbs):
+    32-byte vector loads over an L2-resident buffer of `mib` MiB."""
+    g = ctypes.c_double()
+    check(_abi.load().twos_l2_read_gbs(int(device), int(mib) << 20, int(passes), ctypes.byref(g)))
+    return float(g.value)
 
 
 def estimate_batch(meshes, sites_list, configs, cavities_list=None):
