@@ -255,9 +255,6 @@ typedef struct twos_tuning {
   int32_t units;         /* traversal units (node visits or triangle tests) a
                             lane runs back to back before its warp returns to
                             the refill and step ballots (1..64).  Default 8. */
-  int32_t chain;         /* mixed form: grid steps a lane may take back to back
-                            in one step phase before it rejoins its warp
-                            (1..64).  Default 1. */
   int32_t entry;         /* mixed form: 1 lets a closest-point query whose
                             initial bound is below one entry cell start at
                             the entry-node table's node instead of the root

@@ -17,7 +17,8 @@ C ABI twos_finalize_samples) on identical host-generated samples.
 Tolerances: the device sums in a fixed warp-shuffle order, the oracle in
 numpy's pairwise order, both in FP64.  Estimates agree to 1e-14 of the
 scale sum|a| sum|b| / (n (n - 1)) (the sums' rounding, no cancellation beyond
-that), SEs to 1e-10 relative (the leave-one-out values differ from their mean
+that), means to 1e-13 relative (n terms summed in another order), SEs to
+1e-10 relative (the leave-one-out values differ from their mean
 by ~1/n of their size, which amplifies the rounding of the sums).  Mixed
 precision rounds the samples to float first; the oracle gets the same
 rounded samples.
@@ -59,8 +60,8 @@ def test_compliance_reduction_matches_crossfit_square(mesh, oracle_mod, precisio
         est, se = oracle_mod.crossfit_square(x)
         assert np.all(np.abs(rows["score"] - est) <= 1e-14 * _scale(x, x)), (n_sites, walks)
         np.testing.assert_allclose(rows["score_se"], se, rtol=1e-10, atol=0)
-        np.testing.assert_allclose(rows["u"], x.mean(1), rtol=1e-14, atol=0)
-        np.testing.assert_allclose(rows["same_index"], (x * x).mean(1), rtol=1e-14, atol=0)
+        np.testing.assert_allclose(rows["u"], x.mean(1), rtol=1e-13, atol=0)
+        np.testing.assert_allclose(rows["same_index"], (x * x).mean(1), rtol=1e-13, atol=0)
         np.testing.assert_array_equal(rows["steps"], steps.sum(1, dtype=np.uint64))
         assert np.all(rows["caps"] == 0)
 
@@ -84,9 +85,9 @@ def test_paired_reduction_matches_crossfit_product_on_the_seeded_experiment(mesh
         ref = -oracle_mod.crossfit_product(a, b)
         assert np.all(np.abs(rows["score"] - ref) <= 1e-14 * _scale(a, b)), correlation
         np.testing.assert_allclose(rows["score_se"], oracle_mod.cross_jackknife_se(a, b), rtol=1e-10, atol=0)
-        np.testing.assert_allclose(rows["same_index"], np.mean(a * b, axis=1), rtol=1e-14, atol=0)
-        np.testing.assert_allclose(rows["u"], a.mean(1), rtol=1e-14, atol=0)
-        np.testing.assert_allclose(rows["p"], b.mean(1), rtol=1e-14, atol=0)
+        np.testing.assert_allclose(rows["same_index"], np.mean(a * b, axis=1), rtol=1e-13, atol=0)
+        np.testing.assert_allclose(rows["u"], a.mean(1), rtol=1e-13, atol=0)
+        np.testing.assert_allclose(rows["p"], b.mean(1), rtol=1e-13, atol=0)
 
 
 def test_seeded_experiment_with_the_device_reduction(mesh, oracle_mod):

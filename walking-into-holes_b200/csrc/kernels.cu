@@ -756,10 +756,8 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
     if (ready != 0u && (__popc(ready) >= L.step_threshold || trav == 0u) && phase == kStep) {
       const JobDesc &J = s_jobs[job];
       const GeoDesc &G = s_geos[J.geo];
-      // Up to L.chain steps: a lane whose next radius comes from the grid
-      // takes that step at once instead of waiting for the warp's next batch.
-#pragma unroll 1
-      for (int link = 1;; ++link) {
+      // One pass; `break` leaves it once the lane's next phase is set.
+      do {
         T d = sqrt(best2);
         if (!found) {
           err |= TWOS_DEVERR_QUERY;
@@ -933,9 +931,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
               const unsigned long long slot = atomicAdd(L.trace_count, 1ull);
               if (slot < L.trace_cap) L.trace[slot] = make_float4(pos.x, pos.y, pos.z, bound);
             }
-            // The next step at once while the chain allows, else with the
-            // warp's next batch.
-            if (link < L.chain) continue;
+            // The step itself comes with the warp's next batch.
             break;
           }
           if (!(in_grid && L.entry)) entry_at = 0xffffffffu;
@@ -980,7 +976,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
         iter = 0;
         phase = kTraverse;
         break;
-      }  // chain
+      } while (false);
     }
 
     if (__ballot_sync(full, phase != kIdle) == 0u) {

@@ -152,7 +152,6 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.warm = m->warm;
     L.grid_tau = m->grid_tau;
     L.units = m->units;
-    L.chain = m->chain;
     L.entry = m->entry_start;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;

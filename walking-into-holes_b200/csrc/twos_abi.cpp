@@ -115,15 +115,16 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
 }
 
 // The entry-node table over the distance grid: cells of 2^s grid spacings
-// (4 spacings by default; TWOS_ENTRY_CELLS sets 1, 2, 4, 8 or 16, 0 builds
-// none), each with the node whose subtree holds every triangle within one
-// cell size (plus 4 delta) of the cell.  A query whose initial bound is below
-// one cell size starts there instead of at the root.
+// (2 spacings by default, 16 MB for 2^25 grid vertices; TWOS_ENTRY_CELLS
+// sets 1, 2, 4, 8 or 16, 0 builds none), each with the node whose subtree
+// holds every triangle within one cell size (plus 4 delta) of the cell.  A
+// query whose initial bound is below one cell size starts there instead of at
+// the root.
 void build_entry_table(twos_mesh *m) {
   GeoDesc &g = m->geo_host;
   g.entry = nullptr;
   if (!g.grid) return;
-  uint32_t shift = 2;
+  uint32_t shift = 1;
   if (const char *e = std::getenv("TWOS_ENTRY_CELLS")) {
     const long c = std::strtol(e, nullptr, 10);
     if (c <= 0) return;
@@ -231,7 +232,6 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
-    if (const char *e = std::getenv("TWOS_CHAIN")) m->chain = std::min(64, std::max(1, std::atoi(e)));
     if (const char *e = std::getenv("TWOS_ENTRY")) m->entry_start = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
       const int b = std::atoi(e);
@@ -441,7 +441,6 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.warm = m->warm;
   L.grid_tau = m->grid_tau;
   L.units = m->units;
-  L.chain = m->chain;
   L.entry = m->entry_start;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
@@ -620,7 +619,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
-      t->units < 1 || t->units > 64 || t->chain < 1 || t->chain > 64 || (t->entry != 0 && t->entry != 1))
+      t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1))
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -628,7 +627,6 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->blocks_per_sm = t->blocks_per_sm;
   m->grid_tau = t->grid_threshold;
   m->units = t->units;
-  m->chain = t->chain;
   m->entry_start = t->entry;
   return TWOS_OK;
 }
@@ -641,7 +639,6 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->blocks_per_sm = m->blocks_per_sm;
   t->grid_threshold = m->grid_tau;
   t->units = m->units;
-  t->chain = m->chain;
   t->entry = m->entry_start;
   return TWOS_OK;
 }
@@ -976,7 +973,6 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.warm = m->warm;
     Ls.grid_tau = m->grid_tau;
     Ls.units = m->units;
-    Ls.chain = m->chain;
     Ls.entry = m->entry_start;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
@@ -1552,7 +1548,6 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.warm = m->warm;
         L.grid_tau = m->grid_tau;
         L.units = m->units;
-        L.chain = m->chain;
         L.entry = m->entry_start;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;

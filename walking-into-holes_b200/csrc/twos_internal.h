@@ -207,9 +207,7 @@ struct WosLaunch {
   // Traversal units (node visits / triangle tests) a lane runs back to back
   // per iteration of the warp loop (>= 1).
   int units;
-  // Mixed form: grid steps a lane may take back to back in one step phase
-  // (>= 1), and whether a query may start at the entry-node table's node.
-  int chain;
+  // Mixed form: whether a query may start at the entry-node table's node.
   int entry;
   // Optional record of every grid step (tests): position in the FP32 frame
   // and the bound used, at most trace_cap records; trace_count counts all.

@@ -87,6 +87,5 @@ struct twos_mesh {
   int warm = 1;            // 1: seed each step's query with the previous nearest triangle
   float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
-  int chain = 1;           // grid steps a lane may take back to back in one step phase
   int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
 };

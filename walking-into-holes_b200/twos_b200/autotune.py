@@ -10,6 +10,8 @@ the workload's own request with fewer walks) for every candidate setting of
 * the mixed form's distance-grid threshold (grid spacings a bound must reach
   before a step skips its closest-point query);
 * traversal units a lane runs per iteration of the warp loop;
+* the mixed form's entry-node start (a query whose initial bound is below one
+  entry cell starts at the cell's entry node instead of the BVH root);
 
 and leaves the fastest (walk-kernel device time per walk: every setting runs
 the same walks, and only the grid threshold changes how many steps they
@@ -32,6 +34,7 @@ DEFAULT_GRID = {
     "blocks_per_sm": (0,),
     "grid_threshold": (0.1, 0.25),
     "units": (4, 8, 16),
+    "entry": (0, 1),
 }
 
 
@@ -69,6 +72,7 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
         results.append((tuning, float(np.median(times))))
     best = min(results, key=lambda t: t[1])[0]
     mesh.set_tuning(**best)
+    best = mesh.get_tuning()
     if cache is not None:
         table = json.loads(Path(cache).read_text()) if Path(cache).exists() else {}
         table[key] = best

@@ -131,15 +131,14 @@ class Mesh:
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
     def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8,
-                   chain=1, entry=1):
+                   entry=1):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
         closest-point query, 0 to query every step; units is the number of
-        traversal units a lane runs per warp-loop iteration; chain the grid
-        steps a lane may take back to back; entry 1 starts qualifying
-        mixed-form queries at the entry-node table's node."""
+        traversal units a lane runs per warp-loop iteration; entry 1 starts
+        qualifying mixed-form queries at the entry-node table's node."""
         t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold),
-                        int(units), int(chain), int(entry))
+                        int(units), int(entry))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -148,7 +147,7 @@ class Mesh:
         return {"block": t.block, "refill": t.refill, "step_threshold": t.step_threshold,
                 "blocks_per_sm": t.blocks_per_sm,
                 # The ABI keeps a float; report the shortest decimal that rounds to it (0.1, not 0.10000000149).
-                "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units, "chain": t.chain,
+                "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units,
                 "entry": t.entry}
 
     def info(self) -> dict:
