@@ -109,8 +109,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-autotune", action="store_true", help="keep the session's default launch tuning")
     ap.add_argument("--no-ablation", action="store_true",
                     help="skip the one-step mixed-form run with the distance grid off")
-    ap.add_argument("--cpu-sites", type=int, default=128,
-                    help="sites of the fixed subset timed on the host cores in this arm's cpu_baseline")
+    ap.add_argument("--cpu-sites", type=int, default=0,
+                    help="sites of the fixed subset timed on the host cores in this arm's cpu_baseline "
+                         "(0: 8 per host thread, as one reference-arm step)")
     ap.add_argument("--ref-sites", type=int, default=REF_SUBSET,
                     help="--impl reference: sites of the fixed subset (split over the steps)")
     ap.add_argument("--housing-ref-sites", type=int, default=256, help="housing workload: FP64 reference sites")
@@ -269,6 +270,15 @@ def cpu_reference_leg(V, F, sites, walks, threads=None, workdir=None, repeat_tag
     return {"sites": len(sites), "seconds": dt, "wall": dt, "rate": len(sites) / dt, "threads": threads,
             "h": 1.96 * est["score_se"], "kind": "port",
             "engine": "oracle restatement of wih_twos.cpp (reference algorithm + mt19937_64 stream)"}
+
+
+def cpu_step_sites() -> int:
+    """Sites of one host-CPU sample: 8 per host thread, so the reference's
+    `schedule(dynamic, 4)` site loop (wih_twos.cpp:1825-1841) deals every
+    thread two chunks and no thread idles for want of sites."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import ref_runner
+    return 8 * ref_runner.host_threads()
 
 
 def cpu_model() -> str:
@@ -496,7 +506,7 @@ def run_ours(args):
             accuracy["error_ratio_vs_oracle"] = unit_ball_error_ratio(tb, args.walks)
         cpu = None
         if not args.no_cpu and world == 1:
-            idx = reference_subset(n_all, REF_SUBSET)[: args.cpu_sites]
+            idx = reference_subset(n_all, REF_SUBSET)[: args.cpu_sites or cpu_step_sites()]
             c = cpu_reference_leg(V, F, sites_all[idx], args.walks)
             h_cpu = float(np.median(c["h"]))
             h_gpu = float(np.median(1.96 * rows64["score_se"][idx])) if rows64 is not None else h_cpu
@@ -545,9 +555,10 @@ def run_reference(args):
     """The reference's own compiled backend on the host cores: wih_twos.cpp
     built unchanged (oracle/_ref/wih_twos, with the project's shim headers in
     place of Embree 4 and Eigen), OpenMP over every host thread with
-    OMP_PROC_BIND=true, on the same workload and sites.  The fixed
-    --ref-sites random subset is split over the K timed steps (one process
-    per step, its own timed site loop); warm-up steps run 4 sites each."""
+    OMP_PROC_BIND=true, on the same workload and sites.  Each of the K timed
+    steps is one process over the next 8-per-thread slice of the fixed
+    --ref-sites random subset (cycling through it), timed by the reference's
+    own site loop; warm-up steps run one thread's worth of sites each."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
@@ -555,10 +566,13 @@ def run_reference(args):
     sites_all = workload_sites(grid)
     idx = reference_subset(len(sites_all), args.ref_sites)
     wd = Path(tempfile.mkdtemp(prefix="twos_ref_"))
+    per = min(len(idx), cpu_step_sites())
     for w in range(args.warmup):
-        cpu_reference_leg(V, F, sites_all[idx[4 * w: 4 * w + 4]], args.walks, workdir=wd, repeat_tag=100 + w)
-    chunks = np.array_split(idx, max(1, args.steps))
-    runs = [cpu_reference_leg(V, F, sites_all[c], args.walks, workdir=wd) for c in chunks if len(c)]
+        cpu_reference_leg(V, F, sites_all[idx[:per // 8]], args.walks, workdir=wd, repeat_tag=100 + w)
+    runs = []
+    for k in range(args.steps):
+        take = np.take(idx, np.arange(k * per, (k + 1) * per), mode="wrap")
+        runs.append(cpu_reference_leg(V, F, sites_all[take], args.walks, workdir=wd, repeat_tag=k))
     total_sites = sum(c["sites"] for c in runs)
     total_s = sum(c["seconds"] for c in runs)
     value = total_sites / total_s
@@ -575,8 +589,9 @@ def run_reference(args):
                                      "FP64 GPU form's, so the equal-CI scale is 1"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": runs[0]["kind"],
                          "cpu_model": cpu_model(),
-                         "sample": f"fixed {total_sites}-site random subset (seed {REF_SUBSET_SEED}) of the "
-                                   f"{len(sites_all)} sites over {len(runs)} steps x {args.walks} walks, "
+                         "sample": f"{total_sites} sites over {len(runs)} steps ({per} per step, cycling through the "
+                                   f"fixed {len(idx)}-site random subset, seed {REF_SUBSET_SEED}, of the "
+                                   f"{len(sites_all)} sites) x {args.walks} walks, "
                                    f"{runs[0]['engine']}, OMP_PROC_BIND=true; rate = sites / the reference's own "
                                    "timed site loop"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
