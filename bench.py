@@ -16,7 +16,9 @@ value    mixed form (FP32 query/position, FP64 accumulation) site-estimates/s,
 e2e      the same metric through the host-buffer C-ABI call (twos_estimate):
          pinned host sites in, pinned host rows out, copies inside the timed
          region.
-fp64     the plain all-FP64 GPU form at the same N (the target comparison).
+fp64     the plain all-FP64 GPU form at the same N (the target comparison);
+         beside it the FP64 form given the mixed form's distance grid and
+         entry nodes (fp64_with_grid: the precision change alone).
 accuracy mixed against FP64 per site (z of the TD difference over every
          site), and on the unit ball (closed-form TD u^2 = ((1-|x|^2)/6)^2)
          the ratio of the mixed form's RMS error to the FP64 form's.
@@ -433,6 +435,19 @@ def run_ours(args):
         h64 = float(np.median(1.96 * rows64["score_se"]))
         fp64 = {"rate": units * len(ms64) / (t64 / 1e3), "ms_per_step": t64 / len(ms64), "steps": len(ms64),
                 "h_median": h64, "walk_seconds": float(np.mean([s["walk_seconds"] for s in s64]))}
+    fp64_grid = None
+    if fp64 is not None and not args.no_ablation:
+        # The FP64 form with the mixed form's grid steps and entry nodes: the
+        # like-for-like denominator of the precision change alone.
+        mesh.set_tuning(**dict(tuning, grid_fp64=1))
+        t_g, ms_g, s_g = timed(tb.Config(precision="fp64", **base), 1, 1)
+        rows_g = rows_now()
+        mesh.set_tuning(**tuning)
+        fp64_grid = {"rate_unscaled": units / (t_g / 1e3), "ms_per_step": t_g,
+                     "h_median": float(np.median(1.96 * rows_g["score_se"])),
+                     "walk_seconds": s_g[0]["walk_seconds"],
+                     "steps_per_walk": s_g[0]["steps"] / max(1, s_g[0]["paths"]),
+                     "grid_steps_share": s_g[0]["grid_steps"] / max(1, s_g[0]["steps"])}
     no_grid = None
     if not args.no_ablation:
         mesh.set_tuning(**dict(tuning, grid_threshold=0))
@@ -444,6 +459,8 @@ def run_ours(args):
                    "walk_seconds": s_ng[0]["walk_seconds"],
                    "steps_per_walk": s_ng[0]["steps"] / max(1, s_ng[0]["paths"])}
     h_ref = fp64["h_median"] if fp64 else h_mixed
+    if fp64_grid:
+        fp64_grid["rate"] = fp64_grid["rate_unscaled"] * (fp64_grid["h_median"] / h_ref) ** 2
     if no_grid:
         no_grid["rate"] = no_grid["rate_unscaled"] * (no_grid["h_median"] / h_ref) ** 2
         if fp64:
@@ -534,6 +551,8 @@ def run_ours(args):
             "fp64_form": fp64,
             "mixed_over_fp64": (value / fp64["rate"]) if fp64 else None,
             "mixed_without_grid": no_grid,
+            "fp64_with_grid": fp64_grid,
+            "mixed_over_fp64_with_grid": (value / fp64_grid["rate"]) if fp64_grid else None,
             "accuracy": accuracy,
             "e2e": {"value": rate_e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
                     "d2h_bytes_per_step": int(n * 56), "ms_per_step": t_e2e / args.steps},

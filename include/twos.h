@@ -259,6 +259,10 @@ typedef struct twos_tuning {
                             initial bound is below one entry cell start at
                             the entry-node table's node instead of the root
                             (same result, fewer node visits); 0 = root. */
+  int32_t grid_fp64;     /* 1: the FP64 compliance form (centre source) also
+                            takes the distance grid's steps and entry nodes,
+                            for comparing precision alone; 0 (default): the
+                            plain FP64 form, the reference's algorithm. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);

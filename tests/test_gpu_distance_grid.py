@@ -83,3 +83,26 @@ def test_grid_walks_estimate_the_same_field(tb):
     assert np.max(np.abs(zz)) < 4.5 and abs(np.mean(zz)) < 0.5
     # Same variance per walk: the grid changes the radii, not the estimator.
     assert 0.8 < np.median(on["score_se"] / off["score_se"]) < 1.25
+
+
+def test_fp64_form_with_the_grid_estimates_the_same_field(tb):
+    """grid_fp64 = 1 gives the FP64 compliance form the mixed form's grid steps
+    and entry nodes (a comparison of precision alone): its walks take other
+    radii than the plain FP64 form's, so the two agree within the Monte Carlo
+    error, and both agree with the analytic u on the unit ball."""
+    V, F = tb.geometry.icosphere(5)
+    sites = tb.geometry.uniform_ball(64, 0.9, seed=6)
+    u_exact = (1.0 - np.sum(sites ** 2, axis=1)) / 6.0
+    cfg = tb.Config(walks=2048, precision="fp64", seed=19, epsilon=1e-4, source=tb.sources.constant(1.0))
+    with tb.Mesh(V, F) as mesh:
+        plain, s_plain = mesh.estimate(sites, cfg)
+        mesh.set_tuning(grid_fp64=1)
+        grid, s_grid = mesh.estimate(sites, cfg)
+        smp = mesh.walk_samples(sites, cfg)
+    assert s_plain["grid_steps"] == 0 and s_grid["grid_steps"] > 0.2 * s_grid["steps"]
+    assert s_grid["caps"] == 0 and s_grid["node_tests"] < s_plain["node_tests"]
+    se = smp["u"].std(axis=1, ddof=1) / np.sqrt(cfg.walks)
+    z = (grid["u"] - u_exact) / se
+    assert np.max(np.abs(z)) < 4.5 and np.mean(np.abs(z) < 3) >= 0.95
+    zz = (grid["score"] - plain["score"]) / np.hypot(grid["score_se"], plain["score_se"])
+    assert np.max(np.abs(zz)) < 4.5 and abs(np.mean(zz)) < 0.5

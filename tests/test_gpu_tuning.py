@@ -24,7 +24,8 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
                                          (256, 4, 16, 1)]:
             mesh.set_tuning(block=block, refill=refill, step_threshold=step, blocks_per_sm=bps)
             assert mesh.get_tuning() == {"block": block, "refill": refill, "step_threshold": step,
-                                         "blocks_per_sm": bps, "grid_threshold": 0.1, "units": 8, "entry": 1}
+                                         "blocks_per_sm": bps, "grid_threshold": 0.1, "units": 8, "entry": 1,
+                                         "grid_fp64": 0}
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {block} {refill} {step} {bps}")
@@ -44,7 +45,7 @@ def test_invalid_tuning_is_usage_error(tb, bunny1000):
     with tb.Mesh(*bunny1000) as mesh:
         for bad in [dict(block=96), dict(refill=0), dict(step_threshold=33), dict(blocks_per_sm=-1),
                     dict(grid_threshold=0.05), dict(grid_threshold=-1.0), dict(grid_threshold=float("nan")),
-                    dict(units=0), dict(units=65), dict(entry=2)]:
+                    dict(units=0), dict(units=65), dict(entry=2), dict(grid_fp64=3)]:
             with pytest.raises(tb.TwosError) as e:
                 mesh.set_tuning(**bad)
             assert e.value.code == 2

@@ -190,6 +190,16 @@ __device__ __forceinline__ double gap(double lo, double hi, double p) { return f
 // distance from below; for a nearly flat patch the slab is thin and the
 // bound is close to the true distance, where the box bound is off by up to
 // the box size).
+// An upper bound of sqrt(x), x >= 0, for the distance grid's corner
+// distances: the hardware approximation (sqrt.approx, relative error below
+// 2^-22 per the PTX ISA) raised by 2^-20 relative.  Overstating |p - v|
+// keeps both grid bounds conservative.
+__device__ __forceinline__ float sqrt_up(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r * (1.0f + 0x1.0p-20f);
+}
+
 // 32-byte read-only load (two float4) of 32-byte aligned data: one L1
 // request instead of two.
 __device__ __forceinline__ void ldg32(const void *p, float4 &a, float4 &b) {
@@ -538,7 +548,7 @@ __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
     const uint16_t raw = __ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k);
-    const float dist = sqrtf(dot3(dv, dv));
+    const float dist = sqrt_up(dot3(dv, dv));
     const float dq = static_cast<float>(raw) * g.grid_q;
     best = fmaxf(best, dq - dist);
     if (raw != 0xffffu) up = fminf(up, dq + g.grid_q + dist);
@@ -617,7 +627,7 @@ constexpr int wos_min_blocks(int block) {
                                                                               : 768 / block;
 }
 
-template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false>
+template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false>
 __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
@@ -959,6 +969,25 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             }
           }
         } else {
+          // FP64 form.  With GRID64 it takes the same grid steps and entry
+          // nodes as the mixed form (a comparison of precision alone): the
+          // bound is evaluated at the FP32 image p32 of the position, within
+          // a few 1e-8 of it, and bound <= d(p32) - delta covers that.
+          float bound = 0.f, upper = CUDART_INF_F;
+          uint32_t entry_at = 0xffffffffu;
+          bool in_grid = false;
+          if constexpr (GRID64) {
+            const double p3[3] = {pos.x, pos.y, pos.z};
+            in_grid = L.grid_tau > 0.f && G.grid && grid_bounds(G, to_frame<float>(p3, G), bound, upper, entry_at);
+            const double b = static_cast<double>(bound);
+            if (in_grid && bound >= L.grid_tau * G.grid_h && bound > 2.f * (static_cast<float>(J.epsilon) + G.delta) &&
+                b * b < best2) {
+              best2 = b * b;
+              found = true;
+              ++c_grid;
+              break;
+            }
+          }
           if (L.warm && tri_ok) {
             Vec<T> ta, tb, tc;
             load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
@@ -967,6 +996,15 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             if (w2 < best2) {
               best2 = w2;
               found = true;
+            }
+          }
+          if constexpr (GRID64) {
+            if (in_grid && L.entry && entry_at != 0xffffffffu) {
+              const double ubs = static_cast<double>(upper) + 6.0 * G.delta;
+              if (fmin(sqrt(best2), ubs) < static_cast<double>(G.entry_radius)) {
+                node = __ldg(G.entry + entry_at);
+                if (ubs * ubs < best2) best2 = ubs * ubs;
+              }
             }
           }
         }
@@ -1136,7 +1174,10 @@ template <typename T, int MODE, int BLOCK> static const void *select_src(int src
   return wos_fn<T, MODE, TWOS_SOURCE_CENTER, BLOCK>();
 }
 
-template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src) {
+template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src, int grid64) {
+  if (grid64 && precision == TWOS_PREC_FP64 && mode == TWOS_MODE_COMPLIANCE && src == TWOS_SOURCE_CENTER)
+    return reinterpret_cast<const void *>(
+        &wos_kernel<double, TWOS_MODE_COMPLIANCE, TWOS_SOURCE_CENTER, BLOCK, false, true>);
   if (mode == kModeBoundary)
     return precision == TWOS_PREC_MIXED ? wos_fn<float, kModeBoundary, TWOS_SOURCE_CENTER, BLOCK>()
                                         : wos_fn<double, kModeBoundary, TWOS_SOURCE_CENTER, BLOCK>();
@@ -1153,14 +1194,14 @@ template <int BLOCK> static const void *select_wos_block(int precision, int mode
 }
 
 // Walk kernel instantiations: block sizes 128, 256 and 512 threads.
-static const void *select_wos(int precision, int mode, int src, int block) {
+static const void *select_wos(int precision, int mode, int src, int block, int grid64) {
   switch (block) {
     case 128:
-      return select_wos_block<128>(precision, mode, src);
+      return select_wos_block<128>(precision, mode, src, grid64);
     case 256:
-      return select_wos_block<256>(precision, mode, src);
+      return select_wos_block<256>(precision, mode, src, grid64);
     case 512:
-      return select_wos_block<512>(precision, mode, src);
+      return select_wos_block<512>(precision, mode, src, grid64);
     default:
       return nullptr;
   }
@@ -1192,7 +1233,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
   if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
   if (dyn > 200 * 1024) return cudaErrorInvalidValue;
-  const void *fn = select_wos(precision, mode, src, block);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64);
   if (!fn) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
@@ -1203,7 +1244,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
 
 int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L) {
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
-  const void *fn = select_wos(precision, mode, src, block);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64);
   if (!fn || dyn > 200 * 1024) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;

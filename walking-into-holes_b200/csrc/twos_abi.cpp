@@ -442,6 +442,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.grid_tau = m->grid_tau;
   L.units = m->units;
   L.entry = m->entry_start;
+  L.grid64 = m->grid_fp64;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -619,7 +620,8 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   if ((t->block != 128 && t->block != 256 && t->block != 512) || t->refill < 1 || t->refill > 32 ||
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
-      t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1))
+      t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1) ||
+      (t->grid_fp64 != 0 && t->grid_fp64 != 1))
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -628,6 +630,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->grid_tau = t->grid_threshold;
   m->units = t->units;
   m->entry_start = t->entry;
+  m->grid_fp64 = t->grid_fp64;
   return TWOS_OK;
 }
 
@@ -640,6 +643,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->grid_threshold = m->grid_tau;
   t->units = m->units;
   t->entry = m->entry_start;
+  t->grid_fp64 = m->grid_fp64;
   return TWOS_OK;
 }
 
@@ -974,6 +978,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.grid_tau = m->grid_tau;
     Ls.units = m->units;
     Ls.entry = m->entry_start;
+    Ls.grid64 = m->grid_fp64;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -1549,6 +1554,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.grid_tau = m->grid_tau;
         L.units = m->units;
         L.entry = m->entry_start;
+        L.grid64 = m->grid_fp64;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;

@@ -209,6 +209,9 @@ struct WosLaunch {
   int units;
   // Mixed form: whether a query may start at the entry-node table's node.
   int entry;
+  // FP64 compliance form with the mixed form's distance grid and entry nodes
+  // (a comparison of precision alone; off for the plain FP64 form).
+  int grid64;
   // Optional record of every grid step (tests): position in the FP32 frame
   // and the bound used, at most trace_cap records; trace_count counts all.
   float4 *trace;

@@ -88,4 +88,5 @@ struct twos_mesh {
   float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
   int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
+  int grid_fp64 = 0;       // 1: the FP64 compliance form uses the grid and entry nodes too
 };
