@@ -587,7 +587,7 @@ def run_reference(args):
     wd = Path(tempfile.mkdtemp(prefix="twos_ref_"))
     per = min(len(idx), cpu_step_sites())
     for w in range(args.warmup):
-        cpu_reference_leg(V, F, sites_all[idx[:per // 8]], args.walks, workdir=wd, repeat_tag=100 + w)
+        cpu_reference_leg(V, F, sites_all[idx[:max(1, per // 8)]], args.walks, workdir=wd, repeat_tag=100 + w)
     runs = []
     for k in range(args.steps):
         take = np.take(idx, np.arange(k * per, (k + 1) * per), mode="wrap")
