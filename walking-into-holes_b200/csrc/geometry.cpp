@@ -20,71 +20,90 @@
 
 namespace twos {
 
-void load_ascii_ply(const std::string &path, std::vector<double> &vertices, std::vector<uint32_t> &faces) {
-  std::ifstream input(path);
-  if (!input) throw std::runtime_error("cannot open mesh: " + path);
-  std::string line;
-  size_t vertex_count = 0, face_count = 0;
-  bool ascii = false, header_done = false;
-  while (std::getline(input, line)) {
-    std::istringstream words(line);
-    std::string first;
-    words >> first;
-    if (first == "format") {
-      std::string format;
-      words >> format;
-      ascii = format == "ascii";
-    } else if (first == "element") {
-      std::string type;
-      size_t count = 0;
-      words >> type >> count;
-      if (type == "vertex") vertex_count = count;
-      if (type == "face") face_count = count;
-    } else if (first == "end_header") {
-      header_done = true;
-      break;
+namespace {
+
+// What the header of a PLY file declares, as far as the reader needs it:
+// the format keyword and the last vertex and face element counts.
+struct PlyHeader {
+  bool ascii = false;
+  bool complete = false;  // "end_header" seen
+  size_t vertex_count = 0;
+  size_t face_count = 0;
+};
+
+PlyHeader read_ply_header(std::istream &in) {
+  PlyHeader h;
+  for (std::string line; !h.complete && std::getline(in, line);) {
+    std::istringstream tokens(line);
+    std::string keyword;
+    tokens >> keyword;
+    if (keyword == "end_header") {
+      h.complete = true;
+    } else if (keyword == "format") {
+      std::string kind;
+      tokens >> kind;
+      h.ascii = kind == "ascii";
+    } else if (keyword == "element") {
+      std::string name;
+      size_t n = 0;
+      tokens >> name >> n;
+      if (name == "vertex") h.vertex_count = n;
+      else if (name == "face") h.face_count = n;
     }
   }
-  if (!ascii || !header_done || vertex_count == 0 || face_count == 0)
+  return h;
+}
+
+// Drops whatever follows the values just read on the current line (extra
+// properties of a vertex or face row).
+void skip_rest_of_line(std::istream &in) { in.ignore(std::numeric_limits<std::streamsize>::max(), '\n'); }
+
+}  // namespace
+
+// The reference's reader rules (wih_twos.cpp:437-493): an ASCII header with
+// nonzero vertex and face counts; each vertex row starts with x y z; each
+// face row is "3 a b c" with indices below the vertex count; anything else
+// is an error with the reference's message.
+void load_ascii_ply(const std::string &path, std::vector<double> &vertices, std::vector<uint32_t> &faces) {
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open mesh: " + path);
+  const PlyHeader h = read_ply_header(in);
+  if (!h.ascii || !h.complete || h.vertex_count == 0 || h.face_count == 0)
     throw std::runtime_error("expected a nonempty ASCII triangle PLY mesh");
-  vertices.resize(3 * vertex_count);
-  for (size_t i = 0; i < vertex_count; ++i) {
-    if (!(input >> vertices[3 * i] >> vertices[3 * i + 1] >> vertices[3 * i + 2]))
-      throw std::runtime_error("truncated PLY vertex section");
-    std::getline(input, line);
+  vertices.assign(3 * h.vertex_count, 0.0);
+  for (double *v = vertices.data(), *end = v + vertices.size(); v != end; v += 3) {
+    if (!(in >> v[0] >> v[1] >> v[2])) throw std::runtime_error("truncated PLY vertex section");
+    skip_rest_of_line(in);
   }
-  faces.resize(3 * face_count);
-  for (size_t i = 0; i < face_count; ++i) {
-    unsigned count = 0;
-    uint64_t a = 0, b = 0, c = 0;
-    if (!(input >> count >> a >> b >> c) || count != 3 || a >= vertex_count || b >= vertex_count ||
-        c >= vertex_count)
+  faces.assign(3 * h.face_count, 0u);
+  for (uint32_t *f = faces.data(), *end = f + faces.size(); f != end; f += 3) {
+    unsigned corners = 0;
+    uint64_t idx[3] = {0, 0, 0};
+    const bool parsed = static_cast<bool>(in >> corners >> idx[0] >> idx[1] >> idx[2]);
+    if (!parsed || corners != 3 || std::max({idx[0], idx[1], idx[2]}) >= h.vertex_count)
       throw std::runtime_error("expected valid triangular PLY faces");
-    faces[3 * i] = static_cast<uint32_t>(a);
-    faces[3 * i + 1] = static_cast<uint32_t>(b);
-    faces[3 * i + 2] = static_cast<uint32_t>(c);
-    std::getline(input, line);
+    for (int k = 0; k < 3; ++k) f[k] = static_cast<uint32_t>(idx[k]);
+    skip_rest_of_line(in);
   }
 }
 
+// Points file rules of wih_twos.cpp:508-522: blank lines and lines starting
+// with '#' are skipped, commas count as spaces, a line contributes a point
+// when it starts with three numbers, and a file without points is an error.
 std::vector<double> read_points(const std::string &path) {
-  std::ifstream input(path);
-  if (!input) throw std::runtime_error("cannot open points: " + path);
-  std::vector<double> points;
-  std::string line;
-  while (std::getline(input, line)) {
-    if (line.empty() || line[0] == '#') continue;
-    std::replace(line.begin(), line.end(), ',', ' ');
-    std::istringstream values(line);
-    double x, y, z;
-    if (values >> x >> y >> z) {
-      points.push_back(x);
-      points.push_back(y);
-      points.push_back(z);
-    }
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open points: " + path);
+  std::vector<double> xyz;
+  for (std::string line; std::getline(in, line);) {
+    if (line.empty() || line.front() == '#') continue;
+    for (char &ch : line)
+      if (ch == ',') ch = ' ';
+    std::istringstream row(line);
+    double p[3];
+    if (row >> p[0] >> p[1] >> p[2]) xyz.insert(xyz.end(), p, p + 3);
   }
-  if (points.empty()) throw std::runtime_error("points file contains no points");
-  return points;
+  if (xyz.empty()) throw std::runtime_error("points file contains no points");
+  return xyz;
 }
 
 // ---------------------------------------------------------------- BVH build
