@@ -1114,7 +1114,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
       n_nodes += __shfl_xor_sync(full, n_nodes, o);
       n_planes += __shfl_xor_sync(full, n_planes, o);
       n_tris += __shfl_xor_sync(full, n_tris, o);
-      if (sizeof(T) == 4) n_grid += __shfl_xor_sync(full, n_grid, o);
+      n_grid += __shfl_xor_sync(full, n_grid, o);
     }
     if (lane == 0) {
       atomicAdd(&L.counters[0], n_nodes);
