@@ -1065,42 +1065,47 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           }
           if (!have) {
             phase = kStep;
-          } else if (node >= 0) {
-            ++c_nodes;
-            T dl, dr;
-            int cl, cr;
-            node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
-            const bool vl = dl < best2, vr = dr < best2;
-            if (vl && vr) {
-              if (dr < dl) {
-                const T td = dl;
-                dl = dr;
-                dr = td;
-                const int tc = cl;
-                cl = cr;
-                cr = tc;
-              }
-              if (sp >= kStack) {
-                err |= TWOS_DEVERR_STACK;
-                found = false;
-                phase = kStep;
-              } else {
-                stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
-                ++sp;
+          } else {
+            if (node >= 0) {
+              ++c_nodes;
+              T dl, dr;
+              int cl, cr;
+              node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
+              const bool vl = dl < best2, vr = dr < best2;
+              if (vl && vr) {
+                if (dr < dl) {
+                  const T td = dl;
+                  dl = dr;
+                  dr = td;
+                  const int tc = cl;
+                  cl = cr;
+                  cr = tc;
+                }
+                if (sp >= kStack) {
+                  err |= TWOS_DEVERR_STACK;
+                  found = false;
+                  phase = kStep;
+                } else {
+                  stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+                  ++sp;
+                  node = cl;
+                }
+              } else if (vl) {
                 node = cl;
+              } else if (vr) {
+                node = cr;
+              } else {
+                have = false;
               }
-            } else if (vl) {
-              node = cl;
-            } else if (vr) {
-              node = cr;
-            } else {
+            }
+            // A leaf reached by this unit's visit or pop: its triangle range
+            // is taken in the same unit, so the next unit tests a triangle.
+            if (have && node < 0 && phase == kTraverse) {
+              const uint32_t enc = ~static_cast<uint32_t>(node);
+              tri_cur = enc >> 3;
+              tri_end = tri_cur + (enc & 7u);
               have = false;
             }
-          } else {
-            const uint32_t enc = ~static_cast<uint32_t>(node);
-            tri_cur = enc >> 3;
-            tri_end = tri_cur + (enc & 7u);
-            have = false;
           }
         }
       }
