@@ -482,13 +482,15 @@ def run_ours(args):
         tris = np.mean([s["triangle_tests"] for s in s_mixed])
         walks_launch = n * args.walks
         # Bytes the walk kernel must fetch: 96 B per node visit (two child
-        # boxes + normal slabs + child words), 32 B per triangle plane test
+        # boxes + normal slabs + child words; 192 B for a four-wide node),
+        # 32 B per triangle plane test
         # (plane slab + first vertex), 32 B more per full closest-point test
         # (the other two vertices), counted on the device; four 32 B sectors
         # per distance-grid lookup (the cell's eight corners lie in four
         # (i, j) rows; one lookup after every step).
         grid_lookups = steps if info["grid_dims"][0] else 0.0
-        fetched = 96.0 * nodes + 32.0 * planes + 32.0 * tris + 128.0 * grid_lookups
+        node_bytes = 192.0 if tuning.get("bvh_width", 2) == 4 else 96.0
+        fetched = node_bytes * nodes + 32.0 * planes + 32.0 * tris + 128.0 * grid_lookups
         bvh_queries = queries - grid_steps
         hbm_peak, hbm_kind = measured_peaks()
         l2_peak = tb.l2_read_gbs(local)
@@ -504,8 +506,8 @@ def run_ours(args):
                         "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
                 "ncu_walk_kernel": NCU_WALK_KERNEL,
                 "bytes_per_walk": float(fetched / walks_launch),
-                "bytes_definition": "device-counted: 96 B/node visit + 32 B/plane test + 32 B/full triangle test"
-                                    " + 128 B/distance-grid lookup (one per step)",
+                "bytes_definition": "device-counted: 96 B/node visit (192 B four-wide) + 32 B/plane test + 32 B/full "
+                                    "triangle test + 128 B/distance-grid lookup (one per step)",
                 "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),
                 "bvh_queries_per_launch": float(bvh_queries), "walk_kernel_seconds": walk_s,
                 "bvh_queries_per_second": float(bvh_queries / walk_s),

@@ -263,6 +263,11 @@ typedef struct twos_tuning {
                             takes the distance grid's steps and entry nodes,
                             for comparing precision alone; 0 (default): the
                             plain FP64 form, the reference's algorithm. */
+  int32_t bvh_width;     /* mixed form: 2 traverses the binary BVH, 4 the same
+                            BVH collapsed to four-wide nodes (compliance,
+                            paired and hot modes with the centre or Green
+                            source; the others stay binary).  Same minima,
+                            same rows.  Default 2. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);

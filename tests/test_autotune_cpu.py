@@ -42,7 +42,7 @@ class FakeMesh:
         # threshold adds steps (queries) but fewer seconds per walk.
         per_walk = (1.0 + 0.1 * abs(t["block"] - 256) / 128 + 0.05 * (t["step_threshold"] != 4)
                     + 0.02 * abs(t["units"] - 8) / 4 + 0.3 * t["grid_threshold"] + 0.01 * (t["refill"] != 1)
-                    + 0.1 * (t.get("entry", 1) != 1))
+                    + 0.1 * (t.get("entry", 1) != 1) + 0.05 * (t.get("bvh_width", 2) != 4))
         steps = paths * (30 if t["grid_threshold"] < 0.2 else 25)
         if cfg.repeat == 5000:  # the warm-up run is slow and must be ignored
             per_walk *= 100
@@ -56,7 +56,7 @@ def test_autotune_sweeps_every_setting_and_picks_the_fastest(tmp_path):
     best, results = autotune(mesh, sites, Cfg(), calib_sites=100, calib_walks=64, repeats=2, cache=cache)
     assert len(results) == np.prod([len(v) for v in DEFAULT_GRID.values()])
     assert best == {"block": 256, "refill": 1, "step_threshold": 4, "blocks_per_sm": 0, "grid_threshold": 0.1,
-                    "units": 8, "entry": 1}
+                    "units": 8, "entry": 1, "bvh_width": 4}
     assert mesh.get_tuning() == best
     # Calibration: a seeded subset of the sites, the request's walks capped, one warm-up plus two timed runs.
     assert all(n == 100 and w == 64 for _, w, _, n in mesh.calls)

@@ -12,8 +12,8 @@ eps 1e-4, max 1,024 steps, sites drawn from the bench's interior sites.
   walks) is at most the FP64 distance from the step's position to the mesh
   less delta: the ball a grid step uses (radius bound - delta) never leaves
   the domain.
-* The entry-node start changes no result: rows are equal bit for bit with
-  it switched off (same walks, same minima).
+* The entry-node start and the four-wide BVH change no result: rows are
+  equal bit for bit either way (same walks, same minima).
 """
 import numpy as np
 import pytest
@@ -69,13 +69,13 @@ def test_every_grid_step_stays_inside_the_domain(setup):
     assert np.median(bounds / d64) > 0.5
 
 
-def test_entry_start_changes_no_result(setup):
+def test_entry_start_and_bvh_width_change_no_result(setup):
     tb, mesh, sites = setup
     s = sites[:512]
     base = mesh.get_tuning()
     try:
         ref, _ = mesh.estimate(s, _cfg(tb, "mixed", walks=256))
-        for variant in (dict(entry=0),):
+        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0)):
             mesh.set_tuning(**dict(base, **variant))
             got, _ = mesh.estimate(s, _cfg(tb, "mixed", walks=256))
             np.testing.assert_array_equal(got, ref, err_msg=str(variant))

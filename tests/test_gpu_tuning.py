@@ -25,7 +25,7 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
             mesh.set_tuning(block=block, refill=refill, step_threshold=step, blocks_per_sm=bps)
             assert mesh.get_tuning() == {"block": block, "refill": refill, "step_threshold": step,
                                          "blocks_per_sm": bps, "grid_threshold": 0.1, "units": 8, "entry": 1,
-                                         "grid_fp64": 0}
+                                         "grid_fp64": 0, "bvh_width": 2}
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {block} {refill} {step} {bps}")
@@ -34,18 +34,21 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} units={units}")
-        # The entry-node start changes where a query's traversal begins, never its minimum.
-        mesh.set_tuning(entry=0)
-        out, _ = mesh.estimate(eval_points, cfg)
-        for k in ("u", "score", "score_se", "steps"):
-            np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} entry=0")
+        # The entry-node start and the BVH width change how a query's
+        # traversal runs, never its minimum.
+        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0), dict(bvh_width=4, units=3)):
+            mesh.set_tuning(**variant)
+            out, _ = mesh.estimate(eval_points, cfg)
+            for k in ("u", "score", "score_se", "steps"):
+                np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {variant}")
 
 
 def test_invalid_tuning_is_usage_error(tb, bunny1000):
     with tb.Mesh(*bunny1000) as mesh:
         for bad in [dict(block=96), dict(refill=0), dict(step_threshold=33), dict(blocks_per_sm=-1),
                     dict(grid_threshold=0.05), dict(grid_threshold=-1.0), dict(grid_threshold=float("nan")),
-                    dict(units=0), dict(units=65), dict(entry=2), dict(grid_fp64=3)]:
+                    dict(units=0), dict(units=65), dict(entry=2), dict(grid_fp64=3),
+                    dict(bvh_width=3)]:
             with pytest.raises(tb.TwosError) as e:
                 mesh.set_tuning(**bad)
             assert e.value.code == 2

@@ -710,4 +710,95 @@ std::vector<int32_t> build_entry_table(const HostBvh &bvh, const double origin[3
   return entry;
 }
 
+
+// Collapse of the packed binary BVH into four-wide nodes: slot boxes, slabs
+// and child codes are copied from the binary nodes (so every bound is the
+// same conservative FP32 value), internal slot children become four-wide
+// nodes in turn.
+void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::vector<Node4F> &nodes4,
+                   std::vector<int32_t> &cover) {
+  nodes4.clear();
+  cover.assign(bvh.nodes.size(), 0);
+  if (bvh.nodes.empty()) return;
+  struct Slot {
+    float lo[3], hi[3], n[3], smin, smax;
+    int32_t code;
+  };
+  auto slot_of = [&](int32_t ni, int c) {
+    const NodeF &b = binary[static_cast<size_t>(ni)];
+    const float *x = &b.x.x, *y = &b.y.x, *z = &b.z.x;
+    const float4 &nv = c == 0 ? b.nl : b.nr;
+    Slot s;
+    s.lo[0] = x[c];
+    s.lo[1] = y[c];
+    s.lo[2] = z[c];
+    s.hi[0] = x[2 + c];
+    s.hi[1] = y[2 + c];
+    s.hi[2] = z[2 + c];
+    s.n[0] = nv.x;
+    s.n[1] = nv.y;
+    s.n[2] = nv.z;
+    s.smin = nv.w;
+    s.smax = c == 0 ? b.tail.x : b.tail.y;
+    s.code = bvh.nodes[static_cast<size_t>(ni)].child[c];
+    return s;
+  };
+  // Iterative build: (binary node, four-wide index) pairs still to fill.
+  std::vector<std::pair<int32_t, int32_t>> todo{{0, 0}};
+  nodes4.emplace_back();
+  cover[0] = 0;
+  while (!todo.empty()) {
+    const auto [ni, qi] = todo.back();
+    todo.pop_back();
+    Slot slots[4];
+    int ns = 0;
+    for (int c = 0; c < 2; ++c) {
+      const int32_t code = bvh.nodes[static_cast<size_t>(ni)].child[c];
+      if (code >= 0) {
+        cover[static_cast<size_t>(code)] = qi;  // absorbed into this node
+        slots[ns++] = slot_of(code, 0);
+        slots[ns++] = slot_of(code, 1);
+      } else {
+        slots[ns++] = slot_of(ni, c);
+      }
+    }
+    float *f[11];
+    Node4F q{};
+    float *base = &q.xlo.x;
+    for (int k = 0; k < 11; ++k) f[k] = base + 4 * k;
+    int32_t child[4];
+    for (int k = 0; k < 4; ++k) {
+      if (k < ns) {
+        const Slot &s = slots[k];
+        for (int a = 0; a < 3; ++a) {
+          f[2 * a][k] = s.lo[a];
+          f[2 * a + 1][k] = s.hi[a];
+          f[6 + a][k] = s.n[a];
+        }
+        f[9][k] = s.smin;
+        f[10][k] = s.smax;
+        if (s.code >= 0) {
+          const int32_t qc = static_cast<int32_t>(nodes4.size());
+          nodes4.emplace_back();
+          cover[static_cast<size_t>(s.code)] = qc;
+          todo.push_back({s.code, qc});
+          child[k] = qc;
+        } else {
+          child[k] = s.code;
+        }
+      } else {
+        for (int a = 0; a < 3; ++a) {
+          f[2 * a][k] = std::numeric_limits<float>::infinity();
+          f[2 * a + 1][k] = -std::numeric_limits<float>::infinity();
+          f[6 + a][k] = 0.f;
+        }
+        f[9][k] = f[10][k] = 0.f;
+        child[k] = ~static_cast<int32_t>(0);
+      }
+    }
+    q.child = make_int4(child[0], child[1], child[2], child[3]);
+    nodes4[static_cast<size_t>(qi)] = q;
+  }
+}
+
 }  // namespace twos

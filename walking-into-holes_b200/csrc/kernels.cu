@@ -190,16 +190,6 @@ __device__ __forceinline__ double gap(double lo, double hi, double p) { return f
 // distance from below; for a nearly flat patch the slab is thin and the
 // bound is close to the true distance, where the box bound is off by up to
 // the box size).
-// An upper bound of sqrt(x), x >= 0, for the distance grid's corner
-// distances: the hardware approximation (sqrt.approx, relative error below
-// 2^-22 per the PTX ISA) raised by 2^-20 relative.  Overstating |p - v|
-// keeps both grid bounds conservative.
-__device__ __forceinline__ float sqrt_up(float x) {
-  float r;
-  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r * (1.0f + 0x1.0p-20f);
-}
-
 // 32-byte read-only load (two float4) of 32-byte aligned data: one L1
 // request instead of two.
 __device__ __forceinline__ void ldg32(const void *p, float4 &a, float4 &b) {
@@ -247,6 +237,47 @@ __device__ __forceinline__ void node_dist2(const NodeD *__restrict__ nodes, int 
   dr = fmax(rx * rx + ry * ry + rz * rz, gr * gr);
   cl = ch.x;
   cr = ch.y;
+}
+
+// The same bounds for the four children of a four-wide node (six 32-byte
+// loads); slot k's squared lower bound in d[k], its child code in c[k].  An
+// empty slot's inverted box gives +inf.
+__device__ __forceinline__ void node4_dist2(const Node4F *__restrict__ nodes, int idx, const Vec<float> &p,
+                                            float d[4], int c[4]) {
+  const Node4F *n = nodes + idx;
+  float4 xlo, xhi, ylo, yhi, zlo, zhi, nx, ny, nz, smin, smax, ch;
+  ldg32(&n->xlo, xlo, xhi);
+  ldg32(&n->ylo, ylo, yhi);
+  ldg32(&n->zlo, zlo, zhi);
+  ldg32(&n->nx, nx, ny);
+  ldg32(&n->nz, nz, smin);
+  ldg32(&n->smax, smax, ch);
+  auto slot = [&](float xl, float xh, float yl, float yh, float zl, float zh, float a, float b, float e, float s0,
+                  float s1) {
+    const float gx = gap(xl, xh, p.x), gy = gap(yl, yh, p.y), gz = gap(zl, zh, p.z);
+    const float s = __fmaf_rn(a, p.x, __fmaf_rn(b, p.y, e * p.z));
+    const float gs = gap(s0, s1, s);
+    return fmaxf(__fmaf_rn(gx, gx, __fmaf_rn(gy, gy, gz * gz)), gs * gs);
+  };
+  d[0] = slot(xlo.x, xhi.x, ylo.x, yhi.x, zlo.x, zhi.x, nx.x, ny.x, nz.x, smin.x, smax.x);
+  d[1] = slot(xlo.y, xhi.y, ylo.y, yhi.y, zlo.y, zhi.y, nx.y, ny.y, nz.y, smin.y, smax.y);
+  d[2] = slot(xlo.z, xhi.z, ylo.z, yhi.z, zlo.z, zhi.z, nx.z, ny.z, nz.z, smin.z, smax.z);
+  d[3] = slot(xlo.w, xhi.w, ylo.w, yhi.w, zlo.w, zhi.w, nx.w, ny.w, nz.w, smin.w, smax.w);
+  c[0] = __float_as_int(ch.x);
+  c[1] = __float_as_int(ch.y);
+  c[2] = __float_as_int(ch.z);
+  c[3] = __float_as_int(ch.w);
+}
+
+__device__ __forceinline__ void order2(float &da, int &ca, float &db, int &cb) {
+  if (db < da) {
+    const float t = da;
+    da = db;
+    db = t;
+    const int u = ca;
+    ca = cb;
+    cb = u;
+  }
 }
 
 // Plane-slab lower bound of a triangle (one or two 16-byte loads); the full
@@ -548,7 +579,7 @@ __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
     const uint16_t raw = __ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k);
-    const float dist = sqrt_up(dot3(dv, dv));
+    const float dist = sqrtf(dot3(dv, dv));
     const float dq = static_cast<float>(raw) * g.grid_q;
     best = fmaxf(best, dq - dist);
     if (raw != 0xffffu) up = fminf(up, dq + g.grid_q + dist);
@@ -627,7 +658,7 @@ constexpr int wos_min_blocks(int block) {
                                                                               : 768 / block;
 }
 
-template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false>
+template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false, bool WIDE = false>
 __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
@@ -964,7 +995,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           if (entry_at != 0xffffffffu) {
             const float ubs = upper + 6.f * G.delta;
             if (fminf(sqrtf(best2), ubs) < G.entry_radius) {
-              node = __ldg(G.entry + entry_at);
+              node = __ldg((WIDE ? G.entry4 : G.entry) + entry_at);
               if (ubs * ubs < best2) best2 = ubs * ubs;
             }
           }
@@ -1066,36 +1097,70 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           if (!have) {
             phase = kStep;
           } else {
-            if (node >= 0) {
-              ++c_nodes;
-              T dl, dr;
-              int cl, cr;
-              node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
-              const bool vl = dl < best2, vr = dr < best2;
-              if (vl && vr) {
-                if (dr < dl) {
-                  const T td = dl;
-                  dl = dr;
-                  dr = td;
-                  const int tc = cl;
-                  cl = cr;
-                  cr = tc;
-                }
-                if (sp >= kStack) {
+            if constexpr (WIDE) {
+              if (node >= 0) {
+                // Four-wide node: its valid children sorted nearest first (a
+                // five-comparator network); the nearest is next, the others
+                // are pushed farthest first.
+                ++c_nodes;
+                float d[4];
+                int c[4];
+                node4_dist2(G.nodes4_f, node, pos, d, c);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                  if (!(d[k] < best2)) d[k] = CUDART_INF_F;
+                order2(d[0], c[0], d[1], c[1]);
+                order2(d[2], c[2], d[3], c[3]);
+                order2(d[0], c[0], d[2], c[2]);
+                order2(d[1], c[1], d[3], c[3]);
+                order2(d[1], c[1], d[2], c[2]);
+                const int nv = (d[0] < CUDART_INF_F) + (d[1] < CUDART_INF_F) + (d[2] < CUDART_INF_F) +
+                               (d[3] < CUDART_INF_F);
+                if (nv == 0) {
+                  have = false;
+                } else if (sp + nv - 1 > kStack) {
                   err |= TWOS_DEVERR_STACK;
                   found = false;
                   phase = kStep;
                 } else {
-                  stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
-                  ++sp;
-                  node = cl;
+                  if (nv > 3) stack[(sp++) * BLOCK] = make_uint2(static_cast<uint32_t>(c[3]), __float_as_uint(d[3]));
+                  if (nv > 2) stack[(sp++) * BLOCK] = make_uint2(static_cast<uint32_t>(c[2]), __float_as_uint(d[2]));
+                  if (nv > 1) stack[(sp++) * BLOCK] = make_uint2(static_cast<uint32_t>(c[1]), __float_as_uint(d[1]));
+                  node = c[0];
                 }
-              } else if (vl) {
-                node = cl;
-              } else if (vr) {
-                node = cr;
-              } else {
-                have = false;
+              }
+            } else {
+              if (node >= 0) {
+                ++c_nodes;
+                T dl, dr;
+                int cl, cr;
+                node_dist2(geo_nodes<T>(G), node, pos, dl, dr, cl, cr);
+                const bool vl = dl < best2, vr = dr < best2;
+                if (vl && vr) {
+                  if (dr < dl) {
+                    const T td = dl;
+                    dl = dr;
+                    dr = td;
+                    const int tc = cl;
+                    cl = cr;
+                    cr = tc;
+                  }
+                  if (sp >= kStack) {
+                    err |= TWOS_DEVERR_STACK;
+                    found = false;
+                    phase = kStep;
+                  } else {
+                    stack[sp * BLOCK] = make_uint2(static_cast<uint32_t>(cr), __float_as_uint(lower_f(dr)));
+                    ++sp;
+                    node = cl;
+                  }
+                } else if (vl) {
+                  node = cl;
+                } else if (vr) {
+                  node = cr;
+                } else {
+                  have = false;
+                }
               }
             }
             // A leaf reached by this unit's visit or pop: its triangle range
@@ -1179,7 +1244,18 @@ template <typename T, int MODE, int BLOCK> static const void *select_src(int src
   return wos_fn<T, MODE, TWOS_SOURCE_CENTER, BLOCK>();
 }
 
-template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src, int grid64) {
+template <int MODE, int BLOCK> static const void *select_wide_src(int src) {
+  if (src == TWOS_SOURCE_GREEN)
+    return reinterpret_cast<const void *>(&wos_kernel<float, MODE, TWOS_SOURCE_GREEN, BLOCK, false, false, true>);
+  return reinterpret_cast<const void *>(&wos_kernel<float, MODE, TWOS_SOURCE_CENTER, BLOCK, false, false, true>);
+}
+
+template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src, int grid64, int wide) {
+  if (wide && precision == TWOS_PREC_MIXED && (src == TWOS_SOURCE_CENTER || src == TWOS_SOURCE_GREEN)) {
+    if (mode == TWOS_MODE_COMPLIANCE) return select_wide_src<TWOS_MODE_COMPLIANCE, BLOCK>(src);
+    if (mode == TWOS_MODE_PAIRED) return select_wide_src<TWOS_MODE_PAIRED, BLOCK>(src);
+    if (mode == TWOS_MODE_HOT) return select_wide_src<TWOS_MODE_HOT, BLOCK>(src);
+  }
   if (grid64 && precision == TWOS_PREC_FP64 && mode == TWOS_MODE_COMPLIANCE && src == TWOS_SOURCE_CENTER)
     return reinterpret_cast<const void *>(
         &wos_kernel<double, TWOS_MODE_COMPLIANCE, TWOS_SOURCE_CENTER, BLOCK, false, true>);
@@ -1199,14 +1275,14 @@ template <int BLOCK> static const void *select_wos_block(int precision, int mode
 }
 
 // Walk kernel instantiations: block sizes 128, 256 and 512 threads.
-static const void *select_wos(int precision, int mode, int src, int block, int grid64) {
+static const void *select_wos(int precision, int mode, int src, int block, int grid64, int wide) {
   switch (block) {
     case 128:
-      return select_wos_block<128>(precision, mode, src, grid64);
+      return select_wos_block<128>(precision, mode, src, grid64, wide);
     case 256:
-      return select_wos_block<256>(precision, mode, src, grid64);
+      return select_wos_block<256>(precision, mode, src, grid64, wide);
     case 512:
-      return select_wos_block<512>(precision, mode, src, grid64);
+      return select_wos_block<512>(precision, mode, src, grid64, wide);
     default:
       return nullptr;
   }
@@ -1238,7 +1314,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
   if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
   if (dyn > 200 * 1024) return cudaErrorInvalidValue;
-  const void *fn = select_wos(precision, mode, src, block, L.grid64);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide);
   if (!fn) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
@@ -1249,7 +1325,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
 
 int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L) {
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
-  const void *fn = select_wos(precision, mode, src, block, L.grid64);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide);
   if (!fn || dyn > 200 * 1024) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;

@@ -154,6 +154,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.units = m->units;
     L.entry = m->entry_start;
     L.grid64 = m->grid_fp64;
+    L.wide = m->bvh_width == 4;
     L.counters = totals + 3;
     L.site_best2 = base + lay.first;
     L.total_sites = n_sites;

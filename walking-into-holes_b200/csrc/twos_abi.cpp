@@ -144,6 +144,14 @@ void build_entry_table(twos_mesh *m) {
   m->entry.reserve(table.size() * sizeof(int32_t));
   check(cudaMemcpy(m->entry.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
   g.entry = m->entry.as<int32_t>();
+  // The same entries as four-wide nodes: the node holding each binary one.
+  std::vector<int32_t> table4(table.size());
+  for (size_t i = 0; i < table.size(); ++i) table4[i] = m->cover4[static_cast<size_t>(table[i])];
+  m->entry4.reserve(table4.size() * sizeof(int32_t));
+  check(cudaMemcpy(m->entry4.ptr, table4.data(), table4.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+        "upload");
+  g.entry4 = m->entry4.as<int32_t>();
+  m->resident_bytes += table4.size() * sizeof(int32_t);
   g.entry_shift = shift;
   g.entry_radius = static_cast<float>(cell);
   m->resident_bytes += table.size() * sizeof(int32_t);
@@ -193,6 +201,8 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     std::vector<NodeD> nd;
     std::vector<TriD> td;
     pack_bvh_f32(m->bvh, m->vertices, m->faces, m->center, nf, tf);
+    std::vector<Node4F> n4;
+    pack_bvh4_f32(m->bvh, nf, n4, m->cover4);
     pack_bvh_f64(m->bvh, m->vertices, m->faces, nd, td);
     check(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     m->stream = m->own_stream;
@@ -204,13 +214,17 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     m->nodes_d.reserve(nd.size() * sizeof(NodeD));
     m->tris_d.reserve(td.size() * sizeof(TriD));
     check(cudaMemcpy(m->nodes_f.ptr, nf.data(), nf.size() * sizeof(NodeF), cudaMemcpyHostToDevice), "upload");
+    m->nodes4_f.reserve(n4.size() * sizeof(Node4F));
+    check(cudaMemcpy(m->nodes4_f.ptr, n4.data(), n4.size() * sizeof(Node4F), cudaMemcpyHostToDevice), "upload");
     check(cudaMemcpy(m->tris_f.ptr, tf.data(), tf.size() * sizeof(TriF), cudaMemcpyHostToDevice), "upload");
     check(cudaMemcpy(m->nodes_d.ptr, nd.data(), nd.size() * sizeof(NodeD), cudaMemcpyHostToDevice), "upload");
     check(cudaMemcpy(m->tris_d.ptr, td.data(), td.size() * sizeof(TriD), cudaMemcpyHostToDevice), "upload");
-    m->resident_bytes = nf.size() * sizeof(NodeF) + tf.size() * sizeof(TriF) + nd.size() * sizeof(NodeD) +
+    m->resident_bytes = nf.size() * sizeof(NodeF) + n4.size() * sizeof(Node4F) + tf.size() * sizeof(TriF) +
+                        nd.size() * sizeof(NodeD) +
                         td.size() * sizeof(TriD);
     GeoDesc &g = m->geo_host;
     g.nodes_f = m->nodes_f.as<NodeF>();
+    g.nodes4_f = m->nodes4_f.as<Node4F>();
     g.tris_f = m->tris_f.as<TriF>();
     g.nodes_d = m->nodes_d.as<NodeD>();
     g.tris_d = m->tris_d.as<TriD>();
@@ -233,6 +247,7 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
     if (const char *e = std::getenv("TWOS_ENTRY")) m->entry_start = std::atoi(e) != 0;
+    if (const char *e = std::getenv("TWOS_BVH_WIDTH")) m->bvh_width = std::atoi(e) == 4 ? 4 : 2;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
       const int b = std::atoi(e);
       if (b == 128 || b == 256 || b == 512) m->block = b;
@@ -443,6 +458,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.units = m->units;
   L.entry = m->entry_start;
   L.grid64 = m->grid_fp64;
+  L.wide = m->bvh_width == 4;
   L.counters = m->totals.as<unsigned long long>() + 3;
   L.site_best2 = m->first.ptr;
   L.total_sites = site_total;
@@ -598,7 +614,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
-                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad})
+                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->entry4})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -621,7 +637,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
       t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1) ||
-      (t->grid_fp64 != 0 && t->grid_fp64 != 1))
+      (t->grid_fp64 != 0 && t->grid_fp64 != 1) || (t->bvh_width != 2 && t->bvh_width != 4))
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -631,6 +647,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->units = t->units;
   m->entry_start = t->entry;
   m->grid_fp64 = t->grid_fp64;
+  m->bvh_width = t->bvh_width;
   return TWOS_OK;
 }
 
@@ -644,6 +661,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->units = m->units;
   t->entry = m->entry_start;
   t->grid_fp64 = m->grid_fp64;
+  t->bvh_width = m->bvh_width;
   return TWOS_OK;
 }
 
@@ -979,6 +997,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.units = m->units;
     Ls.entry = m->entry_start;
     Ls.grid64 = m->grid_fp64;
+    Ls.wide = m->bvh_width == 4;
     Ls.counters = m->totals.as<unsigned long long>() + 3;
     m->first.reserve(static_cast<size_t>(n) * sizeof(double));
     first_v.reserve(static_cast<size_t>(k) * sizeof(double));
@@ -1555,6 +1574,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.units = m->units;
         L.entry = m->entry_start;
         L.grid64 = m->grid_fp64;
+        L.wide = m->bvh_width == 4;
         L.counters = m->totals.as<unsigned long long>() + 3;
         L.site_best2 = nullptr;
         L.total_sites = count;

@@ -36,6 +36,19 @@ struct alignas(32) NodeF {
 };
 static_assert(sizeof(NodeF) == 96, "NodeF layout");
 
+// Four-wide FP32 node (the mixed form's BVH width 4, collapsed from the
+// binary BVH: a node's slots are its binary children, each internal child
+// replaced by its own two children): 192 bytes, six 32-byte loads.  Slot c
+// of every float4 is child c: box lo/hi per axis, normal slab (n, smin,
+// smax), child code as in the binary layout.  An empty slot has an inverted
+// box and n = 0, so it is never entered.
+struct alignas(32) Node4F {
+  float4 xlo, xhi, ylo, yhi, zlo, zhi;
+  float4 nx, ny, nz, smin, smax;
+  int4 child;
+};
+static_assert(sizeof(Node4F) == 192, "Node4F layout");
+
 // FP64 node: 192 bytes.  lo/hi pairs (left, right) per axis, slabs, children.
 struct alignas(16) NodeD {
   double2 xlo, xhi, ylo, yhi, zlo, zhi;
@@ -91,6 +104,12 @@ void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &vertices, const
 std::vector<int32_t> build_entry_table(const HostBvh &bvh, const double origin[3], double cell, const uint32_t dims[3],
                                        double radius, double pad);
 
+// The four-wide FP32 BVH collapsed from the packed binary one; cover[n] is,
+// for every binary node n, the four-wide node whose subtree is n's or holds
+// it (n's own node, or its parent's when n was absorbed into it).
+void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::vector<Node4F> &nodes4,
+                   std::vector<int32_t> &cover);
+
 // Host ray-parity membership over the host BVH (EmbreeMesh::inside).
 int inside_parity(const HostBvh &bvh, const std::vector<double> &vertices, const std::vector<uint32_t> &faces,
                   const double p[3], bool &inside, std::string &err);
@@ -104,6 +123,7 @@ std::vector<double> read_points(const std::string &path);
 // One geometry resident on the device.
 struct GeoDesc {
   const NodeF *nodes_f;
+  const Node4F *nodes4_f;  // the same BVH four wide (mixed form, bvh_width 4)
   const TriF *tris_f;
   const NodeD *nodes_d;
   const TriD *tris_d;
@@ -124,6 +144,7 @@ struct GeoDesc {
   // is below entry_radius (every triangle outside that node's subtree is
   // farther).
   const int32_t *entry;
+  const int32_t *entry4;  // the same table in four-wide node indices
   uint32_t entry_shift;  // an entry cell spans 2^entry_shift grid cells per axis
   uint32_t entry_n[3];
   float entry_radius;
@@ -212,6 +233,9 @@ struct WosLaunch {
   // FP64 compliance form with the mixed form's distance grid and entry nodes
   // (a comparison of precision alone; off for the plain FP64 form).
   int grid64;
+  // Mixed form: traverse the four-wide BVH (compliance, paired and hot
+  // modes with the centre or Green-point source; others stay binary).
+  int wide;
   // Optional record of every grid step (tests): position in the FP32 frame
   // and the bound used, at most trace_cap records; trace_count counts all.
   float4 *trace;

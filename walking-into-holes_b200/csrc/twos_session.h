@@ -72,6 +72,8 @@ struct twos_mesh {
   twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
   twos::DevBuf grid;   // distance-bound grid (uint16 per vertex), may be empty
   twos::DevBuf entry;  // entry-node table of the mixed form's queries, may be empty
+  twos::DevBuf nodes4_f, entry4;  // the four-wide BVH and its entry table (mixed form)
+  std::vector<int32_t> cover4;    // binary node -> four-wide node holding its subtree
   twos::DevBuf geo;  // one GeoDesc
   twos::GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
@@ -89,4 +91,5 @@ struct twos_mesh {
   int units = 8;           // traversal units per lane per warp-loop iteration
   int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
   int grid_fp64 = 0;       // 1: the FP64 compliance form uses the grid and entry nodes too
+  int bvh_width = 2;       // mixed form: 2 (binary) or 4 (four-wide) BVH traversal
 };

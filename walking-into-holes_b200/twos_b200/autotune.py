@@ -12,6 +12,8 @@ the workload's own request with fewer walks) for every candidate setting of
 * traversal units a lane runs per iteration of the warp loop;
 * the mixed form's entry-node start (a query whose initial bound is below one
   entry cell starts at the cell's entry node instead of the BVH root);
+* the mixed form's BVH width: the binary BVH or the same BVH collapsed to
+  four-wide nodes;
 
 and leaves the fastest (walk-kernel device time per walk: every setting runs
 the same walks, and only the grid threshold changes how many steps they
@@ -35,6 +37,7 @@ DEFAULT_GRID = {
     "grid_threshold": (0.1, 0.25),
     "units": (4, 8, 16),
     "entry": (0, 1),
+    "bvh_width": (2, 4),
 }
 
 
