@@ -117,6 +117,26 @@ def main(reference: Path) -> None:
         (dst / "argv.json").write_text(json.dumps(keep, indent=1, sort_keys=True) + "\n")
     minimum_benefit(reference, out)
     controlled_experiments(reference, out)
+    sampling_study(reference, out)
+
+
+def sampling_study(reference: Path, out: Path) -> None:
+    """Per-site TD estimates of the 2D sampling study (benchmarks/
+    critical_baselines/sampling.py; output/sampling_fields.csv): repetition
+    0 at 64 walks and repetition 1 at 256 walks, both domains, every method."""
+    import csv
+    dst = out / "critical_baselines"
+    dst.mkdir(exist_ok=True)
+    src = reference / "benchmarks/critical_baselines/output/sampling_fields.csv"
+    with open(src) as f, open(dst / "sampling_fields_subset.csv", "w", newline="") as g:
+        rows = csv.DictReader(f)
+        w = csv.DictWriter(g, fieldnames=rows.fieldnames)
+        w.writeheader()
+        for row in rows:
+            if (row["n"], row["rep"]) in (("64", "0"), ("256", "1")):
+                w.writerow(row)
+    shutil.copyfile(reference / "benchmarks/critical_baselines/output/sampling_manifest.json",
+                    dst / "sampling_manifest.json")
 
 
 def controlled_experiments(reference: Path, out: Path) -> None:
