@@ -268,6 +268,10 @@ typedef struct twos_tuning {
                             paired and hot modes with the centre or Green
                             source; the others stay binary).  Same minima,
                             same rows.  Default 2. */
+  int32_t lane_walks;    /* walks a lane claims from the work queue at once
+                            and runs one after another (1..64); every walk
+                            keeps its own counter stream, so the rows do not
+                            change.  Default 1. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);

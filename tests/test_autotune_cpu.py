@@ -42,21 +42,28 @@ class FakeMesh:
         # threshold adds steps (queries) but fewer seconds per walk.
         per_walk = (1.0 + 0.1 * abs(t["block"] - 256) / 128 + 0.05 * (t["step_threshold"] != 4)
                     + 0.02 * abs(t["units"] - 8) / 4 + 0.3 * t["grid_threshold"] + 0.01 * (t["refill"] != 1)
-                    + 0.1 * (t.get("entry", 1) != 1) + 0.05 * (t.get("bvh_width", 2) != 4))
+                    + 0.1 * (t.get("entry", 1) != 1) + 0.05 * (t.get("bvh_width", 2) != 4)
+                    + 0.03 * abs(t.get("lane_walks", 1) - 2))
         steps = paths * (30 if t["grid_threshold"] < 0.2 else 25)
         if cfg.repeat == 5000:  # the warm-up run is slow and must be ignored
             per_walk *= 100
         return None, {"walk_seconds": per_walk * paths * 1e-9, "paths": paths, "queries": steps + paths}
 
 
-def test_autotune_sweeps_every_setting_and_picks_the_fastest(tmp_path):
+SMALL_GRID = {"block": (128, 256), "refill": (1, 4), "step_threshold": (1, 4), "blocks_per_sm": (0,),
+              "grid_threshold": (0.1, 0.25), "units": (8,), "entry": (0, 1), "bvh_width": (2, 4),
+              "lane_walks": (1, 2)}
+
+
+def test_autotune_sweeps_a_small_grid_whole_and_picks_the_fastest(tmp_path):
     mesh = FakeMesh()
     sites = np.random.default_rng(0).normal(size=(10_000, 3))
     cache = tmp_path / "tuning.json"
-    best, results = autotune(mesh, sites, Cfg(), calib_sites=100, calib_walks=64, repeats=2, cache=cache)
-    assert len(results) == np.prod([len(v) for v in DEFAULT_GRID.values()])
+    best, results = autotune(mesh, sites, Cfg(), grid=SMALL_GRID, calib_sites=100, calib_walks=64, repeats=2,
+                             cache=cache)
+    assert len(results) == np.prod([len(v) for v in SMALL_GRID.values()])
     assert best == {"block": 256, "refill": 1, "step_threshold": 4, "blocks_per_sm": 0, "grid_threshold": 0.1,
-                    "units": 8, "entry": 1, "bvh_width": 4}
+                    "units": 8, "entry": 1, "bvh_width": 4, "lane_walks": 2}
     assert mesh.get_tuning() == best
     # Calibration: a seeded subset of the sites, the request's walks capped, one warm-up plus two timed runs.
     assert all(n == 100 and w == 64 for _, w, _, n in mesh.calls)
@@ -69,6 +76,33 @@ def test_autotune_sweeps_every_setting_and_picks_the_fastest(tmp_path):
     assert again == best and cached == [] and mesh2.calls == [] and mesh2.get_tuning() == best
     # Another precision is another key.
     mesh3 = FakeMesh()
-    _, res3 = autotune(mesh3, sites, Cfg(precision="fp64"), calib_sites=50, calib_walks=32, repeats=1,
-                       cache=cache)
+    _, res3 = autotune(mesh3, sites, Cfg(precision="fp64"), grid=SMALL_GRID, calib_sites=50, calib_walks=32,
+                       repeats=1, cache=cache)
     assert res3 and len(json.loads(cache.read_text())) == 2
+
+
+def test_autotune_descends_the_default_grid_to_the_separable_optimum():
+    """Coordinate descent over the default grid (864 settings) from the
+    mesh's current tuning: the stand-in cost is separable, so descent reaches
+    the grid's optimum, timing each setting once; the default sweeps the grid
+    whole and agrees."""
+    full = int(np.prod([len(v) for v in DEFAULT_GRID.values()]))
+    assert full == 864
+    mesh = FakeMesh(tuning={"block": 128, "refill": 4, "step_threshold": 1, "blocks_per_sm": 0,
+                            "grid_threshold": 0.25, "units": 4, "entry": 0, "bvh_width": 2, "lane_walks": 1})
+    sites = np.random.default_rng(1).normal(size=(1000, 3))
+    best, results = autotune(mesh, sites, Cfg(), calib_sites=100, calib_walks=64, repeats=1, search="descent")
+    assert best == {"block": 256, "refill": 1, "step_threshold": 4, "blocks_per_sm": 0, "grid_threshold": 0.1,
+                    "units": 8, "entry": 1, "bvh_width": 4, "lane_walks": 2}
+    keys = [tuple(sorted(t.items())) for t, _ in results]
+    assert len(set(keys)) == len(keys) and len(keys) < 64
+    # The exhaustive sweep of the same grid agrees.
+    mesh2 = FakeMesh()
+    best2, results2 = autotune(mesh2, sites, Cfg(), calib_sites=20, calib_walks=8, repeats=1)
+    assert best2 == best and len(results2) == full
+
+
+def test_autotune_rejects_an_unknown_search():
+    import pytest
+    with pytest.raises(ValueError):
+        autotune(FakeMesh(), np.zeros((4, 3)), Cfg(), search="random")

@@ -25,7 +25,7 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
             mesh.set_tuning(block=block, refill=refill, step_threshold=step, blocks_per_sm=bps)
             assert mesh.get_tuning() == {"block": block, "refill": refill, "step_threshold": step,
                                          "blocks_per_sm": bps, "grid_threshold": 0.1, "units": 8, "entry": 1,
-                                         "grid_fp64": 0, "bvh_width": 2}
+                                         "grid_fp64": 0, "bvh_width": 2, "lane_walks": 1}
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} {block} {refill} {step} {bps}")
@@ -35,8 +35,11 @@ def test_every_tuning_gives_identical_rows(tb, bunny1000, eval_points, precision
             for k in ("u", "score", "score_se", "steps"):
                 np.testing.assert_array_equal(out[k], ref[k], err_msg=f"{k} units={units}")
         # The entry-node start and the BVH width change how a query's
-        # traversal runs, never its minimum.
-        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0), dict(bvh_width=4, units=3)):
+        # traversal runs, never its minimum; walks per lane only which lane
+        # runs a walk.
+        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0), dict(bvh_width=4, units=3),
+                        dict(lane_walks=2), dict(lane_walks=4, refill=8), dict(lane_walks=64, block=512),
+                        dict(lane_walks=3, bvh_width=4)):
             mesh.set_tuning(**variant)
             out, _ = mesh.estimate(eval_points, cfg)
             for k in ("u", "score", "score_se", "steps"):
@@ -48,7 +51,7 @@ def test_invalid_tuning_is_usage_error(tb, bunny1000):
         for bad in [dict(block=96), dict(refill=0), dict(step_threshold=33), dict(blocks_per_sm=-1),
                     dict(grid_threshold=0.05), dict(grid_threshold=-1.0), dict(grid_threshold=float("nan")),
                     dict(units=0), dict(units=65), dict(entry=2), dict(grid_fp64=3),
-                    dict(bvh_width=3)]:
+                    dict(bvh_width=3), dict(lane_walks=0), dict(lane_walks=65)]:
             with pytest.raises(tb.TwosError) as e:
                 mesh.set_tuning(**bad)
             assert e.value.code == 2
@@ -61,7 +64,10 @@ def test_autotuner_picks_a_grid_point(tb, bunny1000, eval_points, tmp_path):
     with tb.Mesh(*bunny1000) as mesh:
         best, results = autotune(mesh, eval_points, cfg, calib_sites=256, calib_walks=64, repeats=1, cache=cache)
         assert mesh.get_tuning() == best
+        # The default grid is swept whole, each setting once.
+        assert len({tuple(sorted(t.items())) for t, _ in results}) == len(results)
         assert len(results) == np.prod([len(v) for v in DEFAULT_GRID.values()])
+        assert all(best[k] in v for k, v in DEFAULT_GRID.items())
         assert all(t > 0 for _, t in results)
         again, cached = autotune(mesh, eval_points, cfg, cache=cache)
         assert again == best and cached == []

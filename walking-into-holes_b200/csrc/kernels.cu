@@ -658,6 +658,11 @@ constexpr int wos_min_blocks(int block) {
                                                                               : 768 / block;
 }
 
+// Walks a lane claims from the work queue at once.
+__device__ __forceinline__ uint32_t lane_walks_of(const WosLaunch &L) {
+  return L.lane_walks > 1 ? static_cast<uint32_t>(L.lane_walks) : 1u;
+}
+
 template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false, bool WIDE = false>
 __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
@@ -720,24 +725,48 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
   T best2 = T(0);
   int node = 0, sp = 0;
   bool have = false, found = false;
+  // Four-wide form: this query continues on the binary BVH (set when a
+  // four-wide visit would overflow the stack).
+  bool narrow = false;
   uint32_t best_tri = 0;  // leaf-order index of the nearest triangle found for this walk
   bool tri_ok = false;    // best_tri belongs to this walk
   uint32_t tri_cur = 0, tri_end = 0, iter = 0;
+  // Walks a lane claims from the queue at once (run one after another):
+  // s_claim[thread] of them, wid + 1 onwards, are not yet started.  The count
+  // lives in shared memory, read only at refills, so it holds no register
+  // through the traversal.
+  // (The claim size is re-read from the launch parameters where used, so it
+  // holds no register either.)
+  __shared__ uint32_t s_claim[BLOCK];
+  s_claim[threadIdx.x] = 0u;
 
   for (;;) {
-    // ---- refill idle lanes from the work queue
+    // ---- refill idle lanes from their claims and the work queue
     const unsigned idle = __ballot_sync(full, phase == kIdle);
-    if (!exhausted && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
-      unsigned long long base = 0;
-      const int leader = __ffs(idle) - 1;
-      if (static_cast<int>(lane) == leader)
-        base = atomicAdd(L.counter, static_cast<unsigned long long>(__popc(idle)));
-      base = __shfl_sync(full, base, leader);
-      if (base + __popc(idle) >= L.total_walks) exhausted = true;
+    const unsigned pending = (L.lane_walks > 1) ? __ballot_sync(full, s_claim[threadIdx.x] != 0u) : 0u;
+    if ((!exhausted || pending != 0u) && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
+      uint32_t claim_left = (L.lane_walks > 1) ? s_claim[threadIdx.x] : 0u;
+      const unsigned claim = __ballot_sync(full, phase == kIdle && claim_left == 0u);
+      if (!exhausted && claim != 0u) {
+        const uint64_t span = static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim);
+        unsigned long long base = 0;
+        const int leader = __ffs(claim) - 1;
+        if (static_cast<int>(lane) == leader) base = atomicAdd(L.counter, static_cast<unsigned long long>(span));
+        base = __shfl_sync(full, base, leader);
+        if (base + span >= L.total_walks) exhausted = true;
+        if (phase == kIdle && claim_left == 0u) {
+          const uint64_t first = base + static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim & ((1u << lane) - 1u));
+          if (first < L.total_walks) {
+            wid = first - 1;  // wraps for the first walk of the queue; wid + 1 is exact
+            const uint64_t left = L.total_walks - first;
+            claim_left = left < lane_walks_of(L) ? static_cast<uint32_t>(left) : lane_walks_of(L);
+          }
+        }
+      }
       if (phase == kIdle) {
-        const uint64_t id = base + __popc(idle & ((1u << lane) - 1u));
-        if (id < L.total_walks) {
-          wid = id;
+        if (claim_left != 0u) {
+          const uint64_t id = ++wid;
+          --claim_left;
           job = find_job(s_jobs, L.n_jobs, id);
           const JobDesc &J = s_jobs[job];
           const uint64_t local = id - J.walk_begin;
@@ -782,6 +811,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             node = 0;
             sp = 0;
             have = true;
+            narrow = false;
             found = false;
             tri_cur = tri_end = 0;
             iter = 0;
@@ -789,6 +819,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           }
         }
       }
+      if ((L.lane_walks > 1)) s_claim[threadIdx.x] = claim_left;
     }
 
     // ---- batched walk step for lanes whose query has finished
@@ -1041,6 +1072,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
         }
         sp = 0;
         have = true;
+        narrow = false;
         tri_cur = tri_end = 0;
         iter = 0;
         phase = kTraverse;
@@ -1049,7 +1081,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
     }
 
     if (__ballot_sync(full, phase != kIdle) == 0u) {
-      if (exhausted) break;
+      if (exhausted && (!(L.lane_walks > 1) || __ballot_sync(full, s_claim[threadIdx.x] != 0u) == 0u)) break;
       continue;
     }
 
@@ -1098,7 +1130,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             phase = kStep;
           } else {
             if constexpr (WIDE) {
-              if (node >= 0) {
+              if (node >= 0 && !narrow) {
                 // Four-wide node: its valid children sorted nearest first (a
                 // five-comparator network); the nearest is next, the others
                 // are pushed farthest first.
@@ -1119,9 +1151,14 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
                 if (nv == 0) {
                   have = false;
                 } else if (sp + nv - 1 > kStack) {
-                  err |= TWOS_DEVERR_STACK;
-                  found = false;
-                  phase = kStep;
+                  // Up to three pushes per level can outgrow the stack on a
+                  // root-started query with a loose bound.  The query goes
+                  // on from the binary root with the bound found so far
+                  // (one push per level there): every triangle nearer than
+                  // best2 is still reached.
+                  narrow = true;
+                  sp = 0;
+                  node = 0;
                 } else {
                   if (nv > 3) stack[(sp++) * BLOCK] = make_uint2(static_cast<uint32_t>(c[3]), __float_as_uint(d[3]));
                   if (nv > 2) stack[(sp++) * BLOCK] = make_uint2(static_cast<uint32_t>(c[2]), __float_as_uint(d[2]));
@@ -1129,7 +1166,8 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
                   node = c[0];
                 }
               }
-            } else {
+            }
+            if (!WIDE || narrow) {
               if (node >= 0) {
                 ++c_nodes;
                 T dl, dr;

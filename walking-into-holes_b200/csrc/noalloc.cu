@@ -152,6 +152,7 @@ extern "C" int twos_estimate_noalloc(twos_mesh *m, const twos_request *r, const 
     L.warm = m->warm;
     L.grid_tau = m->grid_tau;
     L.units = m->units;
+    L.lane_walks = m->lane_walks;
     L.entry = m->entry_start;
     L.grid64 = m->grid_fp64;
     L.wide = m->bvh_width == 4;

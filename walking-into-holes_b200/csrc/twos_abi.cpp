@@ -246,6 +246,7 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_VOTE")) m->vote = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
+    if (const char *e = std::getenv("TWOS_LANE_WALKS")) m->lane_walks = std::min(64, std::max(1, std::atoi(e)));
     if (const char *e = std::getenv("TWOS_ENTRY")) m->entry_start = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_BVH_WIDTH")) m->bvh_width = std::atoi(e) == 4 ? 4 : 2;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
@@ -456,6 +457,7 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
   L.warm = m->warm;
   L.grid_tau = m->grid_tau;
   L.units = m->units;
+  L.lane_walks = m->lane_walks;
   L.entry = m->entry_start;
   L.grid64 = m->grid_fp64;
   L.wide = m->bvh_width == 4;
@@ -637,7 +639,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
       t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1) ||
-      (t->grid_fp64 != 0 && t->grid_fp64 != 1) || (t->bvh_width != 2 && t->bvh_width != 4))
+      (t->grid_fp64 != 0 && t->grid_fp64 != 1) || (t->bvh_width != 2 && t->bvh_width != 4) || t->lane_walks < 1 || t->lane_walks > 64)
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -648,6 +650,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->entry_start = t->entry;
   m->grid_fp64 = t->grid_fp64;
   m->bvh_width = t->bvh_width;
+  m->lane_walks = t->lane_walks;
   return TWOS_OK;
 }
 
@@ -662,6 +665,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->entry = m->entry_start;
   t->grid_fp64 = m->grid_fp64;
   t->bvh_width = m->bvh_width;
+  t->lane_walks = m->lane_walks;
   return TWOS_OK;
 }
 
@@ -995,6 +999,7 @@ int twos_design_loop(twos_mesh *m, const twos_request *scout, const twos_request
     Ls.warm = m->warm;
     Ls.grid_tau = m->grid_tau;
     Ls.units = m->units;
+    Ls.lane_walks = m->lane_walks;
     Ls.entry = m->entry_start;
     Ls.grid64 = m->grid_fp64;
     Ls.wide = m->bvh_width == 4;
@@ -1572,6 +1577,7 @@ int twos_diffwos(twos_mesh *m, const twos_request *r, double diff_offset, int en
         L.warm = m->warm;
         L.grid_tau = m->grid_tau;
         L.units = m->units;
+        L.lane_walks = m->lane_walks;
         L.entry = m->entry_start;
         L.grid64 = m->grid_fp64;
         L.wide = m->bvh_width == 4;

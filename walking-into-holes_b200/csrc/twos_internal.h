@@ -228,6 +228,9 @@ struct WosLaunch {
   // Traversal units (node visits / triangle tests) a lane runs back to back
   // per iteration of the warp loop (>= 1).
   int units;
+  // Walks a lane claims from the work queue at once and runs one after
+  // another (>= 1).
+  int lane_walks;
   // Mixed form: whether a query may start at the entry-node table's node.
   int entry;
   // FP64 compliance form with the mixed form's distance grid and entry nodes

@@ -89,6 +89,7 @@ struct twos_mesh {
   int warm = 1;            // 1: seed each step's query with the previous nearest triangle
   float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
+  int lane_walks = 1;      // walks a lane claims from the queue at once
   int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
   int grid_fp64 = 0;       // 1: the FP64 compliance form uses the grid and entry nodes too
   int bvh_width = 2;       // mixed form: 2 (binary) or 4 (four-wide) BVH traversal

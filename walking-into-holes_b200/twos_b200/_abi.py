@@ -88,7 +88,8 @@ class MeshInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("refill", ctypes.c_int32), ("step_threshold", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("grid_threshold", ctypes.c_float), ("units", ctypes.c_int32),
-                ("entry", ctypes.c_int32), ("grid_fp64", ctypes.c_int32), ("bvh_width", ctypes.c_int32)]
+                ("entry", ctypes.c_int32), ("grid_fp64", ctypes.c_int32), ("bvh_width", ctypes.c_int32),
+                ("lane_walks", ctypes.c_int32)]
 
 
 class DesignParams(ctypes.Structure):

@@ -14,11 +14,18 @@ the workload's own request with fewer walks) for every candidate setting of
   entry cell starts at the cell's entry node instead of the BVH root);
 * the mixed form's BVH width: the binary BVH or the same BVH collapsed to
   four-wide nodes;
+* walks per lane: walks a lane claims from the work queue at once;
 
 and leaves the fastest (walk-kernel device time per walk: every setting runs
 the same walks, and only the grid threshold changes how many steps they
-take) set on the mesh.  Results can be cached in a JSON file keyed by the mesh's size and
-the request's precision/mode, so a service tunes once per geometry class.
+take) set on the mesh.  A grid of at most `max_grid` settings (the default
+grid has 864, a few seconds of calibration runs) is swept whole, since the
+axes interact (the step threshold and the traversal units above all); a
+larger one by coordinate descent: from the mesh's current tuning, each axis
+in turn takes its fastest value with the others held, until a pass over all
+axes changes nothing.  Results can be
+cached in a JSON file keyed by the mesh's size and the request's
+precision/mode, so a service tunes once per geometry class.
 """
 from __future__ import annotations
 
@@ -38,6 +45,7 @@ DEFAULT_GRID = {
     "units": (4, 8, 16),
     "entry": (0, 1),
     "bvh_width": (2, 4),
+    "lane_walks": (1, 2, 4),
 }
 
 
@@ -47,9 +55,11 @@ def _key(mesh, config) -> str:
 
 
 def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, repeats=2, seed=0,
-             cache: str | Path | None = None, cavities=None):
+             cache: str | Path | None = None, cavities=None, search="auto", max_grid=1024, max_passes=4):
     """Pick the fastest launch tuning for `config` on `mesh`; returns
-    (best tuning dict, list of (tuning, seconds per walk))."""
+    (best tuning dict, list of (tuning, seconds per walk) for every setting
+    timed).  search: "grid" sweeps every setting, "descent" runs coordinate
+    descent, "auto" sweeps grids of at most max_grid settings."""
     key = _key(mesh, config)
     if cache is not None and Path(cache).exists():
         table = json.loads(Path(cache).read_text())
@@ -57,13 +67,19 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
             mesh.set_tuning(**table[key])
             return table[key], []
     grid = grid or DEFAULT_GRID
+    if search not in ("auto", "grid", "descent"):
+        raise ValueError(f"unknown search {search!r}")
     sites = np.asarray(sites, dtype=np.float64).reshape(-1, 3)
     rng = np.random.default_rng(seed)
     pick = sites[rng.choice(len(sites), size=min(calib_sites, len(sites)), replace=False)]
     calib = replace(config, walks=min(config.walks, calib_walks))
-    results = []
     names = list(grid)
-    for values in itertools.product(*(grid[n] for n in names)):
+    results = []
+    timed = {}
+
+    def measure(values):
+        if values in timed:
+            return timed[values]
         tuning = dict(zip(names, values))
         mesh.set_tuning(**tuning)
         times = []
@@ -72,7 +88,27 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
             _, s = mesh.estimate(pick, calib, cavities=cavities)
             if r:  # the first run is a warm-up
                 times.append(s["walk_seconds"] / max(1, s["paths"]))
-        results.append((tuning, float(np.median(times))))
+        timed[values] = float(np.median(times))
+        results.append((tuning, timed[values]))
+        return timed[values]
+
+    size = int(np.prod([len(grid[n]) for n in names]))
+    if search == "grid" or (search == "auto" and size <= max_grid):
+        for values in itertools.product(*(grid[n] for n in names)):
+            measure(values)
+    else:
+        start = mesh.get_tuning()
+        current = [start[n] if start.get(n) in grid[n] else grid[n][0] for n in names]
+        for _ in range(max_passes):
+            moved = False
+            for i, n in enumerate(names):
+                best_v = min(grid[n], key=lambda v: (measure(tuple(current[:i] + [v] + current[i + 1:])),
+                                                     v != current[i]))
+                if best_v != current[i]:
+                    current[i] = best_v
+                    moved = True
+            if not moved:
+                break
     best = min(results, key=lambda t: t[1])[0]
     mesh.set_tuning(**best)
     best = mesh.get_tuning()

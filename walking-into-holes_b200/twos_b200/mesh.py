@@ -131,7 +131,7 @@ class Mesh:
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
     def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8,
-                   entry=1, grid_fp64=0, bvh_width=2):
+                   entry=1, grid_fp64=0, bvh_width=2, lane_walks=1):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
         closest-point query, 0 to query every step; units is the number of
@@ -139,9 +139,10 @@ class Mesh:
         qualifying mixed-form queries at the entry-node table's node;
         grid_fp64 1 gives the FP64 compliance form the grid and entry nodes
         too (a like-for-like comparison of precision); bvh_width 2 or 4 picks
-        the mixed form's binary or four-wide BVH traversal."""
+        the mixed form's binary or four-wide BVH traversal; lane_walks is the
+        number of walks a lane claims from the work queue at once."""
         t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold),
-                        int(units), int(entry), int(grid_fp64), int(bvh_width))
+                        int(units), int(entry), int(grid_fp64), int(bvh_width), int(lane_walks))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -151,7 +152,8 @@ class Mesh:
                 "blocks_per_sm": t.blocks_per_sm,
                 # The ABI keeps a float; report the shortest decimal that rounds to it (0.1, not 0.10000000149).
                 "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units,
-                "entry": t.entry, "grid_fp64": t.grid_fp64, "bvh_width": t.bvh_width}
+                "entry": t.entry, "grid_fp64": t.grid_fp64, "bvh_width": t.bvh_width,
+                "lane_walks": t.lane_walks}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
