@@ -269,9 +269,19 @@ typedef struct twos_tuning {
                             source; the others stay binary).  Same minima,
                             same rows.  Default 2. */
   int32_t lane_walks;    /* walks a lane claims from the work queue at once
-                            and runs one after another (1..64); every walk
-                            keeps its own counter stream, so the rows do not
-                            change.  Default 1. */
+                            and runs one after another (1..64): mixed form,
+                            centre-point source, compliance / paired / hot
+                            modes on the binary BVH (not with bvh_width 4);
+                            the other forms claim one.  Every walk keeps its
+                            own counter stream, so the rows do not change.
+                            Default 1. */
+  int32_t wavefront;     /* mixed form, centre-point source, compliance /
+                            paired / hot modes: 0 runs the persistent walk
+                            kernel; N > 0 (a multiple of 256, at most 2^26)
+                            runs the wavefront form with N walks in flight --
+                            a step kernel over all of them, then a query
+                            kernel over those whose next radius needs a BVH
+                            query, once per step.  Same rows.  Default 0. */
 } twos_tuning;
 
 int twos_mesh_set_tuning(twos_mesh *mesh, const twos_tuning *tuning);
@@ -486,6 +496,13 @@ int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const d
  * ratio r_y (r_y^2 - |x-y|^2) / |x - z|^3 (z the walk's first step point)
  * and each site y weighted by (1-a)^4 / (1+a)^2, a = |x-y| / r_y (reused_means,
  * sampling.py:76-88, in 3D; harmonic problems only: no request->source).
+ * SOBOL: Sobol-over-steps RQMC (sampling.py:49-60 in 3D): walk i of a
+ * (site, batch) holds point i of a Sobol' sequence scrambled once per
+ * (site, batch) (a random lower-triangular digit matrix and a digital shift
+ * per coordinate) and takes coordinates 2k and 2k + 1 at step k, for steps
+ * k < 256; later steps draw the MC stream.  The direction numbers come from
+ * the primitive polynomials over GF(2) in order, with seeded odd initial
+ * values (not the reference's scipy table).
  * A walk's payoff is request->source at each ball centre times r^2/6 plus
  * u_boundary (primal) or p_boundary (adjoint) at its exit point on the mesh.
  * The cross-fitting unit is a whole batch (an independent randomization):
@@ -493,7 +510,7 @@ int twos_estimate_gradient(twos_mesh *mesh, const twos_request *request, const d
  * td[site] = -(sum a sum b - sum ab) / (R (R - 1)) over the R batches
  * (crossfit, sampling.py:90-92).  Capped walks are an error (sampling.py:
  * 72-73).  No reference counterpart in the compiled backend. */
-enum { TWOS_RQMC_MC = 0, TWOS_RQMC_ARRAY = 1, TWOS_RQMC_NEIGHBOUR = 2 };
+enum { TWOS_RQMC_MC = 0, TWOS_RQMC_ARRAY = 1, TWOS_RQMC_NEIGHBOUR = 2, TWOS_RQMC_SOBOL = 3 };
 
 typedef struct twos_rqmc_params {
   int32_t method;    /* TWOS_RQMC_* */
@@ -528,6 +545,15 @@ int twos_trace_grid_steps(twos_mesh *mesh, const twos_request *request, const do
  * walk kernel's load form.  The roofline denominator for kernels whose
  * working set is L2-resident.  No reference counterpart (a measurement). */
 int twos_l2_read_gbs(int device, uint64_t bytes, uint32_t passes, double *gbs);
+
+/* The Sobol' direction numbers of twos_rqmc's SOBOL method, host only:
+ * out [dims][bits], out[d * bits + b] = m_{d,b+1} 2^(31-b) (most significant
+ * digit first).  Dimension 0 is van der Corput's; dimension d >= 1 takes the
+ * d-th primitive polynomial over GF(2) by degree, then coefficient bits,
+ * with odd initial values m_k < 2^k from SplitMix64 and Sobol's recurrence
+ * (the reference's study takes scipy's Joe-Kuo table instead,
+ * critical_baselines/sampling.py:53).  dims <= 65536, bits 1..32. */
+int twos_sobol_directions(uint32_t dims, uint32_t bits, uint32_t *out);
 
 /* The estimator's per-site reduction on caller-supplied per-walk samples:
  * u and p (p may be NULL outside paired mode) [n_sites][walks] as doubles,

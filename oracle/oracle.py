@@ -117,6 +117,8 @@ def lib():
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_sobol_directions.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_sobol_directions.restype = None
         L.oracle_neighbour_means.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32] + \
             [ctypes.c_void_p] * 6
         L.oracle_neighbour_means.restype = None
@@ -320,7 +322,8 @@ class OracleMesh:
 
     def rqmc(self, sites, method, batches, generator, u_boundary, p_boundary, record=False, **kw):
         """The GPU's lockstep Array-RQMC (method 1) / MC (method 0) / MC with
-        neighbour reuse (method 2) in the counter stream: (batch_u, batch_p
+        neighbour reuse (method 2) / Sobol-over-steps RQMC (method 3) in the
+        counter stream: (batch_u, batch_p
         [batches, n_sites], steps, caps), plus the per-walk record dict
         (walk_first, walk_u, walk_p, site_radius) when record is true."""
         p = self._params(**kw)
@@ -336,7 +339,8 @@ class OracleMesh:
         rec = {"walk_first": np.zeros((batches, n, w, 3)), "walk_u": np.zeros((batches, n, w)),
                "walk_p": np.zeros((batches, n, w)), "site_radius": np.zeros(n)}
         keep = record or method == 2
-        rc = lib().oracle_rqmc(self.handle, ctypes.byref(p), 1 if method == 1 else 0, int(batches), int(generator),
+        rc = lib().oracle_rqmc(self.handle, ctypes.byref(p), method if method in (1, 3) else 0, int(batches),
+                               int(generator),
                                _ptr(lo), _ptr(hi), ctypes.cast(ub, ctypes.c_void_p), len(u_boundary),
                                ctypes.cast(pb, ctypes.c_void_p), len(p_boundary), _ptr(s), n, _ptr(bu), _ptr(bp),
                                _ptr(tot), *[_ptr(rec[k]) if keep else None for k in
@@ -497,6 +501,14 @@ def crossfit_square(samples):
     leave_mean = leave.mean(axis=1, keepdims=True)
     se = np.sqrt((n - 1) / n * np.sum((leave - leave_mean) ** 2, axis=1))
     return estimate, se
+
+
+def sobol_directions(dims, bits=10):
+    """The Sobol' direction numbers of twos_rqmc's SOBOL method, [dims, bits]
+    uint32 (most significant digit first): oracle_sobol_directions."""
+    out = np.zeros((int(dims), int(bits)), dtype=np.uint32)
+    lib().oracle_sobol_directions(int(dims), int(bits), out.ctypes.data)
+    return out
 
 
 def crossfit_product(a, b):

@@ -71,6 +71,28 @@ def hilbert2(z, bits=13):
     return h
 
 
+def own_sobol_points(n, dims, rng):
+    """n points of the Sobol' sequence of twos_rqmc's SOBOL method (the
+    oracle's direction numbers: primitive polynomials in order, seeded odd
+    initial values), scrambled as that method scrambles -- a random
+    lower-triangular digit matrix with unit diagonal and a digital shift per
+    coordinate -- with draws from `rng`: [n, dims] in (0, 1)."""
+    import oracle
+    bits = int(np.log2(n))
+    v = oracle.sobol_directions(dims, bits).astype(np.uint64)
+    r = np.arange(32, dtype=np.uint64)
+    rows = rng.integers(0, 2 ** 32, size=(dims, 32), dtype=np.uint64)
+    rows = (rows & ((np.uint64(0xffffffff) << (np.uint64(31) - r)) & np.uint64(0xffffffff))) | \
+        (np.uint64(1) << (np.uint64(31) - r))
+    parity = np.bitwise_count(rows[:, None, :] & v[:, :, None]) & 1
+    dirs = np.bitwise_or.reduce(parity.astype(np.uint64) << (np.uint64(31) - r), axis=-1)
+    x = np.broadcast_to(rng.integers(0, 2 ** 32, size=dims, dtype=np.uint64), (n, dims)).copy()
+    idx = np.arange(n)
+    for b in range(bits):
+        x[(idx >> b) & 1 == 1] ^= dirs[:, b]
+    return (x.astype(np.float64) + 0.5) / 2.0 ** 32
+
+
 def walk_batch(starts, n, seed, domain, method, eps=1e-7, cap=256):
     """n walks from each start; returns (first step points, exit points).
     The random draws follow the study's order exactly: one generator per
@@ -84,6 +106,8 @@ def walk_batch(starts, n, seed, domain, method, eps=1e-7, cap=256):
         m = int(np.log2(n))
         points = np.stack([qmc.Sobol(cap, scramble=True, seed=int(s)).random_base2(m)
                            for s in rng.integers(0, 2 ** 31 - 1, len(starts))])
+    elif method == "sobol_own":  # not in the study: the 3D method's sequence, one coordinate per step
+        points = np.stack([own_sobol_points(n, cap, rng) for _ in starts])
     lattice = (KOROBOV.get(n, 1) * np.arange(n)) % n / n if method == "array" else None
     for step in range(cap):
         r = boundary_distance(z, domain)
@@ -96,7 +120,7 @@ def walk_batch(starts, n, seed, domain, method, eps=1e-7, cap=256):
             shifted = (lattice[None, :] + rng.random((len(starts), 1))) % 1
             u = np.empty_like(shifted)
             np.put_along_axis(u, rank_order, shifted, axis=1)
-        elif method == "rqmc":
+        elif method in ("rqmc", "sobol_own"):
             u = points[:, :, step]
         else:
             u = rng.random(z.shape)

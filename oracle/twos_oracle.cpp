@@ -1650,11 +1650,84 @@ uint32_t oracle_hilbert3(uint32_t x, uint32_t y, uint32_t z) {
 
 }  // namespace
 
+namespace {
+
+// Sobol' direction numbers in the fixed-point form of Bratley and Fox (ACM
+// TOMS 14, 1988): V_k = m_k 2^(32-k), and beyond the degree s of the
+// dimension's polynomial x^s + a_1 x^(s-1) + ... + a_(s-1) x + 1,
+// V_k = a_1 V_(k-1) ^ ... ^ a_(s-1) V_(k-s+1) ^ V_(k-s) ^ (V_(k-s) >> s).
+// Dimension 0 is van der Corput's; dimension d >= 1 the d-th primitive
+// polynomial (by degree, then coefficient bits; primitivity by counting the
+// order of x directly), initial odd m_k < 2^k from SplitMix64 of
+// 0x536f626f6c2d3344 + 64 d + k.
+uint64_t oracle_splitmix(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+bool oracle_primitive(uint32_t p, int deg) {
+  // Powers of x modulo p until they return to 1.
+  const uint32_t top = 1u << deg, want = top - 1u;
+  uint32_t r = 1;
+  for (uint32_t e = 1; e <= want; ++e) {
+    r <<= 1;
+    if (r & top) r ^= p;
+    if (r == 1u) return e == want;
+  }
+  return false;
+}
+
+std::vector<uint32_t> oracle_sobol_table(uint32_t dims, uint32_t bits) {
+  std::vector<uint32_t> polys;
+  for (int deg = 1; polys.size() + 1 < dims; ++deg)
+    for (uint32_t p = (1u << deg) | 1u; p < (2u << deg) && polys.size() + 1 < dims; p += 2)
+      if (oracle_primitive(p, deg)) polys.push_back(p);
+  std::vector<uint32_t> out(static_cast<size_t>(dims) * bits);
+  for (uint32_t d = 0; d < dims; ++d) {
+    std::vector<uint32_t> V(bits + 1, 0u);
+    if (d == 0) {
+      for (uint32_t k = 1; k <= bits; ++k) V[k] = 1u << (32 - k);
+    } else {
+      const uint32_t p = polys[d - 1];
+      int s = 0;
+      while ((p >> (s + 1)) != 0u) ++s;
+      for (uint32_t k = 1; k <= bits; ++k) {
+        if (static_cast<int>(k) <= s) {
+          const uint64_t m = (oracle_splitmix(0x536f626f6c2d3344ull + 64ull * d + k) & ((1ull << k) - 1)) | 1ull;
+          V[k] = static_cast<uint32_t>(m << (32 - k));
+        } else {
+          uint32_t x = V[k - s] ^ (V[k - s] >> s);
+          for (int j = 1; j < s; ++j)
+            if ((p >> (s - j)) & 1u) x ^= V[k - j];
+          V[k] = x;
+        }
+      }
+    }
+    for (uint32_t b = 0; b < bits; ++b) out[static_cast<size_t>(d) * bits + b] = V[b + 1];
+  }
+  return out;
+}
+
+}  // namespace
+
 extern "C" {
 
 uint32_t oracle_hilbert_key(uint32_t x, uint32_t y, uint32_t z) { return oracle_hilbert3(x, y, z); }
 
-// batch_u, batch_p: [batches][n_sites]; steps, caps summed.  method 0 MC, 1 ARRAY.
+// The Sobol' direction numbers twos_rqmc's SOBOL method uses: out [dims][bits].
+void oracle_sobol_directions(uint32_t dims, uint32_t bits, uint32_t *out) {
+  const std::vector<uint32_t> t = oracle_sobol_table(dims, bits);
+  std::copy(t.begin(), t.end(), out);
+}
+
+// batch_u, batch_p: [batches][n_sites]; steps, caps summed.  method 0 MC,
+// 1 ARRAY, 3 SOBOL (Sobol-over-steps: walk i holds point i of the Sobol'
+// sequence scrambled per (site, batch, coordinate) by a lower-triangular
+// digit matrix with unit diagonal and a digital shift, drawn per step from
+// the counter stream; coordinates 2k, 2k + 1 at step k < 256, the MC stream
+// after).
 // Optional record (each may be null): walk_first [batches][n_sites][walks][3]
 // the point after the first step, walk_u / walk_p [batches][n_sites][walks]
 // each walk's payoffs, site_radius [n_sites] the first ball's radius.
@@ -1666,6 +1739,11 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
   const uint32_t n = static_cast<uint32_t>(o->walks);
   uint32_t k0, k1;
   counter_key(o->seed, o->stream, k0, k1);
+  constexpr uint32_t kSobolSteps = 256, kSobolBits = 10;
+  uint32_t sobol_bits = 0;
+  while ((1u << sobol_bits) < n) ++sobol_bits;
+  const std::vector<uint32_t> sobol = method == 3 ? oracle_sobol_table(2 * kSobolSteps, kSobolBits)
+                                                  : std::vector<uint32_t>();
   std::atomic<uint64_t> tsteps{0}, tcaps{0};
   std::atomic<int> failed{0};
 #ifdef _OPENMP
@@ -1728,6 +1806,43 @@ int oracle_rqmc(const oracle_mesh *om, const oracle_params *o, int method, uint3
           double a2 = static_cast<double>((g2 * rank) % n) / n + U2;
           u1[i] = a1 - std::floor(a1);
           u2[i] = a2 - std::floor(a2);
+        }
+      } else if (method == 3 && static_cast<uint32_t>(k) < kSobolSteps) {
+        uint32_t rows[2][32], shift[2], dir[2][kSobolBits];
+        for (uint32_t w = 0; w < 66; ++w) {
+          uint32_t q[4];
+          Philox::block(k0, k1, static_cast<uint32_t>(k), w, site, ctr3 | 5u, q);
+          if (w < 64) {
+            // Row r of the lower-triangular digit matrix: digits 0..r, digit r set.
+            const uint32_t r = w % 32;
+            uint32_t row = 0;
+            for (uint32_t j = 0; j <= r; ++j)
+              if (j == r || ((q[0] >> (31 - j)) & 1u)) row |= 1u << (31 - j);
+            rows[w / 32][r] = row;
+          } else {
+            shift[w - 64] = q[0];
+          }
+        }
+        for (int c = 0; c < 2; ++c)
+          for (uint32_t b = 0; b < sobol_bits; ++b) {
+            const uint32_t v = sobol[(2 * static_cast<size_t>(k) + c) * kSobolBits + b];
+            uint32_t x = 0;
+            for (uint32_t r = 0; r < 32; ++r) {
+              uint32_t parity = 0;
+              for (uint32_t j = 0; j < 32; ++j) parity ^= ((rows[c][r] & v) >> j) & 1u;
+              x |= parity << (31 - r);
+            }
+            dir[c][b] = x;
+          }
+        for (uint32_t i = 0; i < n; ++i) {
+          uint32_t x1 = shift[0], x2 = shift[1];
+          for (uint32_t b = 0; b < sobol_bits; ++b)
+            if ((i >> b) & 1u) {
+              x1 ^= dir[0][b];
+              x2 ^= dir[1][b];
+            }
+          u1[i] = (static_cast<double>(x1) + 0.5) / 4294967296.0;
+          u2[i] = (static_cast<double>(x2) + 0.5) / 4294967296.0;
         }
       } else {
         for (uint32_t i = 0; i < n; ++i) {

@@ -106,3 +106,22 @@ def test_autotune_rejects_an_unknown_search():
     import pytest
     with pytest.raises(ValueError):
         autotune(FakeMesh(), np.zeros((4, 3)), Cfg(), search="random")
+
+
+def test_autotune_skips_settings_the_session_refuses():
+    """Walk claims with the four-wide BVH are refused by the session
+    (TwosError from set_tuning): the sweep skips them and picks a valid one."""
+    from twos_b200._abi import TwosError
+
+    class Refusing(FakeMesh):
+        def set_tuning(self, **t):
+            if t.get("bvh_width") == 4 and t.get("lane_walks", 1) > 1:
+                raise TwosError(2, "invalid tuning")
+            super().set_tuning(**t)
+
+    mesh = Refusing()
+    best, results = autotune(mesh, np.zeros((50, 3)), Cfg(), grid=SMALL_GRID, calib_sites=10, calib_walks=8,
+                             repeats=1)
+    assert all(not (t["bvh_width"] == 4 and t["lane_walks"] > 1) for t, _ in results)
+    assert len(results) == np.prod([len(v) for v in SMALL_GRID.values()]) * 3 // 4
+    assert not (best["bvh_width"] == 4 and best["lane_walks"] > 1)

@@ -69,16 +69,18 @@ def test_every_grid_step_stays_inside_the_domain(setup):
     assert np.median(bounds / d64) > 0.5
 
 
-def test_entry_start_bvh_width_and_lane_walks_change_no_result(setup):
-    """Root-started four-wide queries on the 327,680-triangle mesh outgrow
-    the traversal stack near the root and finish on the binary BVH; the
-    rows stay those of the default tuning."""
+def test_tuning_variants_change_no_result(setup):
+    """Entry-node start off, the four-wide BVH (root-started four-wide
+    queries on the 327,680-triangle mesh outgrow the traversal stack near
+    the root and finish on the binary BVH), walks per lane and the wavefront
+    form: the rows stay those of the default tuning."""
     tb, mesh, sites = setup
     s = sites[:512]
     base = mesh.get_tuning()
     try:
         ref, _ = mesh.estimate(s, _cfg(tb, "mixed", walks=256))
-        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0), dict(lane_walks=4)):
+        for variant in (dict(entry=0), dict(bvh_width=4), dict(bvh_width=4, entry=0), dict(lane_walks=4),
+                        dict(wavefront=1 << 21), dict(wavefront=1 << 16, entry=0)):
             mesh.set_tuning(**dict(base, **variant))
             got, _ = mesh.estimate(s, _cfg(tb, "mixed", walks=256))
             np.testing.assert_array_equal(got, ref, err_msg=str(variant))

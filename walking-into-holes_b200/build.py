@@ -37,7 +37,8 @@ CLI = {
     "wih_compliance_query": ("cli_study.cpp", ["-DTWOS_STUDY_ANALYTIC=1", "-DTWOS_STUDY_AFFINE=1"]),
     "wih_analytic_integral_audit": ("cli_audit.cpp", []),
 }
-HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h", "diffwos.cuh", "ball_green.cuh", "validate.cuh", "rqmc.cuh"]
+HEADERS = ["twos_internal.h", "twos_session.h", "cli_common.h", "diffwos.cuh", "ball_green.cuh", "validate.cuh", "rqmc.cuh",
+           "wavefront.cuh"]
 
 
 def nvcc() -> str:

@@ -801,4 +801,91 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
   }
 }
 
+
+// ---------------------------------------------------------------- Sobol'
+namespace {
+
+// Product a b modulo p over GF(2); deg = degree of p, a and b reduced.
+uint32_t gf2_mulmod(uint32_t a, uint32_t b, uint32_t p, int deg) {
+  uint32_t r = 0;
+  while (b) {
+    if (b & 1u) r ^= a;
+    b >>= 1;
+    a <<= 1;
+    if ((a >> deg) & 1u) a ^= p;
+  }
+  return r;
+}
+
+uint32_t gf2_powmod(uint32_t a, uint64_t e, uint32_t p, int deg) {
+  uint32_t r = 1;
+  while (e) {
+    if (e & 1u) r = gf2_mulmod(r, a, p, deg);
+    a = gf2_mulmod(a, a, p, deg);
+    e >>= 1;
+  }
+  return r;
+}
+
+// p (bit i = coefficient of x^i, degree deg >= 2, constant term 1) is
+// primitive iff x has multiplicative order exactly 2^deg - 1 modulo p: x to
+// that power is 1 and to no quotient by one of its prime factors.
+bool gf2_primitive(uint32_t p, int deg) {
+  const uint64_t order = (1ull << deg) - 1;
+  if (gf2_powmod(2u, order, p, deg) != 1u) return false;
+  uint64_t rest = order;
+  for (uint64_t q = 3; q * q <= rest; q += 2) {
+    if (rest % q) continue;
+    while (rest % q == 0) rest /= q;
+    if (gf2_powmod(2u, order / q, p, deg) == 1u) return false;
+  }
+  return rest == 1 || gf2_powmod(2u, order / rest, p, deg) != 1u;
+}
+
+// SplitMix64 (Steele, Lea and Flood, OOPSLA 2014): one output per state.
+uint64_t splitmix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+}  // namespace
+
+std::vector<uint32_t> sobol_directions(uint32_t dims, uint32_t bits) {
+  if (bits == 0 || bits > 32) throw std::runtime_error("Sobol direction bits must be 1..32");
+  std::vector<uint32_t> polys;  // primitive polynomials, by degree then value
+  if (dims > 1) polys.push_back(3u);  // x + 1
+  for (int deg = 2; polys.size() + 1 < dims; ++deg) {
+    if (deg > 30) throw std::runtime_error("too many Sobol dimensions");
+    for (uint32_t p = (1u << deg) | 1u; p < (2u << deg) && polys.size() + 1 < dims; p += 2)
+      if (gf2_primitive(p, deg)) polys.push_back(p);
+  }
+  std::vector<uint32_t> v(static_cast<size_t>(dims) * bits);
+  std::vector<uint64_t> m(bits + 1);
+  for (uint32_t d = 0; d < dims; ++d) {
+    if (d == 0) {
+      for (uint32_t k = 1; k <= bits; ++k) m[k] = 1;
+    } else {
+      const uint32_t p = polys[d - 1];
+      int deg = 31;
+      while (!((p >> deg) & 1u)) --deg;
+      for (uint32_t k = 1; k <= bits; ++k) {
+        if (k <= static_cast<uint32_t>(deg)) {
+          // Odd initial value below 2^k.
+          const uint64_t h = splitmix64(0x536f626f6c2d3344ull + 64ull * d + k);
+          m[k] = (h & ((1ull << k) - 1)) | 1ull;
+        } else {
+          uint64_t x = m[k - deg] ^ (m[k - deg] << deg);
+          for (int j = 1; j < deg; ++j)
+            if ((p >> (deg - j)) & 1u) x ^= m[k - j] << j;
+          m[k] = x;
+        }
+      }
+    }
+    for (uint32_t b = 0; b < bits; ++b) v[static_cast<size_t>(d) * bits + b] = static_cast<uint32_t>(m[b + 1] << (31 - b));
+  }
+  return v;
+}
+
 }  // namespace twos

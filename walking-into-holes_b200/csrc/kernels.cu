@@ -663,7 +663,8 @@ __device__ __forceinline__ uint32_t lane_walks_of(const WosLaunch &L) {
   return L.lane_walks > 1 ? static_cast<uint32_t>(L.lane_walks) : 1u;
 }
 
-template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false, bool WIDE = false>
+template <typename T, int MODE, int SRC, int BLOCK, bool TRACE = false, bool GRID64 = false, bool WIDE = false,
+          bool CLAIM = false>
 __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wos_kernel(const WosLaunch L) {
   constexpr bool GREEN = SRC == TWOS_SOURCE_GREEN;
   constexpr bool EXACT = SRC == TWOS_SOURCE_EXACT && MODE != kModeBoundary;
@@ -731,95 +732,118 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
   uint32_t best_tri = 0;  // leaf-order index of the nearest triangle found for this walk
   bool tri_ok = false;    // best_tri belongs to this walk
   uint32_t tri_cur = 0, tri_end = 0, iter = 0;
-  // Walks a lane claims from the queue at once (run one after another):
-  // s_claim[thread] of them, wid + 1 onwards, are not yet started.  The count
-  // lives in shared memory, read only at refills, so it holds no register
-  // through the traversal.
-  // (The claim size is re-read from the launch parameters where used, so it
-  // holds no register either.)
-  __shared__ uint32_t s_claim[BLOCK];
-  s_claim[threadIdx.x] = 0u;
+  // CLAIM: walks a lane claims from the queue at once, run one after
+  // another: s_claim[thread] of them, wid + 1 onwards, are not yet started
+  // (shared memory, read only at refills).  A compile-time variant, so the
+  // default kernel's refill stays one atomic per warp and one start per lane.
+  __shared__ uint32_t s_claim[CLAIM ? BLOCK : 1];
+  if (CLAIM) s_claim[threadIdx.x] = 0u;
 
   for (;;) {
-    // ---- refill idle lanes from their claims and the work queue
-    const unsigned idle = __ballot_sync(full, phase == kIdle);
-    const unsigned pending = (L.lane_walks > 1) ? __ballot_sync(full, s_claim[threadIdx.x] != 0u) : 0u;
-    if ((!exhausted || pending != 0u) && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
-      uint32_t claim_left = (L.lane_walks > 1) ? s_claim[threadIdx.x] : 0u;
-      const unsigned claim = __ballot_sync(full, phase == kIdle && claim_left == 0u);
-      if (!exhausted && claim != 0u) {
-        const uint64_t span = static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim);
-        unsigned long long base = 0;
-        const int leader = __ffs(claim) - 1;
-        if (static_cast<int>(lane) == leader) base = atomicAdd(L.counter, static_cast<unsigned long long>(span));
-        base = __shfl_sync(full, base, leader);
-        if (base + span >= L.total_walks) exhausted = true;
-        if (phase == kIdle && claim_left == 0u) {
-          const uint64_t first = base + static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim & ((1u << lane) - 1u));
-          if (first < L.total_walks) {
-            wid = first - 1;  // wraps for the first walk of the queue; wid + 1 is exact
-            const uint64_t left = L.total_walks - first;
-            claim_left = left < lane_walks_of(L) ? static_cast<uint32_t>(left) : lane_walks_of(L);
-          }
+    // Starts walk `wid` on this lane (its first radius from the per-site
+    // pre-pass when there is one).
+    auto start_walk = [&]() {
+      const uint64_t id = wid;
+      job = find_job(s_jobs, L.n_jobs, id);
+      const JobDesc &J = s_jobs[job];
+      const uint64_t local = id - J.walk_begin;
+      site = static_cast<uint32_t>(local / J.walks);
+      walk = static_cast<uint32_t>(local - static_cast<uint64_t>(site) * J.walks);
+      const GeoDesc &G = s_geos[J.geo];
+      bool skip = false;
+      if (L.walk_start) {
+        const double *st = L.walk_start + 3ull * wid;
+        skip = isnan(st[0]);
+        pos = to_frame<T>(st, G);
+      } else {
+        pos = to_frame<T>(L.sites + 3ull * (J.site_begin + site), G);
+      }
+      u = T(0);
+      pv = T(0);
+      steps = 0;
+      tri_ok = false;
+      if (GRAD) g_r0 = T(0);
+      if (!skip && (J.flags & kJobSkipCavitySites)) {
+        const T R = to_T<T>(J.cavity_radius);
+        for (uint32_t c = 0; c < J.n_cav; ++c) {
+          const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
+          const Vec<T> dv = sub(pos, cc);
+          if (sqrt(dot3(dv, dv)) <= R) skip = true;
         }
       }
-      if (phase == kIdle) {
-        if (claim_left != 0u) {
-          const uint64_t id = ++wid;
-          --claim_left;
-          job = find_job(s_jobs, L.n_jobs, id);
-          const JobDesc &J = s_jobs[job];
-          const uint64_t local = id - J.walk_begin;
-          site = static_cast<uint32_t>(local / J.walks);
-          walk = static_cast<uint32_t>(local - static_cast<uint64_t>(site) * J.walks);
-          const GeoDesc &G = s_geos[J.geo];
-          bool skip = false;
-          if (L.walk_start) {
-            const double *st = L.walk_start + 3ull * wid;
-            skip = isnan(st[0]);
-            pos = to_frame<T>(st, G);
-          } else {
-            pos = to_frame<T>(L.sites + 3ull * (J.site_begin + site), G);
-          }
-          u = T(0);
-          pv = T(0);
-          steps = 0;
-          tri_ok = false;
-          if (GRAD) g_r0 = T(0);
-          if (!skip && (J.flags & kJobSkipCavitySites)) {
-            const T R = to_T<T>(J.cavity_radius);
-            for (uint32_t c = 0; c < J.n_cav; ++c) {
-              const Vec<T> cc = to_frame<T>(L.cavities + 3ull * (J.cav_begin + c), G);
-              const Vec<T> dv = sub(pos, cc);
-              if (sqrt(dot3(dv, dv)) <= R) skip = true;
+      if (skip) {
+        if (MODE != kModeBoundary) static_cast<T *>(L.u_out)[wid] = T(0);
+        if (PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
+        if (GRAD)
+          for (int k = 0; k < 6; ++k) static_cast<T *>(L.grad_out)[6ull * wid + k] = T(0);
+        if (MODE == kModeBoundary) L.hits[wid].cavity = -2;
+        L.steps_out[wid] = 0u;
+      } else if (L.site_best2 && MODE != kModeBoundary) {
+        // First query answered by the per-site pre-pass.
+        best2 = static_cast<const T *>(L.site_best2)[J.site_rank + site];
+        found = best2 >= T(0);
+        phase = kStep;
+      } else {
+        best2 = static_cast<T>(J.query_radius2);
+        node = 0;
+        sp = 0;
+        have = true;
+        narrow = false;
+        found = false;
+        tri_cur = tri_end = 0;
+        iter = 0;
+        phase = kTraverse;
+      }
+    };
+
+    // ---- refill idle lanes from the work queue (CLAIM: from their own
+    // claims first)
+    const unsigned idle = __ballot_sync(full, phase == kIdle);
+    if constexpr (CLAIM) {
+      if (idle != 0u) {
+        const unsigned pending = __ballot_sync(full, s_claim[threadIdx.x] != 0u);
+        if ((!exhausted || pending != 0u) && (__popc(idle) >= L.refill || idle == full)) {
+          uint32_t claim_left = s_claim[threadIdx.x];
+          const unsigned claim = __ballot_sync(full, phase == kIdle && claim_left == 0u);
+          if (!exhausted && claim != 0u) {
+            const uint64_t span = static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim);
+            unsigned long long base = 0;
+            const int leader = __ffs(claim) - 1;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(L.counter, static_cast<unsigned long long>(span));
+            base = __shfl_sync(full, base, leader);
+            if (base + span >= L.total_walks) exhausted = true;
+            if (phase == kIdle && claim_left == 0u) {
+              const uint64_t first =
+                  base + static_cast<uint64_t>(lane_walks_of(L)) * __popc(claim & ((1u << lane) - 1u));
+              if (first < L.total_walks) {
+                wid = first - 1;  // wraps for the first walk of the queue; wid + 1 is exact
+                const uint64_t left = L.total_walks - first;
+                claim_left = left < lane_walks_of(L) ? static_cast<uint32_t>(left) : lane_walks_of(L);
+              }
             }
           }
-          if (skip) {
-            if (MODE != kModeBoundary) static_cast<T *>(L.u_out)[wid] = T(0);
-            if (PAIRED) static_cast<T *>(L.p_out)[wid] = T(0);
-            if (GRAD)
-              for (int k = 0; k < 6; ++k) static_cast<T *>(L.grad_out)[6ull * wid + k] = T(0);
-            if (MODE == kModeBoundary) L.hits[wid].cavity = -2;
-            L.steps_out[wid] = 0u;
-          } else if (L.site_best2 && MODE != kModeBoundary) {
-            // First query answered by the per-site pre-pass.
-            best2 = static_cast<const T *>(L.site_best2)[J.site_rank + site];
-            found = best2 >= T(0);
-            phase = kStep;
-          } else {
-            best2 = static_cast<T>(J.query_radius2);
-            node = 0;
-            sp = 0;
-            have = true;
-            narrow = false;
-            found = false;
-            tri_cur = tri_end = 0;
-            iter = 0;
-            phase = kTraverse;
+          if (phase == kIdle && claim_left != 0u) {
+            ++wid;
+            --claim_left;
+            start_walk();
           }
+          s_claim[threadIdx.x] = claim_left;
         }
       }
-      if ((L.lane_walks > 1)) s_claim[threadIdx.x] = claim_left;
+    } else if (!exhausted && idle != 0u && (__popc(idle) >= L.refill || idle == full)) {
+      unsigned long long base = 0;
+      const int leader = __ffs(idle) - 1;
+      if (static_cast<int>(lane) == leader)
+        base = atomicAdd(L.counter, static_cast<unsigned long long>(__popc(idle)));
+      base = __shfl_sync(full, base, leader);
+      if (base + __popc(idle) >= L.total_walks) exhausted = true;
+      if (phase == kIdle) {
+        const uint64_t id = base + __popc(idle & ((1u << lane) - 1u));
+        if (id < L.total_walks) {
+          wid = id;
+          start_walk();
+        }
+      }
     }
 
     // ---- batched walk step for lanes whose query has finished
@@ -1081,7 +1105,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
     }
 
     if (__ballot_sync(full, phase != kIdle) == 0u) {
-      if (exhausted && (!(L.lane_walks > 1) || __ballot_sync(full, s_claim[threadIdx.x] != 0u) == 0u)) break;
+      if (exhausted && (!CLAIM || __ballot_sync(full, s_claim[threadIdx.x] != 0u) == 0u)) break;
       continue;
     }
 
@@ -1288,7 +1312,19 @@ template <int MODE, int BLOCK> static const void *select_wide_src(int src) {
   return reinterpret_cast<const void *>(&wos_kernel<float, MODE, TWOS_SOURCE_CENTER, BLOCK, false, false, true>);
 }
 
-template <int BLOCK> static const void *select_wos_block(int precision, int mode, int src, int grid64, int wide) {
+template <int MODE, int BLOCK> static const void *claim_fn() {
+  return reinterpret_cast<const void *>(
+      &wos_kernel<float, MODE, TWOS_SOURCE_CENTER, BLOCK, false, false, false, true>);
+}
+
+template <int BLOCK>
+static const void *select_wos_block(int precision, int mode, int src, int grid64, int wide, int claim) {
+  // Walk claims (lane_walks > 1): the mixed centre-source modes on the binary BVH.
+  if (claim && !wide && precision == TWOS_PREC_MIXED && src == TWOS_SOURCE_CENTER) {
+    if (mode == TWOS_MODE_COMPLIANCE) return claim_fn<TWOS_MODE_COMPLIANCE, BLOCK>();
+    if (mode == TWOS_MODE_PAIRED) return claim_fn<TWOS_MODE_PAIRED, BLOCK>();
+    if (mode == TWOS_MODE_HOT) return claim_fn<TWOS_MODE_HOT, BLOCK>();
+  }
   if (wide && precision == TWOS_PREC_MIXED && (src == TWOS_SOURCE_CENTER || src == TWOS_SOURCE_GREEN)) {
     if (mode == TWOS_MODE_COMPLIANCE) return select_wide_src<TWOS_MODE_COMPLIANCE, BLOCK>(src);
     if (mode == TWOS_MODE_PAIRED) return select_wide_src<TWOS_MODE_PAIRED, BLOCK>(src);
@@ -1313,14 +1349,14 @@ template <int BLOCK> static const void *select_wos_block(int precision, int mode
 }
 
 // Walk kernel instantiations: block sizes 128, 256 and 512 threads.
-static const void *select_wos(int precision, int mode, int src, int block, int grid64, int wide) {
+static const void *select_wos(int precision, int mode, int src, int block, int grid64, int wide, int claim) {
   switch (block) {
     case 128:
-      return select_wos_block<128>(precision, mode, src, grid64, wide);
+      return select_wos_block<128>(precision, mode, src, grid64, wide, claim);
     case 256:
-      return select_wos_block<256>(precision, mode, src, grid64, wide);
+      return select_wos_block<256>(precision, mode, src, grid64, wide, claim);
     case 512:
-      return select_wos_block<512>(precision, mode, src, grid64, wide);
+      return select_wos_block<512>(precision, mode, src, grid64, wide, claim);
     default:
       return nullptr;
   }
@@ -1352,7 +1388,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
   if (L.n_jobs == 0 || L.n_geos == 0) return cudaErrorInvalidValue;
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
   if (dyn > 200 * 1024) return cudaErrorInvalidValue;
-  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide, L.lane_walks > 1);
   if (!fn) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
@@ -1363,7 +1399,7 @@ cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int
 
 int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L) {
   const uint32_t dyn = wos_dyn_smem(precision, L, block);
-  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide);
+  const void *fn = select_wos(precision, mode, src, block, L.grid64, L.wide, L.lane_walks > 1);
   if (!fn || dyn > 200 * 1024) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)) != cudaSuccess)
     return 0;
@@ -1904,3 +1940,5 @@ cudaError_t launch_topk(const double *keys, uint32_t n, uint32_t k, uint32_t *in
 
 // Array-RQMC / matched MC lockstep walks (use nearest<T>, the stream and warp sums above).
 #include "rqmc.cuh"
+
+#include "wavefront.cuh"

@@ -15,6 +15,8 @@
 // walk draws its own uniforms.  NEIGHBOUR mode runs the MC walks with the
 // per-walk record on (first step point, payoffs, first radius) and then
 // rqmc_reuse_kernel pools the neighbours' walks into each site's batch mean.
+// SOBOL mode gives walk i point i of a scrambled Sobol' sequence, two
+// coordinates per step (the reference's Sobol-over-steps method).
 //
 // Included at the end of kernels.cu.
 #pragma once
@@ -74,6 +76,9 @@ template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const 
   uint32_t *s_rank = reinterpret_cast<uint32_t *>(s_keys + R.walks);
   __shared__ TermT<T> s_terms[3 * TWOS_MAX_TERMS];
   __shared__ double s_red[32][2];
+  // SOBOL: one step's scrambling (lower-triangular matrix rows and digital
+  // shift per coordinate) and scrambled direction numbers.
+  __shared__ uint32_t s_lms[2][32], s_shift[2], s_dir[2][kSobolBits];
   const uint32_t n_terms = R.n_src + R.n_ub + R.n_pb;
   for (uint32_t i = threadIdx.x; i < n_terms; i += blockDim.x) s_terms[i] = to_termT<T>(R.terms[i]);
   __syncthreads();
@@ -149,6 +154,42 @@ template <typename T> __global__ void __launch_bounds__(1024) rqmc_kernel(const 
       a2 -= floor(a2);
       u1 = static_cast<T>(a1);
       u2 = static_cast<T>(a2);
+    } else if (R.method == TWOS_RQMC_SOBOL && static_cast<uint32_t>(k) < kSobolSteps) {
+      // Sobol-over-steps (sampling.py:49-60 in 3D): walk i holds point i of
+      // a Sobol' sequence scrambled once per (site, batch) -- a random
+      // lower-triangular matrix with unit diagonal applied to the digits
+      // (LMS) and a digital shift, per coordinate -- and step k takes its
+      // coordinates 2k and 2k + 1.  Words 0..63 are matrix rows, 64..65 the
+      // shifts; all are keyed by (step, word, site, batch).
+      for (uint32_t w = tid; w < 66u; w += n) {
+        const uint32_t word = philox(R.k0, R.k1, static_cast<uint32_t>(k), w, site, ctr3 | 5u).x;
+        if (w < 64u) {
+          const uint32_t row = w & 31u;
+          s_lms[w >> 5][row] = (word & (~0u << (31u - row))) | (1u << (31u - row));
+        } else {
+          s_shift[w - 64u] = word;
+        }
+      }
+      __syncthreads();
+      if (tid < 2u * R.sobol_bits) {
+        const uint32_t c = tid / R.sobol_bits, b = tid % R.sobol_bits;
+        const uint32_t v = R.sobol_v[(2u * static_cast<uint32_t>(k) + c) * kSobolBits + b];
+        uint32_t out = 0;
+        for (uint32_t row = 0; row < 32u; ++row) out |= (__popc(s_lms[c][row] & v) & 1u) << (31u - row);
+        s_dir[c][b] = out;
+      }
+      __syncthreads();
+      uint32_t x1 = s_shift[0], x2 = s_shift[1];
+      for (uint32_t b = 0; b < R.sobol_bits; ++b)
+        if ((tid >> b) & 1u) {
+          x1 ^= s_dir[0][b];
+          x2 ^= s_dir[1][b];
+        }
+      // Cell midpoints: exact in double, never 0 or 1.
+      u1 = static_cast<T>((static_cast<double>(x1) + 0.5) * 0x1p-32);
+      u2 = static_cast<T>((static_cast<double>(x2) + 0.5) * 0x1p-32);
+      // (The barrier at the end of the step orders these reads before the
+      // next step's writes.)
     } else {
       const Philox4 q = philox(R.k0, R.k1, static_cast<uint32_t>(k), tid, site, ctr3);
       u1 = uniform<T>(q.x, q.y);
@@ -264,6 +305,8 @@ cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s) {
   if (blocks > 0x7fffffffull || R.walks < 32 || R.walks > 1024 || (R.walks & (R.walks - 1)))
     return cudaErrorInvalidValue;
   if ((R.walk_u == nullptr) != (R.walk_p == nullptr)) return cudaErrorInvalidValue;
+  if (R.method == TWOS_RQMC_SOBOL && (!R.sobol_v || (1u << R.sobol_bits) != R.walks || R.sobol_bits > kSobolBits))
+    return cudaErrorInvalidValue;
   const size_t dyn = R.walks * (sizeof(unsigned long long) + sizeof(uint32_t));
   if (precision == TWOS_PREC_MIXED)
     rqmc_kernel<float><<<static_cast<unsigned>(blocks), R.walks, dyn, s>>>(R);

@@ -247,6 +247,10 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     if (const char *e = std::getenv("TWOS_WARM")) m->warm = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_UNITS")) m->units = std::min(64, std::max(1, std::atoi(e)));
     if (const char *e = std::getenv("TWOS_LANE_WALKS")) m->lane_walks = std::min(64, std::max(1, std::atoi(e)));
+    if (const char *e = std::getenv("TWOS_WAVEFRONT")) {
+      const long v = std::atol(e);
+      if (v >= 0 && v <= (1l << 26) && v % 256 == 0) m->wavefront = static_cast<uint32_t>(v);
+    }
     if (const char *e = std::getenv("TWOS_ENTRY")) m->entry_start = std::atoi(e) != 0;
     if (const char *e = std::getenv("TWOS_BVH_WIDTH")) m->bvh_width = std::atoi(e) == 4 ? 4 : 2;
     if (const char *e = std::getenv("TWOS_BLOCK")) {
@@ -485,6 +489,17 @@ void run_launch(twos_mesh *owner, const std::vector<JobSpec> &specs, const doubl
     L.trace_count = trace->count;
     L.trace_cap = trace->cap;
     check(launch_wos_traced(L, per_sm * m->num_sms, m->stream), "traced WoS launch");
+  } else if (m->wavefront > 0 && mixed && green == TWOS_SOURCE_CENTER &&
+             (mode == TWOS_MODE_COMPLIANCE || mode == TWOS_MODE_PAIRED || mode == TWOS_MODE_HOT) &&
+             walk_total < (1ull << 32)) {
+    // Wavefront form: no more slots than walks (rounded up to a step block).
+    const uint32_t slots = static_cast<uint32_t>(std::min<uint64_t>(m->wavefront, (walk_total + 255) / 256 * 256));
+    m->wf.reserve(wf_slot_bytes(slots));
+    int max_steps = 1;
+    for (const JobSpec &js : specs) max_steps = std::max(max_steps, js.r->max_steps);
+    // Every live slot steps once per iteration: a generous bound.
+    const uint64_t bound = (walk_total / slots + 2) * static_cast<uint64_t>(max_steps) + 1024;
+    check(launch_wos_wavefront(mode, L, m->wf.ptr, slots, m->num_sms, bound, m->stream), "wavefront WoS launch");
   } else {
     check(launch_wos(r0->precision, mode, green, L, grid, block, m->stream), "WoS launch");
   }
@@ -616,7 +631,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
-                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->entry4})
+                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->entry4, &m->wf})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -639,7 +654,9 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
       t->step_threshold < 1 || t->step_threshold > 32 || t->blocks_per_sm < 0 ||
       !(t->grid_threshold == 0.0f || (t->grid_threshold >= 0.1f && t->grid_threshold <= 1e6f)) ||
       t->units < 1 || t->units > 64 || (t->entry != 0 && t->entry != 1) ||
-      (t->grid_fp64 != 0 && t->grid_fp64 != 1) || (t->bvh_width != 2 && t->bvh_width != 4) || t->lane_walks < 1 || t->lane_walks > 64)
+      (t->grid_fp64 != 0 && t->grid_fp64 != 1) || (t->bvh_width != 2 && t->bvh_width != 4) || t->lane_walks < 1 || t->lane_walks > 64 ||
+      (t->lane_walks > 1 && t->bvh_width == 4) || t->wavefront < 0 ||
+      t->wavefront > (1 << 26) || t->wavefront % 256 != 0)
     return fail(TWOS_ERR_USAGE, "invalid tuning");
   m->block = t->block;
   m->refill = t->refill;
@@ -651,6 +668,7 @@ int twos_mesh_set_tuning(twos_mesh *m, const twos_tuning *t) {
   m->grid_fp64 = t->grid_fp64;
   m->bvh_width = t->bvh_width;
   m->lane_walks = t->lane_walks;
+  m->wavefront = static_cast<uint32_t>(t->wavefront);
   return TWOS_OK;
 }
 
@@ -666,6 +684,7 @@ int twos_mesh_get_tuning(const twos_mesh *m, twos_tuning *t) {
   t->grid_fp64 = m->grid_fp64;
   t->bvh_width = m->bvh_width;
   t->lane_walks = m->lane_walks;
+  t->wavefront = static_cast<int32_t>(m->wavefront);
   return TWOS_OK;
 }
 
@@ -1344,7 +1363,8 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
     case 1024: generator = 35; break;
     default: return fail(TWOS_ERR_USAGE, "RQMC walks must be a power of two from 32 to 1024");
   }
-  if (rp->method != TWOS_RQMC_MC && rp->method != TWOS_RQMC_ARRAY && rp->method != TWOS_RQMC_NEIGHBOUR)
+  if (rp->method != TWOS_RQMC_MC && rp->method != TWOS_RQMC_ARRAY && rp->method != TWOS_RQMC_NEIGHBOUR &&
+      rp->method != TWOS_RQMC_SOBOL)
     return fail(TWOS_ERR_USAGE, "invalid RQMC method");
   // The Poisson kernel reweights a walk's exit value only: a source's path
   // integral depends on where the walk started (sampling.py runs the
@@ -1370,9 +1390,18 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
   const bool reuse = rp->method == TWOS_RQMC_NEIGHBOUR;
   const bool rec_first = reuse || rp->walk_first || rp->site_radius, rec_walk = reuse || rp->walk_u || rp->walk_p;
   RunOut ro;
-  DevBuf dterms, du, dp, dfirst, dwu, dwp, drad;
+  DevBuf dterms, du, dp, dfirst, dwu, dwp, drad, dsobol;
   try {
     check(cudaSetDevice(m->device), "cudaSetDevice");
+    if (rp->method == TWOS_RQMC_SOBOL) {
+      // Two coordinates per step for the first kSobolSteps steps; computed
+      // once per process (a few hundred primitive polynomials).
+      static const std::vector<uint32_t> table = sobol_directions(2 * kSobolSteps, kSobolBits);
+      dsobol.reserve(table.size() * sizeof(uint32_t));
+      check(cudaMemcpyAsync(dsobol.ptr, table.data(), table.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            m->stream),
+            "upload Sobol directions");
+    }
     m->sites.reserve(static_cast<size_t>(n_sites) * 3 * sizeof(double));
     check(cudaMemcpyAsync(m->sites.ptr, sites, static_cast<size_t>(n_sites) * 3 * sizeof(double),
                           cudaMemcpyHostToDevice, m->stream),
@@ -1422,6 +1451,10 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
     R.walk_p = rec_walk ? dwp.as<double>() : nullptr;
     R.totals = m->totals.as<unsigned long long>();
     R.error = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
+    if (rp->method == TWOS_RQMC_SOBOL) {
+      R.sobol_v = dsobol.as<uint32_t>();
+      while ((1u << R.sobol_bits) < R.walks) ++R.sobol_bits;
+    }
     check(cudaEventRecord(m->ev0, m->stream), "event");
     check(launch_rqmc(r->precision, R, m->stream), "RQMC launch");
     ro.launches = 1;
@@ -1446,10 +1479,10 @@ int twos_rqmc(twos_mesh *m, const twos_request *r, const twos_rqmc_params *rp, c
     check(cudaEventElapsedTime(&ms, m->ev0, m->ev1), "event time");
     ro.kernel_seconds = ro.walk_seconds = ms / 1e3;
   } catch (const std::exception &e) {
-    for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad}) b->release();
+    for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad, &dsobol}) b->release();
     return fail(TWOS_ERR_RUNTIME, e.what());
   }
-  for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad}) b->release();
+  for (DevBuf *b : {&dterms, &du, &dp, &dfirst, &dwu, &dwp, &drad, &dsobol}) b->release();
   // Cross-fitting over batches (crossfit, sampling.py:90-92).
   const double R = rp->batches;
   for (uint32_t s = 0; s < n_sites; ++s) {
@@ -1782,6 +1815,18 @@ int twos_trace_grid_steps(twos_mesh *m, const twos_request *r, const double *sit
   rec.release();
   cnt.release();
   if (ro.error_flags) return fail(TWOS_ERR_RUNTIME, "device error");
+  return TWOS_OK;
+}
+
+int twos_sobol_directions(uint32_t dims, uint32_t bits, uint32_t *out) {
+  if (!out || dims == 0 || dims > 65536 || bits == 0 || bits > 32)
+    return fail(TWOS_ERR_USAGE, "invalid Sobol direction arguments");
+  try {
+    const std::vector<uint32_t> t = sobol_directions(dims, bits);
+    std::copy(t.begin(), t.end(), out);
+  } catch (const std::exception &e) {
+    return fail(TWOS_ERR_RUNTIME, e.what());
+  }
   return TWOS_OK;
 }
 

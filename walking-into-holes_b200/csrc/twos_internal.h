@@ -298,8 +298,24 @@ struct RqmcLaunch {
   double *site_radius;         // optional [n_sites]
   unsigned long long *totals;  // [0] steps, [1] caps
   uint32_t *error;
+  // SOBOL: direction numbers [2 * kSobolSteps][kSobolBits] (sobol_directions)
+  // and log2(walks), the index bits of a walk.
+  const uint32_t *sobol_v;
+  uint32_t sobol_bits;
 };
 cudaError_t launch_rqmc(int precision, const RqmcLaunch &R, cudaStream_t s);
+
+// Sobol-over-steps RQMC: steps 0 .. kSobolSteps - 1 of a walk take the two
+// coordinates (2k, 2k + 1) of its Sobol' point; later steps draw the matched
+// MC stream.  kSobolBits index bits cover up to 1024 walks.
+constexpr uint32_t kSobolSteps = 256, kSobolBits = 10;
+
+// Sobol' direction numbers, `bits` per dimension, most significant digit
+// first: v[d * bits + b] = m_{d, b+1} 2^(31-b).  Dimension 0 is van der
+// Corput's (m = 1); dimension d >= 1 takes the d-th primitive polynomial over
+// GF(2) (by degree, then by coefficient bits) with odd initial m_k < 2^k
+// from SplitMix64 and Sobol's recurrence beyond its degree.
+std::vector<uint32_t> sobol_directions(uint32_t dims, uint32_t bits);
 cudaError_t launch_rqmc_reuse(const RqmcLaunch &R, cudaStream_t s);
 
 // Gradient-mode finalize: one warp per site over u, p, grad u, grad p.
@@ -376,6 +392,24 @@ cudaError_t launch_design_mask(const DesignLaunch &D, cudaStream_t s);
 
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
 cudaError_t launch_wos_traced(const WosLaunch &L, int grid, cudaStream_t s);
+
+// Wavefront form of the mixed-precision walk (wavefront.cuh): the walks in
+// flight live in `slots` slot records in device memory.
+struct WfSlots {
+  float4 *pos;       // FP32-frame position; w: the next step's squared radius
+  uint4 *meta;       // launch walk id, steps, nearest triangle, flags | job << 8
+  float2 *val;       // u, p accumulators
+  int *node;         // start node of the slot's pending query
+  uint32_t *queue;   // slots with a pending query
+  uint32_t *counts;  // [0] queue length, [1] live slots after the step kernel
+  uint32_t slots;
+};
+size_t wf_slot_bytes(uint32_t slots);
+// Runs every walk of L (FP32, centre-point source, compliance / paired /
+// hot; total walks below 2^32) through the wavefront kernels on stream s and
+// waits for it.  max_iterations bounds the iterations (an error beyond).
+cudaError_t launch_wos_wavefront(int mode, const WosLaunch &L, void *slot_mem, uint32_t slots, int num_sms,
+                                 uint64_t max_iterations, cudaStream_t s);
 cudaError_t launch_wos(int precision, int mode, int src, const WosLaunch &L, int grid, int block,
                        cudaStream_t s);
 int wos_max_blocks_per_sm(int precision, int mode, int src, int block, const WosLaunch &L);

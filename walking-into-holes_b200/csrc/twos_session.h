@@ -79,7 +79,7 @@ struct twos_mesh {
   uint64_t resident_bytes = 0;
   // Scratch, grown on demand.
   twos::DevBuf jobs, geos, terms, cavities, sites, out, u, p, grad, steps, first, counter, totals, points, dist, closest,
-      topk;
+      topk, wf;
   size_t max_launch_walks = size_t(1) << 30;
   int block = 128;         // walk-kernel threads per block
   int refill = 1;          // lanes idle before a warp refills from the queue
@@ -90,6 +90,7 @@ struct twos_mesh {
   float grid_tau = 0.1f;   // mixed-form grid steps need a bound of this many spacings; 0 = off
   int units = 8;           // traversal units per lane per warp-loop iteration
   int lane_walks = 1;      // walks a lane claims from the queue at once
+  uint32_t wavefront = 0;  // > 0: mixed centre-source walks run in the wavefront form with this many slots
   int entry_start = 1;     // 1: mixed-form queries start at the entry-node table's node
   int grid_fp64 = 0;       // 1: the FP64 compliance form uses the grid and entry nodes too
   int bvh_width = 2;       // mixed form: 2 (binary) or 4 (four-wide) BVH traversal

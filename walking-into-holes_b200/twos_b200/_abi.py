@@ -29,9 +29,9 @@ EXPORTED = [
     "twos_estimate_batch", "twos_design_loop", "twos_walk_samples", "twos_inside", "twos_topk_device",
     "twos_estimate_noalloc", "twos_mesh_set_tuning", "twos_mesh_get_tuning", "twos_diffwos",
     "twos_ball_green_integral", "twos_validate", "twos_estimate_gradient", "twos_rqmc", "twos_finalize_samples",
-    "twos_l2_read_gbs", "twos_trace_grid_steps",
+    "twos_l2_read_gbs", "twos_trace_grid_steps", "twos_sobol_directions",
 ]
-RQMC_MC, RQMC_ARRAY, RQMC_NEIGHBOUR = 0, 1, 2
+RQMC_MC, RQMC_ARRAY, RQMC_NEIGHBOUR, RQMC_SOBOL = 0, 1, 2, 3
 
 
 class SourceTerm(ctypes.Structure):
@@ -89,7 +89,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("refill", ctypes.c_int32), ("step_threshold", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("grid_threshold", ctypes.c_float), ("units", ctypes.c_int32),
                 ("entry", ctypes.c_int32), ("grid_fp64", ctypes.c_int32), ("bvh_width", ctypes.c_int32),
-                ("lane_walks", ctypes.c_int32)]
+                ("lane_walks", ctypes.c_int32), ("wavefront", ctypes.c_int32)]
 
 
 class DesignParams(ctypes.Structure):
@@ -194,6 +194,7 @@ def load(path: Path | str | None = None):
     L.twos_diffwos.argtypes = [vp, ctypes.POINTER(Request), dbl, i32, vp, u32, vp, u32, vp, vp,
                                ctypes.POINTER(Summary)]
     L.twos_topk_device.argtypes = [vp, vp, u32, u32, vp]
+    L.twos_sobol_directions.argtypes = [u32, u32, vp]
     for name in EXPORTED:
         if name not in ("twos_mesh_close", "twos_last_error"):
             getattr(L, name).restype = ctypes.c_int

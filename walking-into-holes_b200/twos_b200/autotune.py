@@ -14,12 +14,13 @@ the workload's own request with fewer walks) for every candidate setting of
   entry cell starts at the cell's entry node instead of the BVH root);
 * the mixed form's BVH width: the binary BVH or the same BVH collapsed to
   four-wide nodes;
-* walks per lane: walks a lane claims from the work queue at once;
+* walks per lane: walks a lane claims from the work queue at once (not
+  combined with the four-wide BVH, which the session refuses);
 
 and leaves the fastest (walk-kernel device time per walk: every setting runs
 the same walks, and only the grid threshold changes how many steps they
 take) set on the mesh.  A grid of at most `max_grid` settings (the default
-grid has 864, a few seconds of calibration runs) is swept whole, since the
+grid has 864, 576 of them valid; a few seconds of calibration runs) is swept whole, since the
 axes interact (the step threshold and the traversal units above all); a
 larger one by coordinate descent: from the mesh's current tuning, each axis
 in turn takes its fastest value with the others held, until a pass over all
@@ -35,6 +36,8 @@ from dataclasses import replace
 from pathlib import Path
 
 import numpy as np
+
+from ._abi import TwosError
 
 DEFAULT_GRID = {
     "block": (128, 256, 512),
@@ -81,7 +84,11 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
         if values in timed:
             return timed[values]
         tuning = dict(zip(names, values))
-        mesh.set_tuning(**tuning)
+        try:
+            mesh.set_tuning(**tuning)
+        except TwosError:  # a combination the session refuses (walk claims with the four-wide BVH)
+            timed[values] = float("inf")
+            return timed[values]
         times = []
         for r in range(repeats + 1):
             calib.repeat = 5000 + r

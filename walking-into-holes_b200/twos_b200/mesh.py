@@ -131,7 +131,7 @@ class Mesh:
         check(_abi.load().twos_mesh_set_stream(self._h, ctypes.c_void_p(handle or 0)))
 
     def set_tuning(self, block=128, refill=1, step_threshold=1, blocks_per_sm=0, grid_threshold=0.1, units=8,
-                   entry=1, grid_fp64=0, bvh_width=2, lane_walks=1):
+                   entry=1, grid_fp64=0, bvh_width=2, lane_walks=1, wavefront=0):
         """Walk-kernel launch tuning; grid_threshold is the mixed form's
         distance-grid bound (in grid spacings) above which a step skips its
         closest-point query, 0 to query every step; units is the number of
@@ -140,9 +140,11 @@ class Mesh:
         grid_fp64 1 gives the FP64 compliance form the grid and entry nodes
         too (a like-for-like comparison of precision); bvh_width 2 or 4 picks
         the mixed form's binary or four-wide BVH traversal; lane_walks is the
-        number of walks a lane claims from the work queue at once."""
+        number of walks a lane claims from the work queue at once; wavefront
+        > 0 runs the mixed centre-source modes in the wavefront form with that
+        many walks in flight (a multiple of 256)."""
         t = _abi.Tuning(int(block), int(refill), int(step_threshold), int(blocks_per_sm), float(grid_threshold),
-                        int(units), int(entry), int(grid_fp64), int(bvh_width), int(lane_walks))
+                        int(units), int(entry), int(grid_fp64), int(bvh_width), int(lane_walks), int(wavefront))
         check(_abi.load().twos_mesh_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -153,7 +155,7 @@ class Mesh:
                 # The ABI keeps a float; report the shortest decimal that rounds to it (0.1, not 0.10000000149).
                 "grid_threshold": float(str(np.float32(t.grid_threshold))), "units": t.units,
                 "entry": t.entry, "grid_fp64": t.grid_fp64, "bvh_width": t.bvh_width,
-                "lane_walks": t.lane_walks}
+                "lane_walks": t.lane_walks, "wavefront": t.wavefront}
 
     def info(self) -> dict:
         i = _abi.MeshInfo()
@@ -309,8 +311,9 @@ class Mesh:
 
     def rqmc(self, sites, config: Config, u_boundary, p_boundary, method: str = "array", batches: int = 4,
              record: bool = False):
-        """Array-RQMC, matched MC or neighbour reuse (twos_rqmc; the methods
-        'array', 'mc' and 'neighbors' of sampling.py:118-132): returns
+        """Array-RQMC, matched MC, neighbour reuse or Sobol-over-steps RQMC
+        (twos_rqmc; the methods 'array', 'mc', 'neighbors' and 'rqmc' (here
+        also 'sobol') of sampling.py:118-132): returns
         (batch_u, batch_p [batches, n_sites], td [n_sites], summary), td the
         batch cross-fit -(sum a sum b - sum ab)/(R(R-1)) of sampling.py:90-92.
         With record=True the summary also holds the per-walk record:
@@ -319,7 +322,7 @@ class Mesh:
         s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
         p = _abi.RqmcParams()
         p.method = {"mc": _abi.RQMC_MC, "array": _abi.RQMC_ARRAY, "neighbors": _abi.RQMC_NEIGHBOUR,
-                    "neighbours": _abi.RQMC_NEIGHBOUR}[method]
+                    "neighbours": _abi.RQMC_NEIGHBOUR, "rqmc": _abi.RQMC_SOBOL, "sobol": _abi.RQMC_SOBOL}[method]
         p.batches = int(batches)
         p.n_u_boundary, p.n_p_boundary = len(u_boundary), len(p_boundary)
         for i, t in enumerate(u_boundary):
@@ -413,6 +416,15 @@ def l2_read_gbs(device: int = 0, mib: int = 64, passes: int = 20) -> float:
     g = ctypes.c_double()
     check(_abi.load().twos_l2_read_gbs(int(device), int(mib) << 20, int(passes), ctypes.byref(g)))
     return float(g.value)
+
+
+def sobol_directions(dims: int, bits: int = 10) -> np.ndarray:
+    """The Sobol' direction numbers of the 'sobol' RQMC method
+    (twos_sobol_directions, host only): [dims, bits] uint32, most significant
+    digit first."""
+    out = np.zeros((int(dims), int(bits)), dtype=np.uint32)
+    check(_abi.load().twos_sobol_directions(int(dims), int(bits), out.ctypes.data))
+    return out
 
 
 def estimate_batch(meshes, sites_list, configs, cavities_list=None):
