@@ -125,3 +125,27 @@ def test_autotune_skips_settings_the_session_refuses():
     assert all(not (t["bvh_width"] == 4 and t["lane_walks"] > 1) for t, _ in results)
     assert len(results) == np.prod([len(v) for v in SMALL_GRID.values()]) * 3 // 4
     assert not (best["bvh_width"] == 4 and best["lane_walks"] > 1)
+
+
+def test_refine_stage_retimes_the_fastest_on_a_larger_calibration():
+    """refine=k: the k fastest settings of the sweep are timed again on a
+    larger calibration (more sites and walks) and the pick comes from those
+    timings; here the larger calibration reverses the sweep's order."""
+    class TailHeavy(FakeMesh):
+        def estimate(self, sites, cfg, cavities=None):
+            rows, s = super().estimate(sites, cfg, cavities)
+            if len(sites) > 100 and self.tuning["units"] == 8:  # slower at scale
+                s["walk_seconds"] *= 2.0
+            return rows, s
+
+    mesh = TailHeavy()
+    sites = np.random.default_rng(2).normal(size=(5000, 3))
+    grid = dict(SMALL_GRID, units=(4, 8), block=(256,), refill=(1,), step_threshold=(4,), grid_threshold=(0.1,),
+                entry=(1,), bvh_width=(4,), lane_walks=(2,))
+    best, results = autotune(mesh, sites, Cfg(walks=4096), grid=grid, calib_sites=50, calib_walks=16, repeats=1,
+                             refine=2, refine_sites=1000, refine_walks=256)
+    sweep, refined = results[:2], results[2:]
+    assert min(sweep, key=lambda t: t[1])[0]["units"] == 8  # the small calibration prefers 8 units
+    assert len(refined) == 2 and best["units"] == 4
+    big = [c for c in mesh.calls if c[3] == 1000]
+    assert len(big) == 2 * 2 and all(w == 256 for _, w, _, _ in big)

@@ -58,11 +58,16 @@ def _key(mesh, config) -> str:
 
 
 def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, repeats=2, seed=0,
-             cache: str | Path | None = None, cavities=None, search="auto", max_grid=1024, max_passes=4):
+             cache: str | Path | None = None, cavities=None, search="auto", max_grid=1024, max_passes=4,
+             refine=0, refine_sites=32768, refine_walks=512):
     """Pick the fastest launch tuning for `config` on `mesh`; returns
     (best tuning dict, list of (tuning, seconds per walk) for every setting
     timed).  search: "grid" sweeps every setting, "descent" runs coordinate
-    descent, "auto" sweeps grids of at most max_grid settings."""
+    descent, "auto" sweeps grids of at most max_grid settings.  refine > 0
+    re-times the `refine` fastest settings on a larger calibration
+    (refine_sites x refine_walks: a small one is dominated by the tail of
+    the launch, where the last walks run on a nearly empty GPU) and picks
+    among those; their timings follow the sweep's in the list."""
     key = _key(mesh, config)
     if cache is not None and Path(cache).exists():
         table = json.loads(Path(cache).read_text())
@@ -80,6 +85,15 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
     results = []
     timed = {}
 
+    def seconds_per_walk(points, cfg):
+        times = []
+        for r in range(repeats + 1):
+            cfg.repeat = 5000 + r
+            _, s = mesh.estimate(points, cfg, cavities=cavities)
+            if r:  # the first run is a warm-up
+                times.append(s["walk_seconds"] / max(1, s["paths"]))
+        return float(np.median(times))
+
     def measure(values):
         if values in timed:
             return timed[values]
@@ -89,13 +103,7 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
         except TwosError:  # a combination the session refuses (walk claims with the four-wide BVH)
             timed[values] = float("inf")
             return timed[values]
-        times = []
-        for r in range(repeats + 1):
-            calib.repeat = 5000 + r
-            _, s = mesh.estimate(pick, calib, cavities=cavities)
-            if r:  # the first run is a warm-up
-                times.append(s["walk_seconds"] / max(1, s["paths"]))
-        timed[values] = float(np.median(times))
+        timed[values] = seconds_per_walk(pick, calib)
         results.append((tuning, timed[values]))
         return timed[values]
 
@@ -117,6 +125,16 @@ def autotune(mesh, sites, config, grid=None, calib_sites=4096, calib_walks=128, 
             if not moved:
                 break
     best = min(results, key=lambda t: t[1])[0]
+    if refine > 0:
+        pick2 = sites[np.random.default_rng(seed + 1).choice(len(sites), size=min(refine_sites, len(sites)),
+                                                              replace=False)]
+        calib2 = replace(config, walks=min(config.walks, refine_walks))
+        refined = []
+        for tuning, _ in sorted(results, key=lambda t: t[1])[:refine]:
+            mesh.set_tuning(**tuning)
+            refined.append((tuning, seconds_per_walk(pick2, calib2)))
+        results.extend(refined)
+        best = min(refined, key=lambda t: t[1])[0]
     mesh.set_tuning(**best)
     best = mesh.get_tuning()
     if cache is not None:
