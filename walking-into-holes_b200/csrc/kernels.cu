@@ -543,6 +543,16 @@ template <typename T> __device__ __forceinline__ const typename Layout<T>::Tri *
 template <> __device__ __forceinline__ const TriF *geo_tris<float>(const GeoDesc &g) { return g.tris_f; }
 template <> __device__ __forceinline__ const TriD *geo_tris<double>(const GeoDesc &g) { return g.tris_d; }
 
+// An upper bound on sqrtf(x) for x > 0 from rsqrtf, whose stated maximum
+// error is 2 ulp: x rsqrtf(x) is within 1.25 * 2^-22 of sqrt(x) (relative),
+// so raising it by 2^-20 puts it above the correctly rounded sqrtf(x).  The
+// grid bounds only need |p - v| from above (a larger distance lowers the
+// lower bound and raises the upper one), and this takes fewer instructions
+// than the correctly rounded square root.  x = 0 gives NaN, which the
+// bounds' fmaxf / fminf skip: that corner is left out, which only loosens
+// them.
+__device__ __forceinline__ float sqrt_up(float x) { return x * rsqrtf(x) * (1.0f + 0x1.0p-20f); }
+
 // Distance-grid vertex (i, j, k) in the FP32 frame, rounded the same way in
 // the grid build and in the walk step.
 __device__ __forceinline__ Vec<float> grid_vertex(const GeoDesc &g, uint32_t i, uint32_t j, uint32_t k) {
@@ -573,13 +583,13 @@ __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &
   const uint32_t j0 = min(static_cast<uint32_t>(fy), g.grid_n[1] - 2);
   const uint32_t k0 = min(static_cast<uint32_t>(fz), g.grid_n[2] - 2);
   float best = -CUDART_INF_F, up = CUDART_INF_F;
-#pragma unroll
+#pragma unroll 4  // (fully unrolled, the eight corners' values spill the 64-register kernel)
   for (int c = 0; c < 8; ++c) {
     const uint32_t i = i0 + (c >> 2), j = j0 + ((c >> 1) & 1), k = k0 + (c & 1);
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
     const uint16_t raw = __ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k);
-    const float dist = sqrtf(dot3(dv, dv));
+    const float dist = sqrt_up(dot3(dv, dv));
     const float dq = static_cast<float>(raw) * g.grid_q;
     best = fmaxf(best, dq - dist);
     if (raw != 0xffffu) up = fminf(up, dq + g.grid_q + dist);
