@@ -73,10 +73,12 @@ REF_SUBSET_SEED = 1234
 NCU_WALK_KERNEL = {
     "case": "bench.py --walks 256 --grid 24 --steps 1 --warmup 1 --no-cpu --no-fp64 --no-ablation --no-accuracy "
             "--no-autotune",
-    "lts__throughput_pct": 21.1,
-    "smsp__thread_inst_executed_per_inst_executed": 8.59,
-    "smsp__issue_active_pct": 70.2,
+    "lts__throughput_pct": 24.3,
+    "smsp__thread_inst_executed_per_inst_executed": 8.39,
+    "smsp__issue_active_pct": 67.6,
     "sm__warps_active_pct": 48.2,
+    "wavefront_split": {"step_kernel_threads_per_inst": 24.1, "query_kernel_threads_per_inst": 8.4,
+                        "issue_active_pct": 38},
 }
 
 
