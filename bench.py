@@ -73,10 +73,11 @@ REF_SUBSET_SEED = 1234
 NCU_WALK_KERNEL = {
     "case": "bench.py --walks 256 --grid 24 --steps 1 --warmup 1 --no-cpu --no-fp64 --no-ablation --no-accuracy "
             "--no-autotune",
-    "lts__throughput_pct": 24.3,
-    "smsp__thread_inst_executed_per_inst_executed": 8.39,
-    "smsp__issue_active_pct": 67.6,
-    "sm__warps_active_pct": 48.2,
+    "lts__throughput_pct": 21.4,
+    "smsp__thread_inst_executed_per_inst_executed": 8.41,
+    "smsp__issue_active_pct": 50.9,
+    "sm__warps_active_pct": 48.6,
+    "lts__t_sector_hit_rate_pct": 65.1,
     "wavefront_split": {"step_kernel_threads_per_inst": 24.1, "query_kernel_threads_per_inst": 8.4,
                         "issue_active_pct": 38},
 }
@@ -84,12 +85,13 @@ NCU_WALK_KERNEL = {
 
 def dram_traffic_per_launch(walks: int) -> float:
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one walk-
-    kernel launch, from one ncu capture of the full workload: 2.83 GB read +
-    4.33 GB written for 502,403,072 walks, 14.25 B per walk.  The traffic is
-    the per-walk samples and the lines they evict; the BVH (31 MB) and the
-    distance grid (64 MB) stay in L2, so it scales with the walks of the
-    launch."""
-    return 14.25 * walks
+    kernel launch, from one single-pass ncu capture of the full workload
+    (default launch tuning): 1,583.6 GB read + 16.1 GB written for
+    502,403,072 walks, 3,184 B per walk.  With the 2^28-vertex grid (512 MB)
+    and its entry table (1 GiB) the touched cells no longer fit the 126 MB L2:
+    the reads are grid and table lines; the writes are the per-walk samples.
+    Scaled to the walks of the launch."""
+    return 3184.26 * walks
 
 
 EPSILON = 1e-4
@@ -503,7 +505,8 @@ def run_ours(args):
                 "peak_source": "measured in this run: twos_l2_read_gbs, 32-byte loads from every SM over a "
                                "64 MiB L2-resident buffer (the walk kernel's load form)",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-workload walk-kernel "
-                                  "launch, 14.25 B per walk (per-walk samples), scaled to this launch's walks",
+                                  "launch, 3,184 B per walk (grid and entry-table lines read from HBM, per-walk "
+                                  "samples written), scaled to this launch's walks",
                 "hbm": {"peak": hbm_peak, "peak_source": hbm_kind + " hbm_gbs",
                         "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
                 "ncu_walk_kernel": NCU_WALK_KERNEL,

@@ -266,8 +266,9 @@ typedef struct twos_tuning {
   int32_t bvh_width;     /* mixed form: 2 traverses the binary BVH, 4 the same
                             BVH collapsed to four-wide nodes (compliance,
                             paired and hot modes with the centre or Green
-                            source; the others stay binary).  Same minima,
-                            same rows.  Default 2. */
+                            source; the others stay binary).  The same
+                            minima up to FP32 rounding ties between a node
+                            bound and a triangle distance.  Default 2. */
   int32_t lane_walks;    /* walks a lane claims from the work queue at once
                             and runs one after another (1..64): mixed form,
                             centre-point source, compliance / paired / hot

@@ -33,7 +33,7 @@ def test_bound_is_a_lower_bound_and_tight(tb):
     with tb.Mesh(V, F) as mesh:
         info = mesh.info()
         h, delta = info["grid_spacing"], info["mixed_delta"]
-        assert h > 0 and np.prod(info["grid_dims"]) <= 128 * len(F) * 1.5
+        assert h > 0 and np.prod(info["grid_dims"]) <= 1024 * len(F) * 1.5
         lo, hi = np.array(info["bounds_min"]), np.array(info["bounds_max"])
         far = rng.uniform(lo - 0.5 * h, hi + 0.5 * h, (200_000, 3))
         near = V[rng.integers(0, len(V), 100_000)] * (1 + rng.uniform(-3 * h, 3 * h, (100_000, 1)))
@@ -54,7 +54,7 @@ def test_grid_size_and_switch(tb, monkeypatch):
     V, F = tb.geometry.icosphere(3)
     with tb.Mesh(V, F) as mesh:
         dims = mesh.info()["grid_dims"]
-        assert 4096 <= np.prod(dims) <= 1.5 * 128 * len(F)
+        assert 4096 <= np.prod(dims) <= 1.5 * 1024 * len(F)
     monkeypatch.setenv("TWOS_GRID_VERTICES", "0")
     with tb.Mesh(V, F) as mesh:
         assert mesh.info()["grid_dims"] == [0, 0, 0]

@@ -1056,11 +1056,12 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           // table keeps every triangle within a cell size plus 4 delta), so
           // the traversal starts there.  The grid's upper bound plus 6 delta
           // (its 3 delta and the FP32 query's delta, with room) may serve as
-          // b before any triangle is found.
+          // b before any triangle is found.  (The four-wide form keeps the
+          // bound but starts at its root: the table holds binary nodes.)
           if (entry_at != 0xffffffffu) {
             const float ubs = upper + 6.f * G.delta;
             if (fminf(sqrtf(best2), ubs) < G.entry_radius) {
-              node = __ldg((WIDE ? G.entry4 : G.entry) + entry_at);
+              if (!WIDE) node = __ldg(G.entry + entry_at);
               if (ubs * ubs < best2) best2 = ubs * ubs;
             }
           }

@@ -55,9 +55,13 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 
 // Sizes and fills the mixed form's distance-bound grid of a session whose
 // BVH is on the device and whose geo_host describes it (m->geo allocated).
-// About 128 vertices per triangle, at most 2^25, over the bounding box padded
-// by one spacing (environment TWOS_GRID_VERTICES sets the count, up to 2^26;
-// 0 builds none).
+// About 1024 vertices per triangle, at most 2^28 (512 MB), over the bounding
+// box padded by one spacing (environment TWOS_GRID_VERTICES sets the count,
+// up to 2^30; 0 builds none).  On the 327,680-triangle noise sphere the walk
+// kernel took 2.42 / 2.32 / 2.17 / 2.11 / 2.08 s with 2^25 / 2^26 / 2^27 /
+// 2^28 / 2^29 vertices (entry cells of one spacing from 2^26 up): a finer
+// grid answers more steps and its entry cells start queries deeper.  2^28
+// keeps the mesh open within a few seconds.
 // Values are FP32 distances less 2 delta (the mixed form's own error bound,
 // covering the FP32 query and the vertex placement), in steps of h/128.
 void build_entry_table(twos_mesh *m);
@@ -65,9 +69,9 @@ void build_entry_table(twos_mesh *m);
 void build_distance_grid(twos_mesh *m, size_t n_tris) {
   GeoDesc &g = m->geo_host;
   g.grid = nullptr;
-  uint64_t target = std::min<uint64_t>(std::max<uint64_t>(128ull * n_tris, 4096ull), 1ull << 25);
+  uint64_t target = std::min<uint64_t>(std::max<uint64_t>(1024ull * n_tris, 4096ull), 1ull << 28);
   if (const char *e = std::getenv("TWOS_GRID_VERTICES"))
-    target = std::min<uint64_t>(std::strtoull(e, nullptr, 10), 1ull << 26);
+    target = std::min<uint64_t>(std::strtoull(e, nullptr, 10), 1ull << 30);
   const uint64_t cap = std::max<uint64_t>(target, 1ull << 25);
   double ext[3], emax = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -115,8 +119,9 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
 }
 
 // The entry-node table over the distance grid: cells of 2^s grid spacings
-// (2 spacings by default, 16 MB for 2^25 grid vertices; TWOS_ENTRY_CELLS
-// sets 1, 2, 4, 8 or 16, 0 builds none), each with the node whose subtree
+// (by default one spacing while the table takes at most 1 GiB -- 1 GiB for
+// 2^28 grid vertices -- else two; TWOS_ENTRY_CELLS sets 1, 2, 4, 8 or 16, 0
+// builds none), each with the node whose subtree
 // holds every triangle within one cell size (plus 4 delta) of the cell.  A
 // query whose initial bound is below one cell size starts there instead of at
 // the root.
@@ -124,7 +129,8 @@ void build_entry_table(twos_mesh *m) {
   GeoDesc &g = m->geo_host;
   g.entry = nullptr;
   if (!g.grid) return;
-  uint32_t shift = 1;
+  const uint64_t vertices = static_cast<uint64_t>(g.grid_n[0]) * g.grid_n[1] * g.grid_n[2];
+  uint32_t shift = vertices * sizeof(int32_t) <= (1ull << 30) ? 0 : 1;
   if (const char *e = std::getenv("TWOS_ENTRY_CELLS")) {
     const long c = std::strtol(e, nullptr, 10);
     if (c <= 0) return;
@@ -144,14 +150,6 @@ void build_entry_table(twos_mesh *m) {
   m->entry.reserve(table.size() * sizeof(int32_t));
   check(cudaMemcpy(m->entry.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
   g.entry = m->entry.as<int32_t>();
-  // The same entries as four-wide nodes: the node holding each binary one.
-  std::vector<int32_t> table4(table.size());
-  for (size_t i = 0; i < table.size(); ++i) table4[i] = m->cover4[static_cast<size_t>(table[i])];
-  m->entry4.reserve(table4.size() * sizeof(int32_t));
-  check(cudaMemcpy(m->entry4.ptr, table4.data(), table4.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
-        "upload");
-  g.entry4 = m->entry4.as<int32_t>();
-  m->resident_bytes += table4.size() * sizeof(int32_t);
   g.entry_shift = shift;
   g.entry_radius = static_cast<float>(cell);
   m->resident_bytes += table.size() * sizeof(int32_t);
@@ -202,7 +200,8 @@ int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, tw
     std::vector<TriD> td;
     pack_bvh_f32(m->bvh, m->vertices, m->faces, m->center, nf, tf);
     std::vector<Node4F> n4;
-    pack_bvh4_f32(m->bvh, nf, n4, m->cover4);
+    std::vector<int32_t> cover4;
+    pack_bvh4_f32(m->bvh, nf, n4, cover4);
     pack_bvh_f64(m->bvh, m->vertices, m->faces, nd, td);
     check(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     m->stream = m->own_stream;
@@ -631,7 +630,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
-                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->entry4, &m->wf})
+                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->wf})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);

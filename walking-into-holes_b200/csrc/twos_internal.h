@@ -144,7 +144,6 @@ struct GeoDesc {
   // is below entry_radius (every triangle outside that node's subtree is
   // farther).
   const int32_t *entry;
-  const int32_t *entry4;  // the same table in four-wide node indices
   uint32_t entry_shift;  // an entry cell spans 2^entry_shift grid cells per axis
   uint32_t entry_n[3];
   float entry_radius;

@@ -72,8 +72,7 @@ struct twos_mesh {
   twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
   twos::DevBuf grid;   // distance-bound grid (uint16 per vertex), may be empty
   twos::DevBuf entry;  // entry-node table of the mixed form's queries, may be empty
-  twos::DevBuf nodes4_f, entry4;  // the four-wide BVH and its entry table (mixed form)
-  std::vector<int32_t> cover4;    // binary node -> four-wide node holding its subtree
+  twos::DevBuf nodes4_f;  // the four-wide BVH (mixed form, bvh_width 4)
   twos::DevBuf geo;  // one GeoDesc
   twos::GeoDesc geo_host{};
   uint64_t resident_bytes = 0;
