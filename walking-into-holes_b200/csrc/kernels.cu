@@ -583,12 +583,15 @@ __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &
   const uint32_t j0 = min(static_cast<uint32_t>(fy), g.grid_n[1] - 2);
   const uint32_t k0 = min(static_cast<uint32_t>(fz), g.grid_n[2] - 2);
   float best = -CUDART_INF_F, up = CUDART_INF_F;
-#pragma unroll 4  // (fully unrolled, the eight corners' values spill the 64-register kernel)
+  // The cell's eight corner values in one 16-byte record.
+  const uint4 rec = __ldg(g.grid + (static_cast<size_t>(i0) * (g.grid_n[1] - 1) + j0) * (g.grid_n[2] - 1) + k0);
+#pragma unroll
   for (int c = 0; c < 8; ++c) {
     const uint32_t i = i0 + (c >> 2), j = j0 + ((c >> 1) & 1), k = k0 + (c & 1);
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
-    const uint16_t raw = __ldg(g.grid + (static_cast<size_t>(i) * g.grid_n[1] + j) * g.grid_n[2] + k);
+    const uint32_t word = (c >> 1) == 0 ? rec.x : (c >> 1) == 1 ? rec.y : (c >> 1) == 2 ? rec.z : rec.w;
+    const uint32_t raw = (word >> (16 * (c & 1))) & 0xffffu;
     const float dist = sqrt_up(dot3(dv, dv));
     const float dq = static_cast<float>(raw) * g.grid_q;
     best = fmaxf(best, dq - dist);
@@ -1821,6 +1824,32 @@ cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_
   if (n == 0) return cudaSuccess;
   const int grid = static_cast<int>(std::min<uint64_t>((n + 255) / 256, 148ull * 16));
   grid_bound_kernel<<<grid, 256, 0, s>>>(geo_dev, pts, n, out);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) grid_pack_kernel(const uint16_t *__restrict__ v, uint32_t n0, uint32_t n1,
+                                                         uint32_t n2, uint4 *__restrict__ cells) {
+  const uint64_t m1 = n1 - 1, m2 = n2 - 1, count = static_cast<uint64_t>(n0 - 1) * m1 * m2;
+  for (uint64_t cell = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; cell < count;
+       cell += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t k = static_cast<uint32_t>(cell % m2);
+    const uint64_t ij = cell / m2;
+    const uint32_t j = static_cast<uint32_t>(ij % m1), i = static_cast<uint32_t>(ij / m1);
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint64_t at = (static_cast<uint64_t>(i + (c >> 2)) * n1 + (j + ((c >> 1) & 1))) * n2 + (k + (c & 1));
+      w[c >> 1] |= static_cast<uint32_t>(v[at]) << (16 * (c & 1));
+    }
+    cells[cell] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], uint4 *cells, cudaStream_t s) {
+  if (n[0] < 2 || n[1] < 2 || n[2] < 2) return cudaErrorInvalidValue;
+  const uint64_t count = static_cast<uint64_t>(n[0] - 1) * (n[1] - 1) * (n[2] - 1);
+  const int grid = static_cast<int>(std::min<uint64_t>((count + 255) / 256, 148ull * 64));
+  grid_pack_kernel<<<grid, 256, 0, s>>>(vertices, n[0], n[1], n[2], cells);
   return cudaGetLastError();
 }
 

@@ -55,7 +55,8 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 
 // Sizes and fills the mixed form's distance-bound grid of a session whose
 // BVH is on the device and whose geo_host describes it (m->geo allocated).
-// About 1024 vertices per triangle, at most 2^28 (512 MB), over the bounding
+// About 1024 vertices per triangle, at most 2^28 (4 GB of 16-byte cell
+// records; 512 MB of vertex values while it is built), over the bounding
 // box padded by one spacing (environment TWOS_GRID_VERTICES sets the count,
 // up to 2^30; 0 builds none).  On the 327,680-triangle noise sphere the walk
 // kernel took 2.42 / 2.32 / 2.17 / 2.11 / 2.08 s with 2^25 / 2^26 / 2^27 /
@@ -98,11 +99,18 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
   g.grid_inv_h = 1.0f / g.grid_h;
   g.grid_q = g.grid_h / 128.0f;
   const uint64_t count = n[0] * n[1] * n[2];
+  const uint64_t cells = (n[0] - 1) * (n[1] - 1) * (n[2] - 1);
   check(cudaMemcpy(m->geo.ptr, &g, sizeof(GeoDesc), cudaMemcpyHostToDevice), "upload");
-  m->grid.reserve(count * sizeof(uint16_t));
+  // Per-vertex values first, then the per-cell records the walks read.
+  DevBuf values;
+  struct Release {
+    DevBuf &b;
+    ~Release() { b.release(); }
+  } release_values{values};
+  values.reserve(count * sizeof(uint16_t));
   uint32_t *err = reinterpret_cast<uint32_t *>(m->totals.as<unsigned long long>() + 2);
   check(cudaMemset(err, 0, sizeof(uint32_t)), "memset");
-  check(launch_grid_build(m->geo.as<GeoDesc>(), count, 2.0 * m->delta, m->grid.as<uint16_t>(), err, nullptr),
+  check(launch_grid_build(m->geo.as<GeoDesc>(), count, 2.0 * m->delta, values.as<uint16_t>(), err, nullptr),
         "grid build");
   check(cudaDeviceSynchronize(), "grid build");
   uint32_t build_err = 0;
@@ -110,11 +118,13 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
   if (build_err) {
     // A vertex whose query overran its bounds holds 0: still a lower bound,
     // but no upper bound, so the session runs without the grid.
-    m->grid.release();
     return;
   }
-  g.grid = m->grid.as<uint16_t>();
-  m->resident_bytes += count * sizeof(uint16_t);
+  m->grid.reserve(cells * sizeof(uint4));
+  check(launch_grid_pack(values.as<uint16_t>(), g.grid_n, m->grid.as<uint4>(), nullptr), "grid pack");
+  check(cudaDeviceSynchronize(), "grid pack");
+  g.grid = m->grid.as<uint4>();
+  m->resident_bytes += cells * sizeof(uint4);
   build_entry_table(m);
 }
 

@@ -131,10 +131,13 @@ struct GeoDesc {
   float delta;        // FP32 distance error bound (mixed form)
   uint32_t max_iter;  // traversal iteration bound (node + leaf visits)
   // Distance-bound grid of the mixed form (null: none).  Vertex (i, j, k)
-  // sits at grid_lo + (i, j, k) * grid_h in the FP32 frame and holds, at
-  // grid[(i * n1 + j) * n2 + k] * grid_q, a lower bound of its distance to
-  // the surface.
-  const uint16_t *grid;
+  // sits at grid_lo + (i, j, k) * grid_h in the FP32 frame; D(v) * grid_q
+  // is a lower bound of its distance to the surface.  Stored by cell: the
+  // record grid[(i * (n1 - 1) + j) * (n2 - 1) + k] holds the 16-bit D of the
+  // cell's eight corners (i + a, j + b, k + c), corner a * 4 + b * 2 + c in
+  // bits 16 * (corner & 1) of word corner >> 1, so a lookup is one 16-byte
+  // load.
+  const uint4 *grid;
   float grid_lo[3];
   float grid_h, grid_inv_h, grid_q;
   uint32_t grid_n[3];
@@ -444,6 +447,9 @@ cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *
 // in *geo_dev; its `grid` pointer is not read).
 cudaError_t launch_grid_build(const GeoDesc *geo_dev, uint64_t n, double margin, uint16_t *out, uint32_t *error,
                               cudaStream_t s);
+// Packs the per-vertex values (n[0] x n[1] x n[2], k fastest) into the cell
+// records of GeoDesc::grid.
+cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], uint4 *cells, cudaStream_t s);
 // The walk step's grid bound at each point (original coordinates); NaN
 // outside the grid.
 cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_t n, double *out, cudaStream_t s);
