@@ -73,11 +73,11 @@ REF_SUBSET_SEED = 1234
 NCU_WALK_KERNEL = {
     "case": "bench.py --walks 256 --grid 24 --steps 1 --warmup 1 --no-cpu --no-fp64 --no-ablation --no-accuracy "
             "--no-autotune",
-    "lts__throughput_pct": 21.4,
-    "smsp__thread_inst_executed_per_inst_executed": 8.41,
-    "smsp__issue_active_pct": 50.9,
-    "sm__warps_active_pct": 48.6,
-    "lts__t_sector_hit_rate_pct": 65.1,
+    "lts__throughput_pct": 13.8,
+    "smsp__thread_inst_executed_per_inst_executed": 7.84,
+    "smsp__issue_active_pct": 69.8,
+    "sm__warps_active_pct": 48.3,
+    "lts__t_sector_hit_rate_pct": 71.1,
     "wavefront_split": {"step_kernel_threads_per_inst": 24.1, "query_kernel_threads_per_inst": 8.4,
                         "issue_active_pct": 38},
 }
@@ -86,12 +86,12 @@ NCU_WALK_KERNEL = {
 def dram_traffic_per_launch(walks: int) -> float:
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one walk-
     kernel launch, from one single-pass ncu capture of the full workload
-    (default launch tuning): 1,583.6 GB read + 16.1 GB written for
-    502,403,072 walks, 3,184 B per walk.  With the 2^28-vertex grid (512 MB)
-    and its entry table (1 GiB) the touched cells no longer fit the 126 MB L2:
-    the reads are grid and table lines; the writes are the per-walk samples.
-    Scaled to the walks of the launch."""
-    return 3184.26 * walks
+    (default launch tuning): 794.0 GB read + 9.2 GB written for 502,403,072
+    walks, 1,599 B per walk.  With the 2^28-vertex grid (4 GB of cell
+    records) and its entry table (1 GiB) the touched cells no longer fit the
+    126 MB L2: the reads are grid records and table entries; the writes are
+    the per-walk samples.  Scaled to the walks of the launch."""
+    return 1598.70 * walks
 
 
 EPSILON = 1e-4
@@ -494,7 +494,7 @@ def run_ours(args):
         # (i, j) rows; one lookup after every step).
         grid_lookups = steps if info["grid_dims"][0] else 0.0
         node_bytes = 192.0 if tuning.get("bvh_width", 2) == 4 else 96.0
-        fetched = node_bytes * nodes + 32.0 * planes + 32.0 * tris + 128.0 * grid_lookups
+        fetched = node_bytes * nodes + 32.0 * planes + 32.0 * tris + 32.0 * grid_lookups
         bvh_queries = queries - grid_steps
         hbm_peak, hbm_kind = measured_peaks()
         l2_peak = tb.l2_read_gbs(local)
@@ -505,14 +505,15 @@ def run_ours(args):
                 "peak_source": "measured in this run: twos_l2_read_gbs, 32-byte loads from every SM over a "
                                "64 MiB L2-resident buffer (the walk kernel's load form)",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-workload walk-kernel "
-                                  "launch, 3,184 B per walk (grid and entry-table lines read from HBM, per-walk "
-                                  "samples written), scaled to this launch's walks",
+                                  "launch, 1,599 B per walk (grid records and entry-table lines read from HBM, "
+                                  "per-walk samples written), scaled to this launch's walks",
                 "hbm": {"peak": hbm_peak, "peak_source": hbm_kind + " hbm_gbs",
                         "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
                 "ncu_walk_kernel": NCU_WALK_KERNEL,
                 "bytes_per_walk": float(fetched / walks_launch),
                 "bytes_definition": "device-counted: 96 B/node visit (192 B four-wide) + 32 B/plane test + 32 B/full "
-                                    "triangle test + 128 B/distance-grid lookup (one per step)",
+                                    "triangle test + 32 B/distance-grid lookup (one 16-byte cell record, one sector; "
+                                    "one per step)",
                 "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),
                 "bvh_queries_per_launch": float(bvh_queries), "walk_kernel_seconds": walk_s,
                 "bvh_queries_per_second": float(bvh_queries / walk_s),
