@@ -565,12 +565,12 @@ __device__ __forceinline__ Vec<float> grid_vertex(const GeoDesc &g, uint32_t i, 
 // largest D(v) - |p - v| over the eight corners v of p's cell (the distance
 // is 1-Lipschitz, so each is a bound).  Upper (before the FP32 allowance
 // the caller adds): the smallest (D(v) + 1) q + |p - v| over the corners
-// whose value is not saturated -- a vertex stores floor((d_FP32 - 2 delta)/q),
-// so its distance is below (D + 1) q + 3 delta.  `entry_at` is the index of
-// p's cell in the entry-node table (all ones without a table).  False when p
-// lies outside the grid (or is NaN).
+// whose value is held exactly -- a vertex stores floor((d_FP32 - 2 delta)/q),
+// so its distance is below (D + 1) q + 3 delta.  `entry_node` is the cell's
+// entry node (-1: none).  False when p lies outside the grid (or is NaN).
+// One 16-byte record per cell (GeoDesc::grid).
 __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &p, float &bound, float &upper,
-                                            uint32_t &entry_at) {
+                                            int &entry_node) {
   const float fx = (p.x - g.grid_lo[0]) * g.grid_inv_h;
   const float fy = (p.y - g.grid_lo[1]) * g.grid_inv_h;
   const float fz = (p.z - g.grid_lo[2]) * g.grid_inv_h;
@@ -583,31 +583,29 @@ __device__ __forceinline__ bool grid_bounds(const GeoDesc &g, const Vec<float> &
   const uint32_t j0 = min(static_cast<uint32_t>(fy), g.grid_n[1] - 2);
   const uint32_t k0 = min(static_cast<uint32_t>(fz), g.grid_n[2] - 2);
   float best = -CUDART_INF_F, up = CUDART_INF_F;
-  // The cell's eight corner values in one 16-byte record.
   const uint4 rec = __ldg(g.grid + (static_cast<size_t>(i0) * (g.grid_n[1] - 1) + j0) * (g.grid_n[2] - 1) + k0);
+  const uint32_t base = rec.z & 0xffffu;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const uint32_t i = i0 + (c >> 2), j = j0 + ((c >> 1) & 1), k = k0 + (c & 1);
     const Vec<float> v = grid_vertex(g, i, j, k);
     const Vec<float> dv = sub(p, v);
-    const uint32_t word = (c >> 1) == 0 ? rec.x : (c >> 1) == 1 ? rec.y : (c >> 1) == 2 ? rec.z : rec.w;
-    const uint32_t raw = (word >> (16 * (c & 1))) & 0xffffu;
+    const uint32_t off = ((c < 4 ? rec.x : rec.y) >> (8 * (c & 3))) & 0xffu;
     const float dist = sqrt_up(dot3(dv, dv));
-    const float dq = static_cast<float>(raw) * g.grid_q;
+    const float dq = static_cast<float>(off == 0xffu ? base : base + off) * g.grid_q;
     best = fmaxf(best, dq - dist);
-    if (raw != 0xffffu) up = fminf(up, dq + g.grid_q + dist);
+    if (off != 0xffu) up = fminf(up, dq + g.grid_q + dist);
   }
   bound = best;
   upper = up;
-  const uint32_t s = g.entry_shift;
-  entry_at = g.entry ? ((i0 >> s) * g.entry_n[1] + (j0 >> s)) * g.entry_n[2] + (k0 >> s) : 0xffffffffu;
+  entry_node = static_cast<int>(rec.w);
   return true;
 }
 
 __device__ __forceinline__ bool grid_bound(const GeoDesc &g, const Vec<float> &p, float &bound) {
   float upper;
-  uint32_t at;
-  return grid_bounds(g, p, bound, upper, at);
+  int entry_node;
+  return grid_bounds(g, p, bound, upper, entry_node);
 }
 
 __device__ __forceinline__ uint32_t find_job(const JobDesc *jobs, uint32_t n, uint64_t wid) {
@@ -1029,8 +1027,8 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           // step never ends a walk: the bound must clear the termination
           // shell with room to spare.
           float bound, upper = CUDART_INF_F;
-          uint32_t entry_at = 0xffffffffu;
-          const bool in_grid = (L.grid_tau > 0.f || L.entry) && G.grid && grid_bounds(G, pos, bound, upper, entry_at);
+          int entry_node = -1;
+          const bool in_grid = (L.grid_tau > 0.f || L.entry) && G.grid && grid_bounds(G, pos, bound, upper, entry_node);
           if (in_grid && L.grid_tau > 0.f && bound >= L.grid_tau * G.grid_h &&
               bound > 2.f * (static_cast<float>(J.epsilon) + G.delta) && bound * bound < best2) {
             best2 = bound * bound;
@@ -1043,7 +1041,7 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             // The step itself comes with the warp's next batch.
             break;
           }
-          if (!(in_grid && L.entry)) entry_at = 0xffffffffu;
+          if (!(in_grid && L.entry)) entry_node = -1;
           if (L.warm && tri_ok) {
             Vec<T> ta, tb, tc;
             load_tri(geo_tris<T>(G), best_tri, ta, tb, tc);
@@ -1061,10 +1059,10 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           // (its 3 delta and the FP32 query's delta, with room) may serve as
           // b before any triangle is found.  (The four-wide form keeps the
           // bound but starts at its root: the table holds binary nodes.)
-          if (entry_at != 0xffffffffu) {
+          if (entry_node >= 0) {
             const float ubs = upper + 6.f * G.delta;
             if (fminf(sqrtf(best2), ubs) < G.entry_radius) {
-              if (!WIDE) node = __ldg(G.entry + entry_at);
+              if (!WIDE) node = entry_node;
               if (ubs * ubs < best2) best2 = ubs * ubs;
             }
           }
@@ -1074,11 +1072,11 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
           // bound is evaluated at the FP32 image p32 of the position, within
           // a few 1e-8 of it, and bound <= d(p32) - delta covers that.
           float bound = 0.f, upper = CUDART_INF_F;
-          uint32_t entry_at = 0xffffffffu;
+          int entry_node = -1;
           bool in_grid = false;
           if constexpr (GRID64) {
             const double p3[3] = {pos.x, pos.y, pos.z};
-            in_grid = L.grid_tau > 0.f && G.grid && grid_bounds(G, to_frame<float>(p3, G), bound, upper, entry_at);
+            in_grid = L.grid_tau > 0.f && G.grid && grid_bounds(G, to_frame<float>(p3, G), bound, upper, entry_node);
             const double b = static_cast<double>(bound);
             if (in_grid && bound >= L.grid_tau * G.grid_h && bound > 2.f * (static_cast<float>(J.epsilon) + G.delta) &&
                 b * b < best2) {
@@ -1099,10 +1097,10 @@ __global__ void __launch_bounds__(BLOCK, wos_min_blocks<T, MODE, SRC>(BLOCK)) wo
             }
           }
           if constexpr (GRID64) {
-            if (in_grid && L.entry && entry_at != 0xffffffffu) {
+            if (in_grid && L.entry && entry_node >= 0) {
               const double ubs = static_cast<double>(upper) + 6.0 * G.delta;
               if (fmin(sqrt(best2), ubs) < static_cast<double>(G.entry_radius)) {
-                node = __ldg(G.entry + entry_at);
+                node = entry_node;
                 if (ubs * ubs < best2) best2 = ubs * ubs;
               }
             }
@@ -1828,28 +1826,48 @@ cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_
 }
 
 __global__ void __launch_bounds__(256) grid_pack_kernel(const uint16_t *__restrict__ v, uint32_t n0, uint32_t n1,
-                                                         uint32_t n2, uint4 *__restrict__ cells) {
+                                                         uint32_t n2, const int32_t *__restrict__ table,
+                                                         uint32_t shift, uint32_t e1, uint32_t e2,
+                                                         uint4 *__restrict__ cells) {
   const uint64_t m1 = n1 - 1, m2 = n2 - 1, count = static_cast<uint64_t>(n0 - 1) * m1 * m2;
   for (uint64_t cell = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; cell < count;
        cell += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     const uint32_t k = static_cast<uint32_t>(cell % m2);
     const uint64_t ij = cell / m2;
     const uint32_t j = static_cast<uint32_t>(ij % m1), i = static_cast<uint32_t>(ij / m1);
-    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    uint32_t d[8], base = 0xffffu;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const uint64_t at = (static_cast<uint64_t>(i + (c >> 2)) * n1 + (j + ((c >> 1) & 1))) * n2 + (k + (c & 1));
-      w[c >> 1] |= static_cast<uint32_t>(v[at]) << (16 * (c & 1));
+      d[c] = v[(static_cast<uint64_t>(i + (c >> 2)) * n1 + (j + ((c >> 1) & 1))) * n2 + (k + (c & 1))];
+      base = min(base, d[c]);
     }
-    cells[cell] = make_uint4(w[0], w[1], w[2], w[3]);
+    // Byte offsets above the base; 255 for a saturated corner or one too far
+    // above the base (the reader then uses the base: a lower bound still).
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t off = d[c] == 0xffffu || d[c] - base > 254u ? 0xffu : d[c] - base;
+      if (c < 4)
+        lo |= off << (8 * c);
+      else
+        hi |= off << (8 * (c - 4));
+    }
+    const int32_t entry = table ? table[(static_cast<uint64_t>(i >> shift) * e1 + (j >> shift)) * e2 + (k >> shift)]
+                                : -1;
+    cells[cell] = make_uint4(lo, hi, base, static_cast<uint32_t>(entry));
   }
 }
 
-cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], uint4 *cells, cudaStream_t s) {
+cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], const int32_t *table, uint32_t shift,
+                             const uint32_t entry_n[3], uint4 *cells, cudaStream_t s) {
   if (n[0] < 2 || n[1] < 2 || n[2] < 2) return cudaErrorInvalidValue;
+  if (table && (((n[0] - 2) >> shift) >= entry_n[0] || ((n[1] - 2) >> shift) >= entry_n[1] ||
+                ((n[2] - 2) >> shift) >= entry_n[2]))
+    return cudaErrorInvalidValue;
   const uint64_t count = static_cast<uint64_t>(n[0] - 1) * (n[1] - 1) * (n[2] - 1);
   const int grid = static_cast<int>(std::min<uint64_t>((count + 255) / 256, 148ull * 64));
-  grid_pack_kernel<<<grid, 256, 0, s>>>(vertices, n[0], n[1], n[2], cells);
+  grid_pack_kernel<<<grid, 256, 0, s>>>(vertices, n[0], n[1], n[2], table, shift, table ? entry_n[1] : 0,
+                                        table ? entry_n[2] : 0, cells);
   return cudaGetLastError();
 }
 

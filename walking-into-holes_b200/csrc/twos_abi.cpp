@@ -65,7 +65,7 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 // keeps the mesh open within a few seconds.
 // Values are FP32 distances less 2 delta (the mixed form's own error bound,
 // covering the FP32 query and the vertex placement), in steps of h/128.
-void build_entry_table(twos_mesh *m);
+std::vector<int32_t> build_entry_table(twos_mesh *m);
 
 void build_distance_grid(twos_mesh *m, size_t n_tris) {
   GeoDesc &g = m->geo_host;
@@ -120,30 +120,40 @@ void build_distance_grid(twos_mesh *m, size_t n_tris) {
     // but no upper bound, so the session runs without the grid.
     return;
   }
+  // The entry-node table, folded into the records with the corner values.
+  const std::vector<int32_t> table = build_entry_table(m);
+  DevBuf dtable;
+  struct Release2 {
+    DevBuf &b;
+    ~Release2() { b.release(); }
+  } release_table{dtable};
+  if (!table.empty()) {
+    dtable.reserve(table.size() * sizeof(int32_t));
+    check(cudaMemcpy(dtable.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+  }
   m->grid.reserve(cells * sizeof(uint4));
-  check(launch_grid_pack(values.as<uint16_t>(), g.grid_n, m->grid.as<uint4>(), nullptr), "grid pack");
+  check(launch_grid_pack(values.as<uint16_t>(), g.grid_n, table.empty() ? nullptr : dtable.as<int32_t>(),
+                         g.entry_shift, g.entry_n, m->grid.as<uint4>(), nullptr),
+        "grid pack");
   check(cudaDeviceSynchronize(), "grid pack");
   g.grid = m->grid.as<uint4>();
   m->resident_bytes += cells * sizeof(uint4);
-  build_entry_table(m);
 }
 
 // The entry-node table over the distance grid: cells of 2^s grid spacings
 // (by default one spacing while the table takes at most 1 GiB -- 1 GiB for
 // 2^28 grid vertices -- else two; TWOS_ENTRY_CELLS sets 1, 2, 4, 8 or 16, 0
-// builds none), each with the node whose subtree
-// holds every triangle within one cell size (plus 4 delta) of the cell.  A
-// query whose initial bound is below one cell size starts there instead of at
-// the root.
-void build_entry_table(twos_mesh *m) {
+// builds none), each with the node whose subtree holds every triangle within
+// one cell size (plus 4 delta) of the cell.  A query whose initial bound is
+// below one cell size starts there instead of at the root.  Built on the
+// host; the grid's cell records carry it (empty: no table).
+std::vector<int32_t> build_entry_table(twos_mesh *m) {
   GeoDesc &g = m->geo_host;
-  g.entry = nullptr;
-  if (!g.grid) return;
   const uint64_t vertices = static_cast<uint64_t>(g.grid_n[0]) * g.grid_n[1] * g.grid_n[2];
   uint32_t shift = vertices * sizeof(int32_t) <= (1ull << 30) ? 0 : 1;
   if (const char *e = std::getenv("TWOS_ENTRY_CELLS")) {
     const long c = std::strtol(e, nullptr, 10);
-    if (c <= 0) return;
+    if (c <= 0) return {};
     shift = 0;
     while (shift < 4 && (1L << (shift + 1)) <= c) ++shift;
   }
@@ -155,14 +165,9 @@ void build_entry_table(twos_mesh *m) {
     g.entry_n[a] = (g.grid_n[a] - 1 + c - 1) / c;
   }
   const double cell = c * h;
-  const std::vector<int32_t> table =
-      twos::build_entry_table(m->bvh, origin, cell, g.entry_n, cell + 4.0 * m->delta, 0.01 * h);
-  m->entry.reserve(table.size() * sizeof(int32_t));
-  check(cudaMemcpy(m->entry.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-  g.entry = m->entry.as<int32_t>();
   g.entry_shift = shift;
   g.entry_radius = static_cast<float>(cell);
-  m->resident_bytes += table.size() * sizeof(int32_t);
+  return twos::build_entry_table(m->bvh, origin, cell, g.entry_n, cell + 4.0 * m->delta, 0.01 * h);
 }
 
 int open_impl(std::vector<double> &&v, std::vector<uint32_t> &&f, int device, twos_mesh **out) {
@@ -640,7 +645,7 @@ void twos_mesh_close(twos_mesh *m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (DevBuf *b : {&m->nodes_f, &m->tris_f, &m->nodes_d, &m->tris_d, &m->geo, &m->jobs, &m->geos, &m->terms, &m->cavities,
                     &m->sites, &m->out, &m->u, &m->p, &m->steps, &m->first, &m->counter, &m->totals, &m->points, &m->dist,
-                    &m->closest, &m->topk, &m->grid, &m->entry, &m->grad, &m->nodes4_f, &m->wf})
+                    &m->closest, &m->topk, &m->grid, &m->grad, &m->nodes4_f, &m->wf})
     b->release();
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -859,13 +864,12 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
     // job boundary, so two geometries whose data fill much of the L2 should
     // not follow each other.  Jobs go largest, smallest, second largest,
     // second smallest, ... by the bytes their form reads (BVH and triangles,
-    // plus the distance grid and entry table in the mixed form).  Results do
+    // plus the distance grid's cell records in the mixed form).  Results do
     // not depend on the order: every walk's samples are keyed by its own job.
     const bool mixed = requests[0].precision == TWOS_PREC_MIXED;
     auto footprint = [&](uint32_t j) {
       const twos_mesh *mj = meshes[j];
-      return mixed ? mj->nodes_f.bytes + mj->tris_f.bytes + mj->grid.bytes + mj->entry.bytes
-                   : mj->nodes_d.bytes + mj->tris_d.bytes;
+      return mixed ? mj->nodes_f.bytes + mj->tris_f.bytes + mj->grid.bytes : mj->nodes_d.bytes + mj->tris_d.bytes;
     };
     std::vector<uint32_t> by_size(n_jobs);
     for (uint32_t j = 0; j < n_jobs; ++j) by_size[j] = j;

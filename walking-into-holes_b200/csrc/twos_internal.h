@@ -132,22 +132,25 @@ struct GeoDesc {
   uint32_t max_iter;  // traversal iteration bound (node + leaf visits)
   // Distance-bound grid of the mixed form (null: none).  Vertex (i, j, k)
   // sits at grid_lo + (i, j, k) * grid_h in the FP32 frame; D(v) * grid_q
-  // is a lower bound of its distance to the surface.  Stored by cell: the
-  // record grid[(i * (n1 - 1) + j) * (n2 - 1) + k] holds the 16-bit D of the
-  // cell's eight corners (i + a, j + b, k + c), corner a * 4 + b * 2 + c in
-  // bits 16 * (corner & 1) of word corner >> 1, so a lookup is one 16-byte
-  // load.
+  // is a lower bound of its distance to the surface.  Stored by cell, so a
+  // lookup is one 16-byte load: record grid[(i * (n1 - 1) + j) * (n2 - 1) + k]
+  // of cell (i, j, k) holds in .z (low 16 bits) the smallest D of its eight
+  // corners (i + a, j + b, k + c), in byte corner & 3 of .x (corners 0-3) or
+  // .y (corners 4-7), corner = a * 4 + b * 2 + c, each corner's D minus that
+  // base (255: saturated or too far above the base -- the base alone is used
+  // and the corner gives no upper bound), and in .w the cell's entry node
+  // (-1: none).  D varies by at most sqrt(3) h / grid_q + 1 < 224 over a
+  // cell, so the bytes hold every unsaturated corner exactly.
   const uint4 *grid;
   float grid_lo[3];
   float grid_h, grid_inv_h, grid_q;
   uint32_t grid_n[3];
-  // Entry-node table of the mixed form (null: none): entry[(I * e1 + J) * e2
-  // + K] is the BVH node a query may start from at a point of grid cell
-  // (i, j, k), (I, J, K) = (i, j, k) >> entry_shift, when its initial bound
-  // is below entry_radius (every triangle outside that node's subtree is
-  // farther).
-  const int32_t *entry;
-  uint32_t entry_shift;  // an entry cell spans 2^entry_shift grid cells per axis
+  // Entry nodes (in the grid's records): the BVH node a query may start
+  // from at a point of the cell when its initial bound is below
+  // entry_radius (every triangle outside that node's subtree is farther).
+  // The host table behind them has cells of 2^entry_shift grid cells per
+  // axis, entry_n[] of them.
+  uint32_t entry_shift;
   uint32_t entry_n[3];
   float entry_radius;
 };
@@ -447,9 +450,11 @@ cudaError_t launch_closest(int precision, const GeoDesc *geo_dev, const double *
 // in *geo_dev; its `grid` pointer is not read).
 cudaError_t launch_grid_build(const GeoDesc *geo_dev, uint64_t n, double margin, uint16_t *out, uint32_t *error,
                               cudaStream_t s);
-// Packs the per-vertex values (n[0] x n[1] x n[2], k fastest) into the cell
+// Packs the per-vertex values (n[0] x n[1] x n[2], k fastest) and the entry
+// table (may be null; entry_n[] cells of 2^shift grid cells) into the cell
 // records of GeoDesc::grid.
-cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], uint4 *cells, cudaStream_t s);
+cudaError_t launch_grid_pack(const uint16_t *vertices, const uint32_t n[3], const int32_t *table, uint32_t shift,
+                             const uint32_t entry_n[3], uint4 *cells, cudaStream_t s);
 // The walk step's grid bound at each point (original coordinates); NaN
 // outside the grid.
 cudaError_t launch_grid_bound(const GeoDesc *geo_dev, const double *pts, uint64_t n, double *out, cudaStream_t s);

@@ -71,7 +71,6 @@ struct twos_mesh {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
   twos::DevBuf nodes_f, tris_f, nodes_d, tris_d;
   twos::DevBuf grid;   // distance-bound grid (16-byte corner record per cell), may be empty
-  twos::DevBuf entry;  // entry-node table of the mixed form's queries, may be empty
   twos::DevBuf nodes4_f;  // the four-wide BVH (mixed form, bvh_width 4)
   twos::DevBuf geo;  // one GeoDesc
   twos::GeoDesc geo_host{};

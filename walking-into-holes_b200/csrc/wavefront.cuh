@@ -116,15 +116,15 @@ __global__ void __launch_bounds__(kWfStepBlock) wf_step_kernel(const WosLaunch L
       best2 = static_cast<float>(J.query_radius2);
       found = false;
       float bound, upper = CUDART_INF_F;
-      uint32_t entry_at = 0xffffffffu;
-      const bool in_grid = (L.grid_tau > 0.f || L.entry) && G.grid && grid_bounds(G, pos, bound, upper, entry_at);
+      int entry_node = -1;
+      const bool in_grid = (L.grid_tau > 0.f || L.entry) && G.grid && grid_bounds(G, pos, bound, upper, entry_node);
       if (in_grid && L.grid_tau > 0.f && bound >= L.grid_tau * G.grid_h && bound > 2.f * (eps + G.delta) &&
           bound * bound < best2) {
         best2 = bound * bound;
         found = true;
         ++c_grid;
       } else {
-        if (!(in_grid && L.entry)) entry_at = 0xffffffffu;
+        if (!(in_grid && L.entry)) entry_node = -1;
         if (L.warm && tri_ok) {
           Vec<float> ta, tb, tc;
           load_tri(G.tris_f, best_tri, ta, tb, tc);
@@ -135,10 +135,10 @@ __global__ void __launch_bounds__(kWfStepBlock) wf_step_kernel(const WosLaunch L
             found = true;
           }
         }
-        if (entry_at != 0xffffffffu) {
+        if (entry_node >= 0) {
           const float ubs = upper + 6.f * G.delta;
           if (fminf(sqrtf(best2), ubs) < G.entry_radius) {
-            node = __ldg(G.entry + entry_at);
+            node = entry_node;
             if (ubs * ubs < best2) best2 = ubs * ubs;
           }
         }
