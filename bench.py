@@ -73,11 +73,11 @@ REF_SUBSET_SEED = 1234
 NCU_WALK_KERNEL = {
     "case": "bench.py --walks 256 --grid 24 --steps 1 --warmup 1 --no-cpu --no-fp64 --no-ablation --no-accuracy "
             "--no-autotune",
-    "lts__throughput_pct": 13.8,
-    "smsp__thread_inst_executed_per_inst_executed": 7.84,
-    "smsp__issue_active_pct": 69.8,
-    "sm__warps_active_pct": 48.3,
-    "lts__t_sector_hit_rate_pct": 71.1,
+    "lts__throughput_pct": 13.3,
+    "smsp__thread_inst_executed_per_inst_executed": 7.90,
+    "smsp__issue_active_pct": 70.3,
+    "sm__warps_active_pct": 48.2,
+    "lts__t_sector_hit_rate_pct": 73.6,
     "wavefront_split": {"step_kernel_threads_per_inst": 24.1, "query_kernel_threads_per_inst": 8.4,
                         "issue_active_pct": 38},
 }
@@ -86,12 +86,12 @@ NCU_WALK_KERNEL = {
 def dram_traffic_per_launch(walks: int) -> float:
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one walk-
     kernel launch, from one single-pass ncu capture of the full workload
-    (default launch tuning): 794.0 GB read + 9.2 GB written for 502,403,072
-    walks, 1,599 B per walk.  With the 2^28-vertex grid (4 GB of cell
-    records) and its entry table (1 GiB) the touched cells no longer fit the
-    126 MB L2: the reads are grid records and table entries; the writes are
-    the per-walk samples.  Scaled to the walks of the launch."""
-    return 1598.70 * walks
+    (default launch tuning): 691.7 GB read + 8.1 GB written for 502,403,072
+    walks, 1,393 B per walk.  With the 2^28-vertex grid (4 GB of cell
+    records, entry nodes included) the touched cells no longer fit the 126 MB
+    L2: the reads are grid records; the writes are the per-walk samples.
+    Scaled to the walks of the launch."""
+    return 1392.83 * walks
 
 
 EPSILON = 1e-4
@@ -505,8 +505,8 @@ def run_ours(args):
                 "peak_source": "measured in this run: twos_l2_read_gbs, 32-byte loads from every SM over a "
                                "64 MiB L2-resident buffer (the walk kernel's load form)",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-workload walk-kernel "
-                                  "launch, 1,599 B per walk (grid records and entry-table lines read from HBM, "
-                                  "per-walk samples written), scaled to this launch's walks",
+                                  "launch, 1,393 B per walk (grid records read from HBM, per-walk samples "
+                                  "written), scaled to this launch's walks",
                 "hbm": {"peak": hbm_peak, "peak_source": hbm_kind + " hbm_gbs",
                         "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
                 "ncu_walk_kernel": NCU_WALK_KERNEL,
