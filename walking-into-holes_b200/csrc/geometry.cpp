@@ -333,9 +333,10 @@ void cross(const double *a, const double *b, const double *c, double out[3]) {
 }
 
 // Unit mean normal of a triangle range and the interval of n.v over its
-// vertices (the FP64 nodes' normal slab).  Returns false (no slab) when the
-// normals cancel.
-bool range_slab(const TriCoords &tc, Range r, double nq[3], double &smin, double &smax) {
+// vertices.  `nq` receives the direction as the kernel stores it (FP32-rounded
+// for the FP32 layout), and the interval is computed with that direction.
+// Returns false (no slab) when the normals cancel.
+bool range_slab(const TriCoords &tc, Range r, bool fp32, double nq[3], double &smin, double &smax) {
   double N[3] = {0, 0, 0}, total = 0.0;
   for (uint32_t i = r.begin; i < r.end; ++i) {
     const double *t = tc.tri(i);
@@ -348,7 +349,10 @@ bool range_slab(const TriCoords &tc, Range r, double nq[3], double &smin, double
   }
   const double len = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
   if (!(len > 1e-3 * total) || !(len > 0.0)) return false;
-  for (int k = 0; k < 3; ++k) nq[k] = N[k] / len;
+  for (int k = 0; k < 3; ++k) {
+    nq[k] = N[k] / len;
+    if (fp32) nq[k] = static_cast<double>(static_cast<float>(nq[k]));
+  }
   smin = std::numeric_limits<double>::infinity();
   smax = -std::numeric_limits<double>::infinity();
   double mag = 0.0;
@@ -499,7 +503,7 @@ void pack_bvh_f64(const HostBvh &bvh, const std::vector<double> &v, const std::v
     double nv[2][3], smin[2], smax[2];
     for (int c = 0; c < 2; ++c) {
       const Range r = code_range(n.child[c], ranges);
-      if (!(r.end > r.begin && range_slab(tc, r, nv[c], smin[c], smax[c]))) {
+      if (!(r.end > r.begin && range_slab(tc, r, false, nv[c], smin[c], smax[c]))) {
         nv[c][0] = nv[c][1] = nv[c][2] = 0.0;
         smin[c] = smax[c] = 0.0;
       }
