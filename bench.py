@@ -493,7 +493,7 @@ def run_ours(args):
         # per distance-grid lookup (the cell's eight corners lie in four
         # (i, j) rows; one lookup after every step).
         grid_lookups = steps if info["grid_dims"][0] else 0.0
-        node_bytes = 128.0 if tuning.get("bvh_width", 2) == 4 else 64.0
+        node_bytes = 192.0 if tuning.get("bvh_width", 2) == 4 else 96.0
         fetched = node_bytes * nodes + 32.0 * planes + 32.0 * tris + 32.0 * grid_lookups
         bvh_queries = queries - grid_steps
         hbm_peak, hbm_kind = measured_peaks()
@@ -511,7 +511,7 @@ def run_ours(args):
                         "traffic_gbs": traffic / walk_s / 1e9, "frac": traffic / walk_s / 1e9 / hbm_peak},
                 "ncu_walk_kernel": NCU_WALK_KERNEL,
                 "bytes_per_walk": float(fetched / walks_launch),
-                "bytes_definition": "device-counted: 64 B/node visit (128 B four-wide) + 32 B/plane test + 32 B/full "
+                "bytes_definition": "device-counted: 96 B/node visit (192 B four-wide) + 32 B/plane test + 32 B/full "
                                     "triangle test + 32 B/distance-grid lookup (one 16-byte cell record, one sector; "
                                     "one per step)",
                 "distance_evaluations_per_launch": float(queries), "grid_steps_per_launch": float(grid_steps),

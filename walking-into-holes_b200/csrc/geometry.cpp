@@ -439,7 +439,7 @@ void pack_bvh_f32(const HostBvh &bvh, const std::vector<double> &v, const std::v
   nodes.resize(bvh.nodes.size());
   for (size_t ni = 0; ni < bvh.nodes.size(); ++ni) {
     const HostBvh::Node &hn = bvh.nodes[ni];
-    float lo[2][3], hi[2][3];
+    float lo[2][3], hi[2][3], nv[2][3], smin[2], smax[2];
     for (int c = 0; c < 2; ++c) {
       const Range r = code_range(hn.child[c], ranges);
       for (int a = 0; a < 3; ++a) {
@@ -451,12 +451,26 @@ void pack_bvh_f32(const HostBvh &bvh, const std::vector<double> &v, const std::v
           lo[c][a] = std::min(lo[c][a], tri_lo[3 * i + a]);
           hi[c][a] = std::max(hi[c][a], tri_hi[3 * i + a]);
         }
+      double nq[3], s0, s1;
+      if (r.end > r.begin && range_slab(tc, r, true, nq, s0, s1)) {
+        for (int a = 0; a < 3; ++a) nv[c][a] = static_cast<float>(nq[a]);
+        smin[c] = round_down(s0);
+        smax[c] = round_up(s1);
+      } else {
+        nv[c][0] = nv[c][1] = nv[c][2] = 0.f;
+        smin[c] = smax[c] = 0.f;
+      }
     }
     NodeF &o = nodes[ni];
     o.x = make_float4(lo[0][0], lo[1][0], hi[0][0], hi[1][0]);
     o.y = make_float4(lo[0][1], lo[1][1], hi[0][1], hi[1][1]);
     o.z = make_float4(lo[0][2], lo[1][2], hi[0][2], hi[1][2]);
-    o.child = make_int4(hn.child[0], hn.child[1], 0, 0);
+    o.nl = make_float4(nv[0][0], nv[0][1], nv[0][2], smin[0]);
+    o.nr = make_float4(nv[1][0], nv[1][1], nv[1][2], smin[1]);
+    float cl, cr;
+    std::memcpy(&cl, &hn.child[0], 4);
+    std::memcpy(&cr, &hn.child[1], 4);
+    o.tail = make_float4(smax[0], smax[1], cl, cr);
   }
 }
 
@@ -707,12 +721,13 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
   cover.assign(bvh.nodes.size(), 0);
   if (bvh.nodes.empty()) return;
   struct Slot {
-    float lo[3], hi[3];
+    float lo[3], hi[3], n[3], smin, smax;
     int32_t code;
   };
   auto slot_of = [&](int32_t ni, int c) {
     const NodeF &b = binary[static_cast<size_t>(ni)];
     const float *x = &b.x.x, *y = &b.y.x, *z = &b.z.x;
+    const float4 &nv = c == 0 ? b.nl : b.nr;
     Slot s;
     s.lo[0] = x[c];
     s.lo[1] = y[c];
@@ -720,6 +735,11 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
     s.hi[0] = x[2 + c];
     s.hi[1] = y[2 + c];
     s.hi[2] = z[2 + c];
+    s.n[0] = nv.x;
+    s.n[1] = nv.y;
+    s.n[2] = nv.z;
+    s.smin = nv.w;
+    s.smax = c == 0 ? b.tail.x : b.tail.y;
     s.code = bvh.nodes[static_cast<size_t>(ni)].child[c];
     return s;
   };
@@ -742,10 +762,10 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
         slots[ns++] = slot_of(ni, c);
       }
     }
-    float *f[6];
+    float *f[11];
     Node4F q{};
     float *base = &q.xlo.x;
-    for (int k = 0; k < 6; ++k) f[k] = base + 4 * k;
+    for (int k = 0; k < 11; ++k) f[k] = base + 4 * k;
     int32_t child[4];
     for (int k = 0; k < 4; ++k) {
       if (k < ns) {
@@ -753,7 +773,10 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
         for (int a = 0; a < 3; ++a) {
           f[2 * a][k] = s.lo[a];
           f[2 * a + 1][k] = s.hi[a];
+          f[6 + a][k] = s.n[a];
         }
+        f[9][k] = s.smin;
+        f[10][k] = s.smax;
         if (s.code >= 0) {
           const int32_t qc = static_cast<int32_t>(nodes4.size());
           nodes4.emplace_back();
@@ -767,7 +790,9 @@ void pack_bvh4_f32(const HostBvh &bvh, const std::vector<NodeF> &binary, std::ve
         for (int a = 0; a < 3; ++a) {
           f[2 * a][k] = std::numeric_limits<float>::infinity();
           f[2 * a + 1][k] = -std::numeric_limits<float>::infinity();
+          f[6 + a][k] = 0.f;
         }
+        f[9][k] = f[10][k] = 0.f;
         child[k] = ~static_cast<int32_t>(0);
       }
     }

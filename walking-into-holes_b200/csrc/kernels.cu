@@ -201,16 +201,20 @@ __device__ __forceinline__ void ldg32(const void *p, float4 &a, float4 &b) {
 __device__ __forceinline__ void node_dist2(const NodeF *__restrict__ nodes, int idx, const Vec<float> &p,
                                            float &dl, float &dr, int &cl, int &cr) {
   const NodeF *n = nodes + idx;
-  float4 x, y, z, t;
+  float4 x, y, z, nl, nr, t;
   ldg32(&n->x, x, y);
-  ldg32(&n->z, z, t);
+  ldg32(&n->z, z, nl);
+  ldg32(&n->nr, nr, t);
   const float lx = gap(x.x, x.z, p.x), rx = gap(x.y, x.w, p.x);
   const float ly = gap(y.x, y.z, p.y), ry = gap(y.y, y.w, p.y);
   const float lz = gap(z.x, z.z, p.z), rz = gap(z.y, z.w, p.z);
-  dl = __fmaf_rn(lx, lx, __fmaf_rn(ly, ly, lz * lz));
-  dr = __fmaf_rn(rx, rx, __fmaf_rn(ry, ry, rz * rz));
-  cl = __float_as_int(t.x);
-  cr = __float_as_int(t.y);
+  const float sl = __fmaf_rn(nl.x, p.x, __fmaf_rn(nl.y, p.y, nl.z * p.z));
+  const float sr = __fmaf_rn(nr.x, p.x, __fmaf_rn(nr.y, p.y, nr.z * p.z));
+  const float gl = gap(nl.w, t.x, sl), gr = gap(nr.w, t.y, sr);
+  dl = fmaxf(__fmaf_rn(lx, lx, __fmaf_rn(ly, ly, lz * lz)), gl * gl);
+  dr = fmaxf(__fmaf_rn(rx, rx, __fmaf_rn(ry, ry, rz * rz)), gr * gr);
+  cl = __float_as_int(t.z);
+  cr = __float_as_int(t.w);
 }
 
 __device__ __forceinline__ void node_dist2(const NodeD *__restrict__ nodes, int idx, const Vec<double> &p,
@@ -235,25 +239,30 @@ __device__ __forceinline__ void node_dist2(const NodeD *__restrict__ nodes, int 
   cr = ch.y;
 }
 
-// The same bounds for the four children of a four-wide node (four 32-byte
+// The same bounds for the four children of a four-wide node (six 32-byte
 // loads); slot k's squared lower bound in d[k], its child code in c[k].  An
 // empty slot's inverted box gives +inf.
 __device__ __forceinline__ void node4_dist2(const Node4F *__restrict__ nodes, int idx, const Vec<float> &p,
                                             float d[4], int c[4]) {
   const Node4F *n = nodes + idx;
-  float4 xlo, xhi, ylo, yhi, zlo, zhi, ch, pad;
+  float4 xlo, xhi, ylo, yhi, zlo, zhi, nx, ny, nz, smin, smax, ch;
   ldg32(&n->xlo, xlo, xhi);
   ldg32(&n->ylo, ylo, yhi);
   ldg32(&n->zlo, zlo, zhi);
-  ldg32(&n->child, ch, pad);
-  auto slot = [&](float xl, float xh, float yl, float yh, float zl, float zh) {
+  ldg32(&n->nx, nx, ny);
+  ldg32(&n->nz, nz, smin);
+  ldg32(&n->smax, smax, ch);
+  auto slot = [&](float xl, float xh, float yl, float yh, float zl, float zh, float a, float b, float e, float s0,
+                  float s1) {
     const float gx = gap(xl, xh, p.x), gy = gap(yl, yh, p.y), gz = gap(zl, zh, p.z);
-    return __fmaf_rn(gx, gx, __fmaf_rn(gy, gy, gz * gz));
+    const float s = __fmaf_rn(a, p.x, __fmaf_rn(b, p.y, e * p.z));
+    const float gs = gap(s0, s1, s);
+    return fmaxf(__fmaf_rn(gx, gx, __fmaf_rn(gy, gy, gz * gz)), gs * gs);
   };
-  d[0] = slot(xlo.x, xhi.x, ylo.x, yhi.x, zlo.x, zhi.x);
-  d[1] = slot(xlo.y, xhi.y, ylo.y, yhi.y, zlo.y, zhi.y);
-  d[2] = slot(xlo.z, xhi.z, ylo.z, yhi.z, zlo.z, zhi.z);
-  d[3] = slot(xlo.w, xhi.w, ylo.w, yhi.w, zlo.w, zhi.w);
+  d[0] = slot(xlo.x, xhi.x, ylo.x, yhi.x, zlo.x, zhi.x, nx.x, ny.x, nz.x, smin.x, smax.x);
+  d[1] = slot(xlo.y, xhi.y, ylo.y, yhi.y, zlo.y, zhi.y, nx.y, ny.y, nz.y, smin.y, smax.y);
+  d[2] = slot(xlo.z, xhi.z, ylo.z, yhi.z, zlo.z, zhi.z, nx.z, ny.z, nz.z, smin.z, smax.z);
+  d[3] = slot(xlo.w, xhi.w, ylo.w, yhi.w, zlo.w, zhi.w, nx.w, ny.w, nz.w, smin.w, smax.w);
   c[0] = __float_as_int(ch.x);
   c[1] = __float_as_int(ch.y);
   c[2] = __float_as_int(ch.z);

@@ -21,34 +21,33 @@ constexpr int kLeafMax = 4;
 constexpr int kMaxDepth = 24;    // builder bound (<= 4 * 2^24 triangles); one stack entry per level
 constexpr int kStack = 24;
 
-// Each FP64 child also carries a normal slab: a unit direction n (the
-// child's area-weighted mean normal) and the interval [smin, smax] of n.v
-// over its vertices, rounded outward.  A child whose normals cancel gets
-// n = 0 and [0, 0], which bounds nothing.
+// Each child also carries a normal slab: a unit direction n (the child's
+// area-weighted mean normal) and the interval [smin, smax] of n.v over its
+// vertices, rounded outward.  A child whose normals cancel gets n = 0 and
+// [0, 0], which bounds nothing.
 
-// FP32 node: 64 bytes, two 32-byte loads.  x = (l.lo.x, r.lo.x, l.hi.x,
-// r.hi.x), likewise y and z; child = (left child code, right child code, 0,
-// 0).  The FP32 form bounds children by their boxes alone: with queries
-// starting at entry nodes near the surface, the normal slabs the FP64 nodes
-// keep saved fewer node visits (7.37 -> 7.22 per query) than their
-// arithmetic and third load cost.
+// FP32 node: 96 bytes, six 16-byte loads.  x = (l.lo.x, r.lo.x, l.hi.x, r.hi.x),
+// likewise y and z; nl = (l.n, l.smin), nr = (r.n, r.smin);
+// tail = (l.smax, r.smax, left child bits, right child bits).
 struct alignas(32) NodeF {
   float4 x, y, z;
-  int4 child;
+  float4 nl, nr;
+  float4 tail;
 };
-static_assert(sizeof(NodeF) == 64, "NodeF layout");
+static_assert(sizeof(NodeF) == 96, "NodeF layout");
 
 // Four-wide FP32 node (the mixed form's BVH width 4, collapsed from the
 // binary BVH: a node's slots are its binary children, each internal child
-// replaced by its own two children): 128 bytes, four 32-byte loads.  Slot c
-// of every float4 is child c: box lo/hi per axis, child code as in the
-// binary layout.  An empty slot has an inverted box, so it is never entered.
+// replaced by its own two children): 192 bytes, six 32-byte loads.  Slot c
+// of every float4 is child c: box lo/hi per axis, normal slab (n, smin,
+// smax), child code as in the binary layout.  An empty slot has an inverted
+// box and n = 0, so it is never entered.
 struct alignas(32) Node4F {
   float4 xlo, xhi, ylo, yhi, zlo, zhi;
+  float4 nx, ny, nz, smin, smax;
   int4 child;
-  int4 pad;
 };
-static_assert(sizeof(Node4F) == 128, "Node4F layout");
+static_assert(sizeof(Node4F) == 192, "Node4F layout");
 
 // FP64 node: 192 bytes.  lo/hi pairs (left, right) per axis, slabs, children.
 struct alignas(16) NodeD {
