@@ -207,16 +207,19 @@ const char *twos_last_error(void);
 
 /* Build a session from an in-memory triangle mesh: host BVH build, upload of
  * the FP32 and FP64 layouts to `device`, and the distance-bound grid of the
- * mixed form: a uniform grid over the padded bounding box (about 128 vertices
- * per triangle, at most 2^25; environment TWOS_GRID_VERTICES sets it, up to 2^26; 0
- * builds none) holding at each vertex v a lower bound of the distance from v
- * to the surface (the FP32 distance minus twice the mixed form's error bound,
- * rounded down to 1/128 of the spacing h, 16 bits).  The distance function
- * is 1-Lipschitz, so D(v) - |x - v| bounds the distance at any x from below:
- * a mixed-form step may take that as its ball radius -- the ball still lies in
- * the domain, so the walk stays an unbiased walk-on-spheres -- and skip the
- * closest-point query.  Replaces EmbreeMesh's constructor
- * (wih_twos.cpp:298-325; rtcCommitScene is the BVH build). */
+ * mixed form: a uniform grid over the padded bounding box (about 1,024
+ * vertices per triangle, at most 2^28; environment TWOS_GRID_VERTICES sets
+ * it, up to 2^30; 0 builds none) holding at each vertex v a lower bound of
+ * the distance from v to the surface (the FP32 distance minus twice the
+ * mixed form's error bound, rounded down to 1/128 of the spacing h, 16
+ * bits), stored as one 16-byte record per cell with the cell's entry node
+ * (about 16 bytes per vertex: 4 GB at 2^28 vertices, built in a few
+ * seconds).  The distance function is 1-Lipschitz, so D(v) - |x - v| bounds
+ * the distance at any x from below: a mixed-form step may take that as its
+ * ball radius -- the ball still lies in the domain, so the walk stays an
+ * unbiased walk-on-spheres -- and skip the closest-point query.  Replaces
+ * EmbreeMesh's constructor (wih_twos.cpp:298-325; rtcCommitScene is the BVH
+ * build). */
 int twos_mesh_open(const double *vertices, uint64_t n_vertices, const uint32_t *faces,
                    uint64_t n_faces, int device, twos_mesh **out);
 
