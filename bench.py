@@ -718,14 +718,22 @@ def run_batch(args):
         info.append({"level": level, "triangles": int(len(F)), "sites": int(len(pts)), "walks": w})
     total_sites = sum(len(s) for s in sites)
     total_walks = sum(len(s) * c.walks for s, c in zip(sites, cfgs))
-    tb.estimate_batch(meshes, sites, cfgs)  # warm-up
-    t0 = time.perf_counter()
-    _, summ = tb.estimate_batch(meshes, sites, cfgs)
-    t_batch = time.perf_counter() - t0
-    t0 = time.perf_counter()
+    # Warm-ups of both paths, then three timed rounds of each, alternating;
+    # the medians are reported.
+    tb.estimate_batch(meshes, sites, cfgs)
     for m, s, c in zip(meshes, sites, cfgs):
         m.estimate(s, c)
-    t_seq = time.perf_counter() - t0
+    batch_times, seq_times = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        _, summ = tb.estimate_batch(meshes, sites, cfgs)
+        batch_times.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        for m, s, c in zip(meshes, sites, cfgs):
+            m.estimate(s, c)
+        seq_times.append(time.perf_counter() - t0)
+    t_batch = float(np.median(batch_times))
+    t_seq = float(np.median(seq_times))
     big = int(np.argmax([len(s) * c.walks for s, c in zip(sites, cfgs)]))
     best, table = autotune.autotune(meshes[big], sites[big], cfgs[big], refine=4)
     n_ref = min(4, len(table) // 2)  # the refine stage's re-timings close the list
@@ -735,9 +743,10 @@ def run_batch(args):
             "sites": total_sites, "walks": int(total_walks), "dtype": "f32 query/position, f64 accumulation",
             "data": "synthetic",
             "batched": {"seconds": t_batch, "site_estimates_per_s": total_sites / t_batch,
-                        "walks_per_s": total_walks / t_batch, "launches": summ["launches"]},
+                        "walks_per_s": total_walks / t_batch, "launches": summ["launches"],
+                        "rounds_seconds": batch_times},
             "one_call_per_job": {"seconds": t_seq, "site_estimates_per_s": total_sites / t_seq,
-                                 "walks_per_s": total_walks / t_seq},
+                                 "walks_per_s": total_walks / t_seq, "rounds_seconds": seq_times},
             "autotune_largest_job": {"pick": best,
                                      "sweep_seconds_per_walk": {json.dumps(t): s for t, s in table[:-n_ref]},
                                      "refined_seconds_per_walk": {json.dumps(t): s for t, s in table[-n_ref:]}}}

@@ -74,3 +74,27 @@ def test_batch_usage_errors(tb):
     finally:
         for m in meshes:
             m.close()
+
+
+def test_batch_splits_launches_to_keep_tables_in_shared_memory(tb):
+    """Twelve jobs on twelve meshes: their job and geometry descriptors
+    exceed the walk kernel's shared-memory table budget, so the batch runs
+    as several launches (three kernels each) with the same rows as one call
+    per job."""
+    meshes, sites, cfgs = [], [], []
+    try:
+        for j in range(12):
+            V, F = tb.geometry.noise_sphere(1 + j % 2, 50 + j)
+            meshes.append(tb.Mesh(V, F))
+            sites.append(tb.geometry.uniform_ball(9 + j, 0.4, seed=200 + j))
+            cfgs.append(tb.Config(walks=32, precision="mixed", seed=300 + j, epsilon=1e-4,
+                                  source=tb.sources.constant(1.0)))
+        outs, summ = tb.estimate_batch(meshes, sites, cfgs)
+        assert summ["launches"] > 3 and summ["launches"] % 3 == 0
+        for m, s, c, o in zip(meshes, sites, cfgs, outs):
+            ref, _ = m.estimate(s, c)
+            for k in ("u", "score", "score_se", "steps"):
+                np.testing.assert_array_equal(o[k], ref[k], err_msg=k)
+    finally:
+        for m in meshes:
+            m.close()

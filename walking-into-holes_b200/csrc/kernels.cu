@@ -642,6 +642,11 @@ template <typename T> __host__ __device__ inline SmemPlan smem_plan(uint32_t n_j
   return p;
 }
 
+bool launch_tables_in_smem(int precision, uint32_t n_jobs, uint32_t n_geos, uint32_t n_terms) {
+  return precision == TWOS_PREC_MIXED ? smem_plan<float>(n_jobs, n_geos, n_terms).tables
+                                      : smem_plan<double>(n_jobs, n_geos, n_terms).tables;
+}
+
 enum : int { kIdle = 0, kTraverse = 1, kStep = 2 };
 
 // Persistent walk-on-spheres kernel as a per-lane state machine.  Each loop

@@ -881,24 +881,43 @@ int twos_estimate_batch(twos_mesh *const *meshes, const twos_request *requests, 
       if (lo < hi) order.push_back(by_size[--hi]);
     }
     // Group consecutive jobs into launches of at most max_launch_walks walks
-    // (a single larger job runs alone).
+    // (a single larger job runs alone) whose job, geometry and term tables
+    // fit the walk kernel's shared-memory budget: a launch that must read
+    // them from global memory pays for it at every step (measured: 32
+    // jobs in one launch 2.34 s, one launch per job 2.23 s).
     begin_totals(owner);
     std::vector<JobSpec> group;
+    std::vector<const twos_mesh *> group_geos;
     uint64_t group_walks = 0;
+    uint32_t group_terms = 0;
+    const int precision = requests[0].precision;
     for (uint32_t q = 0; q <= n_jobs; ++q) {
       const uint32_t j = q < n_jobs ? order[q] : n_jobs;
       const uint64_t w = j < n_jobs ? static_cast<uint64_t>(n_sites[j]) * requests[j].walks : 0;
-      if (!group.empty() && (j == n_jobs || group_walks + w > owner->max_launch_walks)) {
+      bool fits = true;
+      if (j < n_jobs && !group.empty()) {
+        const bool new_geo = std::find(group_geos.begin(), group_geos.end(), meshes[j]) == group_geos.end();
+        const uint32_t terms = group_terms + static_cast<uint32_t>(requests[j].n_source + requests[j].n_adjoint);
+        fits = launch_tables_in_smem(precision, static_cast<uint32_t>(group.size()) + 1,
+                                     static_cast<uint32_t>(group_geos.size()) + (new_geo ? 1u : 0u),
+                                     std::max(1u, terms));
+      }
+      if (!group.empty() && (j == n_jobs || group_walks + w > owner->max_launch_walks || !fits)) {
         run_launch(owner, group, owner->sites.as<double>(), owner->out.as<twos_site_result>(), ro);
         group.clear();
+        group_geos.clear();
         group_walks = 0;
+        group_terms = 0;
       }
       if (j == n_jobs) break;
       if (n_sites[j] == 0) continue;
       const uint32_t nc = n_cavities ? n_cavities[j] : 0;
       group.push_back(JobSpec{meshes[j], &requests[j], n_sites[j], begin[j], requests[j].site_offset,
                               nc ? cavities[j] : nullptr, nc});
+      if (std::find(group_geos.begin(), group_geos.end(), meshes[j]) == group_geos.end())
+        group_geos.push_back(meshes[j]);
       group_walks += w;
+      group_terms += static_cast<uint32_t>(requests[j].n_source + requests[j].n_adjoint);
     }
     end_totals(owner, ro);
     for (uint32_t j = 0; j < n_jobs; ++j)

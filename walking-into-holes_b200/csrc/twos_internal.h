@@ -397,6 +397,10 @@ cudaError_t launch_design_mask(const DesignLaunch &D, cudaStream_t s);
 
 // Kernel launchers (kernels.cu).  They return cudaGetLastError() of the launch.
 cudaError_t launch_wos_traced(const WosLaunch &L, int grid, cudaStream_t s);
+// Whether a walk-kernel launch of this many jobs, geometries and source
+// terms keeps its descriptor tables in shared memory (else it reads them
+// from global memory at every step).
+bool launch_tables_in_smem(int precision, uint32_t n_jobs, uint32_t n_geos, uint32_t n_terms);
 
 // Wavefront form of the mixed-precision walk (wavefront.cuh): the walks in
 // flight live in `slots` slot records in device memory.
