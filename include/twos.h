@@ -355,14 +355,16 @@ int twos_estimate_noalloc(twos_mesh *mesh, const twos_request *request, const do
                           uint32_t n_sites, const double *cavities, uint32_t n_cavities,
                           twos_site_result *d_out, twos_summary *summary);
 
-/* Several meshes in ONE persistent launch: job j runs request[j] over
- * sites[j] (n_sites[j] sites, 3 doubles each) on meshes[j] with cavities[j]
- * (may be NULL when n_cavities[j] == 0) and writes out[j].  All meshes must be
- * sessions on the same device; all requests must share mode, precision and the
- * Green-point flag.  Walks of every job share one device work queue, so a
- * batch of uneven meshes, site counts and walk counts keeps every SM busy;
- * the queue takes the jobs largest geometry, smallest, second largest, ...
- * so two geometries that each fill much of the L2 are not in flight at once.
+/* Several meshes in persistent launches over one work queue: job j runs
+ * request[j] over sites[j] (n_sites[j] sites, 3 doubles each) on meshes[j]
+ * with cavities[j] (may be NULL when n_cavities[j] == 0) and writes out[j].
+ * All meshes must be sessions on the same device; all requests must share
+ * mode, precision and the Green-point flag.  Walks of the jobs of a launch
+ * share one device work queue, so a batch of uneven meshes, site counts and
+ * walk counts keeps every SM busy; the queue takes the jobs largest
+ * geometry, smallest, second largest, ... so two geometries that each fill
+ * much of the L2 are not in flight at once, and is cut into as few launches
+ * as keep each launch's job and geometry descriptors in shared memory.
  * Results equal those of one twos_estimate call per job with the same
  * requests.  The work runs on meshes[0]'s stream; `summary` totals the batch.
  * Replaces a driver loop of one process call per geometry (e.g.
