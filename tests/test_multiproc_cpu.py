@@ -5,8 +5,8 @@
 * Site sharding (twos_b200.shard): the contiguous cost-weighted partition is
   disjoint and complete; each rank estimates its block with its global site
   indices as the stream's site offset (here the oracle in the GPU's counter
-  stream stands in for the device, as on a GPU box each rank would call its
-  own GPU), the rows are gathered once, and the gathered rows equal the
+  stream stands in for the device, where each rank would call its own GPU),
+  the rows are gathered once, and the gathered rows equal the
   one-rank rows bit for bit; the design loop's maxloc and the top-k merge of
   per-rank shortlists equal the single-array answers.
 """
