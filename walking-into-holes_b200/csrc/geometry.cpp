@@ -6,6 +6,7 @@
 // (437-493), the points reader keeps read_points (508-522), and the BVH
 // builder stands in for rtcCommitScene (320-324).
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -650,62 +651,90 @@ std::vector<int32_t> build_entry_table(const HostBvh &bvh, const double origin[3
     }
     return s;
   };
-  auto work = [&](uint32_t i_begin, uint32_t i_end) {
+  // The deepest node under `start` whose subtree holds every leaf whose box
+  // lies within `radius` of [lo, hi]; -1 when no leaf does.
+  auto lca = [&](int32_t start, const double *lo, const double *hi, std::vector<int32_t> &stack) {
+    uint32_t mn = std::numeric_limits<uint32_t>::max(), mx = 0;
+    stack.clear();
+    stack.push_back(start);
+    while (!stack.empty()) {
+      const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(stack.back())];
+      stack.pop_back();
+      for (int c = 0; c < 2; ++c) {
+        if (!(nd.lo[c][0] <= nd.hi[c][0])) continue;  // empty child
+        if (box_gap2(lo, hi, nd.lo[c], nd.hi[c]) > r2) continue;
+        if (nd.child[c] >= 0) {
+          stack.push_back(nd.child[c]);
+        } else {
+          const Range rg = code_range(nd.child[c], ranges);
+          if (rg.end > rg.begin) {
+            mn = std::min(mn, rg.begin);
+            mx = std::max(mx, rg.end - 1);
+          }
+        }
+      }
+    }
+    if (mn > mx) return -1;
+    int32_t ni = start;
+    for (bool deeper = true; deeper;) {
+      deeper = false;
+      const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(ni)];
+      for (int c = 0; c < 2; ++c) {
+        const int32_t code = nd.child[c];
+        if (code >= 0 && ranges[code].begin <= mn && mx < ranges[code].end) {
+          ni = code;
+          deeper = true;
+          break;
+        }
+      }
+    }
+    return ni;
+  };
+  // Coarse to fine: a block of kB^3 cells first.  Every leaf within radius
+  // of one of its cells is within radius of the block, so a cell's node lies
+  // in the block's subtree and its search starts there; a block with no leaf
+  // within radius (most of the volume) keeps the root everywhere.
+  constexpr uint32_t kB = 8;
+  const uint32_t nb[3] = {(dims[0] + kB - 1) / kB, (dims[1] + kB - 1) / kB, (dims[2] + kB - 1) / kB};
+  // Threads take (bi, bj) block columns from a shared counter: the blocks
+  // near the surface, which carry the work, are unevenly spread.
+  std::atomic<uint64_t> next{0};
+  const uint64_t columns = static_cast<uint64_t>(nb[0]) * nb[1];
+  auto work = [&]() {
     std::vector<int32_t> stack;
     stack.reserve(256);
-    for (uint32_t i = i_begin; i < i_end; ++i)
-      for (uint32_t j = 0; j < dims[1]; ++j)
-        for (uint32_t k = 0; k < dims[2]; ++k) {
-          const uint32_t ijk[3] = {i, j, k};
-          double lo[3], hi[3];
-          for (int a = 0; a < 3; ++a) {
-            lo[a] = origin[a] + cell * ijk[a] - pad;
-            hi[a] = origin[a] + cell * (ijk[a] + 1) + pad;
-          }
-          uint32_t mn = std::numeric_limits<uint32_t>::max(), mx = 0;
-          stack.clear();
-          stack.push_back(0);
-          while (!stack.empty()) {
-            const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(stack.back())];
-            stack.pop_back();
-            for (int c = 0; c < 2; ++c) {
-              if (!(nd.lo[c][0] <= nd.hi[c][0])) continue;  // empty child
-              if (box_gap2(lo, hi, nd.lo[c], nd.hi[c]) > r2) continue;
-              if (nd.child[c] >= 0) {
-                stack.push_back(nd.child[c]);
-              } else {
-                const Range rg = code_range(nd.child[c], ranges);
-                if (rg.end > rg.begin) {
-                  mn = std::min(mn, rg.begin);
-                  mx = std::max(mx, rg.end - 1);
-                }
-              }
-            }
-          }
-          int32_t ni = 0;
-          if (mn <= mx) {
-            for (bool deeper = true; deeper;) {
-              deeper = false;
-              const HostBvh::Node &nd = bvh.nodes[static_cast<size_t>(ni)];
-              for (int c = 0; c < 2; ++c) {
-                const int32_t code = nd.child[c];
-                if (code >= 0 && ranges[code].begin <= mn && mx < ranges[code].end) {
-                  ni = code;
-                  deeper = true;
-                  break;
-                }
-              }
-            }
-          }
-          entry[(static_cast<size_t>(i) * dims[1] + j) * dims[2] + k] = ni;
+    for (uint64_t col = next.fetch_add(1); col < columns; col = next.fetch_add(1)) {
+      const uint32_t bi = static_cast<uint32_t>(col / nb[1]), bj = static_cast<uint32_t>(col % nb[1]);
+      for (uint32_t bk = 0; bk < nb[2]; ++bk) {
+        const uint32_t b0[3] = {bi * kB, bj * kB, bk * kB};
+        uint32_t b1[3];
+        double blo[3], bhi[3];
+        for (int a = 0; a < 3; ++a) {
+          b1[a] = std::min(b0[a] + kB, dims[a]);
+          blo[a] = origin[a] + cell * b0[a] - pad;
+          bhi[a] = origin[a] + cell * b1[a] + pad;
         }
+        const int32_t start = lca(0, blo, bhi, stack);
+        if (start < 0) continue;
+        for (uint32_t i = b0[0]; i < b1[0]; ++i)
+          for (uint32_t j = b0[1]; j < b1[1]; ++j)
+            for (uint32_t k = b0[2]; k < b1[2]; ++k) {
+              const uint32_t ijk[3] = {i, j, k};
+              double lo[3], hi[3];
+              for (int a = 0; a < 3; ++a) {
+                lo[a] = origin[a] + cell * ijk[a] - pad;
+                hi[a] = origin[a] + cell * (ijk[a] + 1) + pad;
+              }
+              const int32_t ni = lca(start, lo, hi, stack);
+              entry[(static_cast<size_t>(i) * dims[1] + j) * dims[2] + k] = ni < 0 ? 0 : ni;
+            }
+      }
+    }
   };
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const uint32_t threads = std::min<uint32_t>(hw, dims[0]);
+  const uint64_t threads = std::min<uint64_t>(hw, columns);
   std::vector<std::thread> pool;
-  for (uint32_t t = 0; t < threads; ++t)
-    pool.emplace_back(work, static_cast<uint32_t>(static_cast<uint64_t>(dims[0]) * t / threads),
-                      static_cast<uint32_t>(static_cast<uint64_t>(dims[0]) * (t + 1) / threads));
+  for (uint64_t t = 0; t < threads; ++t) pool.emplace_back(work);
   for (auto &th : pool) th.join();
   return entry;
 }
